@@ -1,0 +1,314 @@
+"""Benchmark: D3Q19 FP32 IB-LBM sphere flow, one level step per step.
+
+Workload (the D3Q19 FP32 configuration the headline metric is quoted on):
+sphere of diameter 32 cells centred at (64,64,64) in a 256 x 128 x 128 level,
+inflow U = 0.04 (ext_dir) at x-lo, foextrap at x-hi, periodic in y and z,
+Re = 100, marker direct-forcing IBM with implicit velocity correction (golden
+spiral markers), FP32 shifted-population storage.  A step is one
+AdvancePhiAtLevel of that level: IB update_forcing + fused collide-stream.
+
+value  : MLUPS with the state resident in HBM, device time (CUDA events on the
+         library stream), max over ranks; N > 1 runs independent replicas.
+e2e    : the same through the public API with the per-step host inputs copied
+         in (level parameters) and the per-step result read back (the
+         drag/lift force record, as the reference writes force.dat every step).
+roofline: dominant kernel (fused collide-stream), algorithmic bytes 2*Q*4 per
+         cell update, against the measured HBM copy bandwidth.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = dict(nx=256, ny=128, nz=128, D=32.0, center=(64.0, 64.0, 64.0), U=0.04, Re=100.0)
+METRIC = "MLUPS & % HBM roofline (D3Q19 FP32); batched/served MLUPS, p99 vs plain"
+UNIT = "MLUPS"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = "nccl" if os.environ.get("ILBM_BENCH_BACKEND", "nccl") == "nccl" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def allreduce_max(x: float, world: int, device) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference_steps(steps: int, warmup: int, threads: int | None = None):
+    """Times the reference's own CPU path (oracle/_ref, FP32 3D build) on the
+    same workload; returns (MLUPS, seconds per step, threads, sample text)."""
+    from ilbmrex_b200 import cases
+    from oracle import checker
+    from oracle.checker import CpuLevel
+    w = WORKLOAD
+    case, ib, init = cases.sphere(w["nx"], w["ny"], w["nz"], D=w["D"], center=w["center"],
+                                  U=w["U"], Re=w["Re"])
+    kind = "reference" if checker.available("ref", 3, fp32=True) else "port"
+    threads = threads or os.cpu_count() or 1
+    if kind == "reference":
+        L = CpuLevel(case, "ref", fp32=True, threads=threads)
+    else:
+        L = CpuLevel(case, "oracle")
+        threads = 1
+    L.set_macro(*init())
+    L.init_equilibrium()
+    L.ib_create(ib)
+    L.step(max(1, warmup))  # includes the one-time dense LU of the IVC operator
+    t0 = time.perf_counter()
+    L.step(steps)
+    dt = (time.perf_counter() - t0) / steps
+    sample = (f"{steps} full level steps of the {w['nx']}x{w['ny']}x{w['nz']} D3Q19 sphere "
+              f"(after {max(1, warmup)} warm-up steps incl. the one-time IVC LU); "
+              + ("reference sources (Source/LBM, Source/BC, Source/IBM) compiled in place, "
+                 "float, restated AdvancePhiAtLevel pass structure, OpenMP"
+                 if kind == "reference" else "plain-C oracle port, FP64, 1 thread"))
+    return case.cells / dt / 1e6, dt, threads, kind, sample
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 3))
+    mlups, dt, threads, kind, sample = cpu_reference_steps(steps, 1)
+    line = {"metric": METRIC, "value": round(mlups, 3), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": steps, "warmup": 1, "ms_per_step": round(dt * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": workload_config(args),
+            "cpu_baseline": {"value": round(mlups, 3), "unit": UNIT, "cores": threads,
+                             "kind": kind, "sample": sample},
+            "e2e": {"value": round(mlups, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args):
+    w = WORKLOAD
+    return {"workload": f"D3Q19 IB-LBM sphere, single level {w['nx']}x{w['ny']}x{w['nz']}, "
+                        f"D={w['D']:g}, U={w['U']}, Re={w['Re']:g}, IVC marker IB, FP32 shifted storage",
+            "lattice": "D3Q19", "cells": w["nx"] * w["ny"] * w["nz"], "storage": args.storage,
+            "levels": 1, "parallelism": f"replicas{args.gpus}",
+            "l2_policy": "working set 637 MB > 126 MB L2 (no flush needed)"}
+
+
+def run_b200(args):
+    import torch
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    from ilbmrex_b200 import capi, cases
+    from ilbmrex_b200.level import LevelSolver
+
+    w = WORKLOAD
+    case, ib, init = cases.sphere(w["nx"], w["ny"], w["nz"], D=w["D"], center=w["center"],
+                                  U=w["U"], Re=w["Re"])
+    S = LevelSolver(case, args.storage, ib=ib, device=local)
+    S.set_macro(*init())
+    ctx = S.ctx
+    cells = case.cells
+    q = case.lattice.q
+    sbytes = {"f64": 8, "f32": 4, "f16": 2}[args.storage]
+    B_cell = 2 * q * sbytes
+
+    for _ in range(max(3, args.warmup)):
+        S.advance_phi_at_level()
+    ctx.sync()
+    torch.cuda.synchronize(device)
+
+    # ---- device-resident timed region -----------------------------------
+    K = args.steps
+    launches0 = ctx.launches()
+    sampler = ClockSampler(local)
+    with sampler:
+        barrier(world)
+        ctx.sync()
+        ctx.record(0)
+        for s in range(K):
+            # events bracket the fused collide-stream of every step
+            use_macro = S.macro if S.first_step_macro else None
+            b = S._box(S.f, S.f_next, macro_in=use_macro, force=S.force_cur, force_prev=S.force_prev)
+            capi.check(S.L.ilbm_ib_update_forcing(S.ib, C.byref(b), C.byref(S.params), case.dt, S.time), "ib")
+            ctx.record(16 + 2 * s)
+            capi.check(S.L.ilbm_level_step(ctx.h, C.byref(b), 1, C.byref(S.params)), "step")
+            ctx.record(17 + 2 * s)
+            S.f, S.f_next = S.f_next, S.f
+            S.force_cur, S.force_prev = S.force_prev, S.force_cur
+            S.first_step_macro = False
+            S.time += case.dt
+            S.istep += 1
+        ctx.record(1)
+        ctx.sync()
+        barrier(world)
+    launches = ctx.launches() - launches0
+    t_ms = ctx.elapsed_ms(0, 1)
+    step_ms = [ctx.elapsed_ms(16 + 2 * s, 17 + 2 * s) for s in range(K)]
+    t_max = allreduce_max(t_ms, world, device)
+    value = world * cells * K / (t_max * 1e-3) / 1e6
+    kern_ms = float(np.mean(step_ms))
+    peak, peak_kind = peaks()
+    achieved = B_cell * cells / (kern_ms * 1e-3) / 1e9
+    clocks = sampler.summary()
+
+    # ---- end-to-end through the public API --------------------------------
+    Ke = max(3, min(K, 20))
+    ctx.sync()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(Ke):
+        S.advance_phi_at_level(record_force=True)  # reads Cd/Cl back every step
+    ctx.sync()
+    e2e_s = allreduce_max(time.perf_counter() - t0, world, device)
+    e2e = world * cells * Ke / e2e_s / 1e6
+    h2d = C.sizeof(capi.LevelParams_t) + C.sizeof(capi.Box_t) + 16
+    d2h = 3 * 8 + 3 * 8 + 4
+
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get("k_step_d3q19_f32_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    cpu_base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            mlups, dt, threads, kind, sample = cpu_reference_steps(2, 1)
+            cpu_base = {"value": round(mlups, 3), "unit": UNIT, "cores": threads, "kind": kind,
+                        "sample": sample}
+        except Exception as e:  # the checker is optional at run time
+            cpu_base = {"value": None, "unit": UNIT, "cores": 0, "kind": "port",
+                        "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+            "steps": K, "warmup": max(3, args.warmup), "ms_per_step": round(t_max / K, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.storage != "f64" else "f64", "data": "synthetic",
+            "config": workload_config(args),
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "kernel": "k_step<D3Q19,F32_SHIFT> (+ghost prepass)",
+                         "kernel_ms": round(kern_ms, 4), "bytes_per_cell": B_cell,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                         if peak_kind == "measured" else "fallback 6650 GB/s"},
+            "cpu_baseline": cpu_base,
+            "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "ib_markers": S.num_markers(),
+        }
+        print(json.dumps(line), flush=True)
+    S.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--storage", default="f32", choices=["f64", "f32", "f16"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

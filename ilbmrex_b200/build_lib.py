@@ -1,0 +1,72 @@
+"""Builds the in-tree CUDA library ``ilbmrex_b200/lib/libilbm_b200.so`` for sm_100a.
+
+Each ``csrc/*.cu`` is compiled by nvcc (``-gencode arch=compute_100a,
+code=sm_100a -lineinfo -O3``) in parallel and linked into one shared object
+with a static CUDA runtime.  Run ``python -m ilbmrex_b200.build_lib``.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+LIBDIR = PKG / "lib"
+LIB = LIBDIR / "libilbm_b200.so"
+INCLUDE = ROOT / "include"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
+         f"-I{INCLUDE}", f"-I{CSRC}"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _compile(src: Path, obj: Path, extra: list[str]) -> None:
+    cmd = [nvcc(), *ARCH, *FLAGS, *extra, "-c", str(src), "-o", str(obj)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src.name}:\n{r.stderr[-4000:]}")
+
+
+def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> Path:
+    extra = list(extra or [])
+    LIBDIR.mkdir(exist_ok=True)
+    objdir = LIBDIR / "obj"
+    objdir.mkdir(exist_ok=True)
+    srcs = sorted(CSRC.glob("*.cu"))
+    deps = sorted(CSRC.glob("*.cuh")) + [INCLUDE / "ilbm_b200.h"]
+    dep_mtime = max(p.stat().st_mtime for p in deps)
+    jobs = []
+    for s in srcs:
+        o = objdir / (s.stem + ".o")
+        if force or not o.exists() or o.stat().st_mtime < max(s.stat().st_mtime, dep_mtime):
+            jobs.append((s, o))
+    if jobs:
+        with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:
+            futs = [ex.submit(_compile, s, o, extra) for s, o in jobs]
+            for f in futs:
+                f.result()
+    objs = [objdir / (s.stem + ".o") for s in srcs]
+    if force or jobs or not LIB.exists():
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
+    if verbose:
+        print(f"built {LIB}")
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)

@@ -1,0 +1,244 @@
+"""Level and immersed-boundary case descriptions, and the synthetic workloads.
+
+Field names follow the reference's input keys (``amr.n_cell``,
+``geometry.*``, ``amrbc.*``, ``lbmPhysicalParameters.nu``,
+``lbm.prescribed_force``, ``ibm.*``; Source/Core/AmrCoreLBM.cpp:1188-1419 and
+Source/IBM/MarkerIBParams.H).  Lattice units: unless a builder says otherwise
+the base cell is dx = 1, so dt = dx = 1 and tau = 0.5 + 3 nu
+(Source/Core/AmrCoreLBM.cpp:225-238).
+
+The builders produce the synthetic inputs of the benchmark configurations:
+no reference dataset is involved, every field is analytic or seeded.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field, replace
+
+import numpy as np
+
+from .lattice import D2Q9, D3Q19, D3Q27, Lattice
+
+INT_DIR, FOEXTRAP, EXT_DIR, USER_1, USER_2 = 0, 2, 3, 1001, 1002
+
+
+@dataclass
+class LevelCase:
+    lattice: Lattice
+    n_cell: tuple
+    prob_lo: tuple = (0.0, 0.0, 0.0)
+    prob_hi: tuple | None = None
+    periodic: tuple = (True, True, True)
+    bc_lo: tuple = (INT_DIR, INT_DIR, INT_DIR)
+    bc_hi: tuple = (INT_DIR, INT_DIR, INT_DIR)
+    bc_lo_val: tuple = ((0.0,) * 4,) * 3  # per dim (rho, ux, uy, uz)
+    bc_hi_val: tuple = ((0.0,) * 4,) * 3
+    nu: float = 0.1
+    prescribed_force: tuple | None = None
+    nghost: int = 3
+    name: str = "case"
+
+    def __post_init__(self):
+        n = tuple(int(x) for x in self.n_cell) + (1,) * (3 - len(self.n_cell))
+        if self.lattice.dim == 2:
+            n = (n[0], n[1], 1)
+        self.n_cell = n
+        if self.prob_hi is None:
+            self.prob_hi = tuple(float(self.prob_lo[d]) + float(n[d]) for d in range(3))
+        per = tuple(bool(p) for p in self.periodic) + (True,) * (3 - len(self.periodic))
+        self.periodic = per
+
+    @property
+    def dim(self) -> int:
+        return self.lattice.dim
+
+    @property
+    def dx(self) -> float:
+        return (self.prob_hi[0] - self.prob_lo[0]) / self.n_cell[0]
+
+    @property
+    def tau(self) -> float:
+        # AmrCoreLBM.cpp:225: tau_base = 3 nu / dx + 0.5
+        return 3.0 * self.nu / self.dx + 0.5
+
+    @property
+    def dt(self) -> float:
+        return self.dx
+
+    @property
+    def shape(self) -> tuple:
+        """(nz, ny, nx) -- 2D cases have nz = 1."""
+        return (self.n_cell[2], self.n_cell[1], self.n_cell[0])
+
+    @property
+    def cells(self) -> int:
+        return int(np.prod(self.n_cell[: self.dim]))
+
+
+@dataclass
+class MarkerIB:
+    """MarkerIBParams + body (ibm.x0,y0,z0,R) + force evaluation settings."""
+    coupling_method: int = 1      # 0 explicit, 1 ivc (wu_shu), 2 explicit_diag
+    delta_type: int = 4
+    loop_ns: int = 1
+    mdf_relax: float = 1.0
+    explicit_diag_eps: float = 1.0e-8
+    geometry_type: int = 0        # 0 cylinder/sphere, 1 box, 2 pitching NACA
+    box_xlo: float = 0.0
+    box_xhi: float = 0.0
+    box_ylo: float = 0.0
+    box_yhi: float = 0.0
+    box_zlo: float = 0.0
+    box_zhi: float = 0.0
+    box_ds: float = 0.0
+    box_lid_only: int = 0
+    box_lid_ux: float = 0.0
+    box_lid_uy: float = 0.0
+    box_lid_uz: float = 0.0
+    box_wall_tol: float = 0.0
+    n_marker: int = 0
+    rd: float = 0.0
+    ubx: float = 0.0
+    uby: float = 0.0
+    ubz: float = 0.0
+    omx: float = 0.0
+    omy: float = 0.0
+    omz: float = 0.0
+    ivc_diag_reg: float = 1.3
+    ivc_rebuild_matrix: int = 0
+    renormalize_delta: int = 0
+    x0: float = 0.0
+    y0: float = 0.0
+    z0: float = 0.0
+    R: float = 1.0
+    force_eval_method: int = 0    # 0 momentum_exchange, 1 eulerian, 2 marker
+    U0: float = 0.1
+    # pitching NACA (Examples/Pitching_airfoil/IBMUserDefinedGeometry.H:14-20)
+    airfoil: tuple | None = None  # (chord, thickness, mean, amplitude, frequency, phase, pivot_x)
+
+    AIRFOIL_DEFAULT = (20.0, 0.12, 0.0, 0.2617993877991494, 0.0015, 0.0, 0.0)
+
+
+def _bcv(rho=1.0, ux=0.0, uy=0.0, uz=0.0):
+    return (float(rho), float(ux), float(uy), float(uz))
+
+
+# ---------------------------------------------------------------------------
+# synthetic workloads
+# ---------------------------------------------------------------------------
+def taylor_green(n: int = 256, U0: float = 0.01, tau: float = 0.8, lattice: Lattice = D2Q9):
+    """D2Q9 Taylor-Green vortex on a periodic n x n box (lattice units)."""
+    nu = (tau - 0.5) / 3.0
+    case = LevelCase(lattice, (n, n, 1), periodic=(True, True, True), nu=nu, name=f"tgv{n}")
+
+    def init():
+        x = 2.0 * np.pi * (np.arange(n) + 0.5) / n
+        X, Y = np.meshgrid(x, x, indexing="xy")  # [j, i]
+        u = U0 * np.sin(X) * np.cos(Y)
+        v = -U0 * np.cos(X) * np.sin(Y)
+        p = -(U0 ** 2 / 4.0) * (np.cos(2 * X) + np.cos(2 * Y))
+        rho = 1.0 + 3.0 * p
+        sh = (1, n, n)
+        return rho.reshape(sh), u.reshape(sh), v.reshape(sh), np.zeros(sh)
+
+    return case, init
+
+
+def uniform_init(case: LevelCase, rho=1.0, u=(0.0, 0.0, 0.0)):
+    def init():
+        sh = case.shape
+        return (np.full(sh, rho), np.full(sh, u[0]), np.full(sh, u[1]), np.full(sh, u[2]))
+    return init
+
+
+def cylinder(nx=1024, ny=512, D=40.0, center=(256.0, 256.0), U=0.05, Re=100.0, dx=1.0,
+             coupling=1, n_marker=0):
+    """2D flow past a cylinder: ext_dir inflow (rho=1, u=U) at x-lo,
+    foextrap outflow at x-hi, periodic in y, marker IBM with IVC coupling."""
+    nu = U * D / Re
+    case = LevelCase(D2Q9, (nx, ny, 1), prob_hi=(nx * dx, ny * dx, 1.0),
+                     periodic=(False, True, True), bc_lo=(EXT_DIR, INT_DIR, INT_DIR),
+                     bc_hi=(FOEXTRAP, INT_DIR, INT_DIR),
+                     bc_lo_val=(_bcv(1.0, U), _bcv(0.0), _bcv(0.0)), nu=nu,
+                     name=f"cylinder{nx}x{ny}")
+    ib = MarkerIB(coupling_method=coupling, delta_type=4, loop_ns=1, ivc_diag_reg=1.3,
+                  x0=center[0], y0=center[1], R=D / 2.0, U0=U, n_marker=n_marker)
+    return case, ib, uniform_init(case, 1.0, (U, 0.0, 0.0))
+
+
+def sphere(nx=256, ny=128, nz=128, D=32.0, center=(64.0, 64.0, 64.0), U=0.04, Re=100.0,
+           lattice: Lattice = D3Q19, coupling=1, n_marker=0):
+    """3D flow past a sphere: ext_dir inflow at x-lo, foextrap at x-hi,
+    periodic in y and z, golden-spiral markers (IBMarkerDF.cpp:385-421)."""
+    nu = U * D / Re
+    case = LevelCase(lattice, (nx, ny, nz), periodic=(False, True, True),
+                     bc_lo=(EXT_DIR, INT_DIR, INT_DIR), bc_hi=(FOEXTRAP, INT_DIR, INT_DIR),
+                     bc_lo_val=(_bcv(1.0, U), _bcv(0.0), _bcv(0.0)), nu=nu,
+                     name=f"sphere{nx}x{ny}x{nz}")
+    ib = MarkerIB(coupling_method=coupling, delta_type=4, loop_ns=1, ivc_diag_reg=1.3,
+                  x0=center[0], y0=center[1], z0=center[2], R=D / 2.0, U0=U, n_marker=n_marker)
+    return case, ib, uniform_init(case, 1.0, (U, 0.0, 0.0))
+
+
+def square_duct(N=32, L=8, force=1.0e-5, nu=0.06, lattice: Lattice = D3Q19):
+    """Body-force driven laminar square duct (Examples/SquareDuct_flow/inputs):
+    x periodic (length L), face-mirrored user_2 walls on y and z."""
+    case = LevelCase(lattice, (L, N, N), prob_lo=(0.0, -N / 2.0, -N / 2.0),
+                     prob_hi=(float(L), N / 2.0, N / 2.0), periodic=(True, False, False),
+                     bc_lo=(INT_DIR, USER_2, USER_2), bc_hi=(INT_DIR, USER_2, USER_2),
+                     bc_lo_val=(_bcv(0.0), _bcv(1.0), _bcv(1.0)),
+                     bc_hi_val=(_bcv(0.0), _bcv(1.0), _bcv(1.0)), nu=nu,
+                     prescribed_force=(force, 0.0, 0.0), name=f"duct{N}")
+    return case, uniform_init(case)
+
+
+def couette(n=64, U=0.1, nu=0.064):
+    """Couette flow (Examples/Couette_flow/inputs): foextrap in x, ext_dir
+    walls in y (lid velocity U at y-hi)."""
+    case = LevelCase(D2Q9, (n, n, 1), periodic=(False, False, True),
+                     bc_lo=(FOEXTRAP, EXT_DIR, INT_DIR), bc_hi=(FOEXTRAP, EXT_DIR, INT_DIR),
+                     bc_lo_val=(_bcv(0.0), _bcv(1.0, 0.0), _bcv(0.0)),
+                     bc_hi_val=(_bcv(0.0), _bcv(1.0, U), _bcv(0.0)), nu=nu, name=f"couette{n}")
+    return case, uniform_init(case)
+
+
+def channel_bounce_back(nx=32, ny=24, force=1.0e-5, nu=0.1):
+    """Force-driven channel: x periodic, halfway bounce-back (user_1) walls in y."""
+    case = LevelCase(D2Q9, (nx, ny, 1), periodic=(True, False, True),
+                     bc_lo=(INT_DIR, USER_1, INT_DIR), bc_hi=(INT_DIR, USER_1, INT_DIR),
+                     bc_lo_val=(_bcv(0.0), _bcv(1.0), _bcv(0.0)),
+                     bc_hi_val=(_bcv(0.0), _bcv(1.0), _bcv(0.0)), nu=nu,
+                     prescribed_force=(force, 0.0, 0.0), name=f"channel{nx}x{ny}")
+    return case, uniform_init(case)
+
+
+def cavity_lid(n=64, U=0.1, nu=0.064):
+    """Lid-driven cavity with a marker box lid (Examples/Cavity_flow/inputs_ibm_box style)."""
+    case = LevelCase(D2Q9, (n, n, 1), periodic=(False, False, True),
+                     bc_lo=(USER_1, USER_1, INT_DIR), bc_hi=(USER_1, USER_1, INT_DIR),
+                     bc_lo_val=(_bcv(1.0), _bcv(1.0), _bcv(0.0)),
+                     bc_hi_val=(_bcv(1.0), _bcv(1.0), _bcv(0.0)), nu=nu, name=f"cavity{n}")
+    ib = MarkerIB(coupling_method=0, delta_type=4, loop_ns=2, geometry_type=1, box_lid_only=1,
+                  box_lid_ux=U, box_xlo=0.0, box_xhi=float(n), box_ylo=0.0, box_yhi=float(n) - 2.0,
+                  U0=U)
+    return case, ib, uniform_init(case)
+
+
+def pitching_airfoil(nx=512, ny=256, chord=64.0, pivot=(128.0, 128.0), U=0.05, Re=100.0,
+                     amplitude_deg=10.0, reduced_frequency=0.1, quarter_chord=True,
+                     thickness=0.12):
+    """2D NACA 00xx pitching about its quarter chord (user-defined marker
+    geometry, Examples/Pitching_airfoil/IBMUserDefinedGeometry.H; the pivot is
+    moved from the leading edge to c/4).  k = omega c / (2 U)."""
+    nu = U * chord / Re
+    omega = 2.0 * U * reduced_frequency / chord
+    freq = omega / (2.0 * math.pi)
+    case = LevelCase(D2Q9, (nx, ny, 1), periodic=(False, True, True),
+                     bc_lo=(EXT_DIR, INT_DIR, INT_DIR), bc_hi=(FOEXTRAP, INT_DIR, INT_DIR),
+                     bc_lo_val=(_bcv(1.0, U), _bcv(0.0), _bcv(0.0)), nu=nu,
+                     name=f"airfoil{nx}x{ny}")
+    ib = MarkerIB(coupling_method=1, delta_type=4, loop_ns=1, geometry_type=2,
+                  ivc_diag_reg=1.3, x0=pivot[0], y0=pivot[1], R=chord / 2.0, U0=U,
+                  airfoil=(chord, thickness, 0.0, math.radians(amplitude_deg), freq, 0.0,
+                           0.25 * chord if quarter_chord else 0.0))
+    return case, ib, uniform_init(case, 1.0, (U, 0.0, 0.0))

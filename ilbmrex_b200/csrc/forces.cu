@@ -1,0 +1,277 @@
+// Force evaluation on the device: the Eulerian forcing integral of
+// AmrCoreLBM::ComputeIBForce (Source/Core/AmrCoreLBM.cpp:489-509) and the
+// link-wise momentum exchange of IBForceEval
+// (Source/IBM/IBForceEval.cpp:28-191).  Both are two-stage reductions with a
+// fixed summation order, so repeated calls return identical bits.
+#include <algorithm>
+#include <cstring>
+
+#include "ilbm_common.cuh"
+
+using namespace ilbm;
+
+namespace {
+
+constexpr int kRedBlocks = 296;  // 2 x 148 SMs
+constexpr int kRedThreads = 256;
+
+struct RegionArgs {
+  int lo[3], n[3];
+  int mgl[3];
+  int64_t ms0, ms1, ms2;
+  int dim;
+};
+
+template <class R>
+__global__ void __launch_bounds__(kRedThreads) k_force_partial(RegionArgs a, const R *F,
+                                                               double *partial) {
+  __shared__ double sh[3][kRedThreads / 32];
+  const int64_t total = (int64_t)a.n[0] * a.n[1] * a.n[2];
+  const int64_t per = (total + gridDim.x - 1) / gridDim.x;
+  const int64_t t0 = (int64_t)blockIdx.x * per, t1 = min(total, t0 + per);
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+    const int i = a.lo[0] + (int)(t % a.n[0]);
+    const int j = a.lo[1] + (int)((t / a.n[0]) % a.n[1]);
+    const int k = a.lo[2] + (int)(t / ((int64_t)a.n[0] * a.n[1]));
+    const int64_t m = (int64_t)(i - a.mgl[0]) + (int64_t)(j - a.mgl[1]) * a.ms0 +
+                      (int64_t)(k - a.mgl[2]) * a.ms1;
+    acc[0] += double(F[m]);
+    acc[1] += double(F[m + a.ms2]);
+    if (a.dim == 3) acc[2] += double(F[m + 2 * a.ms2]);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int c = 0; c < 3; ++c) {
+    double v = acc[c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[c][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double s = 0.0;
+    for (int w = 0; w < kRedThreads / 32; ++w) s += sh[threadIdx.x][w];
+    partial[blockIdx.x * 3 + threadIdx.x] = s;
+  }
+}
+
+__global__ void k_final_sum(const double *partial, int nparts, double *out) {
+  if (threadIdx.x < 3) {
+    double s = 0.0;
+    for (int b = 0; b < nparts; ++b) s += partial[b * 3 + threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+}
+
+struct MEArgs {
+  int lo[3], hi[3];
+  int fgl[3];
+  int64_t fs0, fs1, fs2;
+  int periodic[3];
+  double plo[3], dx[3];
+  double x0, y0, z0, R;
+  int one_sided;
+  float f16_scale;
+};
+
+__device__ __forceinline__ double sdist(const MEArgs &a, int D, double x, double y, double z) {
+  const double dx = X::sub(x, a.x0), dy = X::sub(y, a.y0);
+  double s = X::add(X::mul(dx, dx), X::mul(dy, dy));
+  if (D == 3) {
+    const double dz = X::sub(z, a.z0);
+    s = X::add(s, X::mul(dz, dz));
+  }
+  return X::sub(__dsqrt_rn(s), a.R);
+}
+
+template <class L, int S>
+__global__ void __launch_bounds__(kRedThreads) k_me_partial(MEArgs a, const void *fptr,
+                                                            double *partial) {
+  using T = typename Store<S>::T;
+  const T *f = static_cast<const T *>(fptr);
+  __shared__ double sh[3][kRedThreads / 32];
+  const int nx = a.hi[0] - a.lo[0] + 1, ny = a.hi[1] - a.lo[1] + 1;
+  const int nz = (L::D == 3) ? a.hi[2] - a.lo[2] + 1 : 1;
+  const int64_t total = (int64_t)nx * ny * nz;
+  const int64_t per = (total + gridDim.x - 1) / gridDim.x;
+  const int64_t t0 = (int64_t)blockIdx.x * per, t1 = min(total, t0 + per);
+  double acc[3] = {0.0, 0.0, 0.0};
+  auto load = [&](int i, int j, int k, int q) -> double {
+    const int64_t b = (int64_t)(i - a.fgl[0]) + (int64_t)(j - a.fgl[1]) * a.fs0 +
+                      (int64_t)(k - a.fgl[2]) * a.fs1 + q * a.fs2;
+    const float s = (S == ILBM_STORAGE_F16_SCALED) ? float(L::w(q)) / a.f16_scale : 1.0f;
+    double v = double(Store<S>::load(f + b, s));
+    if (Store<S>::shifted) v += L::w(q);
+    return v;
+  };
+  for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+    const int i = a.lo[0] + (int)(t % nx);
+    const int j = a.lo[1] + (int)((t / nx) % ny);
+    const int k = (L::D == 3) ? a.lo[2] + (int)(t / ((int64_t)nx * ny)) : 0;
+    const double xc = X::add(a.plo[0], X::mul(X::add(double(i), 0.5), a.dx[0]));
+    const double yc = X::add(a.plo[1], X::mul(X::add(double(j), 0.5), a.dx[1]));
+    const double zc = (L::D == 3) ? X::add(a.plo[2], X::mul(X::add(double(k), 0.5), a.dx[2])) : 0.0;
+    if (!(sdist(a, L::D, xc, yc, zc) > 0.0)) continue;
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) {
+      int in = i + L::cx(q), jn = j + L::cy(q), kn = k + L::cz(q);
+      const int nn[3] = {nx, ny, nz};
+      int c[3] = {in, jn, kn};
+      const int lo[3] = {a.lo[0], a.lo[1], a.lo[2]}, hi[3] = {a.hi[0], a.hi[1], a.hi[2]};
+      bool skip = false;
+#pragma unroll
+      for (int d = 0; d < L::D; ++d) {
+        if (c[d] < lo[d] || c[d] > hi[d]) {
+          if (a.periodic[d]) c[d] = (c[d] < lo[d]) ? c[d] + nn[d] : c[d] - nn[d];
+          else skip = true;
+        }
+      }
+      if (skip) continue;
+      const double xn = X::add(a.plo[0], X::mul(X::add(double(c[0]), 0.5), a.dx[0]));
+      const double yn = X::add(a.plo[1], X::mul(X::add(double(c[1]), 0.5), a.dx[1]));
+      const double zn = (L::D == 3) ? X::add(a.plo[2], X::mul(X::add(double(c[2]), 0.5), a.dx[2])) : 0.0;
+      if (!(sdist(a, L::D, xn, yn, zn) <= 0.0)) continue;
+      const double fo = load(i, j, k, q);
+      double dm;
+      if (a.one_sided) dm = X::mul(2.0, fo);
+      else dm = X::add(fo, load(c[0], c[1], L::D == 3 ? c[2] : 0, opposite<L>(q)));
+      acc[0] += dm * double(L::cx(q));
+      acc[1] += dm * double(L::cy(q));
+      acc[2] += dm * double(L::cz(q));
+    }
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int c = 0; c < 3; ++c) {
+    double v = acc[c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[c][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double s = 0.0;
+    for (int w = 0; w < kRedThreads / 32; ++w) s += sh[threadIdx.x][w];
+    partial[blockIdx.x * 3 + threadIdx.x] = s;
+  }
+}
+
+template <class L, int S>
+int launch_me(ilbm_ctx *ctx, const MEArgs &a, const void *f, double *partial) {
+  k_me_partial<L, S><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(a, f, partial);
+  ctx->launches++;
+  return ILBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ilbm_force_integrals(ilbm_ctx *ctx, const ilbm_box *box, const void *force, const int lo[3],
+                         const int hi[3], double out_sum[3]) {
+  if (!ctx || !box || !force || !out_sum) {
+    set_error("ilbm_force_integrals: null argument");
+    return ILBM_ERR_ARG;
+  }
+  RegionArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.dim = ctx->dim;
+  for (int d = 0; d < 3; ++d) {
+    if (d >= ctx->dim) {
+      a.lo[d] = 0;
+      a.n[d] = 1;
+      a.mgl[d] = 0;
+      continue;
+    }
+    const int l = std::max(lo ? lo[d] : box->lo[d], box->lo[d]);
+    const int h = std::min(hi ? hi[d] : box->hi[d], box->hi[d]);
+    a.lo[d] = l;
+    a.n[d] = std::max(0, h - l + 1);
+    a.mgl[d] = box->lo[d] - box->ngrow_m;
+  }
+  a.ms0 = box->mstride[0];
+  a.ms1 = box->mstride[1];
+  a.ms2 = box->mstride[2];
+  double *scr = static_cast<double *>(ilbm_ctx_scratch(ctx, (kRedBlocks * 3 + 8) * sizeof(double)));
+  if (!scr) {
+    set_error("ilbm_force_integrals: scratch allocation failed");
+    return ILBM_ERR_NOMEM;
+  }
+  if ((int64_t)a.n[0] * a.n[1] * a.n[2] == 0) {
+    out_sum[0] = out_sum[1] = out_sum[2] = 0.0;
+    return ILBM_OK;
+  }
+  if (ctx->storage == ILBM_STORAGE_F64)
+    k_force_partial<double><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(a, static_cast<const double *>(force), scr);
+  else
+    k_force_partial<float><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(a, static_cast<const float *>(force), scr);
+  k_final_sum<<<1, 32, 0, ctx->stream>>>(scr, kRedBlocks, scr + kRedBlocks * 3);
+  ctx->launches += 2;
+  cudaMemcpyAsync(ctx->host_pinned, scr + kRedBlocks * 3, 3 * sizeof(double),
+                  cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals");
+  for (int c = 0; c < 3; ++c) out_sum[c] = ctx->host_pinned[c];
+  return ILBM_OK;
+}
+
+int ilbm_momentum_exchange(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
+                           const void *f, double x0, double y0, double z0, double R,
+                           const double prob_lo[3], const double dx[3], int one_sided,
+                           double out[3]) {
+  if (!ctx || !box || !p || !f || !out || !prob_lo || !dx) {
+    set_error("ilbm_momentum_exchange: null argument");
+    return ILBM_ERR_ARG;
+  }
+  for (int d = 0; d < ctx->dim; ++d)
+    if (box->lo[d] != p->domain_lo[d] || box->hi[d] != p->domain_hi[d]) {
+      set_error("ilbm_momentum_exchange: the box must cover the level domain");
+      return ILBM_ERR_ARG;
+    }
+  MEArgs a;
+  std::memset(&a, 0, sizeof(a));
+  for (int d = 0; d < 3; ++d) {
+    const bool use = d < ctx->dim;
+    a.lo[d] = use ? box->lo[d] : 0;
+    a.hi[d] = use ? box->hi[d] : 0;
+    a.fgl[d] = use ? box->lo[d] - box->ngrow_f : 0;
+    a.periodic[d] = use ? p->periodic[d] : 0;
+    a.plo[d] = prob_lo[d];
+    a.dx[d] = dx[d];
+  }
+  a.fs0 = box->fstride[0];
+  a.fs1 = box->fstride[1];
+  a.fs2 = box->fstride[2];
+  a.x0 = x0;
+  a.y0 = y0;
+  a.z0 = (ctx->dim == 3) ? z0 : 0.0;
+  a.R = R;
+  a.one_sided = one_sided;
+  a.f16_scale = (p->f16_scale > 0) ? float(p->f16_scale) : 1024.0f;
+  double *scr = static_cast<double *>(ilbm_ctx_scratch(ctx, (kRedBlocks * 3 + 8) * sizeof(double)));
+  if (!scr) {
+    set_error("ilbm_momentum_exchange: scratch allocation failed");
+    return ILBM_ERR_NOMEM;
+  }
+  int rc;
+  switch (ctx->q * 4 + ctx->storage) {
+    case 9 * 4 + 0: rc = launch_me<Lat<9>, 0>(ctx, a, f, scr); break;
+    case 9 * 4 + 1: rc = launch_me<Lat<9>, 1>(ctx, a, f, scr); break;
+    case 9 * 4 + 2: rc = launch_me<Lat<9>, 2>(ctx, a, f, scr); break;
+    case 19 * 4 + 0: rc = launch_me<Lat<19>, 0>(ctx, a, f, scr); break;
+    case 19 * 4 + 1: rc = launch_me<Lat<19>, 1>(ctx, a, f, scr); break;
+    case 19 * 4 + 2: rc = launch_me<Lat<19>, 2>(ctx, a, f, scr); break;
+    case 27 * 4 + 0: rc = launch_me<Lat<27>, 0>(ctx, a, f, scr); break;
+    case 27 * 4 + 1: rc = launch_me<Lat<27>, 1>(ctx, a, f, scr); break;
+    case 27 * 4 + 2: rc = launch_me<Lat<27>, 2>(ctx, a, f, scr); break;
+    default: set_error("unsupported lattice/storage"); return ILBM_ERR_UNSUPPORTED;
+  }
+  if (rc) return rc;
+  k_final_sum<<<1, 32, 0, ctx->stream>>>(scr, kRedBlocks, scr + kRedBlocks * 3);
+  ctx->launches++;
+  cudaMemcpyAsync(ctx->host_pinned, scr + kRedBlocks * 3, 3 * sizeof(double),
+                  cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_momentum_exchange");
+  for (int c = 0; c < 3; ++c) out[c] = -ctx->host_pinned[c];
+  return ILBM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,231 @@
+// Shared device-side definitions for the B200 level-step library.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "ilbm_b200.h"
+
+namespace ilbm {
+
+// ---------------------------------------------------------------------------
+// Lattices, in the direction order of the reference decks
+// (D2Q9: Examples/Cylinder_flow/inputs:35-40, D3Q19: Examples/SquareDuct_flow/
+// inputs:36-41, D3Q27: Examples/Sphere_flow/inputs:34-39).  Weights are
+// wis/wim evaluated in double, as AmrCoreLBM.cpp:1218-1221 does at run time.
+// ---------------------------------------------------------------------------
+template <int Q>
+struct Lat;
+
+template <>
+struct Lat<9> {
+  static constexpr int D = 2;
+  static constexpr int Q = 9;
+  __host__ __device__ static constexpr int cx(int q) {
+    constexpr int t[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+    return t[q];
+  }
+  __host__ __device__ static constexpr int cy(int q) {
+    constexpr int t[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+    return t[q];
+  }
+  __host__ __device__ static constexpr int cz(int) { return 0; }
+  __host__ __device__ static constexpr double w(int q) {
+    constexpr double t[9] = {4.0 / 9.0,  1.0 / 9.0,  1.0 / 9.0,  1.0 / 9.0, 1.0 / 9.0,
+                             1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0};
+    return t[q];
+  }
+};
+
+template <>
+struct Lat<19> {
+  static constexpr int D = 3;
+  static constexpr int Q = 19;
+  __host__ __device__ static constexpr int cx(int q) {
+    constexpr int t[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    return t[q];
+  }
+  __host__ __device__ static constexpr int cy(int q) {
+    constexpr int t[19] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1};
+    return t[q];
+  }
+  __host__ __device__ static constexpr int cz(int q) {
+    constexpr int t[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1};
+    return t[q];
+  }
+  __host__ __device__ static constexpr double w(int q) {
+    return q == 0 ? 12.0 / 36.0 : (q < 7 ? 2.0 / 36.0 : 1.0 / 36.0);
+  }
+};
+
+template <>
+struct Lat<27> {
+  static constexpr int D = 3;
+  static constexpr int Q = 27;
+  __host__ __device__ static constexpr int cx(int q) {
+    constexpr int t[27] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 0, 0, 1,
+                           -1, 1, -1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1};
+    return t[q];
+  }
+  __host__ __device__ static constexpr int cy(int q) {
+    constexpr int t[27] = {0, 0, 0, 1, -1, 0, 0, 1, -1, 0, 0, 1, -1, -1,
+                           1, 0, 0, 1, -1, 1, -1, 1, -1, -1, 1, 1, -1};
+    return t[q];
+  }
+  __host__ __device__ static constexpr int cz(int q) {
+    constexpr int t[27] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 1, -1, 1, -1, 0,
+                           0, -1, 1, -1, 1, 1, -1, -1, 1, 1, -1, 1, -1};
+    return t[q];
+  }
+  __host__ __device__ static constexpr double w(int q) {
+    return q == 0 ? 8.0 / 27.0 : (q < 7 ? 2.0 / 27.0 : (q < 19 ? 1.0 / 54.0 : 1.0 / 216.0));
+  }
+};
+
+template <class L>
+__host__ __device__ constexpr int opposite(int q) {
+  for (int p = 0; p < L::Q; ++p)
+    if (L::cx(p) == -L::cx(q) && L::cy(p) == -L::cy(q) && L::cz(p) == -L::cz(q)) return p;
+  return q;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 arithmetic in the reference's operation order, with every product and
+// sum rounded separately (no contraction into FMA), so the FP64 storage form
+// reproduces the reference's results bit for bit.
+// ---------------------------------------------------------------------------
+struct X {
+  __device__ static __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  __device__ static __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  __device__ static __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  __device__ static __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+};
+
+// feqFunction, Source/LBM/feq.H:9-29
+template <class L>
+__device__ __forceinline__ double feq64(int q, double rho, double u, double v, double w) {
+  double eu, uv;
+  if (L::D == 3) {
+    eu = X::add(X::add(X::mul(double(L::cx(q)), u), X::mul(double(L::cy(q)), v)),
+                X::mul(double(L::cz(q)), w));
+    uv = X::add(X::add(X::mul(u, u), X::mul(v, v)), X::mul(w, w));
+  } else {
+    eu = X::add(X::mul(double(L::cx(q)), u), X::mul(double(L::cy(q)), v));
+    uv = X::add(X::mul(u, u), X::mul(v, v));
+  }
+  // wi * rho * (1.0 + 3.0*eu + 4.5*eu*eu - 1.5*uv)
+  const double p = X::sub(X::add(X::add(1.0, X::mul(3.0, eu)), X::mul(X::mul(4.5, eu), eu)),
+                          X::mul(1.5, uv));
+  return X::mul(X::mul(L::w(q), rho), p);
+}
+
+// equilibrium with all three velocity terms (bc_fill.H:189-200,
+// AmrCoreLBM.cpp:2146-2158): always 3D sums, even for 2D lattices
+template <class L>
+__device__ __forceinline__ double feq64_3(int q, double rho, double u, double v, double w) {
+  const double eu = X::add(X::add(X::mul(double(L::cx(q)), u), X::mul(double(L::cy(q)), v)),
+                           X::mul(double(L::cz(q)), w));
+  const double uv = X::add(X::add(X::mul(u, u), X::mul(v, v)), X::mul(w, w));
+  const double p = X::sub(X::add(X::add(1.0, X::mul(3.0, eu)), X::mul(X::mul(4.5, eu), eu)),
+                          X::mul(1.5, uv));
+  return X::mul(X::mul(L::w(q), rho), p);
+}
+
+// BGK relaxation of one population plus its Guo increment
+// (collide.H:48-55, collide_forced.H:81-108).  has_force is the cell's
+// (fx != 0 || fy != 0 || fz != 0) test.
+template <class L>
+__device__ __forceinline__ double collide64_one(int q, double f, double feq, double tau,
+                                                double ux, double uy, double uz, double fx,
+                                                double fy, double fz, bool has_force) {
+  double r = X::sub(X::mul(1.0, f), X::div(X::sub(f, feq), tau));
+  if (!has_force) return r;
+  const double cs2 = 1.0 / 3.0;
+  const double fac = X::sub(1.0, X::div(0.5, tau));
+  const double cx = L::cx(q), cy = L::cy(q), cz = L::cz(q);
+  const double eiu = X::add(X::add(X::mul(cx, ux), X::mul(cy, uy)), X::mul(cz, uz));
+  const double c4 = X::mul(cs2, cs2);
+  const double termx = X::add(X::div(X::sub(cx, ux), cs2), X::mul(X::div(eiu, c4), cx));
+  const double termy = X::add(X::div(X::sub(cy, uy), cs2), X::mul(X::div(eiu, c4), cy));
+  const double termz =
+      (L::D == 3) ? X::add(X::div(X::sub(cz, uz), cs2), X::mul(X::div(eiu, c4), cz)) : 0.0;
+  const double Si = X::mul(X::mul(L::w(q), fac),
+                           X::add(X::add(X::mul(termx, fx), X::mul(termy, fy)), X::mul(termz, fz)));
+  return X::add(r, Si);
+}
+
+// ---------------------------------------------------------------------------
+// Storage forms.  load() returns the working value (f for F64, g = f - w for
+// the shifted forms); store() converts it back.
+// ---------------------------------------------------------------------------
+template <int S>
+struct Store;
+
+template <>
+struct Store<ILBM_STORAGE_F64> {
+  using T = double;
+  using R = double;
+  static constexpr bool shifted = false;
+  __device__ static __forceinline__ R load(const T *p, float) { return *p; }
+  __device__ static __forceinline__ void store(T *p, R v, float) { *p = v; }
+};
+
+template <>
+struct Store<ILBM_STORAGE_F32_SHIFT> {
+  using T = float;
+  using R = float;
+  static constexpr bool shifted = true;
+  __device__ static __forceinline__ R load(const T *p, float) { return __ldg(p); }
+  __device__ static __forceinline__ void store(T *p, R v, float) { *p = v; }
+};
+
+template <>
+struct Store<ILBM_STORAGE_F16_SCALED> {
+  using T = __half;
+  using R = float;
+  static constexpr bool shifted = true;
+  // s: per-direction factor w_q / scale
+  __device__ static __forceinline__ R load(const T *p, float s) { return __half2float(*p) * s; }
+  __device__ static __forceinline__ void store(T *p, R v, float s) { *p = __float2half_rn(v / s); }
+};
+
+// ---------------------------------------------------------------------------
+// Launch helpers
+// ---------------------------------------------------------------------------
+struct Box3 {
+  int lo[3], hi[3];
+};
+
+__host__ __device__ __forceinline__ bool in_box(const int *lo, const int *hi, int i, int j,
+                                                int k) {
+  return i >= lo[0] && i <= hi[0] && j >= lo[1] && j <= hi[1] && k >= lo[2] && k <= hi[2];
+}
+
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+}  // namespace ilbm
+
+struct ilbm_ctx {
+  int q = 0;
+  int dim = 0;
+  int storage = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  cudaEvent_t ev[16] = {};
+  // extra timing events (slots >= 16), created on first use
+  cudaEvent_t *xev = nullptr;
+  int nxev = 0;
+  int64_t launches = 0;
+  // reusable scratch (reductions, level box tables)
+  void *scratch = nullptr;
+  size_t scratch_bytes = 0;
+  double *host_pinned = nullptr;
+};
+
+// grow ctx scratch to at least n bytes (returns nullptr on failure)
+void *ilbm_ctx_scratch(ilbm_ctx *ctx, size_t n);

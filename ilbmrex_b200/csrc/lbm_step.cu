@@ -1,0 +1,1172 @@
+// Fused collide + stream for one level (the per-level hot path).
+//
+// Reference semantics (Source/Core/AdvanceLBMAtLevel.cpp:20-386): the level
+// step FillPatches f^n into a scratch copy with ghosts, collides the valid
+// cells in place (collide_forced with the STORED rho^n, u^n and the new force
+// F^n), refreshes periodic / inter-box ghosts with post-collision values,
+// writes halfway bounce-back ghosts for user_1 faces, pull-streams into f_new
+// and recomputes rho, u with F^n/2.
+//
+// B200 form: one pass.  Each thread owns one cell y, loads its Q populations
+// once (coalesced along i), recovers rho^n and u^n from them (bit-identical to
+// the stored macro because the reference computed it from the same f^n and
+// F^{n-1}; or reads macro_in), collides, and PUSHES f*(y,q) to f_out(y+c_q,q)
+// (wrapping periodic directions).  Populations whose pull source is a ghost
+// that nobody pushes from are completed by the thread that owns the
+// destination: bounce-back (f*(x,q_bar)), the pre-collision ghost value
+// (physical BC / coarse-fine), or, for a ghost covered by another box of the
+// level, that ghost collided in place.  Physical ghosts of layer 1 are
+// synthesised by a small prepass (self-fill mode) with the reference's
+// FillPatch rules, so the main kernel never evaluates boundary formulas.
+// Traffic per cell: Q loads + Q stores of the storage type (plus the force
+// band); no scratch copies.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "ilbm_common.cuh"
+
+namespace ilbm {
+
+static thread_local std::string g_err;
+void set_error(const std::string &msg) { g_err = msg; }
+const char *get_error() { return g_err.c_str(); }
+int cuda_fail(cudaError_t e, const char *what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return ILBM_ERR_CUDA;
+}
+
+constexpr int kMaxLevelBoxes = 64;
+
+struct StepArgs {
+  // box valid region and allocated lower corners
+  int lo[3], hi[3];
+  int fgl[3];  // allocated lower corner of f arrays
+  int mgl[3];  // allocated lower corner of macro / force arrays
+  int64_t fs0, fs1, fs2;
+  int64_t ms0, ms1, ms2;
+  const void *f_in;
+  void *f_out;
+  const void *macro_in;
+  const void *force;
+  const void *force_prev;
+  // level
+  int dlo[3], dhi[3];
+  int periodic[3];
+  int bclo[3], bchi[3];
+  double bvlo[3][4], bvhi[3][4];
+  double tau;
+  int self_fill;
+  int use_uniform;
+  double uf[3];
+  int flo[3], fhi[3];
+  float f16_scale;
+  int nlb;
+  int lb[kMaxLevelBoxes][6];
+};
+
+__device__ __forceinline__ int64_t fidx(const StepArgs &a, int i, int j, int k) {
+  return (int64_t)(i - a.fgl[0]) + (int64_t)(j - a.fgl[1]) * a.fs0 +
+         (int64_t)(k - a.fgl[2]) * a.fs1;
+}
+__device__ __forceinline__ int64_t midx(const StepArgs &a, int i, int j, int k) {
+  return (int64_t)(i - a.mgl[0]) + (int64_t)(j - a.mgl[1]) * a.ms0 +
+         (int64_t)(k - a.mgl[2]) * a.ms1;
+}
+
+template <class L>
+__device__ __forceinline__ bool in_domain(const StepArgs &a, int i, int j, int k) {
+  if (i < a.dlo[0] || i > a.dhi[0] || j < a.dlo[1] || j > a.dhi[1]) return false;
+  if (L::D == 3 && (k < a.dlo[2] || k > a.dhi[2])) return false;
+  return true;
+}
+
+// per-direction storage factor for the F16 form: w_q / scale
+template <class L, int S>
+__device__ __forceinline__ float sfac(const StepArgs &a, int q) {
+  if (S == ILBM_STORAGE_F16_SCALED) return float(L::w(q)) / a.f16_scale;
+  return 1.0f;
+}
+
+template <class L, int S>
+__device__ __forceinline__ typename Store<S>::R ldf(const StepArgs &a, int64_t base, int q) {
+  using T = typename Store<S>::T;
+  return Store<S>::load(static_cast<const T *>(a.f_in) + base + q * a.fs2, sfac<L, S>(a, q));
+}
+
+template <class R>
+__device__ __forceinline__ R ldm(const void *p, int64_t idx) {
+  return static_cast<const R *>(p)[idx];
+}
+
+// force at a cell (F^n or F^{n-1}); zero outside the force region
+template <class L, class R>
+__device__ __forceinline__ void load_force(const StepArgs &a, const void *F, int i, int j,
+                                           int k, R &fx, R &fy, R &fz) {
+  if (F == nullptr) {
+    if (a.use_uniform) {
+      fx = R(a.uf[0]);
+      fy = R(a.uf[1]);
+      fz = R(a.uf[2]);
+    } else {
+      fx = fy = fz = R(0);
+    }
+    return;
+  }
+  if (i < a.flo[0] || i > a.fhi[0] || j < a.flo[1] || j > a.fhi[1] ||
+      (L::D == 3 && (k < a.flo[2] || k > a.fhi[2]))) {
+    fx = fy = fz = R(0);
+    return;
+  }
+  const int64_t m = midx(a, i, j, k);
+  fx = ldm<R>(F, m);
+  fy = ldm<R>(F, m + a.ms2);
+  fz = (L::D == 3) ? ldm<R>(F, m + 2 * a.ms2) : R(0);
+}
+
+// ---------------------------------------------------------------------------
+// Per-cell physics in the two arithmetic forms
+// ---------------------------------------------------------------------------
+
+// rho, u of a cell from its populations and the previous force
+// (calculateMacroForcing.H:155-166, exact order in FP64)
+template <class L>
+__device__ __forceinline__ void moments64(const double *f, double Fx, double Fy, double Fz,
+                                          double &rho, double &u, double &v, double &w) {
+  double r = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    r = X::add(r, f[q]);
+    m1 = X::add(m1, X::mul(double(L::cx(q)), f[q]));
+    m2 = X::add(m2, X::mul(double(L::cy(q)), f[q]));
+    m3 = X::add(m3, X::mul(double(L::cz(q)), f[q]));
+  }
+  rho = r;
+  u = X::div(X::add(m1, X::mul(0.5, Fx)), r);
+  v = X::div(X::add(m2, X::mul(0.5, Fy)), r);
+  w = X::div(X::add(m3, X::mul(0.5, Fz)), r);
+}
+
+// shifted form (g = f - w): drho = rho - 1
+template <class L>
+__device__ __forceinline__ void moments32(const float *g, float Fx, float Fy, float Fz,
+                                          float &drho, float &u, float &v, float &w) {
+  float r = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f;
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    r += g[q];
+    if (L::cx(q)) m1 += float(L::cx(q)) * g[q];
+    if (L::cy(q)) m2 += float(L::cy(q)) * g[q];
+    if (L::cz(q)) m3 += float(L::cz(q)) * g[q];
+  }
+  drho = r;
+  const float inv = 1.0f / (1.0f + r);
+  u = (m1 + 0.5f * Fx) * inv;
+  v = (m2 + 0.5f * Fy) * inv;
+  w = (m3 + 0.5f * Fz) * inv;
+}
+
+// shifted equilibrium: f_eq - w_q
+template <class L>
+__device__ __forceinline__ float feqs(int q, float drho, float u, float v, float w) {
+  const float cu = float(L::cx(q)) * u + float(L::cy(q)) * v + float(L::cz(q)) * w;
+  const float uu = u * u + v * v + w * w;
+  const float P = 3.0f * cu + 4.5f * cu * cu - 1.5f * uu;
+  return float(L::w(q)) * (drho + (1.0f + drho) * P);
+}
+
+template <class L>
+__device__ __forceinline__ float guo32(int q, float omh, float u, float v, float w, float Fx,
+                                       float Fy, float Fz) {
+  const float cx = float(L::cx(q)), cy = float(L::cy(q)), cz = float(L::cz(q));
+  const float cu = cx * u + cy * v + cz * w;
+  const float tx = 3.0f * (cx - u) + 9.0f * cu * cx;
+  const float ty = 3.0f * (cy - v) + 9.0f * cu * cy;
+  const float tz = (L::D == 3) ? 3.0f * (cz - w) + 9.0f * cu * cz : 0.0f;
+  return float(L::w(q)) * omh * (tx * Fx + ty * Fy + tz * Fz);
+}
+
+// ---------------------------------------------------------------------------
+// Ghost synthesis (pre-collision values of physical-boundary ghosts), with the
+// FillPatch semantics the reference relies on: periodic images first, then per
+// ghost cell AMReX's foextrap fill followed by mesoscopicBcFill
+// (Source/BC/bc_fill.H:303-347: user_2 face mirror > user_1 copy > ext_dir
+// non-equilibrium extrapolation, mirror = nearest domain cell).
+// ---------------------------------------------------------------------------
+template <class L>
+__device__ __forceinline__ bool first_face(const StepArgs &a, const int *g, int type, int &bd,
+                                           int &lo_side) {
+#pragma unroll
+  for (int d = 0; d < L::D; ++d) {
+    if (g[d] < a.dlo[d] && a.bclo[d] == type) { bd = d; lo_side = 1; return true; }
+    if (g[d] > a.dhi[d] && a.bchi[d] == type) { bd = d; lo_side = 0; return true; }
+  }
+  return false;
+}
+
+// Resolve a ghost cell to either a source cell in the domain (copy) or a
+// boundary formula on a mirror cell.  kind: 0 copy src, 1 user_1 copy of
+// mirror, 2 ext_dir NEQ, 3 user_2 face-mirror NEQ.
+template <class L>
+__device__ __forceinline__ int ghost_rule(const StepArgs &a, const int *g, int *src, int &bd,
+                                          int &lo_side) {
+  int cur[3] = {g[0], g[1], g[2]};
+  for (int it = 0; it < 4; ++it) {
+    bool inside = true, wrappable = true;
+#pragma unroll
+    for (int d = 0; d < L::D; ++d) {
+      const bool out = cur[d] < a.dlo[d] || cur[d] > a.dhi[d];
+      if (out) {
+        inside = false;
+        if (!a.periodic[d]) wrappable = false;
+      }
+    }
+    if (inside || wrappable) {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        int c = cur[d];
+        if (d < L::D && a.periodic[d]) {
+          const int n = a.dhi[d] - a.dlo[d] + 1;
+          c = a.dlo[d] + (((c - a.dlo[d]) % n) + n) % n;
+        }
+        src[d] = c;
+      }
+      return 0;
+    }
+    if (it == 0) {
+      int m[3] = {cur[0], cur[1], cur[2]};
+#pragma unroll
+      for (int d = 0; d < L::D; ++d) m[d] = min(max(cur[d], a.dlo[d]), a.dhi[d]);
+      if (first_face<L>(a, cur, ILBM_BC_USER_2, bd, lo_side)) { src[0] = m[0]; src[1] = m[1]; src[2] = m[2]; return 3; }
+      if (first_face<L>(a, cur, ILBM_BC_USER_1, bd, lo_side)) { src[0] = m[0]; src[1] = m[1]; src[2] = m[2]; return 1; }
+      if (first_face<L>(a, cur, ILBM_BC_EXT_DIR, bd, lo_side)) { src[0] = m[0]; src[1] = m[1]; src[2] = m[2]; return 2; }
+    }
+    // foextrap: the last dimension with a foextrap face wins (FilccCell order)
+    int dsel = -1;
+#pragma unroll
+    for (int d = 0; d < L::D; ++d) {
+      if (cur[d] < a.dlo[d] && a.bclo[d] == ILBM_BC_FOEXTRAP) dsel = d;
+      else if (cur[d] > a.dhi[d] && a.bchi[d] == ILBM_BC_FOEXTRAP) dsel = d;
+    }
+    if (dsel < 0) break;
+    cur[dsel] = (cur[dsel] < a.dlo[dsel]) ? a.dlo[dsel] : a.dhi[dsel];
+  }
+  src[0] = min(max(g[0], a.dlo[0]), a.dhi[0]);
+  src[1] = min(max(g[1], a.dlo[1]), a.dhi[1]);
+  src[2] = (L::D == 3) ? min(max(g[2], a.dlo[2]), a.dhi[2]) : 0;
+  return 0;
+}
+
+// Fill all Q populations of ghost cell g in f_in (self-fill prepass).
+template <class L, int S>
+__device__ void fill_ghost_cell(const StepArgs &a, const int *g) {
+  using T = typename Store<S>::T;
+  int src[3], bd = 0, lo_side = 1;
+  const int kind = ghost_rule<L>(a, g, src, bd, lo_side);
+  T *fo = static_cast<T *>(const_cast<void *>(a.f_in));
+  const int64_t gi = fidx(a, g[0], g[1], L::D == 3 ? g[2] : 0);
+  const int64_t si = fidx(a, src[0], src[1], L::D == 3 ? src[2] : 0);
+  if (kind <= 1) {
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) fo[gi + q * a.fs2] = fo[si + q * a.fs2];
+    return;
+  }
+  const double *bv = lo_side ? a.bvlo[bd] : a.bvhi[bd];
+  if (S == ILBM_STORAGE_F64) {
+    // applyExtDirMesoscopic / applyFaceMirroredMesoscopic, bc_fill.H:159-261
+    double fnp[L::Q];
+    double rhonp = 0.0, unp = 0.0, vnp = 0.0, wnp = 0.0;
+#pragma unroll
+    for (int n = 0; n < L::Q; ++n) {
+      fnp[n] = ldf<L, S>(a, si, n);
+      rhonp = X::add(rhonp, fnp[n]);
+      unp = X::add(unp, X::mul(double(L::cx(n)), fnp[n]));
+      vnp = X::add(vnp, X::mul(double(L::cy(n)), fnp[n]));
+      wnp = X::add(wnp, X::mul(double(L::cz(n)), fnp[n]));
+    }
+    rhonp = fmax(rhonp, 1.0e-20);
+    unp = X::div(unp, rhonp);
+    vnp = X::div(vnp, rhonp);
+    wnp = X::div(wnp, rhonp);
+    double rt = bv[0], ut = bv[1], vt = bv[2], wt = bv[3];
+    if (kind == 3) {
+      rt = fmax(1.0e-20, X::sub(X::mul(2.0, bv[0]), rhonp));
+      ut = X::sub(X::mul(2.0, bv[1]), unp);
+      vt = X::sub(X::mul(2.0, bv[2]), vnp);
+      wt = X::sub(X::mul(2.0, bv[3]), wnp);
+    }
+#pragma unroll
+    for (int n = 0; n < L::Q; ++n) {
+      const double fe_np = feq64_3<L>(n, rhonp, unp, vnp, wnp);
+      const double fe_t = feq64_3<L>(n, rt, ut, vt, wt);
+      reinterpret_cast<double *>(fo)[gi + n * a.fs2] = X::add(fe_t, X::sub(fnp[n], fe_np));
+    }
+  } else {
+    float gnp[L::Q];
+    float r = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f;
+#pragma unroll
+    for (int n = 0; n < L::Q; ++n) {
+      gnp[n] = ldf<L, S>(a, si, n);
+      r += gnp[n];
+      m1 += float(L::cx(n)) * gnp[n];
+      m2 += float(L::cy(n)) * gnp[n];
+      m3 += float(L::cz(n)) * gnp[n];
+    }
+    const float rho = fmaxf(1.0f + r, 1.0e-20f);
+    const float drho = rho - 1.0f;
+    const float u = m1 / rho, v = m2 / rho, w = m3 / rho;
+    float dr_t = float(bv[0]) - 1.0f, ut = float(bv[1]), vt = float(bv[2]), wt = float(bv[3]);
+    if (kind == 3) {
+      const float rg = fmaxf(1.0e-20f, 2.0f * float(bv[0]) - rho);
+      dr_t = rg - 1.0f;
+      ut = 2.0f * float(bv[1]) - u;
+      vt = 2.0f * float(bv[2]) - v;
+      wt = 2.0f * float(bv[3]) - w;
+    }
+#pragma unroll
+    for (int n = 0; n < L::Q; ++n) {
+      const float val = feqs<L>(n, dr_t, ut, vt, wt) + (gnp[n] - feqs<L>(n, drho, u, v, w));
+      Store<S>::store(fo + gi + n * a.fs2, val, sfac<L, S>(a, n));
+    }
+  }
+}
+
+// Prepass over layer-1 ghosts outside the domain in a non-periodic direction.
+// blockIdx.z selects the face slab (dim, side); a cell is owned by the slab of
+// its lowest out-of-range non-periodic dimension.
+template <class L, int S>
+__global__ void __launch_bounds__(256) k_ghost_fill(StepArgs a) {
+  const int slab = blockIdx.z;
+  const int d = slab >> 1, side = slab & 1;
+  if (d >= L::D || a.periodic[d]) return;
+  // slab coordinates: all other dims over [dlo-1, dhi+1]
+  int ext[3], base[3];
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    if (e >= L::D) { ext[e] = 1; base[e] = 0; continue; }
+    ext[e] = a.dhi[e] - a.dlo[e] + 3;
+    base[e] = a.dlo[e] - 1;
+  }
+  ext[d] = 1;
+  base[d] = side ? a.dhi[d] + 1 : a.dlo[d] - 1;
+  const int64_t n = (int64_t)ext[0] * ext[1] * ext[2];
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int g[3];
+    g[0] = base[0] + (int)(t % ext[0]);
+    g[1] = base[1] + (int)((t / ext[0]) % ext[1]);
+    g[2] = base[2] + (int)(t / ((int64_t)ext[0] * ext[1]));
+    int owner = -1;
+#pragma unroll
+    for (int e = 0; e < L::D; ++e)
+      if (owner < 0 && !a.periodic[e] && (g[e] < a.dlo[e] || g[e] > a.dhi[e])) owner = e;
+    if (owner != d) continue;
+    fill_ghost_cell<L, S>(a, g);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Main fused kernel
+// ---------------------------------------------------------------------------
+template <class L, int S>
+__global__ void __launch_bounds__(256) k_step(StepArgs a) {
+  using T = typename Store<S>::T;
+  using R = typename Store<S>::R;
+  const int i = a.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = a.lo[1] + blockIdx.y;
+  const int k = a.lo[2] + blockIdx.z;
+  if (i > a.hi[0]) return;
+
+  const int64_t base = fidx(a, i, j, k);
+  R f[L::Q];
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) f[q] = ldf<L, S>(a, base, q);
+
+  R Fx, Fy, Fz;
+  load_force<L, R>(a, a.force, i, j, k, Fx, Fy, Fz);
+
+  R fs[L::Q];
+  if (S == ILBM_STORAGE_F64) {
+    double rho, u, v, w;
+    if (a.macro_in) {
+      const int64_t m = midx(a, i, j, k);
+      rho = ldm<double>(a.macro_in, m);
+      u = ldm<double>(a.macro_in, m + a.ms2);
+      v = ldm<double>(a.macro_in, m + 2 * a.ms2);
+      w = (L::D == 3) ? ldm<double>(a.macro_in, m + 3 * a.ms2) : 0.0;
+    } else {
+      double px, py, pz;
+      load_force<L, double>(a, a.force_prev, i, j, k, px, py, pz);
+      moments64<L>(reinterpret_cast<double *>(f), px, py, pz, rho, u, v, w);
+      if (L::D != 3) w = 0.0;
+    }
+    const bool hf = !(double(Fx) == 0.0 && double(Fy) == 0.0 && double(Fz) == 0.0);
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+      const double fe = feq64<L>(q, rho, u, v, w);
+      fs[q] = collide64_one<L>(q, double(f[q]), fe, a.tau, u, v, w, double(Fx), double(Fy),
+                               double(Fz), hf);
+    }
+  } else {
+    float drho, u, v, w;
+    if (a.macro_in) {
+      const int64_t m = midx(a, i, j, k);
+      drho = ldm<float>(a.macro_in, m) - 1.0f;
+      u = ldm<float>(a.macro_in, m + a.ms2);
+      v = ldm<float>(a.macro_in, m + 2 * a.ms2);
+      w = (L::D == 3) ? ldm<float>(a.macro_in, m + 3 * a.ms2) : 0.0f;
+    } else {
+      float px, py, pz;
+      load_force<L, float>(a, a.force_prev, i, j, k, px, py, pz);
+      moments32<L>(reinterpret_cast<float *>(f), px, py, pz, drho, u, v, w);
+    }
+    const float om = float(1.0 / a.tau);
+    const float omh = float(1.0 - 0.5 / a.tau);
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+      const float ge = feqs<L>(q, drho, u, v, w);
+      float val = float(f[q]) + om * (ge - float(f[q]));
+      val += guo32<L>(q, omh, u, v, w, float(Fx), float(Fy), float(Fz));
+      fs[q] = val;
+    }
+  }
+
+  T *fo = static_cast<T *>(a.f_out);
+  // push f*(y,q) to y + c_q
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    int di = i + L::cx(q), dj = j + L::cy(q), dk = k + L::cz(q);
+    bool ok = in_box(a.lo, a.hi, di, dj, dk);
+    if (!ok && a.self_fill) {
+      // single box = domain: wrap periodic directions
+      ok = true;
+      if (L::cx(q) != 0 && (di < a.dlo[0] || di > a.dhi[0])) {
+        if (a.periodic[0]) di = (di < a.dlo[0]) ? a.dhi[0] : a.dlo[0];
+        else ok = false;
+      }
+      if (L::cy(q) != 0 && (dj < a.dlo[1] || dj > a.dhi[1])) {
+        if (a.periodic[1]) dj = (dj < a.dlo[1]) ? a.dhi[1] : a.dlo[1];
+        else ok = false;
+      }
+      if (L::D == 3 && L::cz(q) != 0 && (dk < a.dlo[2] || dk > a.dhi[2])) {
+        if (a.periodic[2]) dk = (dk < a.dlo[2]) ? a.dhi[2] : a.dlo[2];
+        else ok = false;
+      }
+    }
+    if (ok) Store<S>::store(fo + fidx(a, di, dj, dk) + q * a.fs2, fs[q], sfac<L, S>(a, q));
+  }
+
+  // complete pulls whose source is a ghost no thread pushes from
+  const bool edge = (i == a.lo[0] || i == a.hi[0] || j == a.lo[1] || j == a.hi[1] ||
+                     (L::D == 3 && (k == a.lo[2] || k == a.hi[2])));
+  if (!edge) return;
+#pragma unroll
+  for (int q = 1; q < L::Q; ++q) {
+    const int gi = i - L::cx(q), gj = j - L::cy(q), gk = k - L::cz(q);
+    if (in_box(a.lo, a.hi, gi, gj, gk)) continue;
+    const int g[3] = {gi, gj, gk};
+    bool out_np = false, pure_u1 = true;
+#pragma unroll
+    for (int d = 0; d < L::D; ++d) {
+      int side = 0;
+      if (g[d] < a.dlo[d]) side = -1;
+      else if (g[d] > a.dhi[d]) side = 1;
+      if (side == 0) continue;
+      if (a.periodic[d]) {
+        pure_u1 = false;
+      } else {
+        out_np = true;
+        const int bc = side < 0 ? a.bclo[d] : a.bchi[d];
+        if (bc != ILBM_BC_USER_1) pure_u1 = false;
+      }
+    }
+    R val;
+    if (!out_np) {
+      if (a.self_fill) continue;  // delivered by the periodic pusher
+      // caller-filled ghost inside the (periodic) domain
+      int gw[3] = {gi, gj, gk};
+#pragma unroll
+      for (int d = 0; d < L::D; ++d)
+        if (a.periodic[d]) {
+          const int n = a.dhi[d] - a.dlo[d] + 1;
+          gw[d] = a.dlo[d] + (((gw[d] - a.dlo[d]) % n) + n) % n;
+        }
+      bool covered = false;
+      for (int b = 0; b < a.nlb && !covered; ++b)
+        covered = gw[0] >= a.lb[b][0] && gw[0] <= a.lb[b][3] && gw[1] >= a.lb[b][1] &&
+                  gw[1] <= a.lb[b][4] && (L::D == 2 || (gw[2] >= a.lb[b][2] && gw[2] <= a.lb[b][5]));
+      const int64_t gb = fidx(a, gi, gj, gk);
+      const R fg = ldf<L, S>(a, gb, q);
+      if (!covered) {
+        val = fg;
+      } else {
+        // the neighbour box's post-collision value of this population,
+        // recomputed from the caller-filled ghost data
+        R gFx, gFy, gFz;
+        load_force<L, R>(a, a.force, gi, gj, gk, gFx, gFy, gFz);
+        if (S == ILBM_STORAGE_F64) {
+          double rho, u, v, w;
+          if (a.macro_in) {
+            const int64_t m = midx(a, gi, gj, gk);
+            rho = ldm<double>(a.macro_in, m);
+            u = ldm<double>(a.macro_in, m + a.ms2);
+            v = ldm<double>(a.macro_in, m + 2 * a.ms2);
+            w = (L::D == 3) ? ldm<double>(a.macro_in, m + 3 * a.ms2) : 0.0;
+          } else {
+            double fg_all[L::Q];
+#pragma unroll
+            for (int p = 0; p < L::Q; ++p) fg_all[p] = double(ldf<L, S>(a, gb, p));
+            double px, py, pz;
+            load_force<L, double>(a, a.force_prev, gi, gj, gk, px, py, pz);
+            moments64<L>(fg_all, px, py, pz, rho, u, v, w);
+            if (L::D != 3) w = 0.0;
+          }
+          const bool hf = !(double(gFx) == 0.0 && double(gFy) == 0.0 && double(gFz) == 0.0);
+          val = collide64_one<L>(q, double(fg), feq64<L>(q, rho, u, v, w), a.tau, u, v, w,
+                                 double(gFx), double(gFy), double(gFz), hf);
+        } else {
+          float drho, u, v, w;
+          if (a.macro_in) {
+            const int64_t m = midx(a, gi, gj, gk);
+            drho = ldm<float>(a.macro_in, m) - 1.0f;
+            u = ldm<float>(a.macro_in, m + a.ms2);
+            v = ldm<float>(a.macro_in, m + 2 * a.ms2);
+            w = (L::D == 3) ? ldm<float>(a.macro_in, m + 3 * a.ms2) : 0.0f;
+          } else {
+            float g_all[L::Q];
+#pragma unroll
+            for (int p = 0; p < L::Q; ++p) g_all[p] = float(ldf<L, S>(a, gb, p));
+            float px, py, pz;
+            load_force<L, float>(a, a.force_prev, gi, gj, gk, px, py, pz);
+            moments32<L>(g_all, px, py, pz, drho, u, v, w);
+          }
+          const float om = float(1.0 / a.tau);
+          const float omh = float(1.0 - 0.5 / a.tau);
+          const float ge = feqs<L>(q, drho, u, v, w);
+          val = float(fg) + om * (ge - float(fg)) +
+                guo32<L>(q, omh, u, v, w, float(gFx), float(gFy), float(gFz));
+        }
+      }
+    } else if (pure_u1) {
+      val = fs[opposite<L>(q)];  // halfway bounce-back, AdvanceLBMAtLevel.cpp:272-373
+    } else {
+      val = ldf<L, S>(a, fidx(a, gi, gj, gk), q);  // pre-collision BC ghost
+    }
+    Store<S>::store(fo + base + q * a.fs2, val, sfac<L, S>(a, q));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Macro pass (calculateMacroForcing) and equilibrium initialisation
+// ---------------------------------------------------------------------------
+template <class L, int S>
+__global__ void __launch_bounds__(256) k_macro(StepArgs a, int rlo0, int rlo1, int rlo2,
+                                               int rhi0, void *macro_out) {
+  using R = typename Store<S>::R;
+  const int i = rlo0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = rlo1 + blockIdx.y;
+  const int k = rlo2 + blockIdx.z;
+  if (i > rhi0) return;
+  const int64_t base = fidx(a, i, j, k);
+  R f[L::Q];
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) f[q] = ldf<L, S>(a, base, q);
+  R Fx, Fy, Fz;
+  load_force<L, R>(a, a.force, i, j, k, Fx, Fy, Fz);
+  R *mo = static_cast<R *>(macro_out);
+  const int64_t m = midx(a, i, j, k);
+  if (S == ILBM_STORAGE_F64) {
+    double rho, u, v, w;
+    moments64<L>(reinterpret_cast<double *>(f), Fx, Fy, Fz, rho, u, v, w);
+    mo[m] = rho;
+    mo[m + a.ms2] = u;
+    mo[m + 2 * a.ms2] = v;
+    mo[m + 3 * a.ms2] = w;
+  } else {
+    float drho, u, v, w;
+    moments32<L>(reinterpret_cast<float *>(f), Fx, Fy, Fz, drho, u, v, w);
+    mo[m] = 1.0f + drho;
+    mo[m + a.ms2] = u;
+    mo[m + 2 * a.ms2] = v;
+    mo[m + 3 * a.ms2] = w;
+  }
+}
+
+// InitEquilibrium, AmrCoreLBM.cpp:2117-2164, over the allocated f box
+template <class L, int S>
+__global__ void __launch_bounds__(256) k_init_eq(StepArgs a, int ng) {
+  using T = typename Store<S>::T;
+  const int i = a.lo[0] - ng + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = a.lo[1] - ng + blockIdx.y;
+  const int k = (L::D == 3) ? a.lo[2] - ng + blockIdx.z : 0;
+  if (i > a.hi[0] + ng) return;
+  const int64_t m = midx(a, i, j, k);
+  const int64_t b = fidx(a, i, j, k);
+  T *f1 = static_cast<T *>(const_cast<void *>(a.f_in));
+  T *f2 = static_cast<T *>(a.f_out);
+  if (S == ILBM_STORAGE_F64) {
+    const double r = fmax(ldm<double>(a.macro_in, m), 1.e-12);
+    const double u0 = ldm<double>(a.macro_in, m + a.ms2);
+    const double v0 = ldm<double>(a.macro_in, m + 2 * a.ms2);
+    const double w0 = (L::D == 3) ? ldm<double>(a.macro_in, m + 3 * a.ms2) : 0.0;
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+      const double fe = feq64_3<L>(q, r, u0, v0, w0);
+      reinterpret_cast<double *>(f1)[b + q * a.fs2] = fe;
+      reinterpret_cast<double *>(f2)[b + q * a.fs2] = fe;
+    }
+  } else {
+    const float r = fmaxf(ldm<float>(a.macro_in, m), 1.e-12f);
+    const float u0 = ldm<float>(a.macro_in, m + a.ms2);
+    const float v0 = ldm<float>(a.macro_in, m + 2 * a.ms2);
+    const float w0 = (L::D == 3) ? ldm<float>(a.macro_in, m + 3 * a.ms2) : 0.0f;
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+      const float ge = feqs<L>(q, r - 1.0f, u0, v0, w0);
+      Store<S>::store(f1 + b + q * a.fs2, ge, sfac<L, S>(a, q));
+      Store<S>::store(f2 + b + q * a.fs2, ge, sfac<L, S>(a, q));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Band macro for the immersed boundary: rho, u, v, w (FP64) on the cells of
+// the IB support band, including up to two ghost layers outside the domain.
+// Valid cells: from macro_in, or from f^n and F^{n-1} (the value the
+// reference's macro pass stored).  Ghost cells: FillPatchMacro semantics
+// (periodic image, foextrap, macroBcFill: user_2 mirrored state, user_1 /
+// ext_dir prescribed state; Source/BC/bc_fill.H:69-142, 263-301).
+// ---------------------------------------------------------------------------
+template <class L, int S>
+__device__ void macro_at(const StepArgs &a, int i, int j, int k, double *m4) {
+  if (a.macro_in) {
+    const int64_t m = midx(a, i, j, k);
+    if (S == ILBM_STORAGE_F64) {
+      m4[0] = ldm<double>(a.macro_in, m);
+      m4[1] = ldm<double>(a.macro_in, m + a.ms2);
+      m4[2] = ldm<double>(a.macro_in, m + 2 * a.ms2);
+      m4[3] = (L::D == 3) ? ldm<double>(a.macro_in, m + 3 * a.ms2) : 0.0;
+    } else {
+      m4[0] = ldm<float>(a.macro_in, m);
+      m4[1] = ldm<float>(a.macro_in, m + a.ms2);
+      m4[2] = ldm<float>(a.macro_in, m + 2 * a.ms2);
+      m4[3] = (L::D == 3) ? ldm<float>(a.macro_in, m + 3 * a.ms2) : 0.0;
+    }
+    return;
+  }
+  const int64_t b = fidx(a, i, j, k);
+  if (S == ILBM_STORAGE_F64) {
+    double f[L::Q];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) f[q] = ldf<L, S>(a, b, q);
+    double px, py, pz;
+    load_force<L, double>(a, a.force_prev, i, j, k, px, py, pz);
+    moments64<L>(f, px, py, pz, m4[0], m4[1], m4[2], m4[3]);
+    if (L::D != 3) m4[3] = 0.0;
+  } else {
+    float g[L::Q];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) g[q] = ldf<L, S>(a, b, q);
+    float px, py, pz, drho, u, v, w;
+    load_force<L, float>(a, a.force_prev, i, j, k, px, py, pz);
+    moments32<L>(g, px, py, pz, drho, u, v, w);
+    m4[0] = 1.0 + double(drho);
+    m4[1] = u;
+    m4[2] = v;
+    m4[3] = (L::D == 3) ? double(w) : 0.0;
+  }
+}
+
+template <class L, int S>
+__global__ void __launch_bounds__(256) k_band_macro(StepArgs a, int blo0, int blo1, int blo2,
+                                                    int bn0, int bn1, int bn2, double *EV,
+                                                    double *RHO) {
+  const int64_t nb = (int64_t)bn0 * bn1 * bn2;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    int g[3];
+    g[0] = blo0 + (int)(t % bn0);
+    g[1] = blo1 + (int)((t / bn0) % bn1);
+    g[2] = blo2 + (int)(t / ((int64_t)bn0 * bn1));
+    double m4[4];
+    bool in = in_domain<L>(a, g[0], g[1], g[2]);
+    if (in || (a.macro_in && !a.self_fill)) {
+      // caller-filled macros carry their own ghost values
+      macro_at<L, S>(a, g[0], g[1], L::D == 3 ? g[2] : 0, m4);
+    } else {
+      int src[3], bd = 0, lo_side = 1;
+      const int kind = ghost_rule<L>(a, g, src, bd, lo_side);
+      macro_at<L, S>(a, src[0], src[1], L::D == 3 ? src[2] : 0, m4);
+      const double *bv = lo_side ? a.bvlo[bd] : a.bvhi[bd];
+      if (kind == 3) {
+        m4[0] = fmax(1.0e-20, X::sub(X::mul(2.0, bv[0]), m4[0]));
+        m4[1] = X::sub(X::mul(2.0, bv[1]), m4[1]);
+        m4[2] = X::sub(X::mul(2.0, bv[2]), m4[2]);
+        m4[3] = X::sub(X::mul(2.0, bv[3]), m4[3]);
+      } else if (kind == 1 || kind == 2) {
+        m4[0] = bv[0];
+        m4[1] = bv[1];
+        m4[2] = bv[2];
+        m4[3] = bv[3];
+      }
+    }
+    EV[t] = m4[1];
+    EV[t + nb] = m4[2];
+    EV[t + 2 * nb] = (L::D == 3) ? m4[3] : 0.0;
+    RHO[t] = m4[0];
+  }
+}
+
+template <class L, int S>
+static int launch_band_macro(ilbm_ctx *ctx, const StepArgs &a, const int *blo, const int *bn,
+                             double *EV, double *RHO) {
+  const int64_t nb = (int64_t)bn[0] * bn[1] * bn[2];
+  const int blocks = (int)std::min<int64_t>((nb + 255) / 256, 2048);
+  k_band_macro<L, S><<<blocks, 256, 0, ctx->stream>>>(a, blo[0], blo[1], blo[2], bn[0], bn[1],
+                                                      bn[2], EV, RHO);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "band macro launch");
+  return ILBM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+static int fill_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p,
+                     StepArgs &a) {
+  std::memset(&a, 0, sizeof(a));
+  const int D = ctx->dim;
+  for (int d = 0; d < 3; ++d) {
+    a.lo[d] = (d < D) ? b.lo[d] : 0;
+    a.hi[d] = (d < D) ? b.hi[d] : 0;
+    a.fgl[d] = (d < D) ? b.lo[d] - b.ngrow_f : 0;
+    a.mgl[d] = (d < D) ? b.lo[d] - b.ngrow_m : 0;
+  }
+  a.fs0 = b.fstride[0];
+  a.fs1 = b.fstride[1];
+  a.fs2 = b.fstride[2];
+  a.ms0 = b.mstride[0];
+  a.ms1 = b.mstride[1];
+  a.ms2 = b.mstride[2];
+  a.f_in = b.f_in;
+  a.f_out = b.f_out;
+  a.macro_in = b.macro_in;
+  a.force = b.force;
+  a.force_prev = b.force_prev;
+  if (p) {
+    for (int d = 0; d < 3; ++d) {
+      a.dlo[d] = (d < D) ? p->domain_lo[d] : 0;
+      a.dhi[d] = (d < D) ? p->domain_hi[d] : 0;
+      a.periodic[d] = (d < D) ? p->periodic[d] : 0;
+      a.bclo[d] = p->bc_lo[d];
+      a.bchi[d] = p->bc_hi[d];
+      for (int c = 0; c < 4; ++c) {
+        a.bvlo[d][c] = p->bc_val_lo[d][c];
+        a.bvhi[d][c] = p->bc_val_hi[d][c];
+      }
+      a.flo[d] = (d < D) ? p->force_lo[d] : 0;
+      a.fhi[d] = (d < D) ? p->force_hi[d] : 0;
+    }
+    a.tau = p->tau;
+    a.self_fill = (p->ghost_mode == ILBM_GHOST_SELF);
+    a.use_uniform = p->use_uniform_force;
+    for (int d = 0; d < 3; ++d) a.uf[d] = p->uniform_force[d];
+    a.f16_scale = (p->f16_scale > 0) ? float(p->f16_scale) : 1024.0f;
+    if (p->ghost_mode == ILBM_GHOST_CALLER) {
+      if (p->nlevel_boxes > kMaxLevelBoxes) {
+        set_error("level has more boxes than one call supports (64); split the call");
+        return ILBM_ERR_RANGE;
+      }
+      a.nlb = p->nlevel_boxes;
+      for (int n = 0; n < a.nlb; ++n)
+        for (int c = 0; c < 6; ++c) a.lb[n][c] = p->level_boxes[6 * n + c];
+    }
+  } else {
+    a.f16_scale = 1024.0f;
+  }
+  return ILBM_OK;
+}
+
+template <class L, int S>
+static int launch_step(ilbm_ctx *ctx, const StepArgs &a, const ilbm_level_params *p) {
+  const int nx = a.hi[0] - a.lo[0] + 1, ny = a.hi[1] - a.lo[1] + 1;
+  const int nz = (L::D == 3) ? a.hi[2] - a.lo[2] + 1 : 1;
+  if (a.self_fill) {
+    bool any_np = false;
+    for (int d = 0; d < L::D; ++d) any_np = any_np || !a.periodic[d];
+    if (any_np) {
+      int maxslab = 1;
+      for (int d = 0; d < L::D; ++d) {
+        int s = 1;
+        for (int e = 0; e < L::D; ++e)
+          if (e != d) s *= (a.dhi[e] - a.dlo[e] + 3);
+        maxslab = std::max(maxslab, s);
+      }
+      dim3 gg((maxslab + 255) / 256, 1, 2 * L::D);
+      gg.x = std::min<unsigned>(gg.x, 4096u);
+      k_ghost_fill<L, S><<<gg, 256, 0, ctx->stream>>>(a);
+      ctx->launches++;
+    }
+  }
+  const int bx = nx >= 256 ? 256 : ((nx + 31) / 32) * 32;
+  dim3 grid((nx + bx - 1) / bx, ny, nz);
+  k_step<L, S><<<grid, bx, 0, ctx->stream>>>(a);
+  ctx->launches++;
+  (void)p;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "level step launch");
+  return ILBM_OK;
+}
+
+template <class L, int S>
+static int launch_macro(ilbm_ctx *ctx, const StepArgs &a, const int *rlo, const int *rhi,
+                        void *macro_out) {
+  const int nx = rhi[0] - rlo[0] + 1, ny = rhi[1] - rlo[1] + 1;
+  const int nz = (L::D == 3) ? rhi[2] - rlo[2] + 1 : 1;
+  if (nx <= 0 || ny <= 0 || nz <= 0) return ILBM_OK;
+  const int bx = nx >= 256 ? 256 : ((nx + 31) / 32) * 32;
+  dim3 grid((nx + bx - 1) / bx, ny, nz);
+  k_macro<L, S><<<grid, bx, 0, ctx->stream>>>(a, rlo[0], rlo[1], (L::D == 3) ? rlo[2] : 0,
+                                              rhi[0], macro_out);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "macro launch");
+  return ILBM_OK;
+}
+
+template <class L, int S>
+static int launch_init(ilbm_ctx *ctx, const StepArgs &a, int ng) {
+  const int nx = a.hi[0] - a.lo[0] + 1 + 2 * ng, ny = a.hi[1] - a.lo[1] + 1 + 2 * ng;
+  const int nz = (L::D == 3) ? a.hi[2] - a.lo[2] + 1 + 2 * ng : 1;
+  const int bx = nx >= 256 ? 256 : ((nx + 31) / 32) * 32;
+  dim3 grid((nx + bx - 1) / bx, ny, nz);
+  k_init_eq<L, S><<<grid, bx, 0, ctx->stream>>>(a, ng);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "init launch");
+  return ILBM_OK;
+}
+
+#define ILBM_DISPATCH(ctx, FN, ...)                                                        \
+  [&]() -> int {                                                                           \
+    switch ((ctx)->q * 4 + (ctx)->storage) {                                               \
+      case 9 * 4 + ILBM_STORAGE_F64: return FN<Lat<9>, ILBM_STORAGE_F64>(__VA_ARGS__);     \
+      case 9 * 4 + ILBM_STORAGE_F32_SHIFT: return FN<Lat<9>, ILBM_STORAGE_F32_SHIFT>(__VA_ARGS__); \
+      case 9 * 4 + ILBM_STORAGE_F16_SCALED: return FN<Lat<9>, ILBM_STORAGE_F16_SCALED>(__VA_ARGS__); \
+      case 19 * 4 + ILBM_STORAGE_F64: return FN<Lat<19>, ILBM_STORAGE_F64>(__VA_ARGS__);   \
+      case 19 * 4 + ILBM_STORAGE_F32_SHIFT: return FN<Lat<19>, ILBM_STORAGE_F32_SHIFT>(__VA_ARGS__); \
+      case 19 * 4 + ILBM_STORAGE_F16_SCALED: return FN<Lat<19>, ILBM_STORAGE_F16_SCALED>(__VA_ARGS__); \
+      case 27 * 4 + ILBM_STORAGE_F64: return FN<Lat<27>, ILBM_STORAGE_F64>(__VA_ARGS__);   \
+      case 27 * 4 + ILBM_STORAGE_F32_SHIFT: return FN<Lat<27>, ILBM_STORAGE_F32_SHIFT>(__VA_ARGS__); \
+      case 27 * 4 + ILBM_STORAGE_F16_SCALED: return FN<Lat<27>, ILBM_STORAGE_F16_SCALED>(__VA_ARGS__); \
+      default: set_error("unsupported lattice/storage"); return ILBM_ERR_UNSUPPORTED;      \
+    }                                                                                      \
+  }()
+
+static int check_box(const ilbm_ctx *ctx, const ilbm_box &b, bool need_out) {
+  if (!b.f_in || (need_out && !b.f_out)) {
+    set_error("box: f_in/f_out must be set");
+    return ILBM_ERR_ARG;
+  }
+  for (int d = 0; d < ctx->dim; ++d)
+    if (b.hi[d] < b.lo[d]) {
+      set_error("box: empty valid region");
+      return ILBM_ERR_ARG;
+    }
+  if (b.fstride[0] <= 0 || b.fstride[1] <= 0 || b.fstride[2] <= 0) {
+    set_error("box: f strides must be positive");
+    return ILBM_ERR_ARG;
+  }
+  return ILBM_OK;
+}
+
+static int check_params(const ilbm_ctx *ctx, const ilbm_level_params *p) {
+  if (!p) {
+    set_error("level params missing");
+    return ILBM_ERR_ARG;
+  }
+  if (!(p->tau > 0.5)) {
+    set_error("tau must exceed 0.5");
+    return ILBM_ERR_ARG;
+  }
+  for (int d = 0; d < ctx->dim; ++d) {
+    if (p->periodic[d]) continue;
+    for (int s = 0; s < 2; ++s) {
+      const int bc = s ? p->bc_hi[d] : p->bc_lo[d];
+      if (bc != ILBM_BC_FOEXTRAP && bc != ILBM_BC_EXT_DIR && bc != ILBM_BC_USER_1 &&
+          bc != ILBM_BC_USER_2) {
+        set_error("non-periodic face needs BC foextrap(2), ext_dir(3), user_1(1001) or user_2(1002)");
+        return ILBM_ERR_UNSUPPORTED;
+      }
+    }
+  }
+  return ILBM_OK;
+}
+
+// Internal entry for the IB: band macro of box `b` into EV (3 x nb) and RHO.
+int band_macro(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p, const int *blo,
+               const int *bn, double *EV, double *RHO) {
+  StepArgs a;
+  int rc = fill_args(ctx, b, p, a);
+  if (rc) return rc;
+  return ILBM_DISPATCH(ctx, launch_band_macro, ctx, a, blo, bn, EV, RHO);
+}
+
+}  // namespace ilbm
+
+using namespace ilbm;
+
+void *ilbm_ctx_scratch(ilbm_ctx *ctx, size_t n) {
+  if (ctx->scratch_bytes >= n) return ctx->scratch;
+  if (ctx->scratch) cudaFree(ctx->scratch);
+  ctx->scratch = nullptr;
+  ctx->scratch_bytes = 0;
+  if (cudaMalloc(&ctx->scratch, n) != cudaSuccess) return nullptr;
+  ctx->scratch_bytes = n;
+  return ctx->scratch;
+}
+
+extern "C" {
+
+const char *ilbm_last_error(void) { return ilbm::get_error(); }
+
+int ilbm_create(const ilbm_lattice *lat, int storage, int device, void *cuda_stream,
+                ilbm_ctx **out) {
+  if (!lat || !out) {
+    set_error("ilbm_create: null argument");
+    return ILBM_ERR_ARG;
+  }
+  *out = nullptr;
+  if (storage < ILBM_STORAGE_F64 || storage > ILBM_STORAGE_F16_SCALED) {
+    set_error("ilbm_create: unknown storage form");
+    return ILBM_ERR_ARG;
+  }
+  // the lattice must be one of the three deck orderings, with w = wis/wim
+  int dim = 0;
+  auto match = [&](auto L) -> bool {
+    using LL = decltype(L);
+    if (lat->q != LL::Q) return false;
+    for (int q = 0; q < LL::Q; ++q) {
+      if (lat->cx[q] != double(LL::cx(q)) || lat->cy[q] != double(LL::cy(q)) ||
+          lat->cz[q] != double(LL::cz(q)))
+        return false;
+      if (lat->wim[q] == 0.0 || lat->wis[q] / lat->wim[q] != LL::w(q)) return false;
+    }
+    dim = LL::D;
+    return true;
+  };
+  if (!(match(Lat<9>{}) || match(Lat<19>{}) || match(Lat<27>{}))) {
+    set_error("ilbm_create: lattice must be D2Q9, D3Q19 or D3Q27 in the reference deck order");
+    return ILBM_ERR_UNSUPPORTED;
+  }
+  if (lat->dim != 0 && lat->dim != dim) {
+    set_error("ilbm_create: lattice dimension mismatch");
+    return ILBM_ERR_ARG;
+  }
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  auto *c = new ilbm_ctx();
+  c->q = lat->q;
+  c->dim = dim;
+  c->storage = storage;
+  c->device = device;
+  if (cuda_stream) {
+    c->stream = static_cast<cudaStream_t>(cuda_stream);
+  } else {
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete c;
+      return cuda_fail(e, "cudaStreamCreate");
+    }
+    c->own_stream = true;
+  }
+  for (int s = 0; s < 16; ++s) {
+    e = cudaEventCreate(&c->ev[s]);
+    if (e != cudaSuccess) {
+      ilbm_destroy(c);
+      return cuda_fail(e, "cudaEventCreate");
+    }
+  }
+  e = cudaMallocHost(&c->host_pinned, 64 * sizeof(double));
+  if (e != cudaSuccess) {
+    ilbm_destroy(c);
+    return cuda_fail(e, "cudaMallocHost");
+  }
+  *out = c;
+  return ILBM_OK;
+}
+
+int ilbm_destroy(ilbm_ctx *ctx) {
+  if (!ctx) return ILBM_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (int s = 0; s < 16; ++s)
+    if (ctx->ev[s]) cudaEventDestroy(ctx->ev[s]);
+  for (int s = 0; s < ctx->nxev; ++s)
+    if (ctx->xev[s]) cudaEventDestroy(ctx->xev[s]);
+  delete[] ctx->xev;
+  if (ctx->scratch) cudaFree(ctx->scratch);
+  if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return ILBM_OK;
+}
+
+int ilbm_sync(ilbm_ctx *ctx) {
+  if (!ctx) return ILBM_ERR_ARG;
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "stream synchronize");
+  return ILBM_OK;
+}
+
+void *ilbm_stream(ilbm_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+static cudaEvent_t *event_slot(ilbm_ctx *ctx, int slot) {
+  if (slot < 0 || slot >= 16 + 8192) return nullptr;
+  if (slot < 16) return &ctx->ev[slot];
+  const int x = slot - 16;
+  if (x >= ctx->nxev) {
+    const int n = std::max(x + 1, std::max(64, 2 * ctx->nxev));
+    auto *nv = new cudaEvent_t[n];
+    for (int i = 0; i < ctx->nxev; ++i) nv[i] = ctx->xev[i];
+    for (int i = ctx->nxev; i < n; ++i) nv[i] = nullptr;
+    delete[] ctx->xev;
+    ctx->xev = nv;
+    ctx->nxev = n;
+  }
+  if (!ctx->xev[x] && cudaEventCreate(&ctx->xev[x]) != cudaSuccess) return nullptr;
+  return &ctx->xev[x];
+}
+
+int ilbm_event_record(ilbm_ctx *ctx, int slot) {
+  if (!ctx) return ILBM_ERR_ARG;
+  cudaEvent_t *ev = event_slot(ctx, slot);
+  if (!ev) {
+    set_error("event slot out of range (0..8207)");
+    return ILBM_ERR_ARG;
+  }
+  cudaError_t e = cudaEventRecord(*ev, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaEventRecord");
+  return ILBM_OK;
+}
+
+int ilbm_event_elapsed_ms(ilbm_ctx *ctx, int a, int b, float *ms) {
+  if (!ctx || !ms) return ILBM_ERR_ARG;
+  cudaEvent_t *ea = event_slot(ctx, a), *eb = event_slot(ctx, b);
+  if (!ea || !eb) {
+    set_error("event slot out of range");
+    return ILBM_ERR_ARG;
+  }
+  cudaError_t e = cudaEventSynchronize(*eb);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaEventSynchronize");
+  e = cudaEventElapsedTime(ms, *ea, *eb);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaEventElapsedTime");
+  return ILBM_OK;
+}
+
+int64_t ilbm_kernel_launches(const ilbm_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int ilbm_storage_bytes(const ilbm_ctx *ctx, int *sb, int *rb) {
+  if (!ctx) return ILBM_ERR_ARG;
+  const int s = ctx->storage == ILBM_STORAGE_F64 ? 8 : (ctx->storage == ILBM_STORAGE_F32_SHIFT ? 4 : 2);
+  if (sb) *sb = s;
+  if (rb) *rb = ctx->storage == ILBM_STORAGE_F64 ? 8 : 4;
+  return ILBM_OK;
+}
+
+int ilbm_level_step(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const ilbm_level_params *p) {
+  if (!ctx || !boxes || nbox <= 0) {
+    set_error("ilbm_level_step: null argument");
+    return ILBM_ERR_ARG;
+  }
+  int rc = check_params(ctx, p);
+  if (rc) return rc;
+  if (p->ghost_mode == ILBM_GHOST_SELF) {
+    if (nbox != 1) {
+      set_error("self-fill ghost mode needs exactly one box covering the domain");
+      return ILBM_ERR_ARG;
+    }
+    for (int d = 0; d < ctx->dim; ++d)
+      if (boxes[0].lo[d] != p->domain_lo[d] || boxes[0].hi[d] != p->domain_hi[d]) {
+        set_error("self-fill ghost mode: the box must equal the domain");
+        return ILBM_ERR_ARG;
+      }
+    if (boxes[0].ngrow_f < 1) {
+      set_error("self-fill ghost mode needs ngrow_f >= 1 for the synthesised ghost layer");
+      return ILBM_ERR_ARG;
+    }
+  } else if (p->ghost_mode != ILBM_GHOST_CALLER) {
+    set_error("unknown ghost mode");
+    return ILBM_ERR_ARG;
+  }
+  for (int n = 0; n < nbox; ++n) {
+    const ilbm_box &b = boxes[n];
+    if ((rc = check_box(ctx, b, true))) return rc;
+    if (p->ghost_mode == ILBM_GHOST_CALLER && b.ngrow_f < 1) {
+      set_error("caller ghost mode needs ngrow_f >= 1");
+      return ILBM_ERR_ARG;
+    }
+    if (b.f_in == b.f_out) {
+      set_error("f_in and f_out must be distinct (two-lattice scheme)");
+      return ILBM_ERR_ARG;
+    }
+    StepArgs a;
+    if ((rc = fill_args(ctx, b, p, a))) return rc;
+    rc = ILBM_DISPATCH(ctx, launch_step, ctx, a, p);
+    if (rc) return rc;
+    if (b.macro_out) {
+      StepArgs am = a;
+      am.f_in = b.f_out;
+      int rlo[3] = {a.lo[0], a.lo[1], a.lo[2]}, rhi[3] = {a.hi[0], a.hi[1], a.hi[2]};
+      rc = ILBM_DISPATCH(ctx, launch_macro, ctx, am, rlo, rhi, b.macro_out);
+      if (rc) return rc;
+    }
+  }
+  return ILBM_OK;
+}
+
+int ilbm_compute_macro(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
+                       const void *f, const void *force, void *macro_out, const int lo[3],
+                       const int hi[3]) {
+  if (!ctx || !box || !f || !macro_out) {
+    set_error("ilbm_compute_macro: null argument");
+    return ILBM_ERR_ARG;
+  }
+  StepArgs a;
+  int rc = fill_args(ctx, *box, p, a);
+  if (rc) return rc;
+  a.f_in = f;
+  a.force = force;
+  if (!p) {
+    for (int d = 0; d < 3; ++d) {
+      a.flo[d] = -(1 << 30);
+      a.fhi[d] = (1 << 30);
+    }
+  }
+  int rlo[3], rhi[3];
+  for (int d = 0; d < 3; ++d) {
+    const bool use = d < ctx->dim;
+    rlo[d] = use ? std::max(lo ? lo[d] : box->lo[d], box->lo[d]) : 0;
+    rhi[d] = use ? std::min(hi ? hi[d] : box->hi[d], box->hi[d]) : 0;
+  }
+  return ILBM_DISPATCH(ctx, launch_macro, ctx, a, rlo, rhi, macro_out);
+}
+
+int ilbm_init_equilibrium(ilbm_ctx *ctx, const ilbm_box *box) {
+  if (!ctx || !box || !box->f_in || !box->f_out || !box->macro_in) {
+    set_error("ilbm_init_equilibrium: f_in, f_out and macro_in are required");
+    return ILBM_ERR_ARG;
+  }
+  if (box->ngrow_m < box->ngrow_f) {
+    set_error("ilbm_init_equilibrium: macro ghost width must cover the f ghost width");
+    return ILBM_ERR_ARG;
+  }
+  StepArgs a;
+  int rc = fill_args(ctx, *box, nullptr, a);
+  if (rc) return rc;
+  return ILBM_DISPATCH(ctx, launch_init, ctx, a, box->ngrow_f);
+}
+
+}  // extern "C"

@@ -1,0 +1,370 @@
+"""Single-level driver over the C ABI: the host-side mirror of the reference's
+per-level loop.
+
+``LevelSolver.advance_phi_at_level()`` plays the role of
+``AmrCoreLBM::AdvancePhiAtLevel`` (Source/Core/AdvanceLBMAtLevel.cpp:20-394)
+for one level held in one box: optional ``IBMarkerDF::update_forcing`` on the
+level, then the fused collide-stream.  ``compute_ib_force()`` mirrors
+``AmrCoreLBM::ComputeIBForce`` (Source/Core/AmrCoreLBM.cpp:456-631) without the
+``force.dat`` file.  Device memory comes from PyTorch (plumbing only); every
+computation is a call into ``libilbm_b200.so``.
+
+State kept between steps (the reference's f_new / macro_new / forcing):
+  * ``f``      -- f^n, pre-collision populations (storage form);
+  * ``force``  -- F^{n-1}, the Guo force of the last step (IB band only);
+  * the macro fields are not stored: rho^n, u^n are recovered from f^n and
+    F^{n-1} inside the kernels, which reproduces the stored values bit for bit
+    (the reference computes them from the same data).  Step 0 reads the
+    initial macro fields instead.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+
+from . import capi
+from .cases import LevelCase, MarkerIB
+
+_TORCH_DT = {"f64": torch.float64, "f32": torch.float32, "f16": torch.float16}
+_REAL_DT = {"f64": torch.float64, "f32": torch.float32, "f16": torch.float32}
+
+
+def lattice_struct(lat) -> capi.Lattice_t:
+    s = capi.Lattice_t()
+    s.dim, s.q = lat.dim, lat.q
+    for q in range(lat.q):
+        s.cx[q], s.cy[q], s.cz[q] = lat.c[q]
+        s.wis[q], s.wim[q] = lat.wis[q], lat.wim[q]
+    return s
+
+
+def level_params(case: LevelCase, uniform_force: bool, f16_scale: float = 1024.0) -> capi.LevelParams_t:
+    p = capi.LevelParams_t()
+    p.tau = case.tau
+    for d in range(3):
+        p.domain_lo[d] = 0
+        p.domain_hi[d] = case.n_cell[d] - 1 if d < case.dim else 0
+        p.periodic[d] = int(case.periodic[d]) if d < case.dim else 0
+        allp = all(case.periodic[: case.dim])
+        p.bc_lo[d] = case.bc_lo[d] if not allp else 0
+        p.bc_hi[d] = case.bc_hi[d] if not allp else 0
+        for c in range(4):
+            p.bc_val_lo[d][c] = case.bc_lo_val[d][c] if not allp else 0.0
+            p.bc_val_hi[d][c] = case.bc_hi_val[d][c] if not allp else 0.0
+        p.force_lo[d] = 0
+        p.force_hi[d] = -1
+    p.ghost_mode = capi.GHOST_SELF
+    if uniform_force and case.prescribed_force is not None:
+        p.use_uniform_force = 1
+        for d in range(3):
+            p.uniform_force[d] = case.prescribed_force[d]
+    p.f16_scale = f16_scale
+    return p
+
+
+def level_geom(case: LevelCase) -> capi.LevelGeom_t:
+    g = capi.LevelGeom_t()
+    g.dim = case.dim
+    allp = all(case.periodic[: case.dim])
+    for d in range(3):
+        g.n_cell[d] = case.n_cell[d]
+        g.prob_lo[d] = case.prob_lo[d]
+        g.prob_hi[d] = case.prob_hi[d]
+        g.periodic[d] = int(case.periodic[d]) if d < case.dim else 0
+        g.bc_lo[d] = case.bc_lo[d] if not allp else 0
+        g.bc_hi[d] = case.bc_hi[d] if not allp else 0
+        for c in range(4):
+            g.bc_val_lo[d][c] = case.bc_lo_val[d][c] if not allp else 0.0
+            g.bc_val_hi[d][c] = case.bc_hi_val[d][c] if not allp else 0.0
+    return g
+
+
+def ib_params(ib: MarkerIB, dim: int) -> capi.IBParams_t:
+    s = capi.IBParams_t()
+    for name, _ in capi.IBParams_t._fields_:
+        if hasattr(ib, name):
+            setattr(s, name, getattr(ib, name))
+    af = ib.airfoil if ib.airfoil is not None else MarkerIB.AIRFOIL_DEFAULT
+    (s.airfoil_chord, s.airfoil_thickness, s.pitch_mean, s.pitch_amplitude,
+     s.pitch_frequency, s.pitch_phase, s.pivot_x) = af
+    if dim == 2:
+        s.z0 = 0.0
+    return s
+
+
+class Context:
+    """Owns an ``ilbm_ctx`` (lattice + storage form + stream)."""
+
+    def __init__(self, lattice, storage: str = "f64", device: int = 0):
+        self.L = capi.lib()
+        self.storage = storage
+        self._lat = lattice_struct(lattice)
+        h = C.c_void_p()
+        capi.check(self.L.ilbm_create(C.byref(self._lat), capi.STORAGE[storage], device, None,
+                                      C.byref(h)), "ilbm_create")
+        self.h = h
+
+    def sync(self):
+        capi.check(self.L.ilbm_sync(self.h), "ilbm_sync")
+
+    def launches(self) -> int:
+        return int(self.L.ilbm_kernel_launches(self.h))
+
+    def record(self, slot: int):
+        capi.check(self.L.ilbm_event_record(self.h, slot), "event_record")
+
+    def elapsed_ms(self, a: int, b: int) -> float:
+        ms = C.c_float()
+        capi.check(self.L.ilbm_event_elapsed_ms(self.h, a, b, C.byref(ms)), "event_elapsed")
+        return float(ms.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.ilbm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class LevelSolver:
+    """One level held in one box, stepped on the GPU through the C ABI."""
+
+    def __init__(self, case: LevelCase, storage: str = "f64", ib: MarkerIB | None = None,
+                 device: int = 0, f16_scale: float = 1024.0, ctx: Context | None = None):
+        if not torch.cuda.is_available():
+            raise capi.IlbmError("LevelSolver needs a CUDA device")
+        self.case = case
+        self.storage = storage
+        self.dev = torch.device("cuda", device)
+        self.ctx = ctx or Context(case.lattice, storage, device)
+        self.L = self.ctx.L
+        self.q = case.lattice.q
+        self.dim = case.dim
+        self.gf, self.gm = 1, 2
+        nx, ny, nz = case.n_cell
+        gz_f = nz + 2 * self.gf if self.dim == 3 else 1
+        gz_m = nz + 2 * self.gm if self.dim == 3 else 1
+        self.fshape = (self.q, gz_f, ny + 2 * self.gf, nx + 2 * self.gf)
+        self.mshape_g = (gz_m, ny + 2 * self.gm, nx + 2 * self.gm)
+        fdt, rdt = _TORCH_DT[storage], _REAL_DT[storage]
+        self.f = torch.zeros(self.fshape, dtype=fdt, device=self.dev)
+        self.f_next = torch.zeros(self.fshape, dtype=fdt, device=self.dev)
+        self.macro = torch.zeros((4,) + self.mshape_g, dtype=rdt, device=self.dev)
+        self.force_cur = torch.zeros((3,) + self.mshape_g, dtype=rdt, device=self.dev)
+        self.force_prev = torch.zeros((3,) + self.mshape_g, dtype=rdt, device=self.dev)
+        self.f16_scale = f16_scale
+        self.params = level_params(case, uniform_force=(ib is None), f16_scale=f16_scale)
+        self.ib = None
+        self.ib_case = ib
+        if ib is not None:
+            self._geom = level_geom(case)
+            self._ibp = ib_params(ib, self.dim)
+            h = C.c_void_p()
+            capi.check(self.L.ilbm_ib_create(self.ctx.h, C.byref(self._ibp), C.byref(self._geom),
+                                             C.byref(h)), "ilbm_ib_create")
+            self.ib = h
+            lo, hi = (C.c_int * 3)(), (C.c_int * 3)()
+            capi.check(self.L.ilbm_ib_force_region(self.ib, lo, hi), "ib_force_region")
+            for d in range(3):
+                self.params.force_lo[d], self.params.force_hi[d] = lo[d], hi[d]
+            self.force_region = (tuple(lo), tuple(hi))
+        self.time = 0.0
+        self.istep = 0
+        self.first_step_macro = False
+        self.have_prev_body = False
+        self.prev_body = np.zeros(3)
+        self.rec = np.zeros(18)
+
+    # ---- layout helpers ---------------------------------------------------
+    def _box(self, f_in, f_out, macro_in=None, macro_out=None, force=None, force_prev=None):
+        b = capi.Box_t()
+        for d in range(3):
+            b.lo[d] = 0
+            b.hi[d] = self.case.n_cell[d] - 1 if d < self.dim else 0
+        b.ngrow_f, b.ngrow_m = self.gf, self.gm
+        fs = self.f.stride()
+        b.fstride[0], b.fstride[1], b.fstride[2] = fs[2], fs[1], fs[0]
+        ms = self.macro.stride()
+        b.mstride[0], b.mstride[1], b.mstride[2] = ms[2], ms[1], ms[0]
+        b.f_in = f_in.data_ptr()
+        b.f_out = f_out.data_ptr() if f_out is not None else None
+        b.macro_in = macro_in.data_ptr() if macro_in is not None else None
+        b.macro_out = macro_out.data_ptr() if macro_out is not None else None
+        b.force = force.data_ptr() if force is not None else None
+        b.force_prev = force_prev.data_ptr() if force_prev is not None else None
+        return b
+
+    def _valid(self, t, g):
+        nx, ny, nz = self.case.n_cell
+        if self.dim == 3:
+            return t[..., g:g + nz, g:g + ny, g:g + nx]
+        return t[..., :, g:g + ny, g:g + nx]
+
+    # ---- initialisation (MakeNewLevelFromScratch + InitEquilibrium) --------
+    def set_macro(self, rho, ux, uy, uz=None):
+        """Initial macro fields on valid cells ([nz, ny, nx]); f = f_eq(rho, u)."""
+        v = self._valid(self.macro, self.gm)
+        rdt = self.macro.dtype
+        v[0].copy_(torch.as_tensor(np.asarray(rho), dtype=rdt))
+        v[1].copy_(torch.as_tensor(np.asarray(ux), dtype=rdt))
+        v[2].copy_(torch.as_tensor(np.asarray(uy), dtype=rdt))
+        if uz is not None:
+            v[3].copy_(torch.as_tensor(np.asarray(uz), dtype=rdt))
+        torch.cuda.synchronize(self.dev)
+        b = self._box(self.f, self.f_next, macro_in=self.macro)
+        capi.check(self.L.ilbm_init_equilibrium(self.ctx.h, C.byref(b)), "init_equilibrium")
+        self.ctx.sync()
+        self.first_step_macro = True
+        self.time = 0.0
+        self.istep = 0
+
+    def set_f(self, f):
+        """Populations f^n (unshifted, float64, [Q, nz, ny, nx]) on valid cells."""
+        f = torch.as_tensor(np.asarray(f, dtype=np.float64))
+        if self.storage != "f64":
+            w = torch.tensor(self.case.lattice.w, dtype=torch.float64).view(-1, 1, 1, 1)
+            f = f - w
+            if self.storage == "f16":
+                f = f * (self.f16_scale / w)
+        self._valid(self.f, self.gf).copy_(f.to(self.f.dtype))
+        torch.cuda.synchronize(self.dev)
+        self.first_step_macro = False
+
+    def set_force_prev(self, F):
+        """F^{n-1} on valid cells ([3, nz, ny, nx]) -- the force of the step that produced f."""
+        self._valid(self.force_prev, self.gm).copy_(torch.as_tensor(np.asarray(F), dtype=self.force_prev.dtype))
+        torch.cuda.synchronize(self.dev)
+
+    # ---- the level step ---------------------------------------------------
+    def advance_phi_at_level(self, record_force: bool = False):
+        use_macro = self.macro if self.first_step_macro else None
+        ib_on = self.ib is not None
+        b = self._box(self.f, self.f_next, macro_in=use_macro,
+                      force=self.force_cur if ib_on else None,
+                      force_prev=self.force_prev if ib_on else None)
+        if ib_on:
+            capi.check(self.L.ilbm_ib_update_forcing(self.ib, C.byref(b), C.byref(self.params),
+                                                     self.case.dt, self.time), "ib_update_forcing")
+        capi.check(self.L.ilbm_level_step(self.ctx.h, C.byref(b), 1, C.byref(self.params)),
+                   "level_step")
+        self.f, self.f_next = self.f_next, self.f
+        self.force_cur, self.force_prev = self.force_prev, self.force_cur
+        self.first_step_macro = False
+        self.time += self.case.dt
+        self.istep += 1
+        if record_force and ib_on:
+            self.compute_ib_force()
+
+    def step(self, n: int = 1, record_force: bool = False):
+        for _ in range(n):
+            self.advance_phi_at_level(record_force=record_force)
+
+    # ---- force evaluation (ComputeIBForce, AmrCoreLBM.cpp:456-631) --------
+    def compute_ib_force(self):
+        case, ib = self.case, self.ib_case
+        lo, hi = self.force_region
+        b = self._box(self.f, None)
+        s = (C.c_double * 3)()
+        capi.check(self.L.ilbm_force_integrals(self.ctx.h, C.byref(b), self.force_prev.data_ptr(),
+                                               capi.ivec3(lo), capi.ivec3(hi), s), "force_integrals")
+        Fs = np.array([s[0], s[1], s[2] if self.dim == 3 else 0.0])
+        dV = case.dx ** self.dim
+        Feul = -(Fs * dV) / case.dt
+        m = (C.c_double * 3)()
+        capi.check(self.L.ilbm_ib_last_marker_force_sum(self.ib, m), "marker_force_sum")
+        Fm = -np.array([m[0], m[1], m[2]])
+        Fme = Feul.copy()
+        Fb = {0: Fme, 1: Feul, 2: Fm}.get(ib.force_eval_method, Feul)
+        Ftc = 0.5 * (self.prev_body + Fb) if self.have_prev_body else Fb.copy()
+        self.prev_body = Fb.copy()
+        self.have_prev_body = True
+        U = ib.U0
+        denom = (0.5 * 1.0 * U * U * (math.pi * ib.R * ib.R)) if self.dim == 3 else (0.5 * 1.0 * U * U * (2.0 * ib.R))
+        rec = np.zeros(18)
+        rec[0:3], rec[6:9], rec[9:12], rec[12:15], rec[15:18] = Ftc, Fb, Feul, Fm, Fme
+        if denom > 0:
+            rec[3], rec[4] = Ftc[0] / denom, Ftc[1] / denom
+            if self.dim == 3:
+                rec[5] = Ftc[2] / denom
+        self.rec = rec
+        return rec
+
+    # ---- read-back ---------------------------------------------------------
+    def get_f(self) -> np.ndarray:
+        self.ctx.sync()
+        v = self._valid(self.f, self.gf).to(torch.float64)
+        if self.storage != "f64":
+            w = torch.tensor(self.case.lattice.w, dtype=torch.float64, device=self.dev).view(-1, 1, 1, 1)
+            if self.storage == "f16":
+                v = v * (w / self.f16_scale)
+            v = v + w
+        return v.cpu().numpy()
+
+    def get_macro(self) -> np.ndarray:
+        """rho, u, v, w of the current state (calculateMacroForcing with F^{n-1})."""
+        out = torch.zeros_like(self.macro)
+        b = self._box(self.f, None)
+        p = self.params
+        force = self.force_prev if self.ib is not None else None
+        capi.check(self.L.ilbm_compute_macro(self.ctx.h, C.byref(b), C.byref(p), self.f.data_ptr(),
+                                             force.data_ptr() if force is not None else None,
+                                             out.data_ptr(), None, None), "compute_macro")
+        self.ctx.sync()
+        return self._valid(out, self.gm).to(torch.float64).cpu().numpy()
+
+    def get_force(self) -> np.ndarray:
+        """Force F used in the last step ([3, nz, ny, nx])."""
+        self.ctx.sync()
+        if self.ib is None:
+            sh = (3,) + self.case.shape
+            pf = self.case.prescribed_force or (0.0, 0.0, 0.0)
+            return np.stack([np.full(self.case.shape, pf[d]) for d in range(3)]).reshape(sh)
+        return self._valid(self.force_prev, self.gm).to(torch.float64).cpu().numpy()
+
+    def num_markers(self) -> int:
+        n = C.c_int64()
+        capi.check(self.L.ilbm_ib_num_markers(self.ib, C.byref(n)), "num_markers")
+        return int(n.value)
+
+    def marker_force_sum(self) -> np.ndarray:
+        m = (C.c_double * 3)()
+        capi.check(self.L.ilbm_ib_last_marker_force_sum(self.ib, m), "marker_force_sum")
+        return np.array([m[0], m[1], m[2]])
+
+    def markers(self):
+        n = self.num_markers()
+        xyz, uvw, F = (np.zeros(3 * n) for _ in range(3))
+        dp = C.POINTER(C.c_double)
+        capi.check(self.L.ilbm_ib_markers(self.ib, xyz.ctypes.data_as(dp), uvw.ctypes.data_as(dp),
+                                          F.ctypes.data_as(dp)), "ib_markers")
+        return xyz.reshape(3, n).T, uvw.reshape(3, n).T, F.reshape(3, n).T
+
+    def momentum_exchange(self, x0, y0, z0, R, one_sided=False) -> np.ndarray:
+        b = self._box(self.f, None)
+        out = (C.c_double * 3)()
+        dx = [self.case.dx] * 3
+        capi.check(self.L.ilbm_momentum_exchange(self.ctx.h, C.byref(b), C.byref(self.params),
+                                                 self.f.data_ptr(), x0, y0, z0, R,
+                                                 capi.dvec3(self.case.prob_lo), capi.dvec3(dx),
+                                                 int(one_sided), out), "momentum_exchange")
+        return np.array([out[0], out[1], out[2]])
+
+    def close(self):
+        if self.ib is not None:
+            self.L.ilbm_ib_destroy(self.ib)
+            self.ib = None
+        if self.ctx is not None:
+            self.ctx.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

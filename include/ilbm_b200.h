@@ -1,0 +1,242 @@
+/*
+ * ilbm_b200.h -- C ABI of the B200 (sm_100a) level-step library for the
+ * iLBMReX per-level hot path.
+ *
+ * The reference has no plugin or FFI for this path: its seam is a set of C++
+ * member calls inside one binary.  Each entry point below replaces one of
+ * them (reference paths are relative to the reference project root):
+ *
+ *   ilbm_level_step        AmrCoreLBM::AdvancePhiAtLevel, the collide /
+ *                          bounce-back / stream / macro passes
+ *                          (Source/Core/AdvanceLBMAtLevel.cpp:20-21, 196-386)
+ *                          with the ghost fill of FillPatchMesoscopic
+ *                          (Source/Core/AmrCoreLBM.cpp:1531-1628 using
+ *                          mesoscopicBcFill, Source/BC/bc_fill.H:303-347)
+ *   ilbm_compute_macro     calculateMacroForcing pass
+ *                          (Source/LBM/calculateMacroForcing.H:9-32,
+ *                          Source/Core/AdvanceLBMAtLevel.cpp:382-386)
+ *   ilbm_init_equilibrium  AmrCoreLBM::InitEquilibrium
+ *                          (Source/Core/AmrCoreLBM.cpp:2117-2164)
+ *   ilbm_ib_create         IBMarkerDF::IBMarkerDF + build_markers
+ *                          (Source/IBM/IBMarkerDF.H:68-70,
+ *                          Source/IBM/IBMarkerDF.cpp:190-497)
+ *   ilbm_ib_update_forcing IBMarkerDF::update_forcing
+ *                          (Source/IBM/IBMarkerDF.H:76-87,
+ *                          Source/IBM/IBMarkerDF.cpp:1522-1917)
+ *   ilbm_ib_last_marker_force_sum / ilbm_ib_num_markers
+ *                          IBMarkerDF::last_marker_force_sum / num_markers
+ *                          (Source/IBM/IBMarkerDF.H:90-91)
+ *   ilbm_force_integrals   the Eulerian forcing integral of
+ *                          AmrCoreLBM::ComputeIBForce
+ *                          (Source/Core/AmrCoreLBM.cpp:489-509)
+ *   ilbm_momentum_exchange IBForceEval::ComputeMomentumExchangeBodyForce
+ *                          (Source/IBM/IBForceEval.H:24-32,
+ *                          Source/IBM/IBForceEval.cpp:28-191)
+ *
+ * Conventions
+ *   - The caller owns every field buffer (device memory).  The library never
+ *     frees caller memory; it allocates only internal scratch inside a
+ *     context or IB object.
+ *   - Every call returns ILBM_OK (0) or a negative status and never aborts.
+ *     ilbm_last_error() returns the message of the last failure on the
+ *     calling thread.
+ *   - Calls are asynchronous on the context's stream, except the ones that
+ *     return host values (force sums, integrals, marker counts), which
+ *     synchronise that stream.
+ *   - One context per host thread / stream.  There is no global mutable state
+ *     apart from the per-thread error message.
+ *
+ * Field layout (AMReX Array4): element (i,j,k,n) of a box whose allocated
+ * (grown) region starts at glo = lo - ngrow lives at
+ *     ptr[(i-glo.x) + (j-glo.y)*s0 + (k-glo.z)*s1 + n*s2]
+ * with (s0,s1,s2) the box's jstride, kstride and component stride.  In 2D the
+ * k index is 0 and glo.z = 0.
+ *
+ * Storage forms (ilbm_create):
+ *   ILBM_STORAGE_F64         populations f_q stored and collided in double;
+ *                            macro/force arrays are double.
+ *   ILBM_STORAGE_F32_SHIFT   stored g_q = f_q - w_q in float, collided in
+ *                            float; macro/force arrays are float.
+ *   ILBM_STORAGE_F16_SCALED  stored h_q = (f_q - w_q) * scale / w_q in IEEE
+ *                            half, collided in float; macro/force float.
+ */
+#ifndef ILBM_B200_H
+#define ILBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ILBM_OK 0
+#define ILBM_ERR_ARG (-1)
+#define ILBM_ERR_CUDA (-2)
+#define ILBM_ERR_UNSUPPORTED (-3)
+#define ILBM_ERR_NOMEM (-4)
+#define ILBM_ERR_SOLVER (-5)
+#define ILBM_ERR_RANGE (-6)
+
+#define ILBM_STORAGE_F64 0
+#define ILBM_STORAGE_F32_SHIFT 1
+#define ILBM_STORAGE_F16_SCALED 2
+
+/* AMReX BCType codes accepted on non-periodic faces */
+#define ILBM_BC_INT_DIR 0
+#define ILBM_BC_FOEXTRAP 2
+#define ILBM_BC_EXT_DIR 3
+#define ILBM_BC_USER_1 1001
+#define ILBM_BC_USER_2 1002
+
+#define ILBM_MAX_Q 27
+
+typedef struct ilbm_ctx ilbm_ctx;
+typedef struct ilbm_ib ilbm_ib;
+
+/* Discrete velocity set as the reference reads it from its deck
+ * (lbm2d|lbm3d.{ndir,wis,wim,dirx,diry,dirz}, AmrCoreLBM.cpp:1212-1236).
+ * Must be D2Q9, D3Q19 or D3Q27 in the reference decks' direction order. */
+typedef struct {
+  int dim;
+  int q;
+  double cx[ILBM_MAX_Q], cy[ILBM_MAX_Q], cz[ILBM_MAX_Q];
+  double wis[ILBM_MAX_Q], wim[ILBM_MAX_Q];
+} ilbm_lattice;
+
+/* One box of a level (one FAB of f_old/f_new/macro/forcing in AMReX terms). */
+typedef struct {
+  int lo[3], hi[3]; /* valid region, inclusive, level index space */
+  int ngrow_f;      /* ghost width allocated around f_in / f_out */
+  int ngrow_m;      /* ghost width allocated around macro / force arrays */
+  int64_t fstride[3]; /* f arrays: j, k, component strides (elements) */
+  int64_t mstride[3]; /* macro / force arrays: j, k, component strides */
+  void *f_in;       /* f^n (storage type); ghost layer 1 filled per ghost_mode */
+  void *f_out;      /* f^{n+1} on valid cells (storage type) */
+  void *macro_in;   /* rho,u,v,w at step n (real type) or NULL (recomputed) */
+  void *macro_out;  /* rho,u,v,w at step n+1 (real type) or NULL */
+  void *force;      /* F^n = dt*rho*a (3 comps, real type) or NULL */
+  void *force_prev; /* F^{n-1} (3 comps) used when macro_in == NULL, or NULL */
+} ilbm_box;
+
+#define ILBM_GHOST_SELF 0   /* the library synthesises physical/periodic ghosts; one box = domain */
+#define ILBM_GHOST_CALLER 1 /* caller filled f_in/macro_in/force ghosts (AMReX FillPatch) */
+
+typedef struct {
+  double tau;
+  int domain_lo[3], domain_hi[3];
+  int periodic[3];
+  int bc_lo[3], bc_hi[3];
+  double bc_val_lo[3][4]; /* per dim: rho, ux, uy, uz (BCBuf lo_*) */
+  double bc_val_hi[3][4]; /* per dim: rho, ux, uy, uz (BCBuf hi_*) */
+  int ghost_mode;
+  int use_uniform_force;     /* lbm.prescribed_force, applied where force == NULL */
+  double uniform_force[3];
+  int force_lo[3], force_hi[3]; /* cells outside this region have zero force
+                                   (both force and force_prev); ignored for uniform */
+  double f16_scale;          /* ILBM_STORAGE_F16_SCALED only; 0 selects the default */
+  /* ILBM_GHOST_CALLER: boxes of the whole level, to classify ghost cells as
+   * covered (collided like the neighbour's valid cell) or not (kept). */
+  const int *level_boxes; /* host array of nlevel_boxes * 6 ints (lo xyz, hi xyz) or NULL */
+  int nlevel_boxes;
+} ilbm_level_params;
+
+/* ---- context ------------------------------------------------------------ */
+int ilbm_create(const ilbm_lattice *lat, int storage, int device, void *cuda_stream,
+                ilbm_ctx **out);
+int ilbm_destroy(ilbm_ctx *ctx);
+const char *ilbm_last_error(void);
+int ilbm_sync(ilbm_ctx *ctx);
+void *ilbm_stream(ilbm_ctx *ctx);
+/* CUDA events on the context stream, for device-side timing (slots 0..8207;
+ * slots from 16 up are created on first use). */
+int ilbm_event_record(ilbm_ctx *ctx, int slot);
+int ilbm_event_elapsed_ms(ilbm_ctx *ctx, int slot_a, int slot_b, float *ms);
+/* number of kernels this context has launched since creation */
+int64_t ilbm_kernel_launches(const ilbm_ctx *ctx);
+/* storage element size in bytes and real (macro/force) element size */
+int ilbm_storage_bytes(const ilbm_ctx *ctx, int *storage_bytes, int *real_bytes);
+
+/* ---- level step --------------------------------------------------------- */
+/* One level step on nbox boxes: BGK collision with Guo forcing on valid cells,
+ * halfway bounce-back for user_1 faces and pull streaming into f_out, with the
+ * reference's ghost semantics.  If macro_out is set, rho/u of f^{n+1} are
+ * written as well (calculateMacroForcing with F^n). */
+int ilbm_level_step(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox,
+                    const ilbm_level_params *p);
+/* rho,u,v,w of f (valid cells of region [lo,hi] clipped to the box) with the
+ * half-force shift of F (force array, uniform force or zero). */
+int ilbm_compute_macro(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
+                       const void *f, const void *force, void *macro_out,
+                       const int lo[3], const int hi[3]);
+/* f = f_eq(rho,u) over the whole allocated box (valid + ngrow_f ghosts),
+ * written to both f_in and f_out (InitEquilibrium). macro_in must cover the
+ * same region (ngrow_m >= ngrow_f). */
+int ilbm_init_equilibrium(ilbm_ctx *ctx, const ilbm_box *box);
+
+/* ---- marker direct-forcing IBM ----------------------------------------- */
+typedef struct {
+  int dim;
+  int n_cell[3];
+  double prob_lo[3], prob_hi[3];
+  int periodic[3];
+  int bc_lo[3], bc_hi[3];
+  double bc_val_lo[3][4], bc_val_hi[3][4];
+} ilbm_level_geom;
+
+typedef struct {
+  /* MarkerIBParams, Source/IBM/MarkerIBParams.H:8-132 */
+  int coupling_method; /* 0 explicit, 1 ivc (wu_shu), 2 explicit_diag */
+  int delta_type;      /* 0/4: 4-point, 1/3: 3-point */
+  int loop_ns;
+  double mdf_relax;
+  double explicit_diag_eps;
+  int geometry_type;   /* 0 cylinder/sphere, 1 box, 2 user-defined pitching NACA */
+  double box_xlo, box_xhi, box_ylo, box_yhi, box_zlo, box_zhi, box_ds;
+  int box_lid_only;
+  double box_lid_ux, box_lid_uy, box_lid_uz, box_wall_tol;
+  int n_marker;
+  double rd;
+  double ubx, uby, ubz, omx, omy, omz;
+  double ivc_diag_reg;
+  int ivc_rebuild_matrix;
+  int renormalize_delta;
+  double x0, y0, z0, R; /* ibm.x0,y0,z0,R */
+  /* user-defined pitching NACA 00xx (Examples/Pitching_airfoil/
+   * IBMUserDefinedGeometry.H:14-20, 59-175); pivot_x moves the pivot along
+   * the chord (0 = leading edge, as in the reference). */
+  double airfoil_chord, airfoil_thickness;
+  double pitch_mean, pitch_amplitude, pitch_frequency, pitch_phase, pivot_x;
+} ilbm_ib_params;
+
+int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom *g,
+                   ilbm_ib **out);
+int ilbm_ib_destroy(ilbm_ib *ib);
+int ilbm_ib_num_markers(const ilbm_ib *ib, int64_t *n);
+/* Lower/upper corner (inclusive) of the cells whose force the IB may write. */
+int ilbm_ib_force_region(const ilbm_ib *ib, int lo[3], int hi[3]);
+/* update_forcing: reads rho,u (from box->macro_in incl. 2 ghost layers when
+ * set, else from box->f_in + box->force_prev), writes box->force = dt*rho*a on
+ * valid cells of the force region.  Cells of box->force outside that region
+ * are not touched (keep them zero). */
+int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *p,
+                           double dt, double time);
+/* sum over markers of F*dv from the last update_forcing (synchronises) */
+int ilbm_ib_last_marker_force_sum(ilbm_ib *ib, double out[3]);
+/* marker positions / interpolated velocity / force: n*3 doubles each, or NULL */
+int ilbm_ib_markers(ilbm_ib *ib, double *xyz, double *uvw, double *force);
+
+/* ---- force evaluation ---------------------------------------------------- */
+/* sum of the force array over valid cells of [lo,hi] (3 doubles, synchronous) */
+int ilbm_force_integrals(ilbm_ctx *ctx, const ilbm_box *box, const void *force,
+                         const int lo[3], const int hi[3], double out_sum[3]);
+/* link-wise momentum exchange on f (IBForceEval); out = body force (3) */
+int ilbm_momentum_exchange(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
+                           const void *f, double x0, double y0, double z0, double R,
+                           const double prob_lo[3], const double dx[3], int one_sided,
+                           double out[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ILBM_B200_H */

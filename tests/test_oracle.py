@@ -1,0 +1,76 @@
+"""The CPU oracle (oracle/lbm_oracle.c) against the reference's own code.
+
+* ``oracle/_ref`` compiles Source/LBM, Source/BC, Source/IBM of the reference
+  in place; where it is built the oracle must agree with it bit for bit;
+* the committed fixtures in tests/golden were written by that build
+  (tests/golden/make_golden.py) and pin the oracle where the reference tree
+  is not mounted.
+"""
+import numpy as np
+import pytest
+
+from oracle import checker
+from oracle.checker import CpuLevel
+from tests.golden.golden_cases import GOLDEN_CASES
+
+GOLDEN = __import__("pathlib").Path(__file__).resolve().parent / "golden"
+
+
+def _run(backend, name):
+    builder, steps = GOLDEN_CASES[name]
+    case, init, ib = builder()
+    L = CpuLevel(case, backend)
+    L.set_macro(*init())
+    L.init_equilibrium()
+    if ib is not None:
+        L.ib_create(ib)
+    L.step(steps)
+    return L
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN_CASES))
+def test_oracle_matches_golden_fixture(name):
+    """bit-exact: the fixtures are the reference's own outputs"""
+    L = _run("oracle", name)
+    g = np.load(GOLDEN / f"{name}.npz")
+    f = L.get_f()
+    np.testing.assert_array_equal(L.get_macro(), g["macro"])
+    np.testing.assert_array_equal(L.get_force(), g["force"])
+    np.testing.assert_allclose(f.reshape(f.shape[0], -1).sum(axis=1), g["f_sum"], rtol=1e-13, atol=1e-13)
+    if "f" in g:
+        np.testing.assert_array_equal(f, g["f"])
+    if "rec" in g:
+        np.testing.assert_array_equal(L.force_record(), g["rec"])
+        np.testing.assert_array_equal(L.marker_force_sum(), g["fsum"])
+        assert L.num_markers() == int(g["nmark"])
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN_CASES))
+def test_oracle_matches_reference_build(name):
+    case = GOLDEN_CASES[name][0]()[0]
+    if not checker.available("ref", case.dim):
+        pytest.skip("reference build (oracle/_ref/libref*.so) not present")
+    a, b = _run("oracle", name), _run("ref", name)
+    np.testing.assert_array_equal(a.get_f(), b.get_f())
+    np.testing.assert_array_equal(a.get_macro(), b.get_macro())
+
+
+def test_delta_kernel_matches_reference_and_partitions_unity():
+    """IBMarkerDF.cpp:70-99; the 4-point and 3-point kernels sum to 1/h and
+    have first moment 0 on a uniform grid (the reference's own
+    debug_kernel_partition diagnostic, IBMarkerDF.cpp:1585-1689)."""
+    lib = checker._load("oracle", 2)
+    rng = np.random.default_rng(20261203)
+    for kt in (0, 1):
+        for _ in range(50):
+            xp = rng.uniform(0, 1)
+            h = 1.0
+            xs = np.arange(-3, 5) + 0.5
+            vals = np.array([lib.orc_delta_function(x, xp, h, kt) for x in xs])
+            assert abs(vals.sum() * h - 1.0) < 1e-14
+            assert abs(np.sum(vals * (xs - xp)) * h) < 1e-14
+    if checker.available("ref", 2):
+        ref = checker._load("ref", 2)
+        for x in np.linspace(-2.5, 2.5, 101):
+            for kt in (0, 1):
+                assert ref.ref_delta_function(x, 0.1, 1.0, kt) == lib.orc_delta_function(x, 0.1, 1.0, kt)
