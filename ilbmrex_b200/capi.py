@@ -16,6 +16,8 @@ MAXQ = 27
 ILBM_OK = 0
 STORAGE = {"f64": 0, "f32": 1, "f16": 2}
 GHOST_SELF, GHOST_CALLER = 0, 1
+IVC_AUTO, IVC_CG, IVC_DENSE = 0, 1, 2
+IVC_DENSE_MAX = 8192
 BC_INT_DIR, BC_FOEXTRAP, BC_EXT_DIR, BC_USER_1, BC_USER_2 = 0, 2, 3, 1001, 1002
 
 # every symbol the header declares
@@ -24,7 +26,9 @@ EXPORTS = [
     "ilbm_event_record", "ilbm_event_elapsed_ms", "ilbm_kernel_launches", "ilbm_storage_bytes",
     "ilbm_level_step", "ilbm_compute_macro", "ilbm_init_equilibrium",
     "ilbm_ib_create", "ilbm_ib_destroy", "ilbm_ib_num_markers", "ilbm_ib_force_region",
-    "ilbm_ib_update_forcing", "ilbm_ib_last_marker_force_sum", "ilbm_ib_markers",
+    "ilbm_ib_update_forcing", "ilbm_advance_level", "ilbm_ib_last_marker_force_sum",
+    "ilbm_ib_solver_stats", "ilbm_ib_set_ivc_solver",
+    "ilbm_ib_markers",
     "ilbm_force_integrals", "ilbm_momentum_exchange",
 ]
 
@@ -120,7 +124,10 @@ def lib():
         "ilbm_ib_num_markers": (I, [P, C.POINTER(I64)]),
         "ilbm_ib_force_region": (I, [P, ip3, ip3]),
         "ilbm_ib_update_forcing": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), D, D]),
+        "ilbm_advance_level": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P, D, D]),
         "ilbm_ib_last_marker_force_sum": (I, [P, dp]),
+        "ilbm_ib_solver_stats": (I, [P, C.POINTER(I)]),
+        "ilbm_ib_set_ivc_solver": (I, [P, I]),
         "ilbm_ib_markers": (I, [P, dp, dp, dp]),
         "ilbm_force_integrals": (I, [P, C.POINTER(Box_t), P, ip3, ip3, dp]),
         "ilbm_momentum_exchange": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P,

@@ -22,11 +22,17 @@
 #include <cstring>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "ilbm_common.cuh"
+
+namespace cgrp = cooperative_groups;
 
 namespace ilbm {
 int band_macro(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p, const int *blo,
-               const int *bn, double *EV, double *RHO);
+               const int *bn, double *EV, double *RHO, cudaStream_t st);
+int level_step_split(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p,
+                     const int *blo, const int *bhi, cudaEvent_t band_ready);
 }
 
 using namespace ilbm;
@@ -147,56 +153,77 @@ __global__ void k_markers(IBArgs a, double *xyz, const double *ref, double *tgt,
   }
 }
 
-// velocity_interpolation_cic, :612-695; clip box = domain grown by 2
-__global__ void k_interp(IBArgs a, const double *xyz, const double *EV, double *uvw,
-                         int *status) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+// velocity_interpolation_cic, :612-695; clip box = domain grown by 2.
+// One warp per marker: the 5 kernel weights per direction are evaluated once
+// (the reference re-evaluates the same values inside its loops) and the 5^d
+// stencil points are spread over the lanes; products keep the reference's
+// (tU*tV)*tW order, the sum is a fixed-order warp reduction.
+__device__ __forceinline__ void marker_weights(const IBArgs &a, double px, double py, double pz,
+                                               int lane, int &i0, int &j0, int &k0,
+                                               double &wx, double &wy, double &wz) {
+  i0 = cell_of(px, a.plo[0], a.dx[0]);
+  j0 = cell_of(py, a.plo[1], a.dx[1]);
+  k0 = (a.dim == 3) ? cell_of(pz, a.plo[2], a.dx[2]) : 0;
+  const int o = lane % 5 - 2;
+  wx = delta_fn(cell_center(a.plo[0], i0 + o, a.dx[0]), px, a.dx[0], a.kt);
+  wy = delta_fn(cell_center(a.plo[1], j0 + o, a.dx[1]), py, a.dx[1], a.kt);
+  wz = (a.dim == 3) ? delta_fn(cell_center(a.plo[2], k0 + o, a.dx[2]), pz, a.dx[2], a.kt) : 1.0;
+}
+
+__global__ void __launch_bounds__(128) k_interp(IBArgs a, const double *xyz, const double *EV,
+                                                double *uvw, int *status) {
+  const int lane = threadIdx.x & 31;
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (m >= a.n) return;
   const double px = xyz[m], py = xyz[m + a.n], pz = xyz[m + 2 * a.n];
   const double d = (a.dim == 3) ? X::mul(X::mul(a.dx[0], a.dx[1]), a.dx[2]) : X::mul(a.dx[0], a.dx[1]);
-  const int i0 = cell_of(px, a.plo[0], a.dx[0]), j0 = cell_of(py, a.plo[1], a.dx[1]);
-  const int k0 = (a.dim == 3) ? cell_of(pz, a.plo[2], a.dx[2]) : 0;
+  int i0, j0, k0;
+  double wxl, wyl, wzl;
+  marker_weights(a, px, py, pz, lane, i0, j0, k0, wxl, wyl, wzl);
   const int ilo = a.dlo[0] - 2, ihi = a.dhi[0] + 2, jlo = a.dlo[1] - 2, jhi = a.dhi[1] + 2;
   const int klo = (a.dim == 3) ? a.dlo[2] - 2 : 0, khi = (a.dim == 3) ? a.dhi[2] + 2 : 0;
+  const int npts = (a.dim == 3) ? 125 : 25;
   double u = 0.0, v = 0.0, w = 0.0, part = 0.0;
-  for (int ii = -2; ii < 3; ++ii) {
-    const double tU = delta_fn(cell_center(a.plo[0], i0 + ii, a.dx[0]), px, a.dx[0], a.kt);
-    for (int jj = -2; jj < 3; ++jj) {
-      const double tV = delta_fn(cell_center(a.plo[1], j0 + jj, a.dx[1]), py, a.dx[1], a.kt);
-      const int kn = (a.dim == 3) ? 5 : 1;
-      for (int kk = 0; kk < kn; ++kk) {
-        double dvl;
-        const int ip = i0 + ii, jp = j0 + jj;
-        int kp = 0;
-        if (a.dim == 3) {
-          kp = k0 + kk - 2;
-          const double tW = delta_fn(cell_center(a.plo[2], kp, a.dx[2]), pz, a.dx[2], a.kt);
-          if (ip < ilo || ip > ihi || jp < jlo || jp > jhi || kp < klo || kp > khi) continue;
-          dvl = X::mul(X::mul(tU, tV), tW);
-        } else {
-          if (ip < ilo || ip > ihi || jp < jlo || jp > jhi) continue;
-          dvl = X::mul(tU, tV);
-        }
-        if (!in_band(a, ip, jp, kp)) {
-          atomicOr(status, 1);
-          continue;
-        }
-        const int64_t e = bidx(a, ip, jp, kp);
-        part = X::add(part, X::mul(dvl, d));
-        u = X::add(u, X::mul(X::mul(dvl, EV[e]), d));
-        v = X::add(v, X::mul(X::mul(dvl, EV[e + a.nb]), d));
-        if (a.dim == 3) w = X::add(w, X::mul(X::mul(dvl, EV[e + 2 * a.nb]), d));
-      }
+  // every lane runs the same number of iterations so the shuffles stay convergent
+  const int nit = (npts + 31) / 32;
+  for (int it = 0; it < nit; ++it) {
+    const int t = lane + 32 * it;
+    const int tt = t < npts ? t : 0;
+    const int ii = tt / ((a.dim == 3) ? 25 : 5), jj = (tt / ((a.dim == 3) ? 5 : 1)) % 5;
+    const int kk = (a.dim == 3) ? tt % 5 : 2;
+    const double tU = __shfl_sync(0xffffffffu, wxl, ii, 32);
+    const double tV = __shfl_sync(0xffffffffu, wyl, jj, 32);
+    const double tW = __shfl_sync(0xffffffffu, wzl, kk, 32);
+    if (t >= npts) continue;
+    const int ip = i0 + ii - 2, jp = j0 + jj - 2, kp = (a.dim == 3) ? k0 + kk - 2 : 0;
+    if (ip < ilo || ip > ihi || jp < jlo || jp > jhi || kp < klo || kp > khi) continue;
+    if (!in_band(a, ip, jp, kp)) {
+      atomicOr(status, 1);
+      continue;
     }
+    const double dvl = (a.dim == 3) ? X::mul(X::mul(tU, tV), tW) : X::mul(tU, tV);
+    const int64_t e = bidx(a, ip, jp, kp);
+    part = X::add(part, X::mul(dvl, d));
+    u = X::add(u, X::mul(X::mul(dvl, EV[e]), d));
+    v = X::add(v, X::mul(X::mul(dvl, EV[e + a.nb]), d));
+    if (a.dim == 3) w = X::add(w, X::mul(X::mul(dvl, EV[e + 2 * a.nb]), d));
   }
-  if (a.renorm_interp && part > 0.0) {
-    u = X::div(u, part);
-    v = X::div(v, part);
-    w = X::div(w, part);
+  for (int o = 16; o > 0; o >>= 1) {
+    u = X::add(u, __shfl_down_sync(0xffffffffu, u, o));
+    v = X::add(v, __shfl_down_sync(0xffffffffu, v, o));
+    w = X::add(w, __shfl_down_sync(0xffffffffu, w, o));
+    part = X::add(part, __shfl_down_sync(0xffffffffu, part, o));
   }
-  uvw[m] = X::add(uvw[m], u);
-  uvw[m + a.n] = X::add(uvw[m + a.n], v);
-  uvw[m + 2 * a.n] = X::add(uvw[m + 2 * a.n], w);
+  if (lane == 0) {
+    if (a.renorm_interp && part > 0.0) {
+      u = X::div(u, part);
+      v = X::div(v, part);
+      w = X::div(w, part);
+    }
+    uvw[m] = X::add(uvw[m], u);
+    uvw[m + a.n] = X::add(uvw[m + a.n], v);
+    uvw[m + 2 * a.n] = X::add(uvw[m + 2 * a.n], w);
+  }
 }
 
 // rigid_target_velocity / box_target_velocity, :147-182
@@ -299,67 +326,6 @@ __device__ double ivc_entry(const IBArgs &a, const double *xyz, int i, int j, do
   double val = X::mul(X::mul(X::mul(a.dv, sx), sy), sz);
   if (i == j) val = X::add(val, reg);
   return val;
-}
-
-// one CTA: count, scan, fill (status bit 2 on capacity overflow)
-__global__ void __launch_bounds__(1024) k_csr_build(IBArgs a, const double *xyz, double reg,
-                                                    int *rowptr, int *col, double *val,
-                                                    double *diag, int cap, int *status) {
-  __shared__ int warp_tot[32];
-  const int n = a.n;
-  // counts into rowptr[i+1]
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    int c = 0;
-    for (int j = 0; j < n; ++j) c += may_couple(a, xyz, i, j) ? 1 : 0;
-    rowptr[i + 1] = c;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) rowptr[0] = 0;
-  // serial-per-chunk exclusive scan (n is modest; keep it simple and exact)
-  const int chunk = (n + blockDim.x - 1) / blockDim.x;
-  const int s0 = threadIdx.x * chunk, s1 = min(n, s0 + chunk);
-  int local = 0;
-  for (int i = s0; i < s1; ++i) local += rowptr[i + 1];
-  // block-wide exclusive scan of `local`
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int x = local;
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) warp_tot[wid] = x;
-  __syncthreads();
-  if (wid == 0) {
-    int t = (lane < (int)(blockDim.x >> 5)) ? warp_tot[lane] : 0;
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, t, o);
-      if (lane >= o) t += y;
-    }
-    warp_tot[lane] = t;
-  }
-  __syncthreads();
-  int excl = x - local + (wid > 0 ? warp_tot[wid - 1] : 0);
-  for (int i = s0; i < s1; ++i) {
-    const int c = rowptr[i + 1];
-    rowptr[i + 1] = excl + c;
-    excl += c;
-  }
-  __syncthreads();
-  if (rowptr[n] > cap) {
-    if (threadIdx.x == 0) atomicOr(status, 2);
-    return;
-  }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    int p = rowptr[i];
-    for (int j = 0; j < n; ++j) {
-      if (!may_couple(a, xyz, i, j)) continue;
-      const double v = ivc_entry(a, xyz, i, j, reg);
-      col[p] = j;
-      val[p] = v;
-      if (i == j) diag[i] = v;
-      ++p;
-    }
-  }
 }
 
 __device__ double block_sum(double v, double *sh) {
@@ -489,56 +455,407 @@ __global__ void __launch_bounds__(1024) k_ivc_cg(IBArgs a, const double *xyz, co
     for (int c = 0; c < 3; ++c) F[i + c * n] = X::add(F[i + c * n], X_[i + c * n]);
 }
 
-// force_spreading_cic, :1331-1448 (dv folded in, 2D spreads x and y only)
-__global__ void k_spread(IBArgs a, const double *xyz, const double *F, double *EFI, int *status) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+// ---------------------------------------------------------------------------
+// Multi-CTA CSR build (warp per row) and grid-wide CG for large marker sets
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_csr_count(IBArgs a, const double *xyz, int *rowptr) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += nw) {
+    int c = 0;
+    for (int j = lane; j < a.n; j += 32) c += may_couple(a, xyz, i, j) ? 1 : 0;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) rowptr[i + 1] = c;
+  }
+}
+
+// exclusive scan of the row counts; if the total exceeds the capacity the
+// operator is left empty (every row pointer 0) and status bit 2 is set, so no
+// later kernel indexes past the column / value arrays
+__global__ void __launch_bounds__(1024) k_csr_scan(int n, int *rowptr, int cap, int *status) {
+  __shared__ int warp_tot[32];
+  const int chunk = (n + blockDim.x - 1) / blockDim.x;
+  const int s0 = threadIdx.x * chunk, s1 = min(n, s0 + chunk);
+  int local = 0;
+  for (int i = s0; i < s1; ++i) local += rowptr[i + 1];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = local;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int t = (lane < (int)(blockDim.x >> 5)) ? warp_tot[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    warp_tot[lane] = t;
+  }
+  __syncthreads();
+  int excl = x - local + (wid > 0 ? warp_tot[wid - 1] : 0);
+  for (int i = s0; i < s1; ++i) {
+    const int c = rowptr[i + 1];
+    rowptr[i + 1] = excl + c;
+    excl += c;
+  }
+  if (threadIdx.x == 0) rowptr[0] = 0;
+  __syncthreads();
+  const int total = rowptr[n];
+  __syncthreads();
+  if (total > cap) {
+    for (int i = s0; i < s1; ++i) rowptr[i + 1] = 0;
+    if (threadIdx.x == 0) atomicOr(status, 2);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_csr_fill(IBArgs a, const double *xyz, double reg,
+                                                  const int *rowptr, int *col, double *val,
+                                                  double *diag, int cap, int *status) {
+  if ((*status & 2) || rowptr[a.n] > cap) return;  // capacity exceeded (k_csr_scan)
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += nw) {
+    int p = rowptr[i];
+    for (int j0 = 0; j0 < a.n; j0 += 32) {
+      const int j = j0 + lane;
+      const bool c = (j < a.n) && may_couple(a, xyz, i, j);
+      const unsigned m = __ballot_sync(0xffffffffu, c);
+      if (c) {
+        const int slot = p + __popc(m & ((1u << lane) - 1u));
+        const double v = ivc_entry(a, xyz, i, j, reg);
+        col[slot] = j;
+        val[slot] = v;
+        if (i == j) diag[i] = v;
+      }
+      p += __popc(m);
+    }
+  }
+}
+
+// fixed-order reduction of per-block partials (nb blocks x 8 slots); every
+// block computes the same values, so branches on them stay grid-uniform
+__device__ __forceinline__ void reduce_partials(const double *partial, int nblocks, int nval,
+                                                double *out_sh) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (wid < nval) {
+    double s = 0.0;
+    for (int b = lane; b < nblocks; b += 32) s += partial[b * 8 + wid];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out_sh[wid] = s;
+  }
+  __syncthreads();
+}
+
+// block-wide fixed-order sum of nval per-thread values into partial[blockIdx.x*8+c]
+__device__ __forceinline__ void block_partials(const double *v, int nval, double (*sh)[8],
+                                               double *partial) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int c = 0; c < nval; ++c) {
+    double x = v[c];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[wid][c] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < nval) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w][threadIdx.x];
+    partial[blockIdx.x * 8 + threadIdx.x] = t;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) k_ivc_cg_grid(IBArgs a, const double *xyz, const double *tgt,
+                                                     const double *uvw, const int *rowptr,
+                                                     const int *col, const double *val,
+                                                     const double *diag, double *X_, double *work,
+                                                     double *F, double *partial, int maxit,
+                                                     double tol, int warm, int *status,
+                                                     int *iters) {
+  cgrp::grid_group grid = cgrp::this_grid();
+  __shared__ double sh[8][8];
+  __shared__ double red[8];
+  const int n = a.n;
+  double *r = work, *z = work + 3 * n, *p = work + 6 * n, *Ap = work + 9 * n;
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31, nw = gsz >> 5, gw = gtid >> 5;
+  // warm start: x0 = previous solution (the force changes little per step);
+  // r0 = b - A x0, one warp per row
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int row = gw; row < n; row += nw) {
+    double s0 = 0, s1 = 0, s2 = 0;
+    if (warm) {
+      for (int e = rowptr[row] + lane; e < rowptr[row + 1]; e += 32) {
+        const double v = val[e];
+        const int j = col[e];
+        s0 += v * X_[j];
+        s1 += v * X_[j + n];
+        s2 += v * X_[j + 2 * n];
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      }
+    }
+    if (lane == 0) {
+      double Ux, Uy, Uz;
+      target_of(a, row, xyz, tgt, Ux, Uy, Uz);
+      const double U[3] = {Ux, Uy, Uz};
+      const double ax[3] = {s0, s1, s2};
+      for (int c = 0; c < 3; ++c) {
+        const double b = X::div(X::sub(U[c], uvw[row + c * n]), a.dt);
+        if (!warm) X_[row + c * n] = 0.0;
+        const double rr = b - ax[c];
+        const double zz = rr / diag[row];
+        r[row + c * n] = rr;
+        z[row + c * n] = zz;
+        p[row + c * n] = zz;
+        acc[c] += rr * zz;
+        acc[3 + c] += b * b;
+      }
+    }
+  }
+  block_partials(acc, 6, sh, partial);
+  grid.sync();
+  reduce_partials(partial, gridDim.x, 6, red);
+  double rz[3] = {red[0], red[1], red[2]};
+  const double bn[3] = {sqrt(red[3]), sqrt(red[4]), sqrt(red[5])};
+  __syncthreads();
+  int it = 0;
+  bool done = false;
+  if (warm) grid.sync();  // X_ reads of the residual pass are complete before updates
+  for (; it < maxit; ++it) {
+    // Ap = A p, one warp per row; partial p.Ap
+    double pap[3] = {0, 0, 0};
+    for (int row = gw; row < n; row += nw) {
+      double s0 = 0, s1 = 0, s2 = 0;
+      for (int e = rowptr[row] + lane; e < rowptr[row + 1]; e += 32) {
+        const double v = val[e];
+        const int j = col[e];
+        s0 += v * p[j];
+        s1 += v * p[j + n];
+        s2 += v * p[j + 2 * n];
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+        s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+      }
+      if (lane == 0) {
+        Ap[row] = s0;
+        Ap[row + n] = s1;
+        Ap[row + 2 * n] = s2;
+        pap[0] += p[row] * s0;
+        pap[1] += p[row + n] * s1;
+        pap[2] += p[row + 2 * n] * s2;
+      }
+    }
+    block_partials(pap, 3, sh, partial);
+    grid.sync();
+    reduce_partials(partial, gridDim.x, 3, red);
+    double alpha[3];
+    for (int c = 0; c < 3; ++c) alpha[c] = (red[c] != 0.0) ? rz[c] / red[c] : 0.0;
+    __syncthreads();
+    double ac[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = gtid; i < n; i += gsz)
+      for (int c = 0; c < 3; ++c) {
+        X_[i + c * n] += alpha[c] * p[i + c * n];
+        const double rr = r[i + c * n] - alpha[c] * Ap[i + c * n];
+        r[i + c * n] = rr;
+        const double zz = rr / diag[i];
+        z[i + c * n] = zz;
+        ac[c] += rr * zz;
+        ac[3 + c] += rr * rr;
+      }
+    block_partials(ac, 6, sh, partial);
+    grid.sync();
+    reduce_partials(partial, gridDim.x, 6, red);
+    double beta[3];
+    bool ok = true;
+    for (int c = 0; c < 3; ++c) {
+      beta[c] = (rz[c] != 0.0) ? red[c] / rz[c] : 0.0;
+      rz[c] = red[c];
+      ok = ok && (sqrt(red[3 + c]) <= tol * bn[c]);
+    }
+    __syncthreads();
+    if (ok) {
+      done = true;
+      ++it;
+      break;
+    }
+    for (int i = gtid; i < n; i += gsz)
+      for (int c = 0; c < 3; ++c) p[i + c * n] = z[i + c * n] + beta[c] * p[i + c * n];
+    grid.sync();
+  }
+  if (gtid == 0) {
+    *iters = it;
+    if (!done) atomicOr(status, 4);
+  }
+  for (int i = gtid; i < n; i += gsz)
+    for (int c = 0; c < 3; ++c) F[i + c * n] = X::add(F[i + c * n], X_[i + c * n]);
+}
+
+// ---------------------------------------------------------------------------
+// Fixed IVC operator: explicit inverse and one dense solve per step
+// ---------------------------------------------------------------------------
+// When the markers do not move and the matrix is not rebuilt, the reference
+// factorises A = dv*S*S^T + reg*I once (dense LU, IBMarkerDF.cpp) and
+// back-substitutes every step.  Triangular solves are a chain of n dependent
+// steps; on the GPU the same once-per-body work is better spent forming A^-1
+// (in-place Gauss-Jordan, no pivoting: A is symmetric positive definite), so
+// that each step's solve is one bandwidth-bound matvec with three right-hand
+// sides and no grid-wide synchronisation.
+
+// CSR -> dense rows (row stride ld, padding columns stay zero)
+__global__ void __launch_bounds__(256) k_dense_scatter(int n, int ld, const int *rowptr,
+                                                       const int *col, const double *val,
+                                                       double *M) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw)
+    for (int e = rowptr[i] + lane; e < rowptr[i + 1]; e += 32) M[(size_t)i * ld + col[e]] = val[e];
+}
+
+// Gauss-Jordan step k, part 1: pivot row scaled by 1/p, pivot column saved
+__global__ void __launch_bounds__(256) k_gj_panel(double *M, int n, int ld, int k, double *rowk,
+                                                  double *colk, int *status) {
+  const double piv = M[(size_t)k * ld + k];
+  if (!(piv > 0.0)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicOr(status + 1, 8);
+    return;
+  }
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    rowk[t] = (t == k) ? 1.0 / piv : M[(size_t)k * ld + t] / piv;
+    colk[t] = M[(size_t)t * ld + k];
+  }
+}
+
+// part 2, one row per block: a_ij -= a_ik * a_kj/p, a_ik = -a_ik/p, row k = row k/p
+__global__ void __launch_bounds__(256) k_gj_update(double *M, int n, int ld, int k,
+                                                   const double *rowk, const double *colk,
+                                                   const int *status) {
+  if (status[1] & 8) return;
+  const int i = blockIdx.x;
+  double *Mi = M + (size_t)i * ld;
+  if (i == k) {
+    for (int j = threadIdx.x; j < n; j += blockDim.x) Mi[j] = rowk[j];
+    return;
+  }
+  const double ci = colk[i];
+  if (ci == 0.0) return;  // rows not yet coupled to k are unchanged (a_ik stays 0)
+  const double rkk = rowk[k];
+  for (int j = threadIdx.x; j < n; j += blockDim.x)
+    Mi[j] = (j == k) ? -ci * rkk : Mi[j] - ci * rowk[j];
+}
+
+// F += A^-1 b with b = (U_target - U_interp)/dt (the IVC right-hand side of
+// IBMarkerDF.cpp's solve), one warp per row, b staged in shared memory
+__global__ void __launch_bounds__(256) k_ivc_dense(IBArgs a, const double *xyz, const double *tgt,
+                                                   const double *uvw, const double *Ainv, int ld,
+                                                   double *F) {
+  extern __shared__ double bsh[];  // 3 x ld
+  const int n = a.n;
+  for (int j = threadIdx.x; j < ld; j += blockDim.x) {
+    if (j < n) {
+      double Ux, Uy, Uz;
+      target_of(a, j, xyz, tgt, Ux, Uy, Uz);
+      bsh[j] = X::div(X::sub(Ux, uvw[j]), a.dt);
+      bsh[ld + j] = X::div(X::sub(Uy, uvw[j + n]), a.dt);
+      bsh[2 * ld + j] = X::div(X::sub(Uz, uvw[j + 2 * n]), a.dt);
+    } else {
+      bsh[j] = bsh[ld + j] = bsh[2 * ld + j] = 0.0;
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int half = ld >> 1;
+  const double2 *b0 = reinterpret_cast<const double2 *>(bsh);
+  const double2 *b1 = reinterpret_cast<const double2 *>(bsh + ld);
+  const double2 *b2 = reinterpret_cast<const double2 *>(bsh + 2 * ld);
+  for (int row = blockIdx.x * 8 + wid; row < n; row += gridDim.x * 8) {
+    const double2 *Ar = reinterpret_cast<const double2 *>(Ainv + (size_t)row * ld);
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll 4
+    for (int h = lane; h < half; h += 32) {
+      const double2 v = __ldcs(Ar + h);
+      const double2 x0 = b0[h], x1 = b1[h], x2 = b2[h];
+      s0 += v.x * x0.x + v.y * x0.y;
+      s1 += v.x * x1.x + v.y * x1.y;
+      s2 += v.x * x2.x + v.y * x2.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    if (lane == 0) {
+      F[row] = X::add(F[row], s0);
+      F[row + n] = X::add(F[row + n], s1);
+      F[row + 2 * n] = X::add(F[row + 2 * n], s2);
+    }
+  }
+}
+
+// force_spreading_cic, :1331-1448 (dv folded in, 2D spreads x and y only);
+// one warp per marker, lanes over the stencil points, FP64 atomics
+__global__ void __launch_bounds__(128) k_spread(IBArgs a, const double *xyz, const double *F,
+                                                double *EFI, int *status) {
+  const int lane = threadIdx.x & 31;
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (m >= a.n) return;
   const double fx = X::mul(F[m], a.dv), fy = X::mul(F[m + a.n], a.dv), fz = X::mul(F[m + 2 * a.n], a.dv);
   const double px = xyz[m], py = xyz[m + a.n], pz = xyz[m + 2 * a.n];
   const double d = (a.dim == 3) ? X::mul(X::mul(a.dx[0], a.dx[1]), a.dx[2]) : X::mul(a.dx[0], a.dx[1]);
-  const int i0 = cell_of(px, a.plo[0], a.dx[0]), j0 = cell_of(py, a.plo[1], a.dx[1]);
-  const int k0 = (a.dim == 3) ? cell_of(pz, a.plo[2], a.dx[2]) : 0;
+  int i0, j0, k0;
+  double wxl, wyl, wzl;
+  marker_weights(a, px, py, pz, lane, i0, j0, k0, wxl, wyl, wzl);
   const int ilo = a.dlo[0] - 2, ihi = a.dhi[0] + 2, jlo = a.dlo[1] - 2, jhi = a.dhi[1] + 2;
   const int klo = (a.dim == 3) ? a.dlo[2] - 2 : 0, khi = (a.dim == 3) ? a.dhi[2] + 2 : 0;
+  const int npts = (a.dim == 3) ? 125 : 25;
   double scale = 1.0;
-  const int kn = (a.dim == 3) ? 5 : 1;
   if (a.renorm_spread) {
     double part = 0.0;
-    for (int ii = -2; ii < 3; ++ii) {
-      const double tU = delta_fn(cell_center(a.plo[0], i0 + ii, a.dx[0]), px, a.dx[0], a.kt);
-      for (int jj = -2; jj < 3; ++jj) {
-        const double tV = delta_fn(cell_center(a.plo[1], j0 + jj, a.dx[1]), py, a.dx[1], a.kt);
-        for (int kk = 0; kk < kn; ++kk) {
-          const int ip = i0 + ii, jp = j0 + jj, kp = (a.dim == 3) ? k0 + kk - 2 : 0;
-          double t = X::mul(tU, tV);
-          if (a.dim == 3) t = X::mul(t, delta_fn(cell_center(a.plo[2], kp, a.dx[2]), pz, a.dx[2], a.kt));
-          if (ip < ilo || ip > ihi || jp < jlo || jp > jhi || kp < klo || kp > khi) continue;
-          part = X::add(part, X::mul(t, d));
-        }
-      }
+    for (int it = 0; it < (npts + 31) / 32; ++it) {
+      const int t = lane + 32 * it;
+      const int tt = t < npts ? t : 0;
+      const int ii = tt / ((a.dim == 3) ? 25 : 5), jj = (tt / ((a.dim == 3) ? 5 : 1)) % 5;
+      const int kk = (a.dim == 3) ? tt % 5 : 2;
+      const double tU = __shfl_sync(0xffffffffu, wxl, ii, 32);
+      const double tV = __shfl_sync(0xffffffffu, wyl, jj, 32);
+      const double tW = __shfl_sync(0xffffffffu, wzl, kk, 32);
+      if (t >= npts) continue;
+      const int ip = i0 + ii - 2, jp = j0 + jj - 2, kp = (a.dim == 3) ? k0 + kk - 2 : 0;
+      if (ip < ilo || ip > ihi || jp < jlo || jp > jhi || kp < klo || kp > khi) continue;
+      const double t3 = (a.dim == 3) ? X::mul(X::mul(tU, tV), tW) : X::mul(tU, tV);
+      part = X::add(part, X::mul(t3, d));
     }
+    for (int o = 16; o > 0; o >>= 1) part = X::add(part, __shfl_xor_sync(0xffffffffu, part, o));
     if (part > 0.0) scale = X::div(1.0, part);
   }
-  for (int ii = -2; ii < 3; ++ii) {
-    const double tU = delta_fn(cell_center(a.plo[0], i0 + ii, a.dx[0]), px, a.dx[0], a.kt);
-    for (int jj = -2; jj < 3; ++jj) {
-      const double tV = delta_fn(cell_center(a.plo[1], j0 + jj, a.dx[1]), py, a.dx[1], a.kt);
-      for (int kk = 0; kk < kn; ++kk) {
-        const int ip = i0 + ii, jp = j0 + jj, kp = (a.dim == 3) ? k0 + kk - 2 : 0;
-        double t = X::mul(tU, tV);
-        if (a.dim == 3) t = X::mul(t, delta_fn(cell_center(a.plo[2], kp, a.dx[2]), pz, a.dx[2], a.kt));
-        if (ip < ilo || ip > ihi || jp < jlo || jp > jhi || kp < klo || kp > khi) continue;
-        if (!in_band(a, ip, jp, kp)) {
-          atomicOr(status, 1);
-          continue;
-        }
-        const double dvl = X::mul(t, scale);
-        const int64_t e = bidx(a, ip, jp, kp);
-        atomicAdd(&EFI[e], X::mul(dvl, fx));
-        atomicAdd(&EFI[e + a.nb], X::mul(dvl, fy));
-        if (a.dim == 3) atomicAdd(&EFI[e + 2 * a.nb], X::mul(dvl, fz));
-      }
+  for (int it = 0; it < (npts + 31) / 32; ++it) {
+    const int t = lane + 32 * it;
+    const int tt = t < npts ? t : 0;
+    const int ii = tt / ((a.dim == 3) ? 25 : 5), jj = (tt / ((a.dim == 3) ? 5 : 1)) % 5;
+    const int kk = (a.dim == 3) ? tt % 5 : 2;
+    const double tU = __shfl_sync(0xffffffffu, wxl, ii, 32);
+    const double tV = __shfl_sync(0xffffffffu, wyl, jj, 32);
+    const double tW = __shfl_sync(0xffffffffu, wzl, kk, 32);
+    if (t >= npts) continue;
+    const int ip = i0 + ii - 2, jp = j0 + jj - 2, kp = (a.dim == 3) ? k0 + kk - 2 : 0;
+    if (ip < ilo || ip > ihi || jp < jlo || jp > jhi || kp < klo || kp > khi) continue;
+    if (!in_band(a, ip, jp, kp)) {
+      atomicOr(status, 1);
+      continue;
     }
+    const double t3 = (a.dim == 3) ? X::mul(X::mul(tU, tV), tW) : X::mul(tU, tV);
+    const double dvl = X::mul(t3, scale);
+    const int64_t e = bidx(a, ip, jp, kp);
+    atomicAdd(&EFI[e], X::mul(dvl, fx));
+    atomicAdd(&EFI[e + a.nb], X::mul(dvl, fy));
+    if (a.dim == 3) atomicAdd(&EFI[e + 2 * a.nb], X::mul(dvl, fz));
   }
 }
 
@@ -676,6 +993,14 @@ struct ilbm_ib {
   double *d_val = nullptr, *d_diag = nullptr, *d_X = nullptr, *d_work = nullptr;
   int nnz_cap = 0;
   bool csr_ready = false;
+  double *d_partial = nullptr;  // CG block partials
+  int cg_blocks = 0;
+  bool cg_warm = false;  // previous IVC solution available as the CG start
+  // fixed operator solved through its stored inverse (k_ivc_dense)
+  int ivc_solver = ILBM_IVC_AUTO;
+  bool dense = false, dense_ready = false;
+  int ld = 0, dense_blocks = 0;
+  double *d_Ainv = nullptr, *d_gj = nullptr;
   std::vector<void *> allocs;
 };
 
@@ -927,6 +1252,35 @@ IBArgs make_args(const ilbm_ib *ib, double dt, double time) {
   return a;
 }
 
+// storage for the explicit inverse of the fixed IVC operator (n <= ILBM_IVC_DENSE_MAX)
+int enable_dense(ilbm_ib *ib) {
+  if (ib->dense) return ILBM_OK;
+  const int n = ib->n;
+  const int ld = ((n + 31) / 32) * 32;
+  int rc;
+  if ((rc = dmalloc(ib, &ib->d_Ainv, (size_t)n * ld)) || (rc = dmalloc(ib, &ib->d_gj, 2 * (size_t)ld)))
+    return rc;
+  const int smem = 3 * ld * (int)sizeof(double);
+  // the attribute is per function and device: always the largest size, so a
+  // later body with fewer markers cannot lower the limit under this one
+  cudaError_t e = cudaFuncSetAttribute(k_ivc_dense, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       3 * ILBM_IVC_DENSE_MAX * (int)sizeof(double));
+  if (e != cudaSuccess) return cuda_fail(e, "k_ivc_dense shared memory");
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ivc_dense, 256, smem);
+  if (e != cudaSuccess || per_sm < 1) {
+    set_error("k_ivc_dense does not fit on a multiprocessor");
+    return ILBM_ERR_CUDA;
+  }
+  ib->ld = ld;
+  ib->dense_blocks = std::max(1, std::min(per_sm * sms, (n + 7) / 8));
+  ib->dense = true;
+  ib->dense_ready = false;
+  return ILBM_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -995,6 +1349,21 @@ int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom
       ilbm_ib_destroy(ib);
       return rc;
     }
+    // grid-wide CG: as many co-resident blocks as the device holds, at most 2 per SM
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ivc_cg_grid, 256, 0);
+    ib->cg_blocks = std::max(1, std::min(2, per_sm) * sms);
+    if ((rc = dmalloc(ib, &ib->d_partial, 8 * (size_t)std::max(ib->cg_blocks, 16)))) {
+      ilbm_ib_destroy(ib);
+      return rc;
+    }
+    if (!ib->moving && p->ivc_rebuild_matrix == 0 && n <= ILBM_IVC_DENSE_MAX &&
+        (rc = enable_dense(ib))) {
+      ilbm_ib_destroy(ib);
+      return rc;
+    }
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -1032,14 +1401,51 @@ int ilbm_ib_force_region(const ilbm_ib *ib, int lo[3], int hi[3]) {
   return ILBM_OK;
 }
 
-int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *lp,
-                           double dt, double time) {
+}  // extern "C"
+
+// IVC solve by CG on the CSR operator (moving markers, rebuilt or large systems)
+static int launch_cg(ilbm_ib *ib, const IBArgs &a_in, cudaStream_t s) {
+  ilbm_ctx *ctx = ib->ctx;
+  IBArgs a = a_in;
+  // stopping tolerance (relative residual): 1e-14 with FP64 populations, where
+  // results are compared with the reference's dense LU at 1e-12; 1e-10 with
+  // FP32/FP16 populations, whose own rounding is ~1e-7
+  const double cg_tol = (ctx->storage == ILBM_STORAGE_F64) ? 1.0e-14 : 1.0e-10;
+  if (ib->n <= 1024) {
+    k_ivc_cg<<<1, 1024, 0, s>>>(a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_rowptr, ib->d_col,
+                                ib->d_val, ib->d_diag, ib->d_X, ib->d_work, ib->d_F, 500, cg_tol,
+                                ib->d_status, ib->d_iters);
+    return ILBM_OK;
+  }
+  const double *xyz = ib->d_xyz, *tgt = ib->d_tgt, *uvw = ib->d_uvw, *val = ib->d_val,
+               *diag = ib->d_diag;
+  const int *rowptr = ib->d_rowptr, *col = ib->d_col;
+  double *Xv = ib->d_X, *work = ib->d_work, *Fm = ib->d_F, *partial = ib->d_partial;
+  int maxit = 500;
+  double tol = cg_tol;
+  int warm = ib->cg_warm ? 1 : 0;
+  int *status = ib->d_status, *iters = ib->d_iters;
+  void *args[] = {&a, &xyz, &tgt, &uvw, &rowptr, &col, &val, &diag, &Xv, &work, &Fm,
+                  &partial, &maxit, &tol, &warm, &status, &iters};
+  // one warp per ~2 rows keeps the SpMV latency-tolerant; more blocks than
+  // that only make the grid barriers dearer
+  const int blocks = std::max(8, std::min(ib->cg_blocks, (ib->n + 15) / 16));
+  cudaError_t ce = cudaLaunchCooperativeKernel((const void *)k_ivc_cg_grid, dim3(blocks), dim3(256),
+                                               args, 0, s);
+  ib->cg_warm = !ib->moving && ib->p.ivc_rebuild_matrix == 0;
+  if (ce != cudaSuccess) return cuda_fail(ce, "cooperative CG launch");
+  return ILBM_OK;
+}
+
+// update_forcing on stream `s` (the context stream, or its side stream when the
+// chain overlaps the collide-stream of the cells outside the band)
+static int ib_update(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *lp, double dt,
+                     double time, cudaStream_t s) {
   if (!ib || !box || !box->force) {
     set_error("ilbm_ib_update_forcing: ib, box and box->force are required");
     return ILBM_ERR_ARG;
   }
   ilbm_ctx *ctx = ib->ctx;
-  cudaStream_t s = ctx->stream;
   for (int d = 0; d < ib->dim; ++d)
     if (box->lo[d] != 0 || box->hi[d] != ib->g.n_cell[d] - 1) {
       set_error("ilbm_ib_update_forcing: the box must cover the level domain (one box per level)");
@@ -1054,10 +1460,11 @@ int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_pa
     return ILBM_ERR_ARG;
   }
   // EulerVel / rho on the band (:1541-1566)
-  int rc = band_macro(ctx, *box, lp, ib->blo, ib->bn, ib->d_EV, ib->d_RHO);
+  int rc = band_macro(ctx, *box, lp, ib->blo, ib->bn, ib->d_EV, ib->d_RHO, s);
   if (rc) return rc;
   IBArgs a = make_args(ib, dt, time);
   const int nthr = 128, nblk = (ib->n + nthr - 1) / nthr;
+  const int wblk = (ib->n * 32 + 127) / 128;  // one warp per marker
   const int gb = (int)std::min<int64_t>((ib->nb + 255) / 256, 1024);
   cudaMemsetAsync(ib->d_EFT, 0, 3 * ib->nb * sizeof(double), s);
   cudaMemsetAsync(ib->d_fsum, 0, 3 * sizeof(double), s);
@@ -1071,24 +1478,48 @@ int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_pa
     cudaMemsetAsync(ib->d_EFI, 0, 3 * ib->nb * sizeof(double), s);
     k_markers<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_ref, ib->d_tgt, ib->d_uvw, ib->d_F);
     if (any_periodic_band) k_fill_boundary<<<gb, 256, 0, s>>>(a, ib->d_EV);
-    k_interp<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_EV, ib->d_uvw, ib->d_status);
+    k_interp<<<wblk, 128, 0, s>>>(a, ib->d_xyz, ib->d_EV, ib->d_uvw, ib->d_status);
     ctx->launches += 2 + (any_periodic_band ? 1 : 0);
     if (ivc) {
       if (!ib->csr_ready || ib->moving || ib->p.ivc_rebuild_matrix > 0) {
-        k_csr_build<<<1, 1024, 0, s>>>(a, ib->d_xyz, ib->p.ivc_diag_reg, ib->d_rowptr, ib->d_col,
-                                       ib->d_val, ib->d_diag, ib->nnz_cap, ib->d_status);
-        ctx->launches++;
+        const int cb = std::min(4096, (ib->n * 32 + 255) / 256);
+        k_csr_count<<<cb, 256, 0, s>>>(a, ib->d_xyz, ib->d_rowptr);
+        k_csr_scan<<<1, 1024, 0, s>>>(ib->n, ib->d_rowptr, ib->nnz_cap, ib->d_status);
+        k_csr_fill<<<cb, 256, 0, s>>>(a, ib->d_xyz, ib->p.ivc_diag_reg, ib->d_rowptr, ib->d_col,
+                                      ib->d_val, ib->d_diag, ib->nnz_cap, ib->d_status);
+        ctx->launches += 3;
         ib->csr_ready = true;
       }
-      k_ivc_cg<<<1, 1024, 0, s>>>(a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_rowptr, ib->d_col,
-                                  ib->d_val, ib->d_diag, ib->d_X, ib->d_work, ib->d_F, 500, 1.0e-14,
-                                  ib->d_status, ib->d_iters);
+      const bool use_dense = ib->dense && !ib->moving && ib->p.ivc_rebuild_matrix == 0 &&
+                             ib->ivc_solver != ILBM_IVC_CG;
+      if (use_dense) {
+        if (!ib->dense_ready) {
+          // once per body: dense copy of the operator, then Gauss-Jordan in place
+          const int n = ib->n, ld = ib->ld;
+          const int cb = std::min(4096, (n * 32 + 255) / 256);
+          double *rowk = ib->d_gj, *colk = ib->d_gj + ld;
+          cudaMemsetAsync(ib->d_Ainv, 0, (size_t)n * ld * sizeof(double), s);
+          cudaMemsetAsync(ib->d_iters, 0, sizeof(int), s);
+          k_dense_scatter<<<cb, 256, 0, s>>>(n, ld, ib->d_rowptr, ib->d_col, ib->d_val, ib->d_Ainv);
+          const int pb = (n + 255) / 256;
+          for (int k = 0; k < n; ++k) {
+            k_gj_panel<<<pb, 256, 0, s>>>(ib->d_Ainv, n, ld, k, rowk, colk, ib->d_status);
+            k_gj_update<<<n, 256, 0, s>>>(ib->d_Ainv, n, ld, k, rowk, colk, ib->d_status);
+          }
+          ctx->launches += 1 + 2 * (int64_t)n;
+          ib->dense_ready = true;
+        }
+        k_ivc_dense<<<ib->dense_blocks, 256, 3 * ib->ld * sizeof(double), s>>>(
+            a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_Ainv, ib->ld, ib->d_F);
+      } else if ((rc = launch_cg(ib, a, s))) {
+        return rc;
+      }
       ctx->launches++;
     } else {
       k_force_explicit<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_F);
       ctx->launches++;
     }
-    k_spread<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_F, ib->d_EFI, ib->d_status);
+    k_spread<<<wblk, 128, 0, s>>>(a, ib->d_xyz, ib->d_F, ib->d_EFI, ib->d_status);
     ctx->launches++;
     if (any_periodic_band) {
       k_sum_boundary<<<gb, 256, 0, s>>>(a, ib->d_EFI);
@@ -1112,12 +1543,64 @@ int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_pa
   return ILBM_OK;
 }
 
+extern "C" {
+
+int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *lp,
+                           double dt, double time) {
+  if (!ib) {
+    set_error("ilbm_ib_update_forcing: null ib");
+    return ILBM_ERR_ARG;
+  }
+  return ib_update(ib, box, lp, dt, time, ib->ctx->stream);
+}
+
+int ilbm_advance_level(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
+                       ilbm_ib *ib, double dt, double time) {
+  if (!ctx || !box || !p) {
+    set_error("ilbm_advance_level: null argument");
+    return ILBM_ERR_ARG;
+  }
+  if (!ib) return ilbm_level_step(ctx, box, 1, p);
+  if (ib->ctx != ctx) {
+    set_error("ilbm_advance_level: the IB object belongs to another context");
+    return ILBM_ERR_ARG;
+  }
+  ilbm_level_params q = *p;
+  int lo[3], hi[3];
+  ilbm_ib_force_region(ib, lo, hi);
+  for (int d = 0; d < 3; ++d) {
+    q.force_lo[d] = lo[d];
+    q.force_hi[d] = hi[d];
+  }
+  if (p->ghost_mode != ILBM_GHOST_SELF) {
+    // caller-filled ghosts may carry IB forces of neighbouring boxes: serial
+    int rc = ib_update(ib, box, &q, dt, time, ctx->stream);
+    if (rc) return rc;
+    return ilbm_level_step(ctx, box, 1, &q);
+  }
+  // the IB chain runs on the side stream while the collide-stream of every
+  // cell outside its band runs on the main stream; the band waits for it
+  cudaError_t e = cudaEventRecord(ctx->ev_fork, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level fork");
+  int rc = ib_update(ib, box, &q, dt, time, ctx->side);
+  if (rc) return rc;
+  e = cudaEventRecord(ctx->ev_join, ctx->side);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level join");
+  // validate like ilbm_level_step does, then launch the split step
+  if (box->lo[0] != p->domain_lo[0] || box->f_in == box->f_out) {
+    set_error("ilbm_advance_level: self-fill needs one box equal to the domain, f_in != f_out");
+    return ILBM_ERR_ARG;
+  }
+  return level_step_split(ctx, *box, &q, lo, hi, ctx->ev_join);
+}
+
 int ilbm_ib_last_marker_force_sum(ilbm_ib *ib, double out[3]) {
   if (!ib || !out) return ILBM_ERR_ARG;
   ilbm_ctx *ctx = ib->ctx;
   int st[2] = {0, 0};
   cudaMemcpyAsync(ctx->host_pinned, ib->d_fsum, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
-  cudaMemcpyAsync(st, ib->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaMemcpyAsync(st, ib->d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "marker force sum");
   for (int c = 0; c < 3; ++c) out[c] = ctx->host_pinned[c];
@@ -1133,6 +1616,41 @@ int ilbm_ib_last_marker_force_sum(ilbm_ib *ib, double out[3]) {
     set_error("IVC conjugate gradient did not converge");
     return ILBM_ERR_SOLVER;
   }
+  if (st[1] & 8) {
+    set_error("IVC operator has a non-positive pivot (not positive definite); its inverse is invalid");
+    return ILBM_ERR_SOLVER;
+  }
+  return ILBM_OK;
+}
+
+int ilbm_ib_solver_stats(ilbm_ib *ib, int *cg_iterations) {
+  if (!ib || !cg_iterations) return ILBM_ERR_ARG;
+  int it = 0;
+  cudaMemcpyAsync(&it, ib->d_iters, sizeof(int), cudaMemcpyDeviceToHost, ib->ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ib->ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_ib_solver_stats");
+  *cg_iterations = (ib->p.coupling_method == 1) ? it : 0;
+  return ILBM_OK;
+}
+
+int ilbm_ib_set_ivc_solver(ilbm_ib *ib, int solver) {
+  if (!ib || solver < ILBM_IVC_AUTO || solver > ILBM_IVC_DENSE) {
+    set_error("ilbm_ib_set_ivc_solver: bad argument");
+    return ILBM_ERR_ARG;
+  }
+  if (solver == ILBM_IVC_DENSE) {
+    if (ib->p.coupling_method != 1 || ib->moving || ib->p.ivc_rebuild_matrix > 0 ||
+        ib->n > ILBM_IVC_DENSE_MAX) {
+      set_error("ilbm_ib_set_ivc_solver: the stored inverse needs implicit velocity correction, "
+                "fixed markers, no matrix rebuild and at most ILBM_IVC_DENSE_MAX markers");
+      return ILBM_ERR_UNSUPPORTED;
+    }
+    cudaSetDevice(ib->ctx->device);
+    const int rc = enable_dense(ib);
+    if (rc) return rc;
+  }
+  ib->ivc_solver = solver;
+  ib->cg_warm = false;
   return ILBM_OK;
 }
 

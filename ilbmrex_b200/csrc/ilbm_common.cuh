@@ -104,57 +104,72 @@ struct X {
   __device__ static __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
 };
 
-// feqFunction, Source/LBM/feq.H:9-29
-template <class L>
-__device__ __forceinline__ double feq64(int q, double rho, double u, double v, double w) {
+// feqFunction, Source/LBM/feq.H:9-29 (c and w passed as values so the same
+// arithmetic serves compile-time and per-lane directions)
+template <int D>
+__device__ __forceinline__ double feq64v(double cx, double cy, double cz, double wq, double rho,
+                                         double u, double v, double w) {
   double eu, uv;
-  if (L::D == 3) {
-    eu = X::add(X::add(X::mul(double(L::cx(q)), u), X::mul(double(L::cy(q)), v)),
-                X::mul(double(L::cz(q)), w));
+  if (D == 3) {
+    eu = X::add(X::add(X::mul(cx, u), X::mul(cy, v)), X::mul(cz, w));
     uv = X::add(X::add(X::mul(u, u), X::mul(v, v)), X::mul(w, w));
   } else {
-    eu = X::add(X::mul(double(L::cx(q)), u), X::mul(double(L::cy(q)), v));
+    eu = X::add(X::mul(cx, u), X::mul(cy, v));
     uv = X::add(X::mul(u, u), X::mul(v, v));
   }
   // wi * rho * (1.0 + 3.0*eu + 4.5*eu*eu - 1.5*uv)
   const double p = X::sub(X::add(X::add(1.0, X::mul(3.0, eu)), X::mul(X::mul(4.5, eu), eu)),
                           X::mul(1.5, uv));
-  return X::mul(X::mul(L::w(q), rho), p);
+  return X::mul(X::mul(wq, rho), p);
+}
+template <class L>
+__device__ __forceinline__ double feq64(int q, double rho, double u, double v, double w) {
+  return feq64v<L::D>(double(L::cx(q)), double(L::cy(q)), double(L::cz(q)), L::w(q), rho, u, v, w);
 }
 
 // equilibrium with all three velocity terms (bc_fill.H:189-200,
 // AmrCoreLBM.cpp:2146-2158): always 3D sums, even for 2D lattices
-template <class L>
-__device__ __forceinline__ double feq64_3(int q, double rho, double u, double v, double w) {
-  const double eu = X::add(X::add(X::mul(double(L::cx(q)), u), X::mul(double(L::cy(q)), v)),
-                           X::mul(double(L::cz(q)), w));
+__device__ __forceinline__ double feq64_3v(double cx, double cy, double cz, double wq, double rho,
+                                           double u, double v, double w) {
+  const double eu = X::add(X::add(X::mul(cx, u), X::mul(cy, v)), X::mul(cz, w));
   const double uv = X::add(X::add(X::mul(u, u), X::mul(v, v)), X::mul(w, w));
   const double p = X::sub(X::add(X::add(1.0, X::mul(3.0, eu)), X::mul(X::mul(4.5, eu), eu)),
                           X::mul(1.5, uv));
-  return X::mul(X::mul(L::w(q), rho), p);
+  return X::mul(X::mul(wq, rho), p);
+}
+template <class L>
+__device__ __forceinline__ double feq64_3(int q, double rho, double u, double v, double w) {
+  return feq64_3v(double(L::cx(q)), double(L::cy(q)), double(L::cz(q)), L::w(q), rho, u, v, w);
 }
 
 // BGK relaxation of one population plus its Guo increment
 // (collide.H:48-55, collide_forced.H:81-108).  has_force is the cell's
 // (fx != 0 || fy != 0 || fz != 0) test.
-template <class L>
-__device__ __forceinline__ double collide64_one(int q, double f, double feq, double tau,
-                                                double ux, double uy, double uz, double fx,
-                                                double fy, double fz, bool has_force) {
+template <int D>
+__device__ __forceinline__ double collide64v(double cx, double cy, double cz, double wq, double f,
+                                             double feq, double tau, double ux, double uy,
+                                             double uz, double fx, double fy, double fz,
+                                             bool has_force) {
   double r = X::sub(X::mul(1.0, f), X::div(X::sub(f, feq), tau));
   if (!has_force) return r;
   const double cs2 = 1.0 / 3.0;
   const double fac = X::sub(1.0, X::div(0.5, tau));
-  const double cx = L::cx(q), cy = L::cy(q), cz = L::cz(q);
   const double eiu = X::add(X::add(X::mul(cx, ux), X::mul(cy, uy)), X::mul(cz, uz));
   const double c4 = X::mul(cs2, cs2);
   const double termx = X::add(X::div(X::sub(cx, ux), cs2), X::mul(X::div(eiu, c4), cx));
   const double termy = X::add(X::div(X::sub(cy, uy), cs2), X::mul(X::div(eiu, c4), cy));
   const double termz =
-      (L::D == 3) ? X::add(X::div(X::sub(cz, uz), cs2), X::mul(X::div(eiu, c4), cz)) : 0.0;
-  const double Si = X::mul(X::mul(L::w(q), fac),
+      (D == 3) ? X::add(X::div(X::sub(cz, uz), cs2), X::mul(X::div(eiu, c4), cz)) : 0.0;
+  const double Si = X::mul(X::mul(wq, fac),
                            X::add(X::add(X::mul(termx, fx), X::mul(termy, fy)), X::mul(termz, fz)));
   return X::add(r, Si);
+}
+template <class L>
+__device__ __forceinline__ double collide64_one(int q, double f, double feq, double tau,
+                                                double ux, double uy, double uz, double fx,
+                                                double fy, double fz, bool has_force) {
+  return collide64v<L::D>(double(L::cx(q)), double(L::cy(q)), double(L::cz(q)), L::w(q), f, feq,
+                          tau, ux, uy, uz, fx, fy, fz, has_force);
 }
 
 // ---------------------------------------------------------------------------
@@ -225,6 +240,10 @@ struct ilbm_ctx {
   void *scratch = nullptr;
   size_t scratch_bytes = 0;
   double *host_pinned = nullptr;
+  // side stream (high priority) and fork/join events for the overlapped
+  // immersed-boundary chain
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 // grow ctx scratch to at least n bytes (returns nullptr on failure)

@@ -62,6 +62,13 @@ struct StepArgs {
   double uf[3];
   int flo[3], fhi[3];
   float f16_scale;
+  float om32, omh32;  // 1/tau and 1 - 1/(2 tau) rounded to float, from the host
+  // per-direction element offsets: q*fs2 (load) and c_q + q*fs2 (push target)
+  int32_t loff[27], doff[27];
+  // cells handled by this launch: [rlo, rhi], minus [slo, shi] when use_skip
+  int rlo[3], rhi[3];
+  int slo[3], shi[3];
+  int use_skip;
   int nlb;
   int lb[kMaxLevelBoxes][6];
 };
@@ -168,23 +175,32 @@ __device__ __forceinline__ void moments32(const float *g, float Fx, float Fy, fl
 }
 
 // shifted equilibrium: f_eq - w_q
-template <class L>
-__device__ __forceinline__ float feqs(int q, float drho, float u, float v, float w) {
-  const float cu = float(L::cx(q)) * u + float(L::cy(q)) * v + float(L::cz(q)) * w;
+__device__ __forceinline__ float feqsv(float cx, float cy, float cz, float wq, float drho, float u,
+                                       float v, float w) {
+  const float cu = cx * u + cy * v + cz * w;
   const float uu = u * u + v * v + w * w;
   const float P = 3.0f * cu + 4.5f * cu * cu - 1.5f * uu;
-  return float(L::w(q)) * (drho + (1.0f + drho) * P);
+  return wq * (drho + (1.0f + drho) * P);
+}
+template <class L>
+__device__ __forceinline__ float feqs(int q, float drho, float u, float v, float w) {
+  return feqsv(float(L::cx(q)), float(L::cy(q)), float(L::cz(q)), float(L::w(q)), drho, u, v, w);
 }
 
-template <class L>
-__device__ __forceinline__ float guo32(int q, float omh, float u, float v, float w, float Fx,
-                                       float Fy, float Fz) {
-  const float cx = float(L::cx(q)), cy = float(L::cy(q)), cz = float(L::cz(q));
+template <int D>
+__device__ __forceinline__ float guo32v(float cx, float cy, float cz, float wq, float omh, float u,
+                                        float v, float w, float Fx, float Fy, float Fz) {
   const float cu = cx * u + cy * v + cz * w;
   const float tx = 3.0f * (cx - u) + 9.0f * cu * cx;
   const float ty = 3.0f * (cy - v) + 9.0f * cu * cy;
-  const float tz = (L::D == 3) ? 3.0f * (cz - w) + 9.0f * cu * cz : 0.0f;
-  return float(L::w(q)) * omh * (tx * Fx + ty * Fy + tz * Fz);
+  const float tz = (D == 3) ? 3.0f * (cz - w) + 9.0f * cu * cz : 0.0f;
+  return wq * omh * (tx * Fx + ty * Fy + tz * Fz);
+}
+template <class L>
+__device__ __forceinline__ float guo32(int q, float omh, float u, float v, float w, float Fx,
+                                       float Fy, float Fz) {
+  return guo32v<L::D>(float(L::cx(q)), float(L::cy(q)), float(L::cz(q)), float(L::w(q)), omh, u,
+                      v, w, Fx, Fy, Fz);
 }
 
 // ---------------------------------------------------------------------------
@@ -258,303 +274,338 @@ __device__ __forceinline__ int ghost_rule(const StepArgs &a, const int *g, int *
   return 0;
 }
 
-// Fill all Q populations of ghost cell g in f_in (self-fill prepass).
+// Populations that enter the box from its layer-1 ghost shell are pushed here,
+// one thread per ghost cell: the pre-collision boundary value (self-fill: the
+// FillPatch rules above on f^n of the domain; caller-filled: the ghost value
+// as given), or, for a ghost covered by another box of the level, that cell's
+// post-collision value.  Ghosts that are periodic images (self-fill) and
+// halfway bounce-back ghosts are left to the owning cells' push.  A ghost cell
+// is owned by the slab of its lowest dimension outside the box (periodic
+// dimensions excluded in self-fill mode, whose slabs do nothing).
 template <class L, int S>
-__device__ void fill_ghost_cell(const StepArgs &a, const int *g) {
+__global__ void __launch_bounds__(256) k_ghost_push(StepArgs a) {
   using T = typename Store<S>::T;
-  int src[3], bd = 0, lo_side = 1;
-  const int kind = ghost_rule<L>(a, g, src, bd, lo_side);
-  T *fo = static_cast<T *>(const_cast<void *>(a.f_in));
-  const int64_t gi = fidx(a, g[0], g[1], L::D == 3 ? g[2] : 0);
-  const int64_t si = fidx(a, src[0], src[1], L::D == 3 ? src[2] : 0);
-  if (kind <= 1) {
-#pragma unroll
-    for (int q = 0; q < L::Q; ++q) fo[gi + q * a.fs2] = fo[si + q * a.fs2];
-    return;
-  }
-  const double *bv = lo_side ? a.bvlo[bd] : a.bvhi[bd];
-  if (S == ILBM_STORAGE_F64) {
-    // applyExtDirMesoscopic / applyFaceMirroredMesoscopic, bc_fill.H:159-261
-    double fnp[L::Q];
-    double rhonp = 0.0, unp = 0.0, vnp = 0.0, wnp = 0.0;
-#pragma unroll
-    for (int n = 0; n < L::Q; ++n) {
-      fnp[n] = ldf<L, S>(a, si, n);
-      rhonp = X::add(rhonp, fnp[n]);
-      unp = X::add(unp, X::mul(double(L::cx(n)), fnp[n]));
-      vnp = X::add(vnp, X::mul(double(L::cy(n)), fnp[n]));
-      wnp = X::add(wnp, X::mul(double(L::cz(n)), fnp[n]));
-    }
-    rhonp = fmax(rhonp, 1.0e-20);
-    unp = X::div(unp, rhonp);
-    vnp = X::div(vnp, rhonp);
-    wnp = X::div(wnp, rhonp);
-    double rt = bv[0], ut = bv[1], vt = bv[2], wt = bv[3];
-    if (kind == 3) {
-      rt = fmax(1.0e-20, X::sub(X::mul(2.0, bv[0]), rhonp));
-      ut = X::sub(X::mul(2.0, bv[1]), unp);
-      vt = X::sub(X::mul(2.0, bv[2]), vnp);
-      wt = X::sub(X::mul(2.0, bv[3]), wnp);
-    }
-#pragma unroll
-    for (int n = 0; n < L::Q; ++n) {
-      const double fe_np = feq64_3<L>(n, rhonp, unp, vnp, wnp);
-      const double fe_t = feq64_3<L>(n, rt, ut, vt, wt);
-      reinterpret_cast<double *>(fo)[gi + n * a.fs2] = X::add(fe_t, X::sub(fnp[n], fe_np));
-    }
-  } else {
-    float gnp[L::Q];
-    float r = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f;
-#pragma unroll
-    for (int n = 0; n < L::Q; ++n) {
-      gnp[n] = ldf<L, S>(a, si, n);
-      r += gnp[n];
-      m1 += float(L::cx(n)) * gnp[n];
-      m2 += float(L::cy(n)) * gnp[n];
-      m3 += float(L::cz(n)) * gnp[n];
-    }
-    const float rho = fmaxf(1.0f + r, 1.0e-20f);
-    const float drho = rho - 1.0f;
-    const float u = m1 / rho, v = m2 / rho, w = m3 / rho;
-    float dr_t = float(bv[0]) - 1.0f, ut = float(bv[1]), vt = float(bv[2]), wt = float(bv[3]);
-    if (kind == 3) {
-      const float rg = fmaxf(1.0e-20f, 2.0f * float(bv[0]) - rho);
-      dr_t = rg - 1.0f;
-      ut = 2.0f * float(bv[1]) - u;
-      vt = 2.0f * float(bv[2]) - v;
-      wt = 2.0f * float(bv[3]) - w;
-    }
-#pragma unroll
-    for (int n = 0; n < L::Q; ++n) {
-      const float val = feqs<L>(n, dr_t, ut, vt, wt) + (gnp[n] - feqs<L>(n, drho, u, v, w));
-      Store<S>::store(fo + gi + n * a.fs2, val, sfac<L, S>(a, n));
-    }
-  }
-}
-
-// Prepass over layer-1 ghosts outside the domain in a non-periodic direction.
-// blockIdx.z selects the face slab (dim, side); a cell is owned by the slab of
-// its lowest out-of-range non-periodic dimension.
-template <class L, int S>
-__global__ void __launch_bounds__(256) k_ghost_fill(StepArgs a) {
+  using R = typename Store<S>::R;
   const int slab = blockIdx.z;
   const int d = slab >> 1, side = slab & 1;
-  if (d >= L::D || a.periodic[d]) return;
-  // slab coordinates: all other dims over [dlo-1, dhi+1]
+  if (d >= L::D) return;
+  if (a.self_fill && a.periodic[d]) return;
   int ext[3], base[3];
 #pragma unroll
   for (int e = 0; e < 3; ++e) {
     if (e >= L::D) { ext[e] = 1; base[e] = 0; continue; }
-    ext[e] = a.dhi[e] - a.dlo[e] + 3;
-    base[e] = a.dlo[e] - 1;
+    ext[e] = a.hi[e] - a.lo[e] + 3;
+    base[e] = a.lo[e] - 1;
   }
   ext[d] = 1;
-  base[d] = side ? a.dhi[d] + 1 : a.dlo[d] - 1;
+  base[d] = side ? a.hi[d] + 1 : a.lo[d] - 1;
   const int64_t n = (int64_t)ext[0] * ext[1] * ext[2];
+  const T *fin = static_cast<const T *>(a.f_in);
+  T *fo = static_cast<T *>(a.f_out);
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x) {
     int g[3];
     g[0] = base[0] + (int)(t % ext[0]);
     g[1] = base[1] + (int)((t / ext[0]) % ext[1]);
     g[2] = base[2] + (int)(t / ((int64_t)ext[0] * ext[1]));
+    // owner: lowest dimension outside the box whose slab is active (in
+    // self-fill mode periodic slabs are skipped)
     int owner = -1;
 #pragma unroll
     for (int e = 0; e < L::D; ++e)
-      if (owner < 0 && !a.periodic[e] && (g[e] < a.dlo[e] || g[e] > a.dhi[e])) owner = e;
+      if (owner < 0 && (g[e] < a.lo[e] || g[e] > a.hi[e]) && !(a.self_fill && a.periodic[e]))
+        owner = e;
     if (owner != d) continue;
-    fill_ghost_cell<L, S>(a, g);
+    // classify the ghost against the domain
+    bool phys = false, pure_u1 = true;
+#pragma unroll
+    for (int e = 0; e < L::D; ++e) {
+      int sd = 0;
+      if (g[e] < a.dlo[e]) sd = -1;
+      else if (g[e] > a.dhi[e]) sd = 1;
+      if (sd == 0) continue;
+      if (a.periodic[e]) {
+        pure_u1 = false;
+      } else {
+        phys = true;
+        if ((sd < 0 ? a.bclo[e] : a.bchi[e]) != ILBM_BC_USER_1) pure_u1 = false;
+      }
+    }
+    if (a.self_fill && !phys) continue;  // periodic image: the wrapping push delivers it
+    if (phys && pure_u1) continue;       // halfway bounce-back: reflected by the cell
+    const int gk = (L::D == 3) ? g[2] : 0;
+    // source of the ghost's populations
+    int mode;  // 0 copy from src (raw), 1 NEQ boundary formula on src, 2 collide the ghost
+    int src[3] = {g[0], g[1], gk}, bd = 0, lo_side = 1, kind = 0;
+    if (phys && a.self_fill) {
+      kind = ghost_rule<L>(a, g, src, bd, lo_side);
+      mode = (kind <= 1) ? 0 : 1;
+    } else if (phys) {
+      mode = 0;  // caller-filled physical ghost, as given
+    } else {
+      int gw[3] = {g[0], g[1], gk};
+#pragma unroll
+      for (int e = 0; e < L::D; ++e)
+        if (a.periodic[e]) {
+          const int nn = a.dhi[e] - a.dlo[e] + 1;
+          gw[e] = a.dlo[e] + (((gw[e] - a.dlo[e]) % nn) + nn) % nn;
+        }
+      bool covered = false;
+      for (int b = 0; b < a.nlb && !covered; ++b)
+        covered = gw[0] >= a.lb[b][0] && gw[0] <= a.lb[b][3] && gw[1] >= a.lb[b][1] &&
+                  gw[1] <= a.lb[b][4] && (L::D == 2 || (gw[2] >= a.lb[b][2] && gw[2] <= a.lb[b][5]));
+      mode = covered ? 2 : 0;  // not covered: coarse-fine ghost, as given
+    }
+    const int64_t sb = fidx(a, src[0], src[1], L::D == 3 ? src[2] : 0);
+    // per-ghost state for the NEQ formula / the collision
+    double r64 = 0, u64 = 0, v64 = 0, w64 = 0, rt64 = 0, ut64 = 0, vt64 = 0, wt64 = 0;
+    float dr32 = 0, u32 = 0, v32 = 0, w32 = 0, drt32 = 0, ut32 = 0, vt32 = 0, wt32 = 0;
+    R gFx = R(0), gFy = R(0), gFz = R(0);
+    bool ghf = false;
+    if (mode == 1) {
+      // applyExtDirMesoscopic / applyFaceMirroredMesoscopic, bc_fill.H:159-261
+      const double *bv = lo_side ? a.bvlo[bd] : a.bvhi[bd];
+      if (S == ILBM_STORAGE_F64) {
+        double rhonp = 0.0, unp = 0.0, vnp = 0.0, wnp = 0.0;
+#pragma unroll
+        for (int p = 0; p < L::Q; ++p) {
+          const double fp = ldf<L, S>(a, sb, p);
+          rhonp = X::add(rhonp, fp);
+          unp = X::add(unp, X::mul(double(L::cx(p)), fp));
+          vnp = X::add(vnp, X::mul(double(L::cy(p)), fp));
+          wnp = X::add(wnp, X::mul(double(L::cz(p)), fp));
+        }
+        rhonp = fmax(rhonp, 1.0e-20);
+        r64 = rhonp;
+        u64 = X::div(unp, rhonp);
+        v64 = X::div(vnp, rhonp);
+        w64 = X::div(wnp, rhonp);
+        rt64 = bv[0]; ut64 = bv[1]; vt64 = bv[2]; wt64 = bv[3];
+        if (kind == 3) {
+          rt64 = fmax(1.0e-20, X::sub(X::mul(2.0, bv[0]), r64));
+          ut64 = X::sub(X::mul(2.0, bv[1]), u64);
+          vt64 = X::sub(X::mul(2.0, bv[2]), v64);
+          wt64 = X::sub(X::mul(2.0, bv[3]), w64);
+        }
+      } else {
+        float rr = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f;
+#pragma unroll
+        for (int p = 0; p < L::Q; ++p) {
+          const float gp = ldf<L, S>(a, sb, p);
+          rr += gp;
+          if (L::cx(p)) m1 += float(L::cx(p)) * gp;
+          if (L::cy(p)) m2 += float(L::cy(p)) * gp;
+          if (L::cz(p)) m3 += float(L::cz(p)) * gp;
+        }
+        const float rho = fmaxf(1.0f + rr, 1.0e-20f);
+        dr32 = rho - 1.0f;
+        u32 = m1 / rho; v32 = m2 / rho; w32 = m3 / rho;
+        drt32 = float(bv[0]) - 1.0f; ut32 = float(bv[1]); vt32 = float(bv[2]); wt32 = float(bv[3]);
+        if (kind == 3) {
+          drt32 = fmaxf(1.0e-20f, 2.0f * float(bv[0]) - rho) - 1.0f;
+          ut32 = 2.0f * float(bv[1]) - u32;
+          vt32 = 2.0f * float(bv[2]) - v32;
+          wt32 = 2.0f * float(bv[3]) - w32;
+        }
+      }
+    } else if (mode == 2) {
+      load_force<L, R>(a, a.force, g[0], g[1], gk, gFx, gFy, gFz);
+      ghf = !(gFx == R(0) && gFy == R(0) && gFz == R(0));
+      if (a.macro_in) {
+        const int64_t m = midx(a, g[0], g[1], gk);
+        if (S == ILBM_STORAGE_F64) {
+          r64 = ldm<double>(a.macro_in, m);
+          u64 = ldm<double>(a.macro_in, m + a.ms2);
+          v64 = ldm<double>(a.macro_in, m + 2 * a.ms2);
+          w64 = (L::D == 3) ? ldm<double>(a.macro_in, m + 3 * a.ms2) : 0.0;
+        } else {
+          dr32 = ldm<float>(a.macro_in, m) - 1.0f;
+          u32 = ldm<float>(a.macro_in, m + a.ms2);
+          v32 = ldm<float>(a.macro_in, m + 2 * a.ms2);
+          w32 = (L::D == 3) ? ldm<float>(a.macro_in, m + 3 * a.ms2) : 0.0f;
+        }
+      } else if (S == ILBM_STORAGE_F64) {
+        double fg[L::Q];
+#pragma unroll
+        for (int p = 0; p < L::Q; ++p) fg[p] = ldf<L, S>(a, sb, p);
+        double px, py, pz;
+        load_force<L, double>(a, a.force_prev, g[0], g[1], gk, px, py, pz);
+        moments64<L>(fg, px, py, pz, r64, u64, v64, w64);
+        if (L::D != 3) w64 = 0.0;
+      } else {
+        float fg[L::Q];
+#pragma unroll
+        for (int p = 0; p < L::Q; ++p) fg[p] = ldf<L, S>(a, sb, p);
+        float px, py, pz;
+        load_force<L, float>(a, a.force_prev, g[0], g[1], gk, px, py, pz);
+        moments32<L>(fg, px, py, pz, dr32, u32, v32, w32);
+      }
+    }
+#pragma unroll
+    for (int q = 1; q < L::Q; ++q) {
+      const int di = g[0] + L::cx(q), dj = g[1] + L::cy(q), dk = gk + L::cz(q);
+      if (!in_box(a.lo, a.hi, di, dj, dk)) continue;
+      const R fq = ldf<L, S>(a, sb, q);
+      R val;
+      if (mode == 0) {
+        val = fq;
+      } else if (mode == 1) {
+        if (S == ILBM_STORAGE_F64)
+          val = R(X::add(feq64_3<L>(q, rt64, ut64, vt64, wt64),
+                         X::sub(double(fq), feq64_3<L>(q, r64, u64, v64, w64))));
+        else
+          val = R(feqs<L>(q, drt32, ut32, vt32, wt32) + (float(fq) - feqs<L>(q, dr32, u32, v32, w32)));
+      } else {
+        if (S == ILBM_STORAGE_F64)
+          val = R(collide64_one<L>(q, double(fq), feq64<L>(q, r64, u64, v64, w64), a.tau, u64, v64,
+                                   w64, double(gFx), double(gFy), double(gFz), ghf));
+        else {
+          float gv = float(fq) + a.om32 * (feqs<L>(q, dr32, u32, v32, w32) - float(fq));
+          if (ghf) gv += guo32<L>(q, a.omh32, u32, v32, w32, float(gFx), float(gFy), float(gFz));
+          val = R(gv);
+        }
+      }
+      Store<S>::store(fo + fidx(a, di, dj, dk) + q * a.fs2, val, sfac<L, S>(a, q));
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // Main fused kernel
 // ---------------------------------------------------------------------------
+// occupancy target: 4 resident blocks of 256 threads per SM for the 4-byte and
+// 2-byte storage forms of D2Q9/D3Q19 (<= 64 registers), 2 otherwise
 template <class L, int S>
-__global__ void __launch_bounds__(256) k_step(StepArgs a) {
+struct StepOcc {
+  static constexpr int value = (S != ILBM_STORAGE_F64 && L::Q <= 19) ? 4 : 2;
+};
+
+// One cell of the level step: load f^n, recover rho^n/u^n, collide, push.
+// `edge` selects the checked push plus the completion of ghost-sourced pulls;
+// interior cells take the unchecked path.
+template <class L, int S>
+__device__ __forceinline__ void cell_update(const StepArgs &a, int i, int j, int k, bool edge) {
   using T = typename Store<S>::T;
   using R = typename Store<S>::R;
-  const int i = a.lo[0] + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = a.lo[1] + blockIdx.y;
-  const int k = a.lo[2] + blockIdx.z;
-  if (i > a.hi[0]) return;
-
   const int64_t base = fidx(a, i, j, k);
+  const T *fin = static_cast<const T *>(a.f_in) + base;
   R f[L::Q];
 #pragma unroll
-  for (int q = 0; q < L::Q; ++q) f[q] = ldf<L, S>(a, base, q);
+  for (int q = 0; q < L::Q; ++q) f[q] = Store<S>::load(fin + a.loff[q], sfac<L, S>(a, q));
 
   R Fx, Fy, Fz;
   load_force<L, R>(a, a.force, i, j, k, Fx, Fy, Fz);
 
-  R fs[L::Q];
+  // per-cell collision state: rho^n, u^n (stored or recovered) and F^n
+  double rho64 = 0, u64 = 0, v64 = 0, w64 = 0;
+  float drho32 = 0, u32 = 0, v32 = 0, w32 = 0;
   if (S == ILBM_STORAGE_F64) {
-    double rho, u, v, w;
     if (a.macro_in) {
       const int64_t m = midx(a, i, j, k);
-      rho = ldm<double>(a.macro_in, m);
-      u = ldm<double>(a.macro_in, m + a.ms2);
-      v = ldm<double>(a.macro_in, m + 2 * a.ms2);
-      w = (L::D == 3) ? ldm<double>(a.macro_in, m + 3 * a.ms2) : 0.0;
+      rho64 = ldm<double>(a.macro_in, m);
+      u64 = ldm<double>(a.macro_in, m + a.ms2);
+      v64 = ldm<double>(a.macro_in, m + 2 * a.ms2);
+      w64 = (L::D == 3) ? ldm<double>(a.macro_in, m + 3 * a.ms2) : 0.0;
     } else {
       double px, py, pz;
       load_force<L, double>(a, a.force_prev, i, j, k, px, py, pz);
-      moments64<L>(reinterpret_cast<double *>(f), px, py, pz, rho, u, v, w);
-      if (L::D != 3) w = 0.0;
-    }
-    const bool hf = !(double(Fx) == 0.0 && double(Fy) == 0.0 && double(Fz) == 0.0);
-#pragma unroll
-    for (int q = 0; q < L::Q; ++q) {
-      const double fe = feq64<L>(q, rho, u, v, w);
-      fs[q] = collide64_one<L>(q, double(f[q]), fe, a.tau, u, v, w, double(Fx), double(Fy),
-                               double(Fz), hf);
+      moments64<L>(reinterpret_cast<double *>(f), px, py, pz, rho64, u64, v64, w64);
+      if (L::D != 3) w64 = 0.0;
     }
   } else {
-    float drho, u, v, w;
     if (a.macro_in) {
       const int64_t m = midx(a, i, j, k);
-      drho = ldm<float>(a.macro_in, m) - 1.0f;
-      u = ldm<float>(a.macro_in, m + a.ms2);
-      v = ldm<float>(a.macro_in, m + 2 * a.ms2);
-      w = (L::D == 3) ? ldm<float>(a.macro_in, m + 3 * a.ms2) : 0.0f;
+      drho32 = ldm<float>(a.macro_in, m) - 1.0f;
+      u32 = ldm<float>(a.macro_in, m + a.ms2);
+      v32 = ldm<float>(a.macro_in, m + 2 * a.ms2);
+      w32 = (L::D == 3) ? ldm<float>(a.macro_in, m + 3 * a.ms2) : 0.0f;
     } else {
       float px, py, pz;
       load_force<L, float>(a, a.force_prev, i, j, k, px, py, pz);
-      moments32<L>(reinterpret_cast<float *>(f), px, py, pz, drho, u, v, w);
-    }
-    const float om = float(1.0 / a.tau);
-    const float omh = float(1.0 - 0.5 / a.tau);
-#pragma unroll
-    for (int q = 0; q < L::Q; ++q) {
-      const float ge = feqs<L>(q, drho, u, v, w);
-      float val = float(f[q]) + om * (ge - float(f[q]));
-      val += guo32<L>(q, omh, u, v, w, float(Fx), float(Fy), float(Fz));
-      fs[q] = val;
+      moments32<L>(reinterpret_cast<float *>(f), px, py, pz, drho32, u32, v32, w32);
     }
   }
+  // the Guo increment is skipped where F == 0 (collide_forced.H:81-83)
+  const bool hf = !(Fx == R(0) && Fy == R(0) && Fz == R(0));
+  const float om = a.om32;
+  const float omh = a.omh32;
+  auto post_v = [&](int q, R fq) -> R {
+    if (S == ILBM_STORAGE_F64) {
+      const double fe = feq64<L>(q, rho64, u64, v64, w64);
+      return R(collide64_one<L>(q, double(fq), fe, a.tau, u64, v64, w64, double(Fx),
+                                double(Fy), double(Fz), hf));
+    } else {
+      const float ge = feqs<L>(q, drho32, u32, v32, w32);
+      float val = float(fq) + om * (ge - float(fq));
+      if (hf) val += guo32<L>(q, omh, u32, v32, w32, float(Fx), float(Fy), float(Fz));
+      return R(val);
+    }
+  };
 
   T *fo = static_cast<T *>(a.f_out);
-  // push f*(y,q) to y + c_q
+  T *fob = fo + base;
+  // Push: every thread, edge or not, stores f*(y,q) at y + c_q.  For an edge
+  // cell some of these land in the ghost layer of f_out, which is scratch
+  // (never read); they are fixed up below.
 #pragma unroll
-  for (int q = 0; q < L::Q; ++q) {
-    int di = i + L::cx(q), dj = j + L::cy(q), dk = k + L::cz(q);
-    bool ok = in_box(a.lo, a.hi, di, dj, dk);
-    if (!ok && a.self_fill) {
-      // single box = domain: wrap periodic directions
-      ok = true;
-      if (L::cx(q) != 0 && (di < a.dlo[0] || di > a.dhi[0])) {
-        if (a.periodic[0]) di = (di < a.dlo[0]) ? a.dhi[0] : a.dlo[0];
-        else ok = false;
-      }
-      if (L::cy(q) != 0 && (dj < a.dlo[1] || dj > a.dhi[1])) {
-        if (a.periodic[1]) dj = (dj < a.dlo[1]) ? a.dhi[1] : a.dlo[1];
-        else ok = false;
-      }
-      if (L::D == 3 && L::cz(q) != 0 && (dk < a.dlo[2] || dk > a.dhi[2])) {
-        if (a.periodic[2]) dk = (dk < a.dlo[2]) ? a.dhi[2] : a.dlo[2];
-        else ok = false;
-      }
-    }
-    if (ok) Store<S>::store(fo + fidx(a, di, dj, dk) + q * a.fs2, fs[q], sfac<L, S>(a, q));
-  }
-
-  // complete pulls whose source is a ghost no thread pushes from
-  const bool edge = (i == a.lo[0] || i == a.hi[0] || j == a.lo[1] || j == a.hi[1] ||
-                     (L::D == 3 && (k == a.lo[2] || k == a.hi[2])));
+  for (int q = 0; q < L::Q; ++q) Store<S>::store(fob + a.doff[q], post_v(q, f[q]), sfac<L, S>(a, q));
   if (!edge) return;
+  // Edge fix-up for destinations outside the box: periodic image (self-fill)
+  // -> wrapped push; halfway bounce-back wall -> reflected into this cell
+  // (f*(x,q) -> f_out(x, q_bar), AdvanceLBMAtLevel.cpp:272-373); anything
+  // else leaves the box (the populations entering from that ghost come from
+  // k_ghost_push).  The few populations involved are re-collided from a reload.
+  const T *fin_c = static_cast<const T *>(a.f_in) + base;
 #pragma unroll
   for (int q = 1; q < L::Q; ++q) {
-    const int gi = i - L::cx(q), gj = j - L::cy(q), gk = k - L::cz(q);
-    if (in_box(a.lo, a.hi, gi, gj, gk)) continue;
-    const int g[3] = {gi, gj, gk};
-    bool out_np = false, pure_u1 = true;
+    int di = i + L::cx(q), dj = j + L::cy(q), dk = k + L::cz(q);
+    if (in_box(a.lo, a.hi, di, dj, dk)) continue;
+    const int dd[3] = {di, dj, dk};
+    bool phys = false, pure_u1 = true;
 #pragma unroll
-    for (int d = 0; d < L::D; ++d) {
-      int side = 0;
-      if (g[d] < a.dlo[d]) side = -1;
-      else if (g[d] > a.dhi[d]) side = 1;
-      if (side == 0) continue;
-      if (a.periodic[d]) {
+    for (int e = 0; e < L::D; ++e) {
+      int sd = 0;
+      if (dd[e] < a.dlo[e]) sd = -1;
+      else if (dd[e] > a.dhi[e]) sd = 1;
+      if (sd == 0) continue;
+      if (a.periodic[e]) {
         pure_u1 = false;
       } else {
-        out_np = true;
-        const int bc = side < 0 ? a.bclo[d] : a.bchi[d];
-        if (bc != ILBM_BC_USER_1) pure_u1 = false;
+        phys = true;
+        if ((sd < 0 ? a.bclo[e] : a.bchi[e]) != ILBM_BC_USER_1) pure_u1 = false;
       }
     }
-    R val;
-    if (!out_np) {
-      if (a.self_fill) continue;  // delivered by the periodic pusher
-      // caller-filled ghost inside the (periodic) domain
-      int gw[3] = {gi, gj, gk};
-#pragma unroll
-      for (int d = 0; d < L::D; ++d)
-        if (a.periodic[d]) {
-          const int n = a.dhi[d] - a.dlo[d] + 1;
-          gw[d] = a.dlo[d] + (((gw[d] - a.dlo[d]) % n) + n) % n;
-        }
-      bool covered = false;
-      for (int b = 0; b < a.nlb && !covered; ++b)
-        covered = gw[0] >= a.lb[b][0] && gw[0] <= a.lb[b][3] && gw[1] >= a.lb[b][1] &&
-                  gw[1] <= a.lb[b][4] && (L::D == 2 || (gw[2] >= a.lb[b][2] && gw[2] <= a.lb[b][5]));
-      const int64_t gb = fidx(a, gi, gj, gk);
-      const R fg = ldf<L, S>(a, gb, q);
-      if (!covered) {
-        val = fg;
-      } else {
-        // the neighbour box's post-collision value of this population,
-        // recomputed from the caller-filled ghost data
-        R gFx, gFy, gFz;
-        load_force<L, R>(a, a.force, gi, gj, gk, gFx, gFy, gFz);
-        if (S == ILBM_STORAGE_F64) {
-          double rho, u, v, w;
-          if (a.macro_in) {
-            const int64_t m = midx(a, gi, gj, gk);
-            rho = ldm<double>(a.macro_in, m);
-            u = ldm<double>(a.macro_in, m + a.ms2);
-            v = ldm<double>(a.macro_in, m + 2 * a.ms2);
-            w = (L::D == 3) ? ldm<double>(a.macro_in, m + 3 * a.ms2) : 0.0;
-          } else {
-            double fg_all[L::Q];
-#pragma unroll
-            for (int p = 0; p < L::Q; ++p) fg_all[p] = double(ldf<L, S>(a, gb, p));
-            double px, py, pz;
-            load_force<L, double>(a, a.force_prev, gi, gj, gk, px, py, pz);
-            moments64<L>(fg_all, px, py, pz, rho, u, v, w);
-            if (L::D != 3) w = 0.0;
-          }
-          const bool hf = !(double(gFx) == 0.0 && double(gFy) == 0.0 && double(gFz) == 0.0);
-          val = collide64_one<L>(q, double(fg), feq64<L>(q, rho, u, v, w), a.tau, u, v, w,
-                                 double(gFx), double(gFy), double(gFz), hf);
-        } else {
-          float drho, u, v, w;
-          if (a.macro_in) {
-            const int64_t m = midx(a, gi, gj, gk);
-            drho = ldm<float>(a.macro_in, m) - 1.0f;
-            u = ldm<float>(a.macro_in, m + a.ms2);
-            v = ldm<float>(a.macro_in, m + 2 * a.ms2);
-            w = (L::D == 3) ? ldm<float>(a.macro_in, m + 3 * a.ms2) : 0.0f;
-          } else {
-            float g_all[L::Q];
-#pragma unroll
-            for (int p = 0; p < L::Q; ++p) g_all[p] = float(ldf<L, S>(a, gb, p));
-            float px, py, pz;
-            load_force<L, float>(a, a.force_prev, gi, gj, gk, px, py, pz);
-            moments32<L>(g_all, px, py, pz, drho, u, v, w);
-          }
-          const float om = float(1.0 / a.tau);
-          const float omh = float(1.0 - 0.5 / a.tau);
-          const float ge = feqs<L>(q, drho, u, v, w);
-          val = float(fg) + om * (ge - float(fg)) +
-                guo32<L>(q, omh, u, v, w, float(gFx), float(gFy), float(gFz));
-        }
-      }
-    } else if (pure_u1) {
-      val = fs[opposite<L>(q)];  // halfway bounce-back, AdvanceLBMAtLevel.cpp:272-373
+    T *dst;
+    if (phys) {
+      if (!pure_u1) continue;
+      dst = fob + a.loff[opposite<L>(q)];
+    } else if (a.self_fill) {
+      if (L::cx(q) != 0 && (di < a.dlo[0] || di > a.dhi[0])) di = (di < a.dlo[0]) ? a.dhi[0] : a.dlo[0];
+      if (L::cy(q) != 0 && (dj < a.dlo[1] || dj > a.dhi[1])) dj = (dj < a.dlo[1]) ? a.dhi[1] : a.dlo[1];
+      if (L::D == 3 && L::cz(q) != 0 && (dk < a.dlo[2] || dk > a.dhi[2]))
+        dk = (dk < a.dlo[2]) ? a.dhi[2] : a.dlo[2];
+      dst = fo + fidx(a, di, dj, dk) + (int64_t)q * a.fs2;
     } else {
-      val = ldf<L, S>(a, fidx(a, gi, gj, gk), q);  // pre-collision BC ghost
+      continue;  // another box: its ghost shell push delivers
     }
-    Store<S>::store(fo + base + q * a.fs2, val, sfac<L, S>(a, q));
+    const R fq = Store<S>::load(fin_c + a.loff[q], sfac<L, S>(a, q));
+    // (w_q = w_{q_bar}: the FP16 storage factor is the same for a reflection)
+    Store<S>::store(dst, post_v(q, fq), sfac<L, S>(a, q));
   }
+}
+
+// Main kernel: one thread per cell of a row segment (rows on a box face run
+// the checked push as a whole; only the two x-edge cells of a row diverge).
+template <class L, int S>
+__global__ void __launch_bounds__(256, StepOcc<L, S>::value) k_step(StepArgs a) {
+  const int i = a.rlo[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = a.rlo[1] + blockIdx.y;
+  const int k = a.rlo[2] + blockIdx.z;
+  if (i > a.rhi[0]) return;
+  if (a.use_skip && in_box(a.slo, a.shi, i, j, k)) return;
+  const bool edge = (i == a.lo[0] || i == a.hi[0] || j == a.lo[1] || j == a.hi[1] ||
+                     (L::D == 3 && (k == a.lo[2] || k == a.hi[2])));
+  cell_update<L, S>(a, i, j, k, edge);
 }
 
 // ---------------------------------------------------------------------------
@@ -720,11 +771,11 @@ __global__ void __launch_bounds__(256) k_band_macro(StepArgs a, int blo0, int bl
 
 template <class L, int S>
 static int launch_band_macro(ilbm_ctx *ctx, const StepArgs &a, const int *blo, const int *bn,
-                             double *EV, double *RHO) {
+                             double *EV, double *RHO, cudaStream_t st) {
   const int64_t nb = (int64_t)bn[0] * bn[1] * bn[2];
   const int blocks = (int)std::min<int64_t>((nb + 255) / 256, 2048);
-  k_band_macro<L, S><<<blocks, 256, 0, ctx->stream>>>(a, blo[0], blo[1], blo[2], bn[0], bn[1],
-                                                      bn[2], EV, RHO);
+  k_band_macro<L, S><<<blocks, 256, 0, st>>>(a, blo[0], blo[1], blo[2], bn[0], bn[1], bn[2], EV,
+                                              RHO);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "band macro launch");
@@ -744,6 +795,11 @@ static int fill_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_pa
     a.fgl[d] = (d < D) ? b.lo[d] - b.ngrow_f : 0;
     a.mgl[d] = (d < D) ? b.lo[d] - b.ngrow_m : 0;
   }
+  for (int d = 0; d < 3; ++d) {
+    a.rlo[d] = a.lo[d];
+    a.rhi[d] = a.hi[d];
+  }
+  a.use_skip = 0;
   a.fs0 = b.fstride[0];
   a.fs1 = b.fstride[1];
   a.fs2 = b.fstride[2];
@@ -752,6 +808,27 @@ static int fill_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_pa
   a.ms2 = b.mstride[2];
   a.f_in = b.f_in;
   a.f_out = b.f_out;
+  {
+    static const int cx9[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+    static const int cy9[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+    static const int cx19[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    static const int cy19[19] = {0, 0, 0, 1, -1, 0, 0, 1, -1, -1, 1, 0, 0, 0, 0, 1, -1, 1, -1};
+    static const int cz19[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1};
+    for (int q = 0; q < ctx->q; ++q) {
+      int cx = 0, cy = 0, cz = 0;
+      if (ctx->q == 9) { cx = cx9[q]; cy = cy9[q]; }
+      else if (ctx->q == 19) { cx = cx19[q]; cy = cy19[q]; cz = cz19[q]; }
+      else { cx = Lat<27>::cx(q); cy = Lat<27>::cy(q); cz = Lat<27>::cz(q); }
+      const int64_t lo = (int64_t)q * b.fstride[2];
+      const int64_t dof = lo + cx + (int64_t)cy * b.fstride[0] + (int64_t)cz * b.fstride[1];
+      if (lo > INT32_MAX || dof > INT32_MAX || dof < INT32_MIN) {
+        set_error("box too large for 32-bit per-direction offsets (Q * component stride >= 2^31)");
+        return ILBM_ERR_RANGE;
+      }
+      a.loff[q] = (int32_t)lo;
+      a.doff[q] = (int32_t)dof;
+    }
+  }
   a.macro_in = b.macro_in;
   a.force = b.force;
   a.force_prev = b.force_prev;
@@ -766,10 +843,13 @@ static int fill_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_pa
         a.bvlo[d][c] = p->bc_val_lo[d][c];
         a.bvhi[d][c] = p->bc_val_hi[d][c];
       }
-      a.flo[d] = (d < D) ? p->force_lo[d] : 0;
-      a.fhi[d] = (d < D) ? p->force_hi[d] : 0;
+      // never read force outside its allocation
+      a.flo[d] = (d < D) ? std::max(p->force_lo[d], b.lo[d] - b.ngrow_m) : 0;
+      a.fhi[d] = (d < D) ? std::min(p->force_hi[d], b.hi[d] + b.ngrow_m) : 0;
     }
     a.tau = p->tau;
+    a.om32 = float(1.0 / p->tau);
+    a.omh32 = float(1.0 - 0.5 / p->tau);
     a.self_fill = (p->ghost_mode == ILBM_GHOST_SELF);
     a.use_uniform = p->use_uniform_force;
     for (int d = 0; d < 3; ++d) a.uf[d] = p->uniform_force[d];
@@ -790,32 +870,67 @@ static int fill_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_pa
 }
 
 template <class L, int S>
-static int launch_step(ilbm_ctx *ctx, const StepArgs &a, const ilbm_level_params *p) {
-  const int nx = a.hi[0] - a.lo[0] + 1, ny = a.hi[1] - a.lo[1] + 1;
-  const int nz = (L::D == 3) ? a.hi[2] - a.lo[2] + 1 : 1;
-  if (a.self_fill) {
-    bool any_np = false;
-    for (int d = 0; d < L::D; ++d) any_np = any_np || !a.periodic[d];
-    if (any_np) {
-      int maxslab = 1;
-      for (int d = 0; d < L::D; ++d) {
-        int s = 1;
-        for (int e = 0; e < L::D; ++e)
-          if (e != d) s *= (a.dhi[e] - a.dlo[e] + 3);
-        maxslab = std::max(maxslab, s);
-      }
-      dim3 gg((maxslab + 255) / 256, 1, 2 * L::D);
-      gg.x = std::min<unsigned>(gg.x, 4096u);
-      k_ghost_fill<L, S><<<gg, 256, 0, ctx->stream>>>(a);
-      ctx->launches++;
-    }
+static void launch_ghost_push(ilbm_ctx *ctx, const StepArgs &a, cudaStream_t st) {
+  // ghost shell push: needed unless every face is a periodic self-filled one
+  bool need = !a.self_fill;
+  for (int d = 0; d < L::D; ++d) need = need || !a.periodic[d];
+  if (!need) return;
+  int maxslab = 1;
+  for (int d = 0; d < L::D; ++d) {
+    int s = 1;
+    for (int e = 0; e < L::D; ++e)
+      if (e != d) s *= (a.hi[e] - a.lo[e] + 3);
+    maxslab = std::max(maxslab, s);
   }
+  dim3 gg((maxslab + 255) / 256, 1, 2 * L::D);
+  gg.x = std::min<unsigned>(gg.x, 4096u);
+  k_ghost_push<L, S><<<gg, 256, 0, st>>>(a);
+  ctx->launches++;
+}
+
+template <class L, int S>
+static void launch_cells(ilbm_ctx *ctx, const StepArgs &a, cudaStream_t st) {
+  const int nx = a.rhi[0] - a.rlo[0] + 1, ny = a.rhi[1] - a.rlo[1] + 1;
+  const int nz = (L::D == 3) ? a.rhi[2] - a.rlo[2] + 1 : 1;
+  if (nx <= 0 || ny <= 0 || nz <= 0) return;
   const int bx = nx >= 256 ? 256 : ((nx + 31) / 32) * 32;
   dim3 grid((nx + bx - 1) / bx, ny, nz);
-  k_step<L, S><<<grid, bx, 0, ctx->stream>>>(a);
+  k_step<L, S><<<grid, bx, 0, st>>>(a);
   ctx->launches++;
+}
+
+template <class L, int S>
+static int launch_step(ilbm_ctx *ctx, const StepArgs &a, const ilbm_level_params *p) {
   (void)p;
+  launch_ghost_push<L, S>(ctx, a, ctx->stream);
+  launch_cells<L, S>(ctx, a, ctx->stream);
   cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "level step launch");
+  return ILBM_OK;
+}
+
+// Level step whose band [blo,bhi] waits for `band_ready` (recorded on another
+// stream): ghost push and every cell outside the band run first, then the band.
+template <class L, int S>
+static int launch_step_split(ilbm_ctx *ctx, const StepArgs &a, const int *blo, const int *bhi,
+                             cudaEvent_t band_ready) {
+  StepArgs outer = a;
+  outer.use_skip = 1;
+  for (int d = 0; d < 3; ++d) {
+    outer.slo[d] = blo[d];
+    outer.shi[d] = bhi[d];
+  }
+  launch_ghost_push<L, S>(ctx, a, ctx->stream);
+  launch_cells<L, S>(ctx, outer, ctx->stream);
+  cudaError_t e = cudaStreamWaitEvent(ctx->stream, band_ready, 0);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
+  StepArgs inner = a;
+  for (int d = 0; d < 3; ++d) {
+    inner.rlo[d] = blo[d];
+    inner.rhi[d] = bhi[d];
+  }
+  launch_cells<L, S>(ctx, inner, ctx->stream);
+  e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "level step launch");
   return ILBM_OK;
 }
@@ -907,11 +1022,20 @@ static int check_params(const ilbm_ctx *ctx, const ilbm_level_params *p) {
 
 // Internal entry for the IB: band macro of box `b` into EV (3 x nb) and RHO.
 int band_macro(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p, const int *blo,
-               const int *bn, double *EV, double *RHO) {
+               const int *bn, double *EV, double *RHO, cudaStream_t st) {
   StepArgs a;
   int rc = fill_args(ctx, b, p, a);
   if (rc) return rc;
-  return ILBM_DISPATCH(ctx, launch_band_macro, ctx, a, blo, bn, EV, RHO);
+  return ILBM_DISPATCH(ctx, launch_band_macro, ctx, a, blo, bn, EV, RHO, st);
+}
+
+// Level step with the band [blo,bhi] deferred until `band_ready`.
+int level_step_split(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p,
+                     const int *blo, const int *bhi, cudaEvent_t band_ready) {
+  StepArgs a;
+  int rc = fill_args(ctx, b, p, a);
+  if (rc) return rc;
+  return ILBM_DISPATCH(ctx, launch_step_split, ctx, a, blo, bhi, band_ready);
 }
 
 }  // namespace ilbm
@@ -989,6 +1113,19 @@ int ilbm_create(const ilbm_lattice *lat, int storage, int device, void *cuda_str
       return cuda_fail(e, "cudaEventCreate");
     }
   }
+  {
+    // high-priority side stream for the immersed-boundary chain, which then
+    // overlaps the collide-stream of the cells outside its band
+    int lo_pri = 0, hi_pri = 0;
+    cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri);
+    e = cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, hi_pri);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      ilbm_destroy(c);
+      return cuda_fail(e, "side stream");
+    }
+  }
   e = cudaMallocHost(&c->host_pinned, 64 * sizeof(double));
   if (e != cudaSuccess) {
     ilbm_destroy(c);
@@ -1009,6 +1146,12 @@ int ilbm_destroy(ilbm_ctx *ctx) {
   delete[] ctx->xev;
   if (ctx->scratch) cudaFree(ctx->scratch);
   if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
+  if (ctx->side) {
+    cudaStreamSynchronize(ctx->side);
+    cudaStreamDestroy(ctx->side);
+  }
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return ILBM_OK;
@@ -1083,6 +1226,11 @@ int ilbm_level_step(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const ilbm_l
   }
   int rc = check_params(ctx, p);
   if (rc) return rc;
+  for (int n = 0; n < nbox; ++n)
+    if (boxes[n].ngrow_f < 1) {
+      set_error("f arrays need at least one ghost layer (edge cells push into it as scratch)");
+      return ILBM_ERR_ARG;
+    }
   if (p->ghost_mode == ILBM_GHOST_SELF) {
     if (nbox != 1) {
       set_error("self-fill ghost mode needs exactly one box covering the domain");
@@ -1093,10 +1241,7 @@ int ilbm_level_step(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const ilbm_l
         set_error("self-fill ghost mode: the box must equal the domain");
         return ILBM_ERR_ARG;
       }
-    if (boxes[0].ngrow_f < 1) {
-      set_error("self-fill ghost mode needs ngrow_f >= 1 for the synthesised ghost layer");
-      return ILBM_ERR_ARG;
-    }
+
   } else if (p->ghost_mode != ILBM_GHOST_CALLER) {
     set_error("unknown ghost mode");
     return ILBM_ERR_ARG;
@@ -1106,6 +1251,16 @@ int ilbm_level_step(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const ilbm_l
     if ((rc = check_box(ctx, b, true))) return rc;
     if (p->ghost_mode == ILBM_GHOST_CALLER && b.ngrow_f < 1) {
       set_error("caller ghost mode needs ngrow_f >= 1");
+      return ILBM_ERR_ARG;
+    }
+    if (p->ghost_mode == ILBM_GHOST_CALLER && (b.macro_in || b.force || b.force_prev) &&
+        b.ngrow_m < 1) {
+      set_error("caller ghost mode reads macro/force ghosts: needs ngrow_m >= 1");
+      return ILBM_ERR_ARG;
+    }
+    if ((b.macro_in || b.macro_out || b.force || b.force_prev) &&
+        (b.mstride[0] <= 0 || b.mstride[1] <= 0 || b.mstride[2] <= 0)) {
+      set_error("box: macro/force strides must be positive");
       return ILBM_ERR_ARG;
     }
     if (b.f_in == b.f_out) {

@@ -249,11 +249,10 @@ class LevelSolver:
         b = self._box(self.f, self.f_next, macro_in=use_macro,
                       force=self.force_cur if ib_on else None,
                       force_prev=self.force_prev if ib_on else None)
-        if ib_on:
-            capi.check(self.L.ilbm_ib_update_forcing(self.ib, C.byref(b), C.byref(self.params),
-                                                     self.case.dt, self.time), "ib_update_forcing")
-        capi.check(self.L.ilbm_level_step(self.ctx.h, C.byref(b), 1, C.byref(self.params)),
-                   "level_step")
+        # update_forcing + collide-stream (the IB chain overlaps the cells
+        # outside its band inside the library)
+        capi.check(self.L.ilbm_advance_level(self.ctx.h, C.byref(b), C.byref(self.params),
+                                             self.ib, self.case.dt, self.time), "advance_level")
         self.f, self.f_next = self.f_next, self.f
         self.force_cur, self.force_prev = self.force_prev, self.force_cur
         self.first_step_macro = False
@@ -337,6 +336,15 @@ class LevelSolver:
         m = (C.c_double * 3)()
         capi.check(self.L.ilbm_ib_last_marker_force_sum(self.ib, m), "marker_force_sum")
         return np.array([m[0], m[1], m[2]])
+
+    def set_ivc_solver(self, solver: int):
+        """capi.IVC_AUTO / IVC_CG / IVC_DENSE (see ilbm_ib_set_ivc_solver)."""
+        capi.check(self.L.ilbm_ib_set_ivc_solver(self.ib, int(solver)), "ib_set_ivc_solver")
+
+    def cg_iterations(self) -> int:
+        it = C.c_int()
+        capi.check(self.L.ilbm_ib_solver_stats(self.ib, C.byref(it)), "ib_solver_stats")
+        return int(it.value)
 
     def markers(self):
         n = self.num_markers()

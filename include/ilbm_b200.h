@@ -107,11 +107,12 @@ typedef struct {
 /* One box of a level (one FAB of f_old/f_new/macro/forcing in AMReX terms). */
 typedef struct {
   int lo[3], hi[3]; /* valid region, inclusive, level index space */
-  int ngrow_f;      /* ghost width allocated around f_in / f_out */
+  int ngrow_f;      /* ghost width allocated around f_in / f_out (>= 1; the ghost
+                       layer of f_out is scratch written by edge cells) */
   int ngrow_m;      /* ghost width allocated around macro / force arrays */
   int64_t fstride[3]; /* f arrays: j, k, component strides (elements) */
   int64_t mstride[3]; /* macro / force arrays: j, k, component strides */
-  void *f_in;       /* f^n (storage type); ghost layer 1 filled per ghost_mode */
+  void *f_in;       /* f^n (storage type); ghost layer 1 read in caller mode only */
   void *f_out;      /* f^{n+1} on valid cells (storage type) */
   void *macro_in;   /* rho,u,v,w at step n (real type) or NULL (recomputed) */
   void *macro_out;  /* rho,u,v,w at step n+1 (real type) or NULL */
@@ -221,8 +222,37 @@ int ilbm_ib_force_region(const ilbm_ib *ib, int lo[3], int hi[3]);
  * are not touched (keep them zero). */
 int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *p,
                            double dt, double time);
+/* One whole AdvancePhiAtLevel of a level with an immersed body
+ * (Source/Core/AdvanceLBMAtLevel.cpp:20-394): update_forcing into box->force,
+ * then the level step with that force.  In self-fill mode the IB chain runs on
+ * a high-priority side stream concurrently with the collide-stream of every
+ * cell outside the IB band (those cells carry no IB force), and the band
+ * cells follow once the force is ready.  p's force region is set from the IB.
+ * ib may be NULL (plain level step). */
+int ilbm_advance_level(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
+                       ilbm_ib *ib, double dt, double time);
 /* sum over markers of F*dv from the last update_forcing (synchronises) */
 int ilbm_ib_last_marker_force_sum(ilbm_ib *ib, double out[3]);
+/* iterations of the last IVC conjugate-gradient solve (synchronises); the
+ * diagnostic counterpart of ibm.ivc_verbose (IBMarkerDF.cpp:1302-1313);
+ * 0 when the system is solved through the stored inverse */
+int ilbm_ib_solver_stats(ilbm_ib *ib, int *cg_iterations);
+/* How the implicit-velocity-correction system A F = b is solved.
+ * The reference factorises A = dv*S*S^T + reg*I once by dense LU and
+ * back-substitutes each step while the markers stay put
+ * (Source/IBM/IBMarkerDF.cpp:1015-1070, 1131, 1248-1300).  ILBM_IVC_DENSE
+ * is the device counterpart: A^-1 is formed once per body (in-place
+ * Gauss-Jordan on the GPU, n*n doubles, n <= ILBM_IVC_DENSE_MAX) and each step
+ * solves with one dense matvec.  ILBM_IVC_CG solves every step by
+ * preconditioned CG on the sparse operator (warm-started; used for moving
+ * markers and ivc_rebuild_matrix > 0).  ILBM_IVC_AUTO (the default) takes the
+ * stored inverse whenever it applies.  Selecting ILBM_IVC_DENSE where it does
+ * not apply returns ILBM_ERR_UNSUPPORTED. */
+#define ILBM_IVC_AUTO 0
+#define ILBM_IVC_CG 1
+#define ILBM_IVC_DENSE 2
+#define ILBM_IVC_DENSE_MAX 8192
+int ilbm_ib_set_ivc_solver(ilbm_ib *ib, int solver);
 /* marker positions / interpolated velocity / force: n*3 doubles each, or NULL */
 int ilbm_ib_markers(ilbm_ib *ib, double *xyz, double *uvw, double *force);
 

@@ -194,7 +194,7 @@ class CpuLevel:
         self.h = self._fn("create")(C.byref(self._case))
         if not self.h:
             raise RuntimeError(f"{backend}: create failed")
-        self.shape = tuple(spec.n_cell[d] for d in range(self.dim))[::-1]  # (k, j, i)
+        self.shape = tuple(spec.shape)  # (nz, ny, nx); nz = 1 in 2D
         self.ncell = int(np.prod(self.shape))
 
     def _fn(self, name):

@@ -137,6 +137,39 @@ def test_d3q27_duct(storage):
     gpu.close()
 
 
+@pytest.mark.parametrize("solver", [capi.IVC_CG, capi.IVC_DENSE])
+def test_ivc_solvers_sphere_3d(solver):
+    """3D sphere with more than 1024 markers: the grid-wide CG and the stored
+    inverse both against the oracle's dense LU (relative L2 <= 1e-12)."""
+    case, ib, init = cases.sphere(48, 40, 40, D=20.0, center=(16.3, 19.8, 20.1), U=0.04, Re=40.0)
+    cpu = CpuLevel(case, "oracle")
+    cpu.set_macro(*init())
+    cpu.init_equilibrium()
+    cpu.ib_create(ib)
+    cpu.step(4)
+    gpu = LevelSolver(case, "f64", ib=ib)
+    gpu.set_ivc_solver(solver)
+    gpu.set_macro(*init())
+    gpu.step(4, record_force=True)
+    assert gpu.num_markers() == cpu.num_markers() > 1024
+    assert rel_l2(gpu.get_f(), cpu.get_f()) <= 1e-12
+    assert rel_l2(gpu.get_force(), cpu.get_force()) <= 1e-11
+    np.testing.assert_allclose(gpu.marker_force_sum(), cpu.marker_force_sum(), rtol=1e-9, atol=1e-14)
+    it = gpu.cg_iterations()
+    assert (it > 0) if solver == capi.IVC_CG else (it == 0)
+    gpu.close()
+
+
+def test_ivc_dense_refused_for_moving_markers():
+    from tests.golden.golden_cases import GOLDEN_CASES as G
+    case, init, ib = G["airfoil96x64_pitching_ivc"][0]()
+    gpu = LevelSolver(case, "f64", ib=ib)
+    with pytest.raises(capi.IlbmError):
+        gpu.set_ivc_solver(capi.IVC_DENSE)
+    gpu.set_ivc_solver(capi.IVC_CG)
+    gpu.close()
+
+
 def test_momentum_exchange_matches_oracle():
     case, init = cases.taylor_green(48, U0=0.02, tau=0.7)
     cpu = CpuLevel(case, "oracle")
