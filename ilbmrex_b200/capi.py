@@ -14,6 +14,8 @@ LIB_PATH = Path(__file__).resolve().parent / "lib" / "libilbm_b200.so"
 MAXQ = 27
 
 ILBM_OK = 0
+ILBM_ERR_ARG, ILBM_ERR_CUDA, ILBM_ERR_UNSUPPORTED = -1, -2, -3
+ILBM_ERR_NOMEM, ILBM_ERR_SOLVER, ILBM_ERR_RANGE = -4, -5, -6
 STORAGE = {"f64": 0, "f32": 1, "f16": 2}
 GHOST_SELF, GHOST_CALLER = 0, 1
 IVC_AUTO, IVC_CG, IVC_DENSE = 0, 1, 2
@@ -29,7 +31,7 @@ EXPORTS = [
     "ilbm_ib_update_forcing", "ilbm_advance_level", "ilbm_ib_last_marker_force_sum",
     "ilbm_ib_solver_stats", "ilbm_ib_set_ivc_solver",
     "ilbm_ib_markers",
-    "ilbm_force_integrals", "ilbm_momentum_exchange",
+    "ilbm_force_integrals", "ilbm_force_integrals_noalloc", "ilbm_momentum_exchange",
 ]
 
 
@@ -130,6 +132,7 @@ def lib():
         "ilbm_ib_set_ivc_solver": (I, [P, I]),
         "ilbm_ib_markers": (I, [P, dp, dp, dp]),
         "ilbm_force_integrals": (I, [P, C.POINTER(Box_t), P, ip3, ip3, dp]),
+        "ilbm_force_integrals_noalloc": (I, [P, C.POINTER(Box_t), P, ip3, ip3, dp]),
         "ilbm_momentum_exchange": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P,
                                        D, D, D, D, dp, dp, I, dp]),
     }

@@ -4,6 +4,7 @@
 // (Source/IBM/IBForceEval.cpp:28-191).  Both are two-stage reductions with a
 // fixed summation order, so repeated calls return identical bits.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 
 #include "ilbm_common.cuh"
@@ -271,6 +272,125 @@ int ilbm_momentum_exchange(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "ilbm_momentum_exchange");
   for (int c = 0; c < 3; ++c) out[c] = -ctx->host_pinned[c];
+  return ILBM_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Force integral that allocates nothing
+// ---------------------------------------------------------------------------
+// ilbm_force_integrals grows the context's scratch with cudaMalloc on first
+// use.  Some hosts cannot allocate once they are running: AMReX's default
+// arena reserves most of the device memory at start-up, so a later cudaMalloc
+// by a library can fail; a serving loop that admits cases against a fixed
+// memory budget must not grow behind its back; and cudaMalloc / cudaFree can
+// synchronise the device, stalling work queued on other streams.  This
+// variant keeps its partial sums in a fixed array in the library's own
+// device image instead.
+//
+// The region is cut into ceil(cells / kNoAllocChunkCells) equal chunks, one
+// partial triple per chunk, so the summation order depends on the region
+// only.  The array holds kNoAllocChunks partials plus the 3-double result:
+// regions up to kNoAllocChunks * kNoAllocChunkCells cells (8,388,608).  Nothing in it has to start at
+// zero: every partial that k_final_sum reads is written by k_force_partial
+// earlier in the same call, and the result slot is written by k_final_sum.
+
+namespace {
+
+constexpr int kNoAllocChunks = 2048;
+constexpr int64_t kNoAllocChunkCells = 4096;
+constexpr int kNoAllocMaxDevices = 64;
+
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocChunks * 3 + 3];
+
+// device address of g_noalloc_scratch, looked up once per device
+double *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+int noalloc_scratch(int device, double **out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) {
+    set_error("ilbm_force_integrals_noalloc: device ordinal out of range");
+    return ILBM_ERR_ARG;
+  }
+  if (!g_noalloc_ptr[device]) {
+    int prev = 0;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals_noalloc: cudaGetDevice");
+    if (prev != device && (e = cudaSetDevice(device)) != cudaSuccess)
+      return cuda_fail(e, "ilbm_force_integrals_noalloc: cudaSetDevice");
+    void *ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (prev != device) cudaSetDevice(prev);
+    if (e != cudaSuccess || !ptr)
+      return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol,
+                       "ilbm_force_integrals_noalloc: cudaGetSymbolAddress");
+    g_noalloc_ptr[device] = static_cast<double *>(ptr);
+  }
+  *out = g_noalloc_ptr[device];
+  return ILBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ilbm_force_integrals_noalloc(ilbm_ctx *ctx, const ilbm_box *box, const void *force,
+                                 const int lo[3], const int hi[3], double out_sum[3]) {
+  if (!ctx || !box || !force || !out_sum) {
+    set_error("ilbm_force_integrals_noalloc: null argument");
+    return ILBM_ERR_ARG;
+  }
+  RegionArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.dim = ctx->dim;
+  for (int d = 0; d < 3; ++d) {
+    if (d >= ctx->dim) {
+      a.lo[d] = 0;
+      a.n[d] = 1;
+      a.mgl[d] = 0;
+      continue;
+    }
+    const int l = std::max(lo ? lo[d] : box->lo[d], box->lo[d]);
+    const int h = std::min(hi ? hi[d] : box->hi[d], box->hi[d]);
+    a.lo[d] = l;
+    a.n[d] = std::max(0, h - l + 1);
+    a.mgl[d] = box->lo[d] - box->ngrow_m;
+  }
+  a.ms0 = box->mstride[0];
+  a.ms1 = box->mstride[1];
+  a.ms2 = box->mstride[2];
+  const int64_t cells = (int64_t)a.n[0] * a.n[1] * a.n[2];
+  const int64_t max_cells = (int64_t)kNoAllocChunks * kNoAllocChunkCells;
+  if (cells > max_cells) {
+    char msg[200];
+    std::snprintf(msg, sizeof(msg),
+                  "ilbm_force_integrals_noalloc: region has %lld cells; the static scratch covers at "
+                  "most %lld (%d chunks of %lld cells); use ilbm_force_integrals",
+                  (long long)cells, (long long)max_cells, kNoAllocChunks,
+                  (long long)kNoAllocChunkCells);
+    set_error(msg);
+    return ILBM_ERR_RANGE;
+  }
+  double *scr = nullptr;
+  int rc = noalloc_scratch(ctx->device, &scr);
+  if (rc) return rc;
+  if (cells == 0) {
+    out_sum[0] = out_sum[1] = out_sum[2] = 0.0;
+    return ILBM_OK;
+  }
+  const int nchunks = (int)((cells + kNoAllocChunkCells - 1) / kNoAllocChunkCells);
+  if (ctx->storage == ILBM_STORAGE_F64)
+    k_force_partial<double><<<nchunks, kRedThreads, 0, ctx->stream>>>(a, static_cast<const double *>(force), scr);
+  else
+    k_force_partial<float><<<nchunks, kRedThreads, 0, ctx->stream>>>(a, static_cast<const float *>(force), scr);
+  k_final_sum<<<1, 32, 0, ctx->stream>>>(scr, nchunks, scr + kNoAllocChunks * 3);
+  ctx->launches += 2;
+  double res[3] = {0.0, 0.0, 0.0};
+  cudaMemcpyAsync(res, scr + kNoAllocChunks * 3, 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                  ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals_noalloc");
+  for (int c = 0; c < 3; ++c) out_sum[c] = res[c];
   return ILBM_OK;
 }
 

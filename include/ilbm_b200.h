@@ -260,6 +260,28 @@ int ilbm_ib_markers(ilbm_ib *ib, double *xyz, double *uvw, double *force);
 /* sum of the force array over valid cells of [lo,hi] (3 doubles, synchronous) */
 int ilbm_force_integrals(ilbm_ctx *ctx, const ilbm_box *box, const void *force,
                          const int lo[3], const int hi[3], double out_sum[3]);
+/* The same sum as ilbm_force_integrals, for callers that cannot allocate
+ * device memory while they run (no counterpart in the reference).  Hosts
+ * such as AMReX reserve most of the device memory in their own arena at
+ * start-up, serving loops admit work against a fixed memory budget, and
+ * cudaMalloc / cudaFree can synchronise the device; ilbm_force_integrals
+ * grows the context's scratch with cudaMalloc on first use, this call never
+ * allocates: its partial sums live in a fixed array inside the library.
+ *   - Limit: the clipped region may hold at most 8,388,608 cells (2048
+ *     chunks of up to 4096 cells); larger regions return ILBM_ERR_RANGE
+ *     without launching anything.
+ *   - The first call on a device does a one-time set-up (it looks up the
+ *     array's device address, which may load the library's device code on
+ *     that device); make it before any stream capture begins.
+ *   - There is one array per device: calls that overlap on a device (from
+ *     two host threads, or on two contexts of the same device) race on it
+ *     and give wrong sums.  Each call synchronises the context's stream
+ *     before returning, so calls from one host thread never overlap.
+ *   - Results may differ from ilbm_force_integrals in the last bits (the
+ *     partial sums are grouped differently); repeated calls on the same
+ *     region return identical bits. */
+int ilbm_force_integrals_noalloc(ilbm_ctx *ctx, const ilbm_box *box, const void *force,
+                                 const int lo[3], const int hi[3], double out_sum[3]);
 /* link-wise momentum exchange on f (IBForceEval); out = body force (3) */
 int ilbm_momentum_exchange(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
                            const void *f, double x0, double y0, double z0, double R,
