@@ -170,8 +170,15 @@ __device__ __forceinline__ void marker_weights(const IBArgs &a, double px, doubl
   wz = (a.dim == 3) ? delta_fn(cell_center(a.plo[2], k0 + o, a.dx[2]), pz, a.dx[2], a.kt) : 1.0;
 }
 
+__device__ __forceinline__ void target_of(const IBArgs &a, int m, const double *xyz,
+                                          const double *tgt, double &ux, double &uy,
+                                          double &uz);
+
+// rhs (optional, row stride ld): the IVC right-hand side (U_target - U)/dt of
+// the marker, written once here instead of by every block of the solve
 __global__ void __launch_bounds__(128) k_interp(IBArgs a, const double *xyz, const double *EV,
-                                                double *uvw, int *status) {
+                                                double *uvw, int *status, const double *tgt,
+                                                double *rhs, int ld) {
   const int lane = threadIdx.x & 31;
   const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (m >= a.n) return;
@@ -220,9 +227,19 @@ __global__ void __launch_bounds__(128) k_interp(IBArgs a, const double *xyz, con
       v = X::div(v, part);
       w = X::div(w, part);
     }
-    uvw[m] = X::add(uvw[m], u);
-    uvw[m + a.n] = X::add(uvw[m + a.n], v);
-    uvw[m + 2 * a.n] = X::add(uvw[m + 2 * a.n], w);
+    u = X::add(uvw[m], u);
+    v = X::add(uvw[m + a.n], v);
+    w = X::add(uvw[m + 2 * a.n], w);
+    uvw[m] = u;
+    uvw[m + a.n] = v;
+    uvw[m + 2 * a.n] = w;
+    if (rhs) {
+      double Ux, Uy, Uz;
+      target_of(a, m, xyz, tgt, Ux, Uy, Uz);
+      rhs[m] = X::div(X::sub(Ux, u), a.dt);
+      rhs[m + ld] = X::div(X::sub(Uy, v), a.dt);
+      rhs[m + 2 * ld] = X::div(X::sub(Uz, w), a.dt);
+    }
   }
 }
 
@@ -752,50 +769,45 @@ __global__ void __launch_bounds__(256) k_gj_update(double *M, int n, int ld, int
 }
 
 // F += A^-1 b with b = (U_target - U_interp)/dt (the IVC right-hand side of
-// IBMarkerDF.cpp's solve), one warp per row, b staged in shared memory
-__global__ void __launch_bounds__(256) k_ivc_dense(IBArgs a, const double *xyz, const double *tgt,
-                                                   const double *uvw, const double *Ainv, int ld,
-                                                   double *F) {
-  extern __shared__ double bsh[];  // 3 x ld
-  const int n = a.n;
-  for (int j = threadIdx.x; j < ld; j += blockDim.x) {
-    if (j < n) {
-      double Ux, Uy, Uz;
-      target_of(a, j, xyz, tgt, Ux, Uy, Uz);
-      bsh[j] = X::div(X::sub(Ux, uvw[j]), a.dt);
-      bsh[ld + j] = X::div(X::sub(Uy, uvw[j + n]), a.dt);
-      bsh[2 * ld + j] = X::div(X::sub(Uz, uvw[j + 2 * n]), a.dt);
-    } else {
-      bsh[j] = bsh[ld + j] = bsh[2 * ld + j] = 0.0;
-    }
+// IBMarkerDF.cpp's solve, written by k_interp with row stride ld, padding
+// zero).  One block per row: the 256 threads issue all their loads of the row
+// at once (coalesced, up to 8 x 16 bytes each), b comes through L1, and a
+// fixed-order block reduction gives the three components.
+constexpr int kDenseThreads = 256;
+__global__ void __launch_bounds__(kDenseThreads) k_ivc_dense(IBArgs a, const double *rhs,
+                                                             const double *Ainv, int ld, double *F) {
+  __shared__ double red[kDenseThreads / 32][3];
+  const int n = a.n, row = blockIdx.x;
+  const int half = ld >> 1;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const double2 *Ar = reinterpret_cast<const double2 *>(Ainv + (size_t)row * ld);
+  const double2 *b0 = reinterpret_cast<const double2 *>(rhs);
+  const double2 *b1 = reinterpret_cast<const double2 *>(rhs + ld);
+  const double2 *b2 = reinterpret_cast<const double2 *>(rhs + 2 * ld);
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll 8
+  for (int h = threadIdx.x; h < half; h += kDenseThreads) {
+    const double2 v = __ldcs(Ar + h);
+    const double2 x0 = __ldg(b0 + h), x1 = __ldg(b1 + h), x2 = __ldg(b2 + h);
+    s0 += v.x * x0.x + v.y * x0.y;
+    s1 += v.x * x1.x + v.y * x1.y;
+    s2 += v.x * x2.x + v.y * x2.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if (lane == 0) {
+    red[wid][0] = s0;
+    red[wid][1] = s1;
+    red[wid][2] = s2;
   }
   __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int half = ld >> 1;
-  const double2 *b0 = reinterpret_cast<const double2 *>(bsh);
-  const double2 *b1 = reinterpret_cast<const double2 *>(bsh + ld);
-  const double2 *b2 = reinterpret_cast<const double2 *>(bsh + 2 * ld);
-  for (int row = blockIdx.x * 8 + wid; row < n; row += gridDim.x * 8) {
-    const double2 *Ar = reinterpret_cast<const double2 *>(Ainv + (size_t)row * ld);
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-#pragma unroll 4
-    for (int h = lane; h < half; h += 32) {
-      const double2 v = __ldcs(Ar + h);
-      const double2 x0 = b0[h], x1 = b1[h], x2 = b2[h];
-      s0 += v.x * x0.x + v.y * x0.y;
-      s1 += v.x * x1.x + v.y * x1.y;
-      s2 += v.x * x2.x + v.y * x2.y;
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-    }
-    if (lane == 0) {
-      F[row] = X::add(F[row], s0);
-      F[row + n] = X::add(F[row + n], s1);
-      F[row + 2 * n] = X::add(F[row + 2 * n], s2);
-    }
+  if (threadIdx.x < 3) {
+    double t = 0.0;
+    for (int w = 0; w < kDenseThreads / 32; ++w) t += red[w][threadIdx.x];
+    F[row + threadIdx.x * n] = X::add(F[row + threadIdx.x * n], t);
   }
 }
 
@@ -999,8 +1011,9 @@ struct ilbm_ib {
   // fixed operator solved through its stored inverse (k_ivc_dense)
   int ivc_solver = ILBM_IVC_AUTO;
   bool dense = false, dense_ready = false;
-  int ld = 0, dense_blocks = 0;
-  double *d_Ainv = nullptr, *d_gj = nullptr;
+  int ld = 0;
+  double *d_Ainv = nullptr, *d_gj = nullptr, *d_rhs = nullptr;
+  bool fsum_deferred = false;  // marker force sum still to be launched (ib_finish)
   std::vector<void *> allocs;
 };
 
@@ -1258,24 +1271,13 @@ int enable_dense(ilbm_ib *ib) {
   const int n = ib->n;
   const int ld = ((n + 31) / 32) * 32;
   int rc;
-  if ((rc = dmalloc(ib, &ib->d_Ainv, (size_t)n * ld)) || (rc = dmalloc(ib, &ib->d_gj, 2 * (size_t)ld)))
+  if ((rc = dmalloc(ib, &ib->d_Ainv, (size_t)n * ld)) || (rc = dmalloc(ib, &ib->d_gj, 2 * (size_t)ld)) ||
+      (rc = dmalloc(ib, &ib->d_rhs, 3 * (size_t)ld)))
     return rc;
-  const int smem = 3 * ld * (int)sizeof(double);
-  // the attribute is per function and device: always the largest size, so a
-  // later body with fewer markers cannot lower the limit under this one
-  cudaError_t e = cudaFuncSetAttribute(k_ivc_dense, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       3 * ILBM_IVC_DENSE_MAX * (int)sizeof(double));
-  if (e != cudaSuccess) return cuda_fail(e, "k_ivc_dense shared memory");
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ivc_dense, 256, smem);
-  if (e != cudaSuccess || per_sm < 1) {
-    set_error("k_ivc_dense does not fit on a multiprocessor");
-    return ILBM_ERR_CUDA;
-  }
+  // the padding of the right-hand side meets zero columns of A^-1: keep it finite
+  cudaError_t e = cudaMemset(ib->d_rhs, 0, 3 * (size_t)ld * sizeof(double));
+  if (e != cudaSuccess) return cuda_fail(e, "enable_dense");
   ib->ld = ld;
-  ib->dense_blocks = std::max(1, std::min(per_sm * sms, (n + 7) / 8));
   ib->dense = true;
   ib->dense_ready = false;
   return ILBM_OK;
@@ -1439,8 +1441,11 @@ static int launch_cg(ilbm_ib *ib, const IBArgs &a_in, cudaStream_t s) {
 
 // update_forcing on stream `s` (the context stream, or its side stream when the
 // chain overlaps the collide-stream of the cells outside the band)
+// defer_sum: with one MDF iteration, leave the marker force sum (which only
+// the force evaluation reads) to ib_finish, so it can run after the exported
+// force has been handed to the level step
 static int ib_update(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *lp, double dt,
-                     double time, cudaStream_t s) {
+                     double time, cudaStream_t s, bool defer_sum) {
   if (!ib || !box || !box->force) {
     set_error("ilbm_ib_update_forcing: ib, box and box->force are required");
     return ILBM_ERR_ARG;
@@ -1466,11 +1471,16 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *
   const int nthr = 128, nblk = (ib->n + nthr - 1) / nthr;
   const int wblk = (ib->n * 32 + 127) / 128;  // one warp per marker
   const int gb = (int)std::min<int64_t>((ib->nb + 255) / 256, 1024);
-  cudaMemsetAsync(ib->d_EFT, 0, 3 * ib->nb * sizeof(double), s);
-  cudaMemsetAsync(ib->d_fsum, 0, 3 * sizeof(double), s);
-  cudaMemsetAsync(ib->d_status, 0, sizeof(int), s);
   const bool ivc = ib->p.coupling_method == 1;
   const int nloop = ivc ? 1 : std::max(ib->p.loop_ns, 1);
+  const bool use_dense = ivc && ib->dense && !ib->moving && ib->p.ivc_rebuild_matrix == 0 &&
+                         ib->ivc_solver != ILBM_IVC_CG;
+  // with one MDF iteration the total force is the iteration's force, and the
+  // velocity correction has no later reader: export straight from EFI
+  const bool single = (nloop == 1);
+  if (!single) cudaMemsetAsync(ib->d_EFT, 0, 3 * ib->nb * sizeof(double), s);
+  cudaMemsetAsync(ib->d_fsum, 0, 3 * sizeof(double), s);
+  cudaMemsetAsync(ib->d_status, 0, sizeof(int), s);
   bool any_periodic_band = false;
   for (int d = 0; d < ib->dim; ++d)
     any_periodic_band = any_periodic_band || (ib->g.periodic[d] && ib->blo[d] < 0);
@@ -1478,7 +1488,8 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *
     cudaMemsetAsync(ib->d_EFI, 0, 3 * ib->nb * sizeof(double), s);
     k_markers<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_ref, ib->d_tgt, ib->d_uvw, ib->d_F);
     if (any_periodic_band) k_fill_boundary<<<gb, 256, 0, s>>>(a, ib->d_EV);
-    k_interp<<<wblk, 128, 0, s>>>(a, ib->d_xyz, ib->d_EV, ib->d_uvw, ib->d_status);
+    k_interp<<<wblk, 128, 0, s>>>(a, ib->d_xyz, ib->d_EV, ib->d_uvw, ib->d_status, ib->d_tgt,
+                                  use_dense ? ib->d_rhs : nullptr, ib->ld);
     ctx->launches += 2 + (any_periodic_band ? 1 : 0);
     if (ivc) {
       if (!ib->csr_ready || ib->moving || ib->p.ivc_rebuild_matrix > 0) {
@@ -1490,8 +1501,6 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *
         ctx->launches += 3;
         ib->csr_ready = true;
       }
-      const bool use_dense = ib->dense && !ib->moving && ib->p.ivc_rebuild_matrix == 0 &&
-                             ib->ivc_solver != ILBM_IVC_CG;
       if (use_dense) {
         if (!ib->dense_ready) {
           // once per body: dense copy of the operator, then Gauss-Jordan in place
@@ -1509,8 +1518,7 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *
           ctx->launches += 1 + 2 * (int64_t)n;
           ib->dense_ready = true;
         }
-        k_ivc_dense<<<ib->dense_blocks, 256, 3 * ib->ld * sizeof(double), s>>>(
-            a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_Ainv, ib->ld, ib->d_F);
+        k_ivc_dense<<<ib->n, kDenseThreads, 0, s>>>(a, ib->d_rhs, ib->d_Ainv, ib->ld, ib->d_F);
       } else if ((rc = launch_cg(ib, a, s))) {
         return rc;
       }
@@ -1525,21 +1533,39 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *
       k_sum_boundary<<<gb, 256, 0, s>>>(a, ib->d_EFI);
       ctx->launches++;
     }
-    k_marker_sum<<<1, 1024, 0, s>>>(a, ib->d_F, ib->d_fsum);
-    k_correct<<<gb, 256, 0, s>>>(a, ib->d_EV, ib->d_EFI, ib->d_EFT);
-    ctx->launches += 2;
+    ib->fsum_deferred = single && defer_sum;
+    if (!ib->fsum_deferred) {
+      k_marker_sum<<<1, 1024, 0, s>>>(a, ib->d_F, ib->d_fsum);
+      ctx->launches++;
+    }
+    if (!single) {
+      k_correct<<<gb, 256, 0, s>>>(a, ib->d_EV, ib->d_EFI, ib->d_EFT);
+      ctx->launches++;
+    }
   }
+  const double *EFT = single ? ib->d_EFI : ib->d_EFT;
   const int mgl0 = box->lo[0] - box->ngrow_m, mgl1 = box->lo[1] - box->ngrow_m;
   const int mgl2 = (ib->dim == 3) ? box->lo[2] - box->ngrow_m : 0;
   if (ctx->storage == ILBM_STORAGE_F64)
-    k_export<double><<<gb, 256, 0, s>>>(a, ib->d_EFT, ib->d_RHO, static_cast<double *>(box->force),
+    k_export<double><<<gb, 256, 0, s>>>(a, EFT, ib->d_RHO, static_cast<double *>(box->force),
                                         mgl0, mgl1, mgl2, box->mstride[0], box->mstride[1], box->mstride[2]);
   else
-    k_export<float><<<gb, 256, 0, s>>>(a, ib->d_EFT, ib->d_RHO, static_cast<float *>(box->force),
+    k_export<float><<<gb, 256, 0, s>>>(a, EFT, ib->d_RHO, static_cast<float *>(box->force),
                                        mgl0, mgl1, mgl2, box->mstride[0], box->mstride[1], box->mstride[2]);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "ilbm_ib_update_forcing");
+  return ILBM_OK;
+}
+
+// the work ib_update deferred (the marker force sum), on stream s
+static int ib_finish(ilbm_ib *ib, cudaStream_t s) {
+  if (!ib->fsum_deferred) return ILBM_OK;
+  k_marker_sum<<<1, 1024, 0, s>>>(make_args(ib, 1.0, 0.0), ib->d_F, ib->d_fsum);
+  ib->ctx->launches++;
+  ib->fsum_deferred = false;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "marker force sum");
   return ILBM_OK;
 }
 
@@ -1551,7 +1577,7 @@ int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_pa
     set_error("ilbm_ib_update_forcing: null ib");
     return ILBM_ERR_ARG;
   }
-  return ib_update(ib, box, lp, dt, time, ib->ctx->stream);
+  return ib_update(ib, box, lp, dt, time, ib->ctx->stream, false);
 }
 
 int ilbm_advance_level(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
@@ -1574,7 +1600,7 @@ int ilbm_advance_level(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_para
   }
   if (p->ghost_mode != ILBM_GHOST_SELF) {
     // caller-filled ghosts may carry IB forces of neighbouring boxes: serial
-    int rc = ib_update(ib, box, &q, dt, time, ctx->stream);
+    int rc = ib_update(ib, box, &q, dt, time, ctx->stream, false);
     if (rc) return rc;
     return ilbm_level_step(ctx, box, 1, &q);
   }
@@ -1583,16 +1609,23 @@ int ilbm_advance_level(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_para
   cudaError_t e = cudaEventRecord(ctx->ev_fork, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0);
   if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level fork");
-  int rc = ib_update(ib, box, &q, dt, time, ctx->side);
-  if (rc) return rc;
-  e = cudaEventRecord(ctx->ev_join, ctx->side);
-  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level join");
-  // validate like ilbm_level_step does, then launch the split step
+  // validate like ilbm_level_step does before anything is launched
   if (box->lo[0] != p->domain_lo[0] || box->f_in == box->f_out) {
     set_error("ilbm_advance_level: self-fill needs one box equal to the domain, f_in != f_out");
     return ILBM_ERR_ARG;
   }
-  return level_step_split(ctx, *box, &q, lo, hi, ctx->ev_join);
+  int rc = ib_update(ib, box, &q, dt, time, ctx->side, true);
+  if (rc) return rc;
+  e = cudaEventRecord(ctx->ev_join, ctx->side);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level join");
+  // the marker force sum runs beside the band's collide-stream
+  if ((rc = ib_finish(ib, ctx->side))) return rc;
+  e = cudaEventRecord(ctx->ev_done, ctx->side);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level done");
+  if ((rc = level_step_split(ctx, *box, &q, lo, hi, ctx->ev_join))) return rc;
+  e = cudaStreamWaitEvent(ctx->stream, ctx->ev_done, 0);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level wait");
+  return ILBM_OK;
 }
 
 int ilbm_ib_last_marker_force_sum(ilbm_ib *ib, double out[3]) {

@@ -243,7 +243,7 @@ struct ilbm_ctx {
   // side stream (high priority) and fork/join events for the overlapped
   // immersed-boundary chain
   cudaStream_t side = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_done = nullptr;
 };
 
 // grow ctx scratch to at least n bytes (returns nullptr on failure)

@@ -26,6 +26,7 @@
 #include <string>
 
 #include "ilbm_common.cuh"
+#include "step_args.cuh"
 
 namespace ilbm {
 
@@ -37,41 +38,6 @@ int cuda_fail(cudaError_t e, const char *what) {
   return ILBM_ERR_CUDA;
 }
 
-constexpr int kMaxLevelBoxes = 64;
-
-struct StepArgs {
-  // box valid region and allocated lower corners
-  int lo[3], hi[3];
-  int fgl[3];  // allocated lower corner of f arrays
-  int mgl[3];  // allocated lower corner of macro / force arrays
-  int64_t fs0, fs1, fs2;
-  int64_t ms0, ms1, ms2;
-  const void *f_in;
-  void *f_out;
-  const void *macro_in;
-  const void *force;
-  const void *force_prev;
-  // level
-  int dlo[3], dhi[3];
-  int periodic[3];
-  int bclo[3], bchi[3];
-  double bvlo[3][4], bvhi[3][4];
-  double tau;
-  int self_fill;
-  int use_uniform;
-  double uf[3];
-  int flo[3], fhi[3];
-  float f16_scale;
-  float om32, omh32;  // 1/tau and 1 - 1/(2 tau) rounded to float, from the host
-  // per-direction element offsets: q*fs2 (load) and c_q + q*fs2 (push target)
-  int32_t loff[27], doff[27];
-  // cells handled by this launch: [rlo, rhi], minus [slo, shi] when use_skip
-  int rlo[3], rhi[3];
-  int slo[3], shi[3];
-  int use_skip;
-  int nlb;
-  int lb[kMaxLevelBoxes][6];
-};
 
 __device__ __forceinline__ int64_t fidx(const StepArgs &a, int i, int j, int k) {
   return (int64_t)(i - a.fgl[0]) + (int64_t)(j - a.fgl[1]) * a.fs0 +
@@ -282,14 +248,16 @@ __device__ __forceinline__ int ghost_rule(const StepArgs &a, const int *g, int *
 // halfway bounce-back ghosts are left to the owning cells' push.  A ghost cell
 // is owned by the slab of its lowest dimension outside the box (periodic
 // dimensions excluded in self-fill mode, whose slabs do nothing).
+// The work runs in the leading blocks of the k_step launch (it writes only
+// slots that no cell's push writes, and reads only f^n), so its strided
+// accesses overlap the main stream instead of preceding it.
 template <class L, int S>
-__global__ void __launch_bounds__(256) k_ghost_push(StepArgs a) {
+__device__ __noinline__ void ghost_push(const StepArgs &a, int64_t gid, int64_t gstride) {
   using T = typename Store<S>::T;
   using R = typename Store<S>::R;
-  const int slab = blockIdx.z;
+  for (int slab = 0; slab < 2 * L::D; ++slab) {
   const int d = slab >> 1, side = slab & 1;
-  if (d >= L::D) return;
-  if (a.self_fill && a.periodic[d]) return;
+  if (a.self_fill && a.periodic[d]) continue;
   int ext[3], base[3];
 #pragma unroll
   for (int e = 0; e < 3; ++e) {
@@ -302,8 +270,7 @@ __global__ void __launch_bounds__(256) k_ghost_push(StepArgs a) {
   const int64_t n = (int64_t)ext[0] * ext[1] * ext[2];
   const T *fin = static_cast<const T *>(a.f_in);
   T *fo = static_cast<T *>(a.f_out);
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t t = gid; t < n; t += gstride) {
     int g[3];
     g[0] = base[0] + (int)(t % ext[0]);
     g[1] = base[1] + (int)((t / ext[0]) % ext[1]);
@@ -468,6 +435,7 @@ __global__ void __launch_bounds__(256) k_ghost_push(StepArgs a) {
       Store<S>::store(fo + fidx(a, di, dj, dk) + q * a.fs2, val, sfac<L, S>(a, q));
     }
   }
+  }  // slab
 }
 
 // ---------------------------------------------------------------------------
@@ -596,17 +564,70 @@ __device__ __forceinline__ void cell_update(const StepArgs &a, int i, int j, int
 
 // Main kernel: one thread per cell of a row segment (rows on a box face run
 // the checked push as a whole; only the two x-edge cells of a row diverge).
+// the edge fix-up is needed only on faces whose outgoing populations come
+// back into the box (self-filled periodic: wrapped; user_1: reflected)
+template <class L>
+__device__ __forceinline__ bool needs_fixup(const StepArgs &a, int i, int j, int k) {
+  return (i == a.lo[0] && a.act_lo[0]) || (i == a.hi[0] && a.act_hi[0]) ||
+         (j == a.lo[1] && a.act_lo[1]) || (j == a.hi[1] && a.act_hi[1]) ||
+         (L::D == 3 && ((k == a.lo[2] && a.act_lo[2]) || (k == a.hi[2] && a.act_hi[2])));
+}
+
+// The first `ghost_slices` z-slices of the grid push the ghost shell's
+// populations (ghost_push); the rest run one cell per thread.
 template <class L, int S>
-__global__ void __launch_bounds__(256, StepOcc<L, S>::value) k_step(StepArgs a) {
+__global__ void __launch_bounds__(256, StepOcc<L, S>::value) k_step(const __grid_constant__ StepArgs a) {
+  if ((int)blockIdx.z < a.ghost_slices) {
+    const int64_t blk = blockIdx.x + (int64_t)gridDim.x * (blockIdx.y + (int64_t)gridDim.y * blockIdx.z);
+    ghost_push<L, S>(a, blk * blockDim.x + threadIdx.x,
+                     (int64_t)a.ghost_slices * gridDim.x * gridDim.y * blockDim.x);
+    return;
+  }
   const int i = a.rlo[0] + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = a.rlo[1] + blockIdx.y;
-  const int k = a.rlo[2] + blockIdx.z;
+  const int k = a.rlo[2] + (int)blockIdx.z - a.ghost_slices;
   if (i > a.rhi[0]) return;
   if (a.use_skip && in_box(a.slo, a.shi, i, j, k)) return;
-  const bool edge = (i == a.lo[0] || i == a.hi[0] || j == a.lo[1] || j == a.hi[1] ||
-                     (L::D == 3 && (k == a.lo[2] || k == a.hi[2])));
-  cell_update<L, S>(a, i, j, k, edge);
+  cell_update<L, S>(a, i, j, k, needs_fixup<L>(a, i, j, k));
 }
+
+// ---------------------------------------------------------------------------
+// Batched level step: many independent cases (each one box = its level
+// domain, self-filled ghosts) in one persistent launch.  Blocks walk a tile
+// table of row segments and ghost-push chunks over all cases; the arguments
+// of a tile's case are copied to shared memory, so the per-direction offsets
+// stay on chip and cannot alias the population stores.
+// ---------------------------------------------------------------------------
+template <class L, int S>
+__global__ void __launch_bounds__(256, StepOcc<L, S>::value)
+    k_step_batch(const StepArgs *__restrict__ args, const StepTile *__restrict__ tiles, int ntiles) {
+  __shared__ StepArgs sa;
+  __shared__ int cur;
+  if (threadIdx.x == 0) cur = -1;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const StepTile tl = tiles[t];
+    __syncthreads();  // every thread is done with the previous tile's arguments
+    if (tl.c != cur) {
+      const int *src = reinterpret_cast<const int *>(args + tl.c);
+      int *dst = reinterpret_cast<int *>(&sa);
+      for (int w = threadIdx.x; w < (int)(sizeof(StepArgs) / sizeof(int)); w += blockDim.x)
+        dst[w] = src[w];
+      __syncthreads();
+      if (threadIdx.x == 0) cur = tl.c;
+    }
+    __syncthreads();
+    if (tl.i0 < 0) {
+      ghost_push<L, S>(sa, (int64_t)(-1 - tl.i0) * blockDim.x + threadIdx.x,
+                       (int64_t)tl.j * blockDim.x);
+      continue;
+    }
+    const int i = tl.i0 + threadIdx.x;
+    if (i > sa.hi[0]) continue;
+    cell_update<L, S>(sa, i, tl.j, tl.k, needs_fixup<L>(sa, i, tl.j, tl.k));
+  }
+}
+
+
 
 // ---------------------------------------------------------------------------
 // Macro pass (calculateMacroForcing) and equilibrium initialisation
@@ -730,12 +751,10 @@ __device__ void macro_at(const StepArgs &a, int i, int j, int k, double *m4) {
 }
 
 template <class L, int S>
-__global__ void __launch_bounds__(256) k_band_macro(StepArgs a, int blo0, int blo1, int blo2,
-                                                    int bn0, int bn1, int bn2, double *EV,
-                                                    double *RHO) {
-  const int64_t nb = (int64_t)bn0 * bn1 * bn2;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb;
-       t += (int64_t)gridDim.x * blockDim.x) {
+__device__ __forceinline__ void band_macro_cell(const StepArgs &a, int blo0, int blo1, int blo2,
+                                                int bn0, int bn1, int64_t nb, int64_t t,
+                                                double *EV, double *RHO) {
+  {
     int g[3];
     g[0] = blo0 + (int)(t % bn0);
     g[1] = blo1 + (int)((t / bn0) % bn1);
@@ -766,6 +785,29 @@ __global__ void __launch_bounds__(256) k_band_macro(StepArgs a, int blo0, int bl
     EV[t + nb] = m4[2];
     EV[t + 2 * nb] = (L::D == 3) ? m4[3] : 0.0;
     RHO[t] = m4[0];
+  }
+}
+
+template <class L, int S>
+__global__ void __launch_bounds__(256) k_band_macro(StepArgs a, int blo0, int blo1, int blo2,
+                                                    int bn0, int bn1, int bn2, double *EV,
+                                                    double *RHO) {
+  const int64_t nb = (int64_t)bn0 * bn1 * bn2;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb;
+       t += (int64_t)gridDim.x * blockDim.x)
+    band_macro_cell<L, S>(a, blo0, blo1, blo2, bn0, bn1, nb, t, EV, RHO);
+}
+
+template <class L, int S>
+__global__ void __launch_bounds__(256) k_band_macro_batch(const StepArgs *args, const BandDesc *bands,
+                                                          const int64_t *off, int ncase) {
+  const int64_t total = off[ncase];
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int c = case_of(off, ncase, t);
+    const BandDesc &b = bands[c];
+    band_macro_cell<L, S>(args[c], b.blo[0], b.blo[1], b.blo[2], b.bn[0], b.bn[1], b.nb, t - off[c],
+                          b.EV, b.RHO);
   }
 }
 
@@ -854,6 +896,15 @@ static int fill_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_pa
     a.use_uniform = p->use_uniform_force;
     for (int d = 0; d < 3; ++d) a.uf[d] = p->uniform_force[d];
     a.f16_scale = (p->f16_scale > 0) ? float(p->f16_scale) : 1024.0f;
+    // faces that send outgoing populations back into the box: domain faces
+    // that are periodic with self-filled ghosts (wrapped push) or user_1
+    // (halfway bounce-back); every other face leaves them to ghost_push
+    for (int d = 0; d < D; ++d) {
+      const bool plo = a.periodic[d] ? a.self_fill : (a.bclo[d] == ILBM_BC_USER_1);
+      const bool phi = a.periodic[d] ? a.self_fill : (a.bchi[d] == ILBM_BC_USER_1);
+      a.act_lo[d] = (a.lo[d] == a.dlo[d]) && plo;
+      a.act_hi[d] = (a.hi[d] == a.dhi[d]) && phi;
+    }
     if (p->ghost_mode == ILBM_GHOST_CALLER) {
       if (p->nlevel_boxes > kMaxLevelBoxes) {
         set_error("level has more boxes than one call supports (64); split the call");
@@ -869,32 +920,39 @@ static int fill_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_pa
   return ILBM_OK;
 }
 
-template <class L, int S>
-static void launch_ghost_push(ilbm_ctx *ctx, const StepArgs &a, cudaStream_t st) {
-  // ghost shell push: needed unless every face is a periodic self-filled one
-  bool need = !a.self_fill;
-  for (int d = 0; d < L::D; ++d) need = need || !a.periodic[d];
-  if (!need) return;
-  int maxslab = 1;
+// ghost cells whose populations ghost_push delivers (0 when every face is a
+// self-filled periodic one)
+template <class L>
+static int64_t ghost_work(const StepArgs &a) {
+  int64_t n = 0;
   for (int d = 0; d < L::D; ++d) {
-    int s = 1;
+    if (a.self_fill && a.periodic[d]) continue;
+    int64_t s = 1;
     for (int e = 0; e < L::D; ++e)
       if (e != d) s *= (a.hi[e] - a.lo[e] + 3);
-    maxslab = std::max(maxslab, s);
+    n += 2 * s;
   }
-  dim3 gg((maxslab + 255) / 256, 1, 2 * L::D);
-  gg.x = std::min<unsigned>(gg.x, 4096u);
-  k_ghost_push<L, S><<<gg, 256, 0, st>>>(a);
-  ctx->launches++;
+  return n;
 }
 
+// k_step over [rlo, rhi] (minus the skip box), with the ghost shell push in
+// leading z-slices when with_ghosts is set
 template <class L, int S>
-static void launch_cells(ilbm_ctx *ctx, const StepArgs &a, cudaStream_t st) {
+static void launch_cells(ilbm_ctx *ctx, const StepArgs &a_in, cudaStream_t st, bool with_ghosts) {
+  StepArgs a = a_in;
   const int nx = a.rhi[0] - a.rlo[0] + 1, ny = a.rhi[1] - a.rlo[1] + 1;
   const int nz = (L::D == 3) ? a.rhi[2] - a.rlo[2] + 1 : 1;
   if (nx <= 0 || ny <= 0 || nz <= 0) return;
   const int bx = nx >= 256 ? 256 : ((nx + 31) / 32) * 32;
-  dim3 grid((nx + bx - 1) / bx, ny, nz);
+  const int gx = (nx + bx - 1) / bx;
+  a.ghost_slices = 0;
+  if (with_ghosts) {
+    // about one ghost cell per thread
+    const int64_t per_slice = (int64_t)gx * ny * bx;
+    const int64_t w = ghost_work<L>(a);
+    if (w > 0) a.ghost_slices = (int)std::min<int64_t>(64, (w + per_slice - 1) / per_slice);
+  }
+  dim3 grid(gx, ny, nz + a.ghost_slices);
   k_step<L, S><<<grid, bx, 0, st>>>(a);
   ctx->launches++;
 }
@@ -902,8 +960,7 @@ static void launch_cells(ilbm_ctx *ctx, const StepArgs &a, cudaStream_t st) {
 template <class L, int S>
 static int launch_step(ilbm_ctx *ctx, const StepArgs &a, const ilbm_level_params *p) {
   (void)p;
-  launch_ghost_push<L, S>(ctx, a, ctx->stream);
-  launch_cells<L, S>(ctx, a, ctx->stream);
+  launch_cells<L, S>(ctx, a, ctx->stream, true);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "level step launch");
   return ILBM_OK;
@@ -920,8 +977,7 @@ static int launch_step_split(ilbm_ctx *ctx, const StepArgs &a, const int *blo, c
     outer.slo[d] = blo[d];
     outer.shi[d] = bhi[d];
   }
-  launch_ghost_push<L, S>(ctx, a, ctx->stream);
-  launch_cells<L, S>(ctx, outer, ctx->stream);
+  launch_cells<L, S>(ctx, outer, ctx->stream, true);
   cudaError_t e = cudaStreamWaitEvent(ctx->stream, band_ready, 0);
   if (e != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
   StepArgs inner = a;
@@ -929,7 +985,7 @@ static int launch_step_split(ilbm_ctx *ctx, const StepArgs &a, const int *blo, c
     inner.rlo[d] = blo[d];
     inner.rhi[d] = bhi[d];
   }
-  launch_cells<L, S>(ctx, inner, ctx->stream);
+  launch_cells<L, S>(ctx, inner, ctx->stream, false);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "level step launch");
   return ILBM_OK;
@@ -1038,6 +1094,100 @@ int level_step_split(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *
   return ILBM_DISPATCH(ctx, launch_step_split, ctx, a, blo, bhi, band_ready);
 }
 
+// ---- internal entries of the batch engine (batch.cu) ----------------------
+
+// StepArgs of one batched case: self-filled ghosts, one box equal to the
+// domain, distinct f_in / f_out with a ghost layer, macro recovered from f
+// (macro_in is not read: the case has taken its first step already).
+int batch_case_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p,
+                    StepArgs *out) {
+  int rc = check_params(ctx, p);
+  if (rc) return rc;
+  if (p->ghost_mode != ILBM_GHOST_SELF) {
+    set_error("batched cases use self-filled ghosts (ILBM_GHOST_SELF)");
+    return ILBM_ERR_ARG;
+  }
+  for (int d = 0; d < ctx->dim; ++d)
+    if (b.lo[d] != p->domain_lo[d] || b.hi[d] != p->domain_hi[d]) {
+      set_error("batched case: the box must equal the domain");
+      return ILBM_ERR_ARG;
+    }
+  if ((rc = check_box(ctx, b, true))) return rc;
+  if (b.ngrow_f < 1 || b.f_in == b.f_out) {
+    set_error("batched case: f arrays need a ghost layer and f_in != f_out");
+    return ILBM_ERR_ARG;
+  }
+  if ((b.force || b.force_prev) && (b.mstride[0] <= 0 || b.mstride[1] <= 0 || b.mstride[2] <= 0)) {
+    set_error("batched case: force strides must be positive");
+    return ILBM_ERR_ARG;
+  }
+  ilbm_box bb = b;
+  bb.macro_in = nullptr;
+  bb.macro_out = nullptr;
+  if ((rc = fill_args(ctx, bb, p, *out))) return rc;
+  out->ghost_slices = 0;
+  return ILBM_OK;
+}
+
+// ghost-push chunks of w threads for one case (each thread takes at most one
+// ghost cell per slab); 0 when every face is a self-filled periodic one
+int batch_ghost_chunks(const ilbm_ctx *ctx, const StepArgs &a, int w) {
+  int64_t maxslab = 0;
+  for (int d = 0; d < ctx->dim; ++d) {
+    if (a.self_fill && a.periodic[d]) continue;
+    int64_t s = 1;
+    for (int e = 0; e < ctx->dim; ++e)
+      if (e != d) s *= (a.hi[e] - a.lo[e] + 3);
+    maxslab = std::max(maxslab, s);
+  }
+  return (int)((maxslab + w - 1) / w);
+}
+
+template <class L, int S>
+static int launch_step_batch(ilbm_ctx *ctx, const StepArgs *d_args, const StepTile *d_tiles,
+                             int ntiles, int w, int blocks, cudaStream_t st) {
+  k_step_batch<L, S><<<blocks, w, 0, st>>>(d_args, d_tiles, ntiles);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "batched level step launch");
+  return ILBM_OK;
+}
+
+int batch_step_launch(ilbm_ctx *ctx, const StepArgs *d_args, const StepTile *d_tiles, int ntiles,
+                      int w, int blocks, cudaStream_t st) {
+  if (ntiles <= 0) return ILBM_OK;
+  return ILBM_DISPATCH(ctx, launch_step_batch, ctx, d_args, d_tiles, ntiles, w, blocks, st);
+}
+
+template <class L, int S>
+static int launch_band_macro_batch(ilbm_ctx *ctx, const StepArgs *d_args, const BandDesc *d_bands,
+                                   const int64_t *d_off, int ncase, int64_t total, cudaStream_t st) {
+  const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
+  k_band_macro_batch<L, S><<<blocks, 256, 0, st>>>(d_args, d_bands, d_off, ncase);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "batched band macro launch");
+  return ILBM_OK;
+}
+
+int batch_band_macro_launch(ilbm_ctx *ctx, const StepArgs *d_args, const BandDesc *d_bands,
+                            const int64_t *d_off, int ncase, int64_t total, cudaStream_t st) {
+  if (total <= 0) return ILBM_OK;
+  return ILBM_DISPATCH(ctx, launch_band_macro_batch, ctx, d_args, d_bands, d_off, ncase, total, st);
+}
+
+template <class L, int S>
+static int occupancy_step_batch(const ilbm_ctx *, int w, int *per_sm) {
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, k_step_batch<L, S>, w, 0);
+  if (e != cudaSuccess) return cuda_fail(e, "batched level step occupancy");
+  return ILBM_OK;
+}
+
+// resident blocks of w threads per SM for the batched level step
+int batch_step_occupancy(const ilbm_ctx *ctx, int w, int *per_sm) {
+  return ILBM_DISPATCH(ctx, occupancy_step_batch, ctx, w, per_sm);
+}
+
 }  // namespace ilbm
 
 using namespace ilbm;
@@ -1121,6 +1271,7 @@ int ilbm_create(const ilbm_lattice *lat, int storage, int device, void *cuda_str
     e = cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, hi_pri);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming);
     if (e != cudaSuccess) {
       ilbm_destroy(c);
       return cuda_fail(e, "side stream");
@@ -1152,6 +1303,7 @@ int ilbm_destroy(ilbm_ctx *ctx) {
   }
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  if (ctx->ev_done) cudaEventDestroy(ctx->ev_done);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return ILBM_OK;

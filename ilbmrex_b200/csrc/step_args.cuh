@@ -1,0 +1,76 @@
+// Kernel arguments of one box of a level step, shared by the level-step
+// kernels (lbm_step.cu), the immersed boundary (ib.cu) and the batch engine
+// (batch.cu), which keeps one StepArgs per case and buffer parity in device
+// memory.
+#pragma once
+
+#include <stdint.h>
+
+namespace ilbm {
+
+constexpr int kMaxLevelBoxes = 64;
+
+struct StepArgs {
+  // box valid region and allocated lower corners
+  int lo[3], hi[3];
+  int fgl[3];  // allocated lower corner of f arrays
+  int mgl[3];  // allocated lower corner of macro / force arrays
+  int64_t fs0, fs1, fs2;
+  int64_t ms0, ms1, ms2;
+  const void *f_in;
+  void *f_out;
+  const void *macro_in;
+  const void *force;
+  const void *force_prev;
+  // level
+  int dlo[3], dhi[3];
+  int periodic[3];
+  int bclo[3], bchi[3];
+  double bvlo[3][4], bvhi[3][4];
+  double tau;
+  int self_fill;
+  int use_uniform;
+  double uf[3];
+  int flo[3], fhi[3];
+  float f16_scale;
+  float om32, omh32;  // 1/tau and 1 - 1/(2 tau) rounded to float, from the host
+  // per-direction element offsets: q*fs2 (load) and c_q + q*fs2 (push target)
+  int32_t loff[27], doff[27];
+  // cells handled by this launch: [rlo, rhi], minus [slo, shi] when use_skip
+  int rlo[3], rhi[3];
+  int slo[3], shi[3];
+  int use_skip;
+  int ghost_slices;          // leading z-slices of the k_step grid that run ghost_push
+  int act_lo[3], act_hi[3];  // face returns outgoing populations (wrap / reflect)
+  int nlb;
+  int lb[kMaxLevelBoxes][6];
+};
+
+// One work item of the batched level step (k_step_batch): a row segment of
+// blockDim.x cells of case c starting at (i0, j, k), or, when i0 < 0, chunk
+// (-1 - i0) of the case's ghost shell push, which has j chunks in all.
+struct StepTile {
+  int c, i0, j, k;
+};
+
+// Support band of an immersed body on a case's level (EV: 3 velocity
+// components, RHO: density, both band-sized).
+struct BandDesc {
+  int blo[3], bn[3];
+  int64_t nb;
+  double *EV, *RHO;
+};
+
+// Case owning item t of a concatenation whose case c starts at off[c]
+// (off has ncase + 1 entries, nondecreasing).
+__device__ __forceinline__ int case_of(const int64_t *off, int ncase, int64_t t) {
+  int lo = 0, hi = ncase - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (off[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+}  // namespace ilbm
