@@ -32,6 +32,9 @@ EXPORTS = [
     "ilbm_ib_solver_stats", "ilbm_ib_set_ivc_solver",
     "ilbm_ib_markers",
     "ilbm_force_integrals", "ilbm_force_integrals_noalloc", "ilbm_momentum_exchange",
+    "ilbm_batch_create", "ilbm_batch_destroy", "ilbm_batch_add", "ilbm_batch_remove",
+    "ilbm_batch_step", "ilbm_batch_case_state", "ilbm_batch_records", "ilbm_batch_set_tiles",
+    "ilbm_batch_tune", "ilbm_batch_size",
 ]
 
 
@@ -133,6 +136,17 @@ def lib():
         "ilbm_ib_markers": (I, [P, dp, dp, dp]),
         "ilbm_force_integrals": (I, [P, C.POINTER(Box_t), P, ip3, ip3, dp]),
         "ilbm_force_integrals_noalloc": (I, [P, C.POINTER(Box_t), P, ip3, ip3, dp]),
+        "ilbm_batch_create": (I, [P, I, C.POINTER(P)]),
+        "ilbm_batch_destroy": (I, [P]),
+        "ilbm_batch_add": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P, D, D, I,
+                               C.POINTER(I)]),
+        "ilbm_batch_remove": (I, [P, I]),
+        "ilbm_batch_step": (I, [P, I]),
+        "ilbm_batch_case_state": (I, [P, I, C.POINTER(I), C.POINTER(I64), dp]),
+        "ilbm_batch_records": (I, [P, I, dp, I, C.POINTER(I)]),
+        "ilbm_batch_set_tiles": (I, [P, I, I]),
+        "ilbm_batch_tune": (I, [P, I, C.POINTER(I), C.POINTER(I), C.POINTER(C.c_float)]),
+        "ilbm_batch_size": (I, [P, C.POINTER(I), C.POINTER(I64)]),
         "ilbm_momentum_exchange": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P,
                                        D, D, D, D, dp, dp, I, dp]),
     }

@@ -242,3 +242,34 @@ def pitching_airfoil(nx=512, ny=256, chord=64.0, pivot=(128.0, 128.0), U=0.05, R
                   airfoil=(chord, thickness, 0.0, math.radians(amplitude_deg), freq, 0.0,
                            0.25 * chord if quarter_chord else 0.0))
     return case, ib, uniform_init(case, 1.0, (U, 0.0, 0.0))
+
+
+def batch_mix(n_cases: int = 64, seed: int = 20261203, U: float = 0.05):
+    """The batched D2Q9 workload: n_cases independent single-level cases with
+    seeded grid sizes from 256 x 128 to 1024 x 512 (multiples of 8), each a
+    cylinder (D uniform in [16, 48] cells, Re uniform in [20, 200]) or a NACA
+    0012 pitching about its quarter chord (chord uniform in [64, 128] cells,
+    amplitude uniform in [2, 15] degrees, reduced frequency uniform in
+    [0.05, 0.3], Re 100), inflow U.  Returns (case, ib, init) triples."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(n_cases):
+        nx = int(rng.integers(256 // 8, 1024 // 8 + 1)) * 8
+        ny = int(rng.integers(128 // 8, 512 // 8 + 1)) * 8
+        if rng.random() < 0.5:
+            D = float(rng.uniform(16.0, 48.0))
+            D = min(D, 0.3 * ny)
+            Re = float(rng.uniform(20.0, 200.0))
+            cx, cy = 0.25 * nx + 0.37, 0.5 * ny - 0.21
+            case, ib, init = cylinder(nx=nx, ny=ny, D=D, center=(cx, cy), U=U, Re=Re)
+        else:
+            chord = float(rng.uniform(64.0, 128.0))
+            chord = min(chord, 0.45 * nx, 0.9 * ny)
+            amp = float(rng.uniform(2.0, 15.0))
+            k = float(rng.uniform(0.05, 0.3))
+            px, py = 0.25 * nx + 0.37, 0.5 * ny - 0.21
+            case, ib, init = pitching_airfoil(nx=nx, ny=ny, chord=chord, pivot=(px, py), U=U,
+                                              Re=100.0, amplitude_deg=amp, reduced_frequency=k)
+        case.name = f"{case.name}#{c}"
+        out.append((case, ib, init))
+    return out

@@ -1,0 +1,56 @@
+// Internal interface between the batch engine (batch.cu) and the level-step
+// (lbm_step.cu) and immersed-boundary (ib.cu) translation units.  Not part
+// of the C ABI.
+#pragma once
+
+#include <vector>
+
+#include "ilbm_common.cuh"
+#include "step_args.cuh"
+
+struct ilbm_ib;
+
+namespace ilbm {
+
+// ---- lbm_step.cu --------------------------------------------------------
+// StepArgs of one batched case (self-filled ghosts, one box = domain)
+int batch_case_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p,
+                    StepArgs *out);
+// ghost-push chunks of w threads one case needs
+int batch_ghost_chunks(const ilbm_ctx *ctx, const StepArgs &a, int w);
+// k_step_batch over a tile table (w threads per block, `blocks` persistent blocks)
+int batch_step_launch(ilbm_ctx *ctx, const StepArgs *d_args, const StepTile *d_tiles, int ntiles,
+                      int w, int blocks, cudaStream_t st);
+// band macro of every case's body
+int batch_band_macro_launch(ilbm_ctx *ctx, const StepArgs *d_args, const BandDesc *d_bands,
+                            const int64_t *d_off, int ncase, int64_t total, cudaStream_t st);
+// resident blocks of w threads per SM of k_step_batch
+int batch_step_occupancy(const ilbm_ctx *ctx, int w, int *per_sm);
+
+// ---- ib.cu ----------------------------------------------------------------
+struct IBBatch;
+
+struct IBBatchCase {
+  ilbm_ib *ib;     // NULL: a case without an immersed body
+  double dt;       // time step of the case's level
+  double time0;    // time of the case's next step
+  int kin_steps;   // steps the kinematics table covers (moving bodies)
+};
+
+// device tables for a set of cases; fails if a body has not taken its first
+// step through ilbm_advance_level / ilbm_ib_update_forcing, or uses several
+// MDF iterations
+int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int rec_slots,
+                    IBBatch **out);
+void ib_batch_destroy(IBBatch *b);
+// update_forcing of every case for one step; d_args: the step's StepArgs table
+int ib_batch_forcing(IBBatch *b, const StepArgs *d_args, cudaStream_t s);
+// per-case force record of the step and step counter + 1
+int ib_batch_record(IBBatch *b, const StepArgs *d_args, cudaStream_t s);
+// record rings (ncase x rec_slots x 8 doubles), step counters (ncase) and
+// status words (ncase) to the host; synchronises s
+int ib_batch_read(IBBatch *b, std::vector<double> &rec, std::vector<int> &steps,
+                  std::vector<int> &status, cudaStream_t s);
+int ib_batch_rec_slots(const IBBatch *b);
+
+}  // namespace ilbm

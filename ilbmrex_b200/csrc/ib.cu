@@ -123,18 +123,18 @@ __device__ __forceinline__ bool in_band(const IBArgs &a, int i, int j, int k) {
 // update_lagrangian_marker (user-defined kinematics) + zeroing, :499-609.
 // Static geometries keep the positions computed at creation; the
 // Redistribute periodic wrap is applied here.
-__global__ void k_markers(IBArgs a, double *xyz, const double *ref, double *tgt, double *uvw,
-                          double *F) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= a.n) return;
+// kc, ks, komega: cos / sin of the pitch angle and its rate at this step
+__device__ __forceinline__ void markers_one(const IBArgs &a, double kc, double ks, double komega,
+                                            int m, double *xyz, const double *ref, double *tgt,
+                                            double *uvw, double *F) {
   if (a.geometry_type == 2) {
     // IBMUserDefinedGeometry.H:144-175
     const double xr = X::sub(ref[m], a.pivot_x), yr = ref[m + a.n], zr = ref[m + 2 * a.n];
-    double x = X::sub(X::add(a.x0, X::mul(a.kc, xr)), X::mul(a.ks, yr));
-    double y = X::add(X::add(a.y0, X::mul(a.ks, xr)), X::mul(a.kc, yr));
+    double x = X::sub(X::add(a.x0, X::mul(kc, xr)), X::mul(ks, yr));
+    double y = X::add(X::add(a.y0, X::mul(ks, xr)), X::mul(kc, yr));
     double z = X::add(a.z0, zr);
-    tgt[m] = X::mul(-a.komega, X::sub(y, a.y0));
-    tgt[m + a.n] = X::mul(a.komega, X::sub(x, a.x0));
+    tgt[m] = X::mul(-komega, X::sub(y, a.y0));
+    tgt[m + a.n] = X::mul(komega, X::sub(x, a.x0));
     tgt[m + 2 * a.n] = 0.0;
     double pos[3] = {x, y, z};
     for (int d = 0; d < a.dim; ++d) {
@@ -151,6 +151,13 @@ __global__ void k_markers(IBArgs a, double *xyz, const double *ref, double *tgt,
     uvw[m + c * a.n] = 0.0;
     F[m + c * a.n] = 0.0;
   }
+}
+
+__global__ void k_markers(IBArgs a, double *xyz, const double *ref, double *tgt, double *uvw,
+                          double *F) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.n) return;
+  markers_one(a, a.kc, a.ks, a.komega, m, xyz, ref, tgt, uvw, F);
 }
 
 // velocity_interpolation_cic, :612-695; clip box = domain grown by 2.
@@ -176,12 +183,9 @@ __device__ __forceinline__ void target_of(const IBArgs &a, int m, const double *
 
 // rhs (optional, row stride ld): the IVC right-hand side (U_target - U)/dt of
 // the marker, written once here instead of by every block of the solve
-__global__ void __launch_bounds__(128) k_interp(IBArgs a, const double *xyz, const double *EV,
-                                                double *uvw, int *status, const double *tgt,
-                                                double *rhs, int ld) {
-  const int lane = threadIdx.x & 31;
-  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (m >= a.n) return;
+__device__ __forceinline__ void interp_one(const IBArgs &a, int m, int lane, const double *xyz,
+                                           const double *EV, double *uvw, int *status,
+                                           const double *tgt, double *rhs, int ld) {
   const double px = xyz[m], py = xyz[m + a.n], pz = xyz[m + 2 * a.n];
   const double d = (a.dim == 3) ? X::mul(X::mul(a.dx[0], a.dx[1]), a.dx[2]) : X::mul(a.dx[0], a.dx[1]);
   int i0, j0, k0;
@@ -243,6 +247,15 @@ __global__ void __launch_bounds__(128) k_interp(IBArgs a, const double *xyz, con
   }
 }
 
+__global__ void __launch_bounds__(128) k_interp(IBArgs a, const double *xyz, const double *EV,
+                                                double *uvw, int *status, const double *tgt,
+                                                double *rhs, int ld) {
+  const int lane = threadIdx.x & 31;
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (m >= a.n) return;
+  interp_one(a, m, lane, xyz, EV, uvw, status, tgt, rhs, ld);
+}
+
 // rigid_target_velocity / box_target_velocity, :147-182
 __device__ __forceinline__ void rigid_target(const IBArgs &a, double x, double y, double z,
                                              double &ux, double &uy, double &uz) {
@@ -278,10 +291,8 @@ __device__ __forceinline__ void target_of(const IBArgs &a, int m, const double *
 }
 
 // compute_lagrangian_force_explicit, :741-873
-__global__ void k_force_explicit(IBArgs a, const double *xyz, const double *tgt,
-                                 const double *uvw, double *F) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= a.n) return;
+__device__ __forceinline__ void force_explicit_one(const IBArgs &a, int m, const double *xyz,
+                                                   const double *tgt, const double *uvw, double *F) {
   double Ux, Uy, Uz;
   target_of(a, m, xyz, tgt, Ux, Uy, Uz);
   double denom = a.dt;
@@ -319,6 +330,13 @@ __global__ void k_force_explicit(IBArgs a, const double *xyz, const double *tgt,
   F[m] = X::add(F[m], X::div(X::mul(a.relax, X::sub(Ux, uvw[m])), denom));
   F[m + a.n] = X::add(F[m + a.n], X::div(X::mul(a.relax, X::sub(Uy, uvw[m + a.n])), denom));
   F[m + 2 * a.n] = X::add(F[m + 2 * a.n], X::div(X::mul(a.relax, X::sub(Uz, uvw[m + 2 * a.n])), denom));
+}
+
+__global__ void k_force_explicit(IBArgs a, const double *xyz, const double *tgt,
+                                 const double *uvw, double *F) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.n) return;
+  force_explicit_one(a, m, xyz, tgt, uvw, F);
 }
 
 // ---------------------------------------------------------------------------
@@ -363,12 +381,11 @@ __device__ double block_sum(double v, double *sh) {
 
 // Solves A x = b for the three force components at once.  rhs: b = (U_d-U)/dt.
 // work: 4 vectors of 3n doubles (r, z, p, Ap).  F += x on exit.
-__global__ void __launch_bounds__(1024) k_ivc_cg(IBArgs a, const double *xyz, const double *tgt,
-                                                 const double *uvw, const int *rowptr,
-                                                 const int *col, const double *val,
-                                                 const double *diag, double *X_, double *work,
-                                                 double *F, int maxit, double tol, int *status,
-                                                 int *iters) {
+__device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz, const double *tgt,
+                                             const double *uvw, const int *rowptr, const int *col,
+                                             const double *val, const double *diag, double *X_,
+                                             double *work, double *F, int maxit, double tol,
+                                             int *status, int *iters) {
   __shared__ double sh[33];
   __shared__ double s_rz[3], s_alpha[3], s_beta[3], s_bn[3], s_rn[3];
   __shared__ int s_done;
@@ -472,24 +489,37 @@ __global__ void __launch_bounds__(1024) k_ivc_cg(IBArgs a, const double *xyz, co
     for (int c = 0; c < 3; ++c) F[i + c * n] = X::add(F[i + c * n], X_[i + c * n]);
 }
 
+__global__ void __launch_bounds__(1024) k_ivc_cg(IBArgs a, const double *xyz, const double *tgt,
+                                                 const double *uvw, const int *rowptr,
+                                                 const int *col, const double *val,
+                                                 const double *diag, double *X_, double *work,
+                                                 double *F, int maxit, double tol, int *status,
+                                                 int *iters) {
+  ivc_cg_block(a, xyz, tgt, uvw, rowptr, col, val, diag, X_, work, F, maxit, tol, status, iters);
+}
+
 // ---------------------------------------------------------------------------
 // Multi-CTA CSR build (warp per row) and grid-wide CG for large marker sets
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void csr_count_row(const IBArgs &a, const double *xyz, int *rowptr, int i,
+                                              int lane) {
+  int c = 0;
+  for (int j = lane; j < a.n; j += 32) c += may_couple(a, xyz, i, j) ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if (lane == 0) rowptr[i + 1] = c;
+}
+
 __global__ void __launch_bounds__(256) k_csr_count(IBArgs a, const double *xyz, int *rowptr) {
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += nw) {
-    int c = 0;
-    for (int j = lane; j < a.n; j += 32) c += may_couple(a, xyz, i, j) ? 1 : 0;
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if (lane == 0) rowptr[i + 1] = c;
-  }
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += nw)
+    csr_count_row(a, xyz, rowptr, i, lane);
 }
 
 // exclusive scan of the row counts; if the total exceeds the capacity the
 // operator is left empty (every row pointer 0) and status bit 2 is set, so no
 // later kernel indexes past the column / value arrays
-__global__ void __launch_bounds__(1024) k_csr_scan(int n, int *rowptr, int cap, int *status) {
+__device__ __forceinline__ void csr_scan_block(int n, int *rowptr, int cap, int *status) {
   __shared__ int warp_tot[32];
   const int chunk = (n + blockDim.x - 1) / blockDim.x;
   const int s0 = threadIdx.x * chunk, s1 = min(n, s0 + chunk);
@@ -528,13 +558,14 @@ __global__ void __launch_bounds__(1024) k_csr_scan(int n, int *rowptr, int cap, 
   }
 }
 
-__global__ void __launch_bounds__(256) k_csr_fill(IBArgs a, const double *xyz, double reg,
-                                                  const int *rowptr, int *col, double *val,
-                                                  double *diag, int cap, int *status) {
-  if ((*status & 2) || rowptr[a.n] > cap) return;  // capacity exceeded (k_csr_scan)
-  const int lane = threadIdx.x & 31;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += nw) {
+__global__ void __launch_bounds__(1024) k_csr_scan(int n, int *rowptr, int cap, int *status) {
+  csr_scan_block(n, rowptr, cap, status);
+}
+
+__device__ __forceinline__ void csr_fill_row(const IBArgs &a, const double *xyz, double reg,
+                                             const int *rowptr, int *col, double *val,
+                                             double *diag, int i, int lane) {
+  {
     int p = rowptr[i];
     for (int j0 = 0; j0 < a.n; j0 += 32) {
       const int j = j0 + lane;
@@ -550,6 +581,16 @@ __global__ void __launch_bounds__(256) k_csr_fill(IBArgs a, const double *xyz, d
       p += __popc(m);
     }
   }
+}
+
+__global__ void __launch_bounds__(256) k_csr_fill(IBArgs a, const double *xyz, double reg,
+                                                  const int *rowptr, int *col, double *val,
+                                                  double *diag, int cap, int *status) {
+  if ((*status & 2) || rowptr[a.n] > cap) return;  // capacity exceeded (k_csr_scan)
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += nw)
+    csr_fill_row(a, xyz, reg, rowptr, col, val, diag, i, lane);
 }
 
 // fixed-order reduction of per-block partials (nb blocks x 8 slots); every
@@ -774,10 +815,10 @@ __global__ void __launch_bounds__(256) k_gj_update(double *M, int n, int ld, int
 // at once (coalesced, up to 8 x 16 bytes each), b comes through L1, and a
 // fixed-order block reduction gives the three components.
 constexpr int kDenseThreads = 256;
-__global__ void __launch_bounds__(kDenseThreads) k_ivc_dense(IBArgs a, const double *rhs,
-                                                             const double *Ainv, int ld, double *F) {
+__device__ __forceinline__ void dense_row(const IBArgs &a, const double *rhs, const double *Ainv,
+                                          int ld, double *F, int row) {
   __shared__ double red[kDenseThreads / 32][3];
-  const int n = a.n, row = blockIdx.x;
+  const int n = a.n;
   const int half = ld >> 1;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const double2 *Ar = reinterpret_cast<const double2 *>(Ainv + (size_t)row * ld);
@@ -811,13 +852,15 @@ __global__ void __launch_bounds__(kDenseThreads) k_ivc_dense(IBArgs a, const dou
   }
 }
 
+__global__ void __launch_bounds__(kDenseThreads) k_ivc_dense(IBArgs a, const double *rhs,
+                                                             const double *Ainv, int ld, double *F) {
+  dense_row(a, rhs, Ainv, ld, F, blockIdx.x);
+}
+
 // force_spreading_cic, :1331-1448 (dv folded in, 2D spreads x and y only);
 // one warp per marker, lanes over the stencil points, FP64 atomics
-__global__ void __launch_bounds__(128) k_spread(IBArgs a, const double *xyz, const double *F,
-                                                double *EFI, int *status) {
-  const int lane = threadIdx.x & 31;
-  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (m >= a.n) return;
+__device__ __forceinline__ void spread_one(const IBArgs &a, int m, int lane, const double *xyz,
+                                           const double *F, double *EFI, int *status) {
   const double fx = X::mul(F[m], a.dv), fy = X::mul(F[m + a.n], a.dv), fz = X::mul(F[m + 2 * a.n], a.dv);
   const double px = xyz[m], py = xyz[m + a.n], pz = xyz[m + 2 * a.n];
   const double d = (a.dim == 3) ? X::mul(X::mul(a.dx[0], a.dx[1]), a.dx[2]) : X::mul(a.dx[0], a.dx[1]);
@@ -871,17 +914,24 @@ __global__ void __launch_bounds__(128) k_spread(IBArgs a, const double *xyz, con
   }
 }
 
+__global__ void __launch_bounds__(128) k_spread(IBArgs a, const double *xyz, const double *F,
+                                                double *EFI, int *status) {
+  const int lane = threadIdx.x & 31;
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (m >= a.n) return;
+  spread_one(a, m, lane, xyz, F, EFI, status);
+}
+
 // SumBoundary (periodic): ghost-cell contributions added into their valid image
-__global__ void k_sum_boundary(IBArgs a, double *EFI) {
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.nb;
-       t += (int64_t)gridDim.x * blockDim.x) {
+__device__ __forceinline__ void sum_boundary_cell(const IBArgs &a, double *EFI, int64_t t) {
+  {
     const int i = a.blo[0] + (int)(t % a.bn[0]);
     const int j = a.blo[1] + (int)((t / a.bn[0]) % a.bn[1]);
     const int k = a.blo[2] + (int)(t / ((int64_t)a.bn[0] * a.bn[1]));
     const int g[3] = {i, j, k};
     bool inside = true;
     for (int d = 0; d < a.dim; ++d) inside = inside && g[d] >= a.dlo[d] && g[d] <= a.dhi[d];
-    if (!inside) continue;
+    if (!inside) return;
     // visit every periodic image of this cell that lies in the band
     int nsh[3] = {1, 1, 1};
     for (int d = 0; d < a.dim; ++d) nsh[d] = a.periodic[d] ? 3 : 1;
@@ -902,8 +952,14 @@ __global__ void k_sum_boundary(IBArgs a, double *EFI) {
   }
 }
 
+__global__ void k_sum_boundary(IBArgs a, double *EFI) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.nb;
+       t += (int64_t)gridDim.x * blockDim.x)
+    sum_boundary_cell(a, EFI, t);
+}
+
 // marker force sum (:1781-1819), deterministic single-CTA reduction
-__global__ void __launch_bounds__(1024) k_marker_sum(IBArgs a, const double *F, double *fsum) {
+__device__ __forceinline__ void marker_sum_block(const IBArgs &a, const double *F, double *fsum) {
   __shared__ double sh[33];
   for (int c = 0; c < 3; ++c) {
     double s = 0.0;
@@ -911,6 +967,10 @@ __global__ void __launch_bounds__(1024) k_marker_sum(IBArgs a, const double *F, 
     s = block_sum(s, sh);
     if (threadIdx.x == 0) fsum[c] = X::add(fsum[c], s);
   }
+}
+
+__global__ void __launch_bounds__(1024) k_marker_sum(IBArgs a, const double *F, double *fsum) {
+  marker_sum_block(a, F, fsum);
 }
 
 // velocity_correction (valid cells) and EulerForceTotal += EulerForceIter, :1878-1879;
@@ -932,9 +992,8 @@ __global__ void k_correct(IBArgs a, double *EV, const double *EFI, double *EFT) 
   }
 }
 
-__global__ void k_fill_boundary(IBArgs a, double *EV) {
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.nb;
-       t += (int64_t)gridDim.x * blockDim.x) {
+__device__ __forceinline__ void fill_boundary_cell(const IBArgs &a, double *EV, int64_t t) {
+  {
     int g[3];
     g[0] = a.blo[0] + (int)(t % a.bn[0]);
     g[1] = a.blo[1] + (int)((t / a.bn[0]) % a.bn[1]);
@@ -947,37 +1006,49 @@ __global__ void k_fill_boundary(IBArgs a, double *EV) {
         if (!a.periodic[d]) wrappable = false;
       }
     }
-    if (inside || !wrappable) continue;
+    if (inside || !wrappable) return;
     int w[3] = {g[0], g[1], g[2]};
     for (int d = 0; d < a.dim; ++d) {
       const int nn = a.dhi[d] - a.dlo[d] + 1;
       w[d] = a.dlo[d] + (((w[d] - a.dlo[d]) % nn) + nn) % nn;
     }
-    if (!in_band(a, w[0], w[1], w[2])) continue;
+    if (!in_band(a, w[0], w[1], w[2])) return;
     const int64_t e = bidx(a, w[0], w[1], w[2]);
     for (int c = 0; c < 3; ++c) EV[t + c * a.nb] = EV[e + c * a.nb];
   }
 }
 
+__global__ void k_fill_boundary(IBArgs a, double *EV) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.nb;
+       t += (int64_t)gridDim.x * blockDim.x)
+    fill_boundary_cell(a, EV, t);
+}
+
 // export, :1889-1911: F = dt * rho * a on valid band cells
+template <class R>
+__device__ __forceinline__ void export_cell(const IBArgs &a, const double *EFT, const double *RHO,
+                                            R *F, int mgl0, int mgl1, int mgl2, int64_t ms0,
+                                            int64_t ms1, int64_t ms2, int64_t t) {
+  const int i = a.blo[0] + (int)(t % a.bn[0]);
+  const int j = a.blo[1] + (int)((t / a.bn[0]) % a.bn[1]);
+  const int k = a.blo[2] + (int)(t / ((int64_t)a.bn[0] * a.bn[1]));
+  const int g[3] = {i, j, k};
+  bool inside = true;
+  for (int d = 0; d < a.dim; ++d) inside = inside && g[d] >= a.dlo[d] && g[d] <= a.dhi[d];
+  if (!inside) return;
+  const int64_t m = (int64_t)(i - mgl0) + (int64_t)(j - mgl1) * ms0 + (int64_t)(k - mgl2) * ms1;
+  const double dr = X::mul(a.dt, RHO[t]);
+  F[m] = R(X::mul(dr, EFT[t]));
+  F[m + ms2] = R(X::mul(dr, EFT[t + a.nb]));
+  if (a.dim == 3) F[m + 2 * ms2] = R(X::mul(dr, EFT[t + 2 * a.nb]));
+}
+
 template <class R>
 __global__ void k_export(IBArgs a, const double *EFT, const double *RHO, R *F, int mgl0,
                          int mgl1, int mgl2, int64_t ms0, int64_t ms1, int64_t ms2) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.nb;
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int i = a.blo[0] + (int)(t % a.bn[0]);
-    const int j = a.blo[1] + (int)((t / a.bn[0]) % a.bn[1]);
-    const int k = a.blo[2] + (int)(t / ((int64_t)a.bn[0] * a.bn[1]));
-    const int g[3] = {i, j, k};
-    bool inside = true;
-    for (int d = 0; d < a.dim; ++d) inside = inside && g[d] >= a.dlo[d] && g[d] <= a.dhi[d];
-    if (!inside) continue;
-    const int64_t m = (int64_t)(i - mgl0) + (int64_t)(j - mgl1) * ms0 + (int64_t)(k - mgl2) * ms1;
-    const double dr = X::mul(a.dt, RHO[t]);
-    F[m] = R(X::mul(dr, EFT[t]));
-    F[m + ms2] = R(X::mul(dr, EFT[t + a.nb]));
-    if (a.dim == 3) F[m + 2 * ms2] = R(X::mul(dr, EFT[t + 2 * a.nb]));
-  }
+       t += (int64_t)gridDim.x * blockDim.x)
+    export_cell<R>(a, EFT, RHO, F, mgl0, mgl1, mgl2, ms0, ms1, ms2, t);
 }
 
 }  // namespace
@@ -1700,3 +1771,459 @@ int ilbm_ib_markers(ilbm_ib *ib, double *xyz, double *uvw, double *force) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched update_forcing for the batch engine (batch.cu): every stage runs as
+// one launch over all cases.  The items of a stage (markers, band cells, rows
+// of a stored inverse) are concatenated over the cases and mapped back with
+// case_of; each case's IBArgs and arrays sit in a device table.  Cases have
+// taken their first step through ib_update already (operator and inverse
+// built), use one MDF iteration, and read the time-dependent pitching
+// kinematics from a per-step table filled on the host with the same
+// arithmetic as make_args.
+// ---------------------------------------------------------------------------
+#include "batch_internal.h"
+
+namespace {
+
+struct IBCase {
+  IBArgs a;
+  double *xyz;
+  const double *ref;
+  double *tgt, *uvw, *F, *EV, *EFI, *RHO, *fsum;
+  int *status, *iters;
+  int mode;     // 0 explicit, 1 stored inverse, 2 CG
+  int rebuild;  // CG operator rebuilt every step (moving markers / ivc_rebuild_matrix)
+  int moving, periodic_band;
+  int *rowptr, *col;
+  double *val, *diag, *X, *work;
+  int nnz_cap;
+  double reg, cg_tol;
+  const double *Ainv;
+  double *rhs;
+  int ld;
+  const double *kin;  // per step: komega, cos, sin, 0
+  int kin_steps;
+  double *rec;        // rec_slots x 8: Eulerian force sum (3), marker force sum (3), step, 0
+};
+
+__global__ void __launch_bounds__(256) k_b_markers(const IBCase *cs, const int64_t *off, int nc,
+                                                   const int *steps) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < off[nc];
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int c = case_of(off, nc, t);
+    const IBCase &k = cs[c];
+    const int m = (int)(t - off[c]);
+    if (m == 0) {
+      k.fsum[0] = k.fsum[1] = k.fsum[2] = 0.0;
+      k.status[0] = 0;
+    }
+    double kc = 1.0, ks = 0.0, om = 0.0;
+    if (k.moving) {
+      int s = steps[c];
+      if (s >= k.kin_steps) {
+        if (m == 0) atomicOr(k.status, 16);  // ran past its kinematics table
+        s = k.kin_steps - 1;
+      }
+      om = k.kin[4 * s];
+      kc = k.kin[4 * s + 1];
+      ks = k.kin[4 * s + 2];
+    }
+    markers_one(k.a, kc, ks, om, m, k.xyz, k.ref, k.tgt, k.uvw, k.F);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_b_band(const IBCase *cs, const int64_t *off, int nc, int op) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < off[nc];
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int c = case_of(off, nc, t);
+    const IBCase &k = cs[c];
+    const int64_t u = t - off[c];
+    if (op == 0) {
+      k.EFI[u] = 0.0;
+      k.EFI[u + k.a.nb] = 0.0;
+      k.EFI[u + 2 * k.a.nb] = 0.0;
+    } else if (op == 1) {
+      if (k.periodic_band) fill_boundary_cell(k.a, k.EV, u);
+    } else {
+      if (k.periodic_band) sum_boundary_cell(k.a, k.EFI, u);
+    }
+  }
+}
+
+// one warp per marker; stage 0 interpolation, 1 explicit force, 2 spreading,
+// 3 CSR row count, 4 CSR row fill
+__global__ void __launch_bounds__(128) k_b_marker_warp(const IBCase *cs, const int64_t *off, int nc,
+                                                       int stage) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < off[nc]; w += nw) {
+    const int c = case_of(off, nc, w);
+    const IBCase &k = cs[c];
+    const int m = (int)(w - off[c]);
+    if (stage == 0) {
+      interp_one(k.a, m, lane, k.xyz, k.EV, k.uvw, k.status, k.tgt, k.mode == 1 ? k.rhs : nullptr,
+                 k.ld);
+    } else if (stage == 1) {
+      if (k.mode == 0 && lane == 0) force_explicit_one(k.a, m, k.xyz, k.tgt, k.uvw, k.F);
+    } else if (stage == 2) {
+      spread_one(k.a, m, lane, k.xyz, k.F, k.EFI, k.status);
+    } else if (stage == 3) {
+      if (k.mode == 2 && k.rebuild) csr_count_row(k.a, k.xyz, k.rowptr, m, lane);
+    } else {
+      if (k.mode == 2 && k.rebuild && !(k.status[0] & 2) && k.rowptr[k.a.n] <= k.nnz_cap)
+        csr_fill_row(k.a, k.xyz, k.reg, k.rowptr, k.col, k.val, k.diag, m, lane);
+    }
+  }
+}
+
+// one block per CG case: the CSR scan, or the whole solve
+__global__ void __launch_bounds__(1024) k_b_cg(const IBCase *cs, const int *cg_case, int stage) {
+  const IBCase &k = cs[cg_case[blockIdx.x]];
+  if (stage == 0) {
+    if (k.rebuild) csr_scan_block(k.a.n, k.rowptr, k.nnz_cap, k.status);
+  } else {
+    ivc_cg_block(k.a, k.xyz, k.tgt, k.uvw, k.rowptr, k.col, k.val, k.diag, k.X, k.work, k.F, 500,
+                 k.cg_tol, k.status, k.iters);
+  }
+}
+
+// one block per row of every stored inverse
+__global__ void __launch_bounds__(kDenseThreads) k_b_dense(const IBCase *cs, const int *dcase,
+                                                           const int64_t *doff, int nd) {
+  const int di = case_of(doff, nd, blockIdx.x);
+  const IBCase &k = cs[dcase[di]];
+  dense_row(k.a, k.rhs, k.Ainv, k.ld, k.F, (int)(blockIdx.x - doff[di]));
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_b_export(const IBCase *cs, const int64_t *off, int nc,
+                                                  const StepArgs *args) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < off[nc];
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int c = case_of(off, nc, t);
+    const IBCase &k = cs[c];
+    const StepArgs &sa = args[c];
+    export_cell<R>(k.a, k.EFI, k.RHO, static_cast<R *>(const_cast<void *>(sa.force)), sa.mgl[0],
+                   sa.mgl[1], sa.mgl[2], sa.ms0, sa.ms1, sa.ms2, t - off[c]);
+  }
+}
+
+// one block (1024 threads) per case: marker force sum and Eulerian force sum
+// over the force region, written to the case's record ring; step counter + 1
+template <class R>
+__global__ void __launch_bounds__(1024) k_b_record(const IBCase *cs, const StepArgs *args, int *steps,
+                                                   int rec_slots) {
+  __shared__ double sh[33];
+  const int c = blockIdx.x;
+  const IBCase &k = cs[c];
+  const StepArgs &sa = args[c];
+  double fe[3] = {0.0, 0.0, 0.0};
+  if (k.a.n > 0) {
+    marker_sum_block(k.a, k.F, k.fsum);
+    const R *F = static_cast<const R *>(sa.force);
+    for (int comp = 0; comp < k.a.dim; ++comp) {
+      double s = 0.0;
+      for (int64_t t = threadIdx.x; t < k.a.nb; t += blockDim.x) {
+        const int i = k.a.blo[0] + (int)(t % k.a.bn[0]);
+        const int j = k.a.blo[1] + (int)((t / k.a.bn[0]) % k.a.bn[1]);
+        const int kk = k.a.blo[2] + (int)(t / ((int64_t)k.a.bn[0] * k.a.bn[1]));
+        const int g[3] = {i, j, kk};
+        bool inside = true;
+        for (int d = 0; d < k.a.dim; ++d) inside = inside && g[d] >= k.a.dlo[d] && g[d] <= k.a.dhi[d];
+        if (!inside) continue;
+        const int64_t m = (int64_t)(i - sa.mgl[0]) + (int64_t)(j - sa.mgl[1]) * sa.ms0 +
+                          (int64_t)(kk - sa.mgl[2]) * sa.ms1;
+        s += double(F[m + comp * sa.ms2]);
+      }
+      fe[comp] = block_sum(s, sh);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int s = steps[c];
+    double *r = k.rec + (size_t)(s % rec_slots) * 8;
+    r[0] = fe[0];
+    r[1] = fe[1];
+    r[2] = fe[2];
+    r[3] = (k.a.n > 0) ? k.fsum[0] : 0.0;
+    r[4] = (k.a.n > 0) ? k.fsum[1] : 0.0;
+    r[5] = (k.a.n > 0) ? k.fsum[2] : 0.0;
+    r[6] = double(s);
+    r[7] = 0.0;
+    steps[c] = s + 1;
+  }
+}
+
+}  // namespace
+
+namespace ilbm {
+
+struct IBBatch {
+  ilbm_ctx *ctx = nullptr;
+  int nc = 0, rec_slots = 1;
+  std::vector<void *> allocs;
+  IBCase *d_cases = nullptr;
+  BandDesc *d_bands = nullptr;
+  int64_t *d_moff = nullptr, *d_boff = nullptr, *d_doff = nullptr;
+  int64_t total_m = 0, total_b = 0, total_drows = 0;
+  int *d_dcase = nullptr, *d_cgcase = nullptr;
+  int nd = 0, ncg = 0;
+  bool any_periodic = false, any_explicit = false, any_rebuild = false;
+  int *d_steps = nullptr;
+  double *d_rec = nullptr;
+  int *d_status_copy = nullptr;
+  std::vector<int *> status_ptrs;
+};
+
+template <class T>
+static int bmalloc(IBBatch *b, T **p, size_t count) {
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc (IB batch)");
+  b->allocs.push_back(q);
+  *p = static_cast<T *>(q);
+  return ILBM_OK;
+}
+template <class T>
+static int bupload(IBBatch *b, T **p, const std::vector<T> &h) {
+  int rc = bmalloc(b, p, h.size());
+  if (rc) return rc;
+  if (!h.empty()) {
+    cudaError_t e = cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "IB batch upload");
+  }
+  return ILBM_OK;
+}
+static int grid_for(int64_t items, int threads) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((items + threads - 1) / threads, 4096));
+}
+
+void ib_batch_destroy(IBBatch *b) {
+  if (!b) return;
+  for (void *q : b->allocs) cudaFree(q);
+  delete b;
+}
+
+int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int rec_slots,
+                    IBBatch **out) {
+  *out = nullptr;
+  auto *b = new IBBatch();
+  b->ctx = ctx;
+  b->nc = (int)cases.size();
+  b->rec_slots = std::max(1, rec_slots);
+  std::vector<IBCase> hc(b->nc);
+  std::vector<BandDesc> hb(b->nc);
+  std::vector<int64_t> moff(b->nc + 1, 0), boff(b->nc + 1, 0), doff(1, 0);
+  std::vector<int> dcase, cgcase;
+  std::vector<std::vector<double>> kin(b->nc);
+  for (int c = 0; c < b->nc; ++c) {
+    IBCase &k = hc[c];
+    std::memset(&k, 0, sizeof(k));
+    BandDesc &bd = hb[c];
+    std::memset(&bd, 0, sizeof(bd));
+    ilbm_ib *ib = cases[c].ib;
+    moff[c + 1] = moff[c];
+    boff[c + 1] = boff[c];
+    b->status_ptrs.push_back(nullptr);
+    if (!ib) continue;
+    if (ib->ctx != ctx) {
+      set_error("batch: an IB object belongs to another context");
+      ib_batch_destroy(b);
+      return ILBM_ERR_ARG;
+    }
+    const bool ivc = ib->p.coupling_method == 1;
+    if (!ivc && ib->p.loop_ns > 1) {
+      set_error("batch: explicit coupling with several MDF iterations (loop_ns > 1) is not batched");
+      ib_batch_destroy(b);
+      return ILBM_ERR_UNSUPPORTED;
+    }
+    if (ivc && !ib->csr_ready) {
+      set_error("batch: a body joins after its first step (its IVC operator is not built yet)");
+      ib_batch_destroy(b);
+      return ILBM_ERR_ARG;
+    }
+    k.a = make_args(ib, cases[c].dt, cases[c].time0);
+    k.xyz = ib->d_xyz;
+    k.ref = ib->d_ref;
+    k.tgt = ib->d_tgt;
+    k.uvw = ib->d_uvw;
+    k.F = ib->d_F;
+    k.EV = ib->d_EV;
+    k.EFI = ib->d_EFI;
+    k.RHO = ib->d_RHO;
+    k.fsum = ib->d_fsum;
+    k.status = ib->d_status;
+    k.iters = ib->d_iters;
+    k.moving = ib->moving ? 1 : 0;
+    for (int d = 0; d < ib->dim; ++d)
+      k.periodic_band = k.periodic_band || (ib->g.periodic[d] && ib->blo[d] < 0);
+    const bool dense = ivc && ib->dense && ib->dense_ready && !ib->moving &&
+                       ib->p.ivc_rebuild_matrix == 0 && ib->ivc_solver != ILBM_IVC_CG;
+    k.mode = !ivc ? 0 : (dense ? 1 : 2);
+    k.rebuild = (k.mode == 2 && (ib->moving || ib->p.ivc_rebuild_matrix > 0)) ? 1 : 0;
+    k.rowptr = ib->d_rowptr;
+    k.col = ib->d_col;
+    k.val = ib->d_val;
+    k.diag = ib->d_diag;
+    k.X = ib->d_X;
+    k.work = ib->d_work;
+    k.nnz_cap = ib->nnz_cap;
+    k.reg = ib->p.ivc_diag_reg;
+    k.cg_tol = (ctx->storage == ILBM_STORAGE_F64) ? 1.0e-14 : 1.0e-10;
+    k.Ainv = ib->d_Ainv;
+    k.rhs = ib->d_rhs;
+    k.ld = ib->ld;
+    if (ib->moving) {
+      // IBMUserDefinedGeometry.H:151-160 with the time accumulated step by
+      // step as the caller does (time += dt), host trigonometry as make_args
+      const int ns = std::max(1, cases[c].kin_steps);
+      kin[c].assign(4 * (size_t)ns, 0.0);
+      double t = cases[c].time0;
+      const double twopi = 2.0 * kPi;
+      for (int s = 0; s < ns; ++s) {
+        const double phase = twopi * ib->p.pitch_frequency * t + ib->p.pitch_phase;
+        const double angle = ib->p.pitch_mean + ib->p.pitch_amplitude * std::sin(phase);
+        kin[c][4 * s] = twopi * ib->p.pitch_frequency * ib->p.pitch_amplitude * std::cos(phase);
+        kin[c][4 * s + 1] = std::cos(angle);
+        kin[c][4 * s + 2] = std::sin(angle);
+        t += cases[c].dt;
+      }
+      k.kin_steps = ns;
+    }
+    moff[c + 1] = moff[c] + ib->n;
+    boff[c + 1] = boff[c] + ib->nb;
+    for (int d = 0; d < 3; ++d) {
+      bd.blo[d] = ib->blo[d];
+      bd.bn[d] = ib->bn[d];
+    }
+    bd.nb = ib->nb;
+    bd.EV = ib->d_EV;
+    bd.RHO = ib->d_RHO;
+    if (k.mode == 1) {
+      dcase.push_back(c);
+      doff.push_back(doff.back() + ib->n);
+    }
+    if (k.mode == 2) cgcase.push_back(c);
+    b->any_periodic = b->any_periodic || k.periodic_band;
+    b->any_explicit = b->any_explicit || k.mode == 0;
+    b->any_rebuild = b->any_rebuild || k.rebuild;
+    b->status_ptrs.back() = ib->d_status;
+  }
+  int rc;
+  for (int c = 0; c < b->nc; ++c) {
+    if (kin[c].empty()) continue;
+    double *dk = nullptr;
+    if ((rc = bupload(b, &dk, kin[c]))) { ib_batch_destroy(b); return rc; }
+    hc[c].kin = dk;
+  }
+  double *rec = nullptr;
+  if ((rc = bmalloc(b, &rec, (size_t)b->nc * b->rec_slots * 8)) || (rc = bmalloc(b, &b->d_steps, b->nc))) {
+    ib_batch_destroy(b);
+    return rc;
+  }
+  cudaMemset(rec, 0, (size_t)b->nc * b->rec_slots * 8 * sizeof(double));
+  cudaMemset(b->d_steps, 0, b->nc * sizeof(int));
+  b->d_rec = rec;
+  for (int c = 0; c < b->nc; ++c) hc[c].rec = rec + (size_t)c * b->rec_slots * 8;
+  b->total_m = moff.back();
+  b->total_b = boff.back();
+  b->nd = (int)dcase.size();
+  b->total_drows = doff.back();
+  b->ncg = (int)cgcase.size();
+  if ((rc = bupload(b, &b->d_cases, hc)) || (rc = bupload(b, &b->d_bands, hb)) ||
+      (rc = bupload(b, &b->d_moff, moff)) || (rc = bupload(b, &b->d_boff, boff)) ||
+      (rc = bupload(b, &b->d_doff, doff)) || (rc = bupload(b, &b->d_dcase, dcase)) ||
+      (rc = bupload(b, &b->d_cgcase, cgcase))) {
+    ib_batch_destroy(b);
+    return rc;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    ib_batch_destroy(b);
+    return cuda_fail(e, "ib_batch_create");
+  }
+  *out = b;
+  return ILBM_OK;
+}
+
+int ib_batch_forcing(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
+  ilbm_ctx *ctx = b->ctx;
+  if (b->total_m == 0) return ILBM_OK;
+  int rc = batch_band_macro_launch(ctx, d_args, b->d_bands, b->d_boff, b->nc, b->total_b, s);
+  if (rc) return rc;
+  const int gb = grid_for(b->total_b, 256), gm = grid_for(b->total_m, 256);
+  const int gw = grid_for(b->total_m * 32, 128);
+  k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 0);
+  k_b_markers<<<gm, 256, 0, s>>>(b->d_cases, b->d_moff, b->nc, b->d_steps);
+  ctx->launches += 2;
+  if (b->any_periodic) {
+    k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 1);
+    ctx->launches++;
+  }
+  k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 0);
+  ctx->launches++;
+  if (b->any_rebuild) {
+    k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 3);
+    k_b_cg<<<b->ncg, 1024, 0, s>>>(b->d_cases, b->d_cgcase, 0);
+    k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 4);
+    ctx->launches += 3;
+  }
+  if (b->nd > 0) {
+    k_b_dense<<<(unsigned)b->total_drows, kDenseThreads, 0, s>>>(b->d_cases, b->d_dcase, b->d_doff, b->nd);
+    ctx->launches++;
+  }
+  if (b->ncg > 0) {
+    k_b_cg<<<b->ncg, 1024, 0, s>>>(b->d_cases, b->d_cgcase, 1);
+    ctx->launches++;
+  }
+  if (b->any_explicit) {
+    k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 1);
+    ctx->launches++;
+  }
+  k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 2);
+  ctx->launches++;
+  if (b->any_periodic) {
+    k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 2);
+    ctx->launches++;
+  }
+  if (ctx->storage == ILBM_STORAGE_F64)
+    k_b_export<double><<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, d_args);
+  else
+    k_b_export<float><<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, d_args);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "batched update_forcing");
+  return ILBM_OK;
+}
+
+int ib_batch_record(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
+  if (b->nc == 0) return ILBM_OK;
+  if (b->ctx->storage == ILBM_STORAGE_F64)
+    k_b_record<double><<<b->nc, 1024, 0, s>>>(b->d_cases, d_args, b->d_steps, b->rec_slots);
+  else
+    k_b_record<float><<<b->nc, 1024, 0, s>>>(b->d_cases, d_args, b->d_steps, b->rec_slots);
+  b->ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "batched force record");
+  return ILBM_OK;
+}
+
+int ib_batch_read(IBBatch *b, std::vector<double> &rec, std::vector<int> &steps,
+                  std::vector<int> &status, cudaStream_t s) {
+  rec.assign((size_t)b->nc * b->rec_slots * 8, 0.0);
+  steps.assign(b->nc, 0);
+  status.assign(b->nc, 0);
+  cudaMemcpyAsync(rec.data(), b->d_rec, rec.size() * sizeof(double), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(steps.data(), b->d_steps, steps.size() * sizeof(int), cudaMemcpyDeviceToHost, s);
+  for (int c = 0; c < b->nc; ++c)
+    if (b->status_ptrs[c])
+      cudaMemcpyAsync(&status[c], b->status_ptrs[c], sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "batch record read-back");
+  return ILBM_OK;
+}
+
+int ib_batch_rec_slots(const IBBatch *b) { return b->rec_slots; }
+
+}  // namespace ilbm

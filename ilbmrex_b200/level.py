@@ -143,6 +143,7 @@ class LevelSolver:
         self.case = case
         self.storage = storage
         self.dev = torch.device("cuda", device)
+        self._own_ctx = ctx is None
         self.ctx = ctx or Context(case.lattice, storage, device)
         self.L = self.ctx.L
         self.q = case.lattice.q
@@ -267,18 +268,27 @@ class LevelSolver:
 
     # ---- force evaluation (ComputeIBForce, AmrCoreLBM.cpp:456-631) --------
     def compute_ib_force(self):
-        case, ib = self.case, self.ib_case
         lo, hi = self.force_region
         b = self._box(self.f, None)
         s = (C.c_double * 3)()
         capi.check(self.L.ilbm_force_integrals(self.ctx.h, C.byref(b), self.force_prev.data_ptr(),
                                                capi.ivec3(lo), capi.ivec3(hi), s), "force_integrals")
-        Fs = np.array([s[0], s[1], s[2] if self.dim == 3 else 0.0])
-        dV = case.dx ** self.dim
-        Feul = -(Fs * dV) / case.dt
         m = (C.c_double * 3)()
         capi.check(self.L.ilbm_ib_last_marker_force_sum(self.ib, m), "marker_force_sum")
-        Fm = -np.array([m[0], m[1], m[2]])
+        self.rec = self.force_record(np.array([s[0], s[1], s[2]]), np.array([m[0], m[1], m[2]]))
+        return self.rec
+
+    def force_record(self, eul_sum, marker_sum):
+        """One line of the force record from the Eulerian force sum over the IB
+        force region and the marker force sum of a step (ComputeIBForce,
+        AmrCoreLBM.cpp:489-631): body force, time-centred with the previous
+        step's, and Cd / Cl.  Layout: Ftc(3), Cd, Cl, Cz, Fb(3), Feul(3),
+        Fmarker(3), Fme(3)."""
+        case, ib = self.case, self.ib_case
+        Fs = np.array([eul_sum[0], eul_sum[1], eul_sum[2] if self.dim == 3 else 0.0])
+        dV = case.dx ** self.dim
+        Feul = -(Fs * dV) / case.dt
+        Fm = -np.asarray(marker_sum, dtype=np.float64)
         Fme = Feul.copy()
         Fb = {0: Fme, 1: Feul, 2: Fm}.get(ib.force_eval_method, Feul)
         Ftc = 0.5 * (self.prev_body + Fb) if self.have_prev_body else Fb.copy()
@@ -292,7 +302,6 @@ class LevelSolver:
             rec[3], rec[4] = Ftc[0] / denom, Ftc[1] / denom
             if self.dim == 3:
                 rec[5] = Ftc[2] / denom
-        self.rec = rec
         return rec
 
     # ---- read-back ---------------------------------------------------------
@@ -368,8 +377,9 @@ class LevelSolver:
         if self.ib is not None:
             self.L.ilbm_ib_destroy(self.ib)
             self.ib = None
-        if self.ctx is not None:
+        if self.ctx is not None and self._own_ctx:
             self.ctx.close()
+        self.ctx = None
 
     def __del__(self):
         try:

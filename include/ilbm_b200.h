@@ -288,6 +288,48 @@ int ilbm_momentum_exchange(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_
                            const double prob_lo[3], const double dx[3], int one_sided,
                            double out[3]);
 
+/* ---- batch engine (no counterpart in the reference) ---------------------
+ * Many independent single-level cases of the context's lattice and storage
+ * form, advanced together: per step one launch per immersed-boundary stage
+ * for all cases and one persistent collide-stream kernel over a tile table of
+ * every case's cells; two consecutive steps are replayed as a CUDA graph.
+ * A case is one box equal to its level domain with self-filled ghosts
+ * (ILBM_GHOST_SELF).  It joins after its first step has been taken through
+ * ilbm_advance_level (which reads the stored macro fields and builds the IVC
+ * operator); from then on its state lives in the buffers of `box`, whose
+ * f_in/f_out and force/force_prev swap every step.  Bodies use one MDF
+ * iteration.  Adding, removing or re-tiling settles the batch (synchronises
+ * and rebuilds its tables at the next step). */
+typedef struct ilbm_batch ilbm_batch;
+/* rec_slots: per-case force records kept on the device between read-backs
+ * (0 selects 256) */
+int ilbm_batch_create(ilbm_ctx *ctx, int rec_slots, ilbm_batch **out);
+int ilbm_batch_destroy(ilbm_batch *b);
+/* time: time of the case's next step; max_steps: steps the case may take in
+ * the batch (sizes the pitching-kinematics table) */
+int ilbm_batch_add(ilbm_batch *b, const ilbm_box *box, const ilbm_level_params *p, ilbm_ib *ib,
+                   double dt, double time, int max_steps, int *case_id);
+int ilbm_batch_remove(ilbm_batch *b, int case_id);
+/* advances every case by nsteps (asynchronous, except for record read-backs
+ * every rec_slots steps) */
+int ilbm_batch_step(ilbm_batch *b, int nsteps);
+/* parity 0: box.f_in (and box.force for F^{n-1}) hold the current state,
+ * 1: box.f_out (box.force_prev); synchronises */
+int ilbm_batch_case_state(ilbm_batch *b, int case_id, int *parity, int64_t *steps_done,
+                          double *time);
+/* the case's per-step force records, oldest first, 6 doubles each: Eulerian
+ * force sum over the IB force region (3) and marker force sum (3); with out
+ * NULL, *nrec = number available.  Synchronises. */
+int ilbm_batch_records(ilbm_batch *b, int case_id, double *out, int max_rec, int *nrec);
+/* tile width (threads per block: 64, 128, 256) and resident blocks per SM
+ * (0: as many as fit) of the batched collide-stream */
+int ilbm_batch_set_tiles(ilbm_batch *b, int tile_w, int ctas_per_sm);
+/* times every tile width and block count on the batch itself (advancing every
+ * case by the trial steps of each candidate) and keeps the fastest */
+int ilbm_batch_tune(ilbm_batch *b, int trial_steps, int *tile_w, int *ctas_per_sm,
+                    float *ms_per_step);
+int ilbm_batch_size(ilbm_batch *b, int *ncase, int64_t *cells);
+
 #ifdef __cplusplus
 }
 #endif
