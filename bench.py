@@ -180,6 +180,108 @@ def workload_config(args):
             "l2_policy": "working set 637 MB > 126 MB L2 (no flush needed)"}
 
 
+def run_batched(args, world, device):
+    """Batched D2Q9 FP32 workload (64 seeded cylinder / pitching-airfoil cases)
+    through the batch engine, against the same cases run one after another
+    through the plain single-case call (ilbm_advance_level)."""
+    import torch
+    from ilbmrex_b200 import cases
+    from ilbmrex_b200.batch import Batch
+    from ilbmrex_b200.lattice import D2Q9
+    from ilbmrex_b200.level import LevelSolver
+    mix = cases.batch_mix(args.batch_cases)
+    cells = sum(c.cells for c, _, _ in mix)
+    K = args.batch_steps
+    B = Batch(D2Q9, "f32", device=device.index or 0, rec_slots=512)
+    for c, ib, init in mix:
+        B.add(B.solver(c, ib, init), max_steps=K + 200)
+    tile_w, cps, _ = B.tune(trial_steps=4)
+    B.step(4)
+    B.ctx.sync()
+    barrier(world)
+    launches0 = B.ctx.launches()
+    B.ctx.record(4)
+    B.step(K)
+    B.ctx.record(5)
+    B.ctx.sync()
+    launches = B.ctx.launches() - launches0
+    t_b = allreduce_max(B.ctx.elapsed_ms(4, 5), world, device)
+    batched = world * cells * K / (t_b * 1e-3) / 1e6
+    B.close()
+    # plain: case by case through the single-case call
+    Kp = args.batch_plain_steps
+    t_plain = 0.0
+    for c, ib, init in (mix if Kp > 0 else []):
+        S = LevelSolver(c, "f32", ib=ib, device=device.index or 0)
+        S.set_macro(*init())
+        S.step(3)
+        S.ctx.sync()
+        S.ctx.record(6)
+        S.step(Kp)
+        S.ctx.record(7)
+        S.ctx.sync()
+        t_plain += S.ctx.elapsed_ms(6, 7) / Kp
+        S.close()
+        torch.cuda.empty_cache()
+    t_plain = allreduce_max(t_plain, world, device)
+    plain = world * cells / (t_plain * 1e-3) / 1e6 if Kp > 0 else None
+    return {"metric": "batched MLUPS (64 D2Q9 FP32 IB cases)", "value": round(batched, 2),
+            "unit": "MLUPS", "plain_case_by_case": round(plain, 2) if plain else None,
+            "speedup_vs_plain": round(batched / plain, 2) if plain else None,
+            "cases": len(mix), "cells": cells,
+            "steps": K, "plain_steps_per_case": Kp, "ms_per_step": round(t_b / K, 4),
+            "tile_w": tile_w, "ctas_per_sm": cps, "gpu_launches": int(launches),
+            "workload": "seeded mix: grids 256x128..1024x512, cylinders D 16-48 Re 20-200, "
+                        "NACA0012 pitching (chord 64-128, 2-15 deg, k 0.05-0.3), FP32 storage; "
+                        "each case steps through its own IB (stored IVC inverse or CG)"}
+
+
+def run_served(args, world, device):
+    """Served mixed workload: Poisson arrivals (seeded) of D2Q9 cylinder /
+    airfoil, D3Q19 duct and D3Q19 sphere requests through the continuous-
+    batching server, against the same requests served one at a time through
+    the plain single-case call (FIFO, same arrivals)."""
+    from ilbmrex_b200.serve import Server, make_request, poisson_arrivals, run_alone
+    rng = np.random.default_rng(20261203)
+    n = args.serve_requests
+    kinds = rng.choice(["cylinder", "duct", "sphere"], p=[0.5, 0.25, 0.25], size=n)
+    reqs = [make_request(i, str(k), rng, int(rng.integers(args.serve_min_steps, args.serve_max_steps + 1)),
+                         scale=args.serve_scale) for i, k in enumerate(kinds)]
+    arr = poisson_arrivals(n, args.serve_rate, rng)
+    for r, t in zip(reqs, arr):
+        r.arrival = float(t)
+    lups = sum(r.case.cells * r.steps for r in reqs)
+    srv = Server("f32", device=device.index or 0, chunk=args.serve_chunk)
+    stats = srv.run(reqs)
+    srv.close()
+    # plain: one request at a time through the single-case call
+    service = []
+    for r in reqs:
+        t0 = time.perf_counter()
+        run_alone(r, "f32", device=device.index or 0)
+        service.append(time.perf_counter() - t0)
+    done, lat = 0.0, []
+    for r, sv in zip(reqs, service):
+        done = max(done, r.arrival) + sv
+        lat.append(done - r.arrival)
+    plain_mlups = lups / sum(service) / 1e6
+    sizes = [r.case.cells for r in reqs]
+    return {"metric": "served MLUPS, mixed D2Q9/D3Q19 FP32 requests", "value": round(stats["mlups"], 2),
+            "unit": "MLUPS", "p50_latency_s": round(stats["p50_latency_s"], 4),
+            "p99_latency_s": round(stats["p99_latency_s"], 4),
+            "plain_mlups": round(plain_mlups, 2),
+            "plain_p50_latency_s": round(float(np.percentile(lat, 50)), 4),
+            "plain_p99_latency_s": round(float(np.percentile(lat, 99)), 4),
+            "speedup_vs_plain": round(stats["mlups"] / plain_mlups, 2),
+            "requests": n, "arrival_rate_per_s": args.serve_rate, "makespan_s": round(stats["makespan_s"], 3),
+            "cells_min_max": [int(min(sizes)), int(max(sizes))],
+            "steps_min_max": [args.serve_min_steps, args.serve_max_steps],
+            "workload": f"seeded Poisson arrivals; 50% D2Q9 cylinder/airfoil, 25% D3Q19 duct N x N x 4N, "
+                        f"25% D3Q19 sphere; grid edges scaled by {args.serve_scale} and step counts "
+                        f"{args.serve_min_steps}-{args.serve_max_steps} (the served configuration's "
+                        f"1e5-3e7 cells x 1000-20000 steps shrunk to a bench-sized run)"}
+
+
 def run_b200(args):
     import torch
     world, rank, local = dist_setup()
@@ -187,6 +289,12 @@ def run_b200(args):
     device = torch.device("cuda", local)
     from ilbmrex_b200 import capi, cases
     from ilbmrex_b200.level import LevelSolver
+
+    if args.only_batched:  # profiling aid: the batched workload alone
+        out = run_batched(args, world, device)
+        if rank == 0:
+            print(json.dumps(out), flush=True)
+        return
 
     w = WORKLOAD
     case, ib, init = cases.sphere(w["nx"], w["ny"], w["nz"], D=w["D"], center=w["center"],
@@ -293,6 +401,13 @@ def run_b200(args):
             cpu_base = {"value": None, "unit": UNIT, "cores": 0, "kind": "port",
                         "sample": f"unavailable: {e}"}
 
+    batched = None
+    if not args.no_batched:
+        batched = run_batched(args, world, device)
+    served = None
+    if not args.no_served:
+        served = run_served(args, world, device)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
@@ -314,6 +429,8 @@ def run_b200(args):
             "ib_markers": S.num_markers(),
             "ivc_cg_iterations": S.cg_iterations(),
             "first_step_ms_incl_ivc_setup": round(first_step_ms, 2),
+            "batched": batched,
+            "served": served,
         }
         print(json.dumps(line), flush=True)
     S.close()
@@ -330,6 +447,19 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f64", "f32", "f16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched workload")
+    ap.add_argument("--no-served", action="store_true", help="skip the served workload")
+    ap.add_argument("--serve-requests", type=int, default=24)
+    ap.add_argument("--serve-rate", type=float, default=40.0, help="arrivals per second")
+    ap.add_argument("--serve-scale", type=float, default=0.5)
+    ap.add_argument("--serve-min-steps", type=int, default=300)
+    ap.add_argument("--serve-max-steps", type=int, default=1500)
+    ap.add_argument("--serve-chunk", type=int, default=50)
+    ap.add_argument("--only-batched", action="store_true",
+                    help="run only the batched workload and print its result (profiling aid)")
+    ap.add_argument("--batch-cases", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=40)
+    ap.add_argument("--batch-plain-steps", type=int, default=8)
     ap.add_argument("--serial", action="store_true",
                     help="run the IB chain and the level step one after the other (no overlap)")
     args = ap.parse_args()

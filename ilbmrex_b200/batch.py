@@ -98,7 +98,8 @@ class Batch:
 
     def sync(self, cid: int) -> LevelSolver:
         """Brings the solver up to date with the case (buffer roles, time,
-        step count, force record of the last step)."""
+        step count, force record of the last step; every step's record is
+        appended to ``solver.rec_history`` when the solver has that list)."""
         s = self.members[cid]
         par, steps, t = C.c_int(), C.c_int64(), C.c_double()
         capi.check(self.L.ilbm_batch_case_state(self.h, int(cid), C.byref(par), C.byref(steps),
@@ -106,8 +107,11 @@ class Batch:
         new = steps.value - self._taken[cid]
         if new > 0:
             if s.ib is not None:
+                hist = getattr(s, "rec_history", None)
                 for r in self.records(cid)[self._taken[cid]:steps.value]:
                     s.rec = s.force_record(r[0:3], r[3:6])
+                    if hist is not None:
+                        hist.append(s.rec.copy())
             s.istep += new
             self._taken[cid] = steps.value
         # parity 0: the state is in the buffers as added; 1: roles swapped

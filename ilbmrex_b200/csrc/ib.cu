@@ -381,26 +381,44 @@ __device__ double block_sum(double v, double *sh) {
 
 // Solves A x = b for the three force components at once.  rhs: b = (U_d-U)/dt.
 // work: 4 vectors of 3n doubles (r, z, p, Ap).  F += x on exit.
+// warm: start from the previous solution in X_ (the force changes little
+// from one step to the next), else from zero
 __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz, const double *tgt,
                                              const double *uvw, const int *rowptr, const int *col,
                                              const double *val, const double *diag, double *X_,
                                              double *work, double *F, int maxit, double tol,
-                                             int *status, int *iters) {
+                                             int *status, int *iters, int warm) {
   __shared__ double sh[33];
   __shared__ double s_rz[3], s_alpha[3], s_beta[3], s_bn[3], s_rn[3];
   __shared__ int s_done;
   const int n = a.n;
   double *r = work, *z = work + 3 * n, *p = work + 6 * n, *Ap = work + 9 * n;
-  // b, x = 0, r = b, z = r / diag, p = z
+  // b (kept in Ap until the residual is formed), x0 = 0 or the previous x
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double Ux, Uy, Uz;
     target_of(a, i, xyz, tgt, Ux, Uy, Uz);
     const double U[3] = {Ux, Uy, Uz};
     for (int c = 0; c < 3; ++c) {
-      const double b = X::div(X::sub(U[c], uvw[i + c * n]), a.dt);
-      r[i + c * n] = b;
-      X_[i + c * n] = 0.0;
-      const double zz = b / diag[i];
+      Ap[i + c * n] = X::div(X::sub(U[c], uvw[i + c * n]), a.dt);
+      if (!warm) X_[i + c * n] = 0.0;
+    }
+  }
+  __syncthreads();
+  // r = b - A x0, z = r / diag, p = z
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double ax[3] = {0.0, 0.0, 0.0};
+    if (warm)
+      for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
+        const double v = val[e];
+        const int j = col[e];
+        ax[0] += v * X_[j];
+        ax[1] += v * X_[j + n];
+        ax[2] += v * X_[j + 2 * n];
+      }
+    for (int c = 0; c < 3; ++c) {
+      const double rr = Ap[i + c * n] - ax[c];
+      r[i + c * n] = rr;
+      const double zz = rr / diag[i];
       z[i + c * n] = zz;
       p[i + c * n] = zz;
     }
@@ -410,7 +428,7 @@ __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz,
     double rz = 0.0, bb = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       rz += r[i + c * n] * z[i + c * n];
-      bb += r[i + c * n] * r[i + c * n];
+      bb += Ap[i + c * n] * Ap[i + c * n];
     }
     rz = block_sum(rz, sh);
     bb = block_sum(bb, sh);
@@ -494,8 +512,9 @@ __global__ void __launch_bounds__(1024) k_ivc_cg(IBArgs a, const double *xyz, co
                                                  const int *col, const double *val,
                                                  const double *diag, double *X_, double *work,
                                                  double *F, int maxit, double tol, int *status,
-                                                 int *iters) {
-  ivc_cg_block(a, xyz, tgt, uvw, rowptr, col, val, diag, X_, work, F, maxit, tol, status, iters);
+                                                 int *iters, int warm) {
+  ivc_cg_block(a, xyz, tgt, uvw, rowptr, col, val, diag, X_, work, F, maxit, tol, status, iters,
+               warm);
 }
 
 // ---------------------------------------------------------------------------
@@ -1487,7 +1506,8 @@ static int launch_cg(ilbm_ib *ib, const IBArgs &a_in, cudaStream_t s) {
   if (ib->n <= 1024) {
     k_ivc_cg<<<1, 1024, 0, s>>>(a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_rowptr, ib->d_col,
                                 ib->d_val, ib->d_diag, ib->d_X, ib->d_work, ib->d_F, 500, cg_tol,
-                                ib->d_status, ib->d_iters);
+                                ib->d_status, ib->d_iters, ib->cg_warm ? 1 : 0);
+    ib->cg_warm = true;  // later solves start from this one
     return ILBM_OK;
   }
   const double *xyz = ib->d_xyz, *tgt = ib->d_tgt, *uvw = ib->d_uvw, *val = ib->d_val,
@@ -1505,7 +1525,7 @@ static int launch_cg(ilbm_ib *ib, const IBArgs &a_in, cudaStream_t s) {
   const int blocks = std::max(8, std::min(ib->cg_blocks, (ib->n + 15) / 16));
   cudaError_t ce = cudaLaunchCooperativeKernel((const void *)k_ivc_cg_grid, dim3(blocks), dim3(256),
                                                args, 0, s);
-  ib->cg_warm = !ib->moving && ib->p.ivc_rebuild_matrix == 0;
+  ib->cg_warm = true;  // the next solve starts from this one (an initial guess only)
   if (ce != cudaSuccess) return cuda_fail(ce, "cooperative CG launch");
   return ILBM_OK;
 }
@@ -1884,7 +1904,7 @@ __global__ void __launch_bounds__(1024) k_b_cg(const IBCase *cs, const int *cg_c
     if (k.rebuild) csr_scan_block(k.a.n, k.rowptr, k.nnz_cap, k.status);
   } else {
     ivc_cg_block(k.a, k.xyz, k.tgt, k.uvw, k.rowptr, k.col, k.val, k.diag, k.X, k.work, k.F, 500,
-                 k.cg_tol, k.status, k.iters);
+                 k.cg_tol, k.status, k.iters, 1);
   }
 }
 
@@ -1909,49 +1929,73 @@ __global__ void __launch_bounds__(256) k_b_export(const IBCase *cs, const int64_
   }
 }
 
-// one block (1024 threads) per case: marker force sum and Eulerian force sum
-// over the force region, written to the case's record ring; step counter + 1
+// kRecParts blocks per case: Eulerian force sum over the force region (the
+// band clipped to the domain) in fixed partial slots; the case's last block to
+// finish combines them in order, forms the marker force sum, writes the
+// case's record ring and advances its step counter
+constexpr int kRecParts = 8;
+constexpr int kRecThreads = 256;
 template <class R>
-__global__ void __launch_bounds__(1024) k_b_record(const IBCase *cs, const StepArgs *args, int *steps,
-                                                   int rec_slots) {
+__global__ void __launch_bounds__(kRecThreads) k_b_record(const IBCase *cs, const StepArgs *args,
+                                                          int *steps, int rec_slots, double *part,
+                                                          unsigned *done) {
   __shared__ double sh[33];
-  const int c = blockIdx.x;
+  __shared__ bool last;
+  const int c = blockIdx.x / kRecParts, pt = blockIdx.x % kRecParts;
   const IBCase &k = cs[c];
   const StepArgs &sa = args[c];
+  if (k.a.n > 0) {
+    const R *F = static_cast<const R *>(sa.force);
+    int lo[3], nn[3];
+    for (int d = 0; d < 3; ++d) {
+      const int l = (d < k.a.dim) ? max(k.a.blo[d], k.a.dlo[d]) : 0;
+      const int h = (d < k.a.dim) ? min(k.a.blo[d] + k.a.bn[d] - 1, k.a.dhi[d]) : 0;
+      lo[d] = l;
+      nn[d] = max(0, h - l + 1);
+    }
+    const int items = nn[0] * nn[1] * nn[2];
+    for (int comp = 0; comp < 3; ++comp) {
+      double sm = 0.0;
+      if (comp < k.a.dim) {
+        const R *Fc = F + comp * sa.ms2;
+        for (int f = pt * kRecThreads + threadIdx.x; f < items; f += kRecParts * kRecThreads) {
+          const int i = lo[0] + f % nn[0], r = f / nn[0];
+          const int j = lo[1] + r % nn[1], kk = lo[2] + r / nn[1];
+          sm += double(Fc[(int64_t)(i - sa.mgl[0]) + (int64_t)(j - sa.mgl[1]) * sa.ms0 +
+                          (int64_t)(kk - sa.mgl[2]) * sa.ms1]);
+        }
+      }
+      sm = block_sum(sm, sh);
+      if (threadIdx.x == 0) part[((size_t)c * kRecParts + pt) * 3 + comp] = sm;
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = (atomicAdd(done + c, 1u) == kRecParts - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
   double fe[3] = {0.0, 0.0, 0.0};
   if (k.a.n > 0) {
     marker_sum_block(k.a, k.F, k.fsum);
-    const R *F = static_cast<const R *>(sa.force);
-    for (int comp = 0; comp < k.a.dim; ++comp) {
-      double s = 0.0;
-      for (int64_t t = threadIdx.x; t < k.a.nb; t += blockDim.x) {
-        const int i = k.a.blo[0] + (int)(t % k.a.bn[0]);
-        const int j = k.a.blo[1] + (int)((t / k.a.bn[0]) % k.a.bn[1]);
-        const int kk = k.a.blo[2] + (int)(t / ((int64_t)k.a.bn[0] * k.a.bn[1]));
-        const int g[3] = {i, j, kk};
-        bool inside = true;
-        for (int d = 0; d < k.a.dim; ++d) inside = inside && g[d] >= k.a.dlo[d] && g[d] <= k.a.dhi[d];
-        if (!inside) continue;
-        const int64_t m = (int64_t)(i - sa.mgl[0]) + (int64_t)(j - sa.mgl[1]) * sa.ms0 +
-                          (int64_t)(kk - sa.mgl[2]) * sa.ms1;
-        s += double(F[m + comp * sa.ms2]);
-      }
-      fe[comp] = block_sum(s, sh);
-    }
+    for (int p2 = 0; p2 < kRecParts; ++p2)
+      for (int comp = 0; comp < 3; ++comp) fe[comp] += __ldcg(part + ((size_t)c * kRecParts + p2) * 3 + comp);
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    const int s = steps[c];
-    double *r = k.rec + (size_t)(s % rec_slots) * 8;
+    const int st = steps[c];
+    double *r = k.rec + (size_t)(st % rec_slots) * 8;
     r[0] = fe[0];
     r[1] = fe[1];
     r[2] = fe[2];
     r[3] = (k.a.n > 0) ? k.fsum[0] : 0.0;
     r[4] = (k.a.n > 0) ? k.fsum[1] : 0.0;
     r[5] = (k.a.n > 0) ? k.fsum[2] : 0.0;
-    r[6] = double(s);
+    r[6] = double(st);
     r[7] = 0.0;
-    steps[c] = s + 1;
+    steps[c] = st + 1;
+    done[c] = 0u;  // ready for the next step
   }
 }
 
@@ -1971,7 +2015,8 @@ struct IBBatch {
   int nd = 0, ncg = 0;
   bool any_periodic = false, any_explicit = false, any_rebuild = false;
   int *d_steps = nullptr;
-  double *d_rec = nullptr;
+  double *d_rec = nullptr, *d_part = nullptr;
+  unsigned *d_done = nullptr;
   int *d_status_copy = nullptr;
   std::vector<int *> status_ptrs;
 };
@@ -2100,6 +2145,7 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
     bd.nb = ib->nb;
     bd.EV = ib->d_EV;
     bd.RHO = ib->d_RHO;
+    bd.EFI = ib->d_EFI;
     if (k.mode == 1) {
       dcase.push_back(c);
       doff.push_back(doff.back() + ib->n);
@@ -2118,12 +2164,14 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
     hc[c].kin = dk;
   }
   double *rec = nullptr;
-  if ((rc = bmalloc(b, &rec, (size_t)b->nc * b->rec_slots * 8)) || (rc = bmalloc(b, &b->d_steps, b->nc))) {
+  if ((rc = bmalloc(b, &rec, (size_t)b->nc * b->rec_slots * 8)) || (rc = bmalloc(b, &b->d_steps, b->nc)) ||
+      (rc = bmalloc(b, &b->d_part, (size_t)b->nc * kRecParts * 3)) || (rc = bmalloc(b, &b->d_done, b->nc))) {
     ib_batch_destroy(b);
     return rc;
   }
   cudaMemset(rec, 0, (size_t)b->nc * b->rec_slots * 8 * sizeof(double));
   cudaMemset(b->d_steps, 0, b->nc * sizeof(int));
+  cudaMemset(b->d_done, 0, b->nc * sizeof(unsigned));
   b->d_rec = rec;
   for (int c = 0; c < b->nc; ++c) hc[c].rec = rec + (size_t)c * b->rec_slots * 8;
   b->total_m = moff.back();
@@ -2154,9 +2202,9 @@ int ib_batch_forcing(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
   if (rc) return rc;
   const int gb = grid_for(b->total_b, 256), gm = grid_for(b->total_m, 256);
   const int gw = grid_for(b->total_m * 32, 128);
-  k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 0);
+  // (the band macro also zeroed EFI)
   k_b_markers<<<gm, 256, 0, s>>>(b->d_cases, b->d_moff, b->nc, b->d_steps);
-  ctx->launches += 2;
+  ctx->launches += 1;
   if (b->any_periodic) {
     k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 1);
     ctx->launches++;
@@ -2199,10 +2247,13 @@ int ib_batch_forcing(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
 
 int ib_batch_record(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
   if (b->nc == 0) return ILBM_OK;
+  const unsigned g = (unsigned)b->nc * kRecParts;
   if (b->ctx->storage == ILBM_STORAGE_F64)
-    k_b_record<double><<<b->nc, 1024, 0, s>>>(b->d_cases, d_args, b->d_steps, b->rec_slots);
+    k_b_record<double><<<g, kRecThreads, 0, s>>>(b->d_cases, d_args, b->d_steps, b->rec_slots,
+                                                 b->d_part, b->d_done);
   else
-    k_b_record<float><<<b->nc, 1024, 0, s>>>(b->d_cases, d_args, b->d_steps, b->rec_slots);
+    k_b_record<float><<<g, kRecThreads, 0, s>>>(b->d_cases, d_args, b->d_steps, b->rec_slots,
+                                                b->d_part, b->d_done);
   b->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "batched force record");

@@ -602,20 +602,18 @@ template <class L, int S>
 __global__ void __launch_bounds__(256, StepOcc<L, S>::value)
     k_step_batch(const StepArgs *__restrict__ args, const StepTile *__restrict__ tiles, int ntiles) {
   __shared__ StepArgs sa;
-  __shared__ int cur;
-  if (threadIdx.x == 0) cur = -1;
+  int cur = -1;  // every thread walks the same tiles, so this stays block-uniform
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const StepTile tl = tiles[t];
-    __syncthreads();  // every thread is done with the previous tile's arguments
     if (tl.c != cur) {
+      __syncthreads();  // every thread is done with the previous case's arguments
       const int *src = reinterpret_cast<const int *>(args + tl.c);
       int *dst = reinterpret_cast<int *>(&sa);
       for (int w = threadIdx.x; w < (int)(sizeof(StepArgs) / sizeof(int)); w += blockDim.x)
         dst[w] = src[w];
       __syncthreads();
-      if (threadIdx.x == 0) cur = tl.c;
+      cur = tl.c;
     }
-    __syncthreads();
     if (tl.i0 < 0) {
       ghost_push<L, S>(sa, (int64_t)(-1 - tl.i0) * blockDim.x + threadIdx.x,
                        (int64_t)tl.j * blockDim.x);
@@ -806,8 +804,10 @@ __global__ void __launch_bounds__(256) k_band_macro_batch(const StepArgs *args, 
        t += (int64_t)gridDim.x * blockDim.x) {
     const int c = case_of(off, ncase, t);
     const BandDesc &b = bands[c];
-    band_macro_cell<L, S>(args[c], b.blo[0], b.blo[1], b.blo[2], b.bn[0], b.bn[1], b.nb, t - off[c],
-                          b.EV, b.RHO);
+    const int64_t u = t - off[c];
+    band_macro_cell<L, S>(args[c], b.blo[0], b.blo[1], b.blo[2], b.bn[0], b.bn[1], b.nb, u, b.EV,
+                          b.RHO);
+    if (b.EFI) b.EFI[u] = b.EFI[u + b.nb] = b.EFI[u + 2 * b.nb] = 0.0;  // spread target of this step
   }
 }
 

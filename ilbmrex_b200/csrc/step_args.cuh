@@ -54,11 +54,12 @@ struct StepTile {
 };
 
 // Support band of an immersed body on a case's level (EV: 3 velocity
-// components, RHO: density, both band-sized).
+// components, RHO: density, EFI: 3 spread-force components, zeroed by the
+// batched band macro when set; all band-sized).
 struct BandDesc {
   int blo[3], bn[3];
   int64_t nb;
-  double *EV, *RHO;
+  double *EV, *RHO, *EFI;
 };
 
 // Case owning item t of a concatenation whose case c starts at off[c]

@@ -133,6 +133,24 @@ class Context:
             pass
 
 
+def ib_footprint(case: LevelCase, ib: MarkerIB) -> int:
+    """Estimated device bytes of an IB object: band arrays (10 doubles per
+    cell of the support band), marker arrays and the IVC operator (stored
+    inverse for fixed bodies up to 8192 markers, else CSR + CG vectors)."""
+    d = case.dim
+    ext = 2.0 * ib.R + 16.0
+    if ib.geometry_type == 2 and ib.airfoil is not None:
+        ext = ib.airfoil[0] + 16.0
+    nb = int(ext ** d)
+    h = case.dx
+    area = (2.0 * math.pi * ib.R) if d == 2 else (4.0 * math.pi * ib.R * ib.R)
+    n = int(max(ib.n_marker, area / (h ** (d - 1)) if ib.geometry_type == 0 else 4.0 * ext / h))
+    ld = (n + 31) // 32 * 32
+    op = n * ld * 8 if (ib.coupling_method == 1 and ib.geometry_type != 2 and n <= 8192) else 0
+    op += n * (512 if d == 3 else 96) * 12 + n * 15 * 8 * 3
+    return int(nb * 10 * 8 + n * 15 * 8 + op)
+
+
 class LevelSolver:
     """One level held in one box, stepped on the GPU through the C ABI."""
 
@@ -326,6 +344,27 @@ class LevelSolver:
                                              out.data_ptr(), None, None), "compute_macro")
         self.ctx.sync()
         return self._valid(out, self.gm).to(torch.float64).cpu().numpy()
+
+    def mean_velocity(self) -> np.ndarray:
+        """Domain-mean velocity of the current state (reduced on the device)."""
+        out = torch.zeros_like(self.macro)
+        b = self._box(self.f, None)
+        force = self.force_prev if self.ib is not None else None
+        capi.check(self.L.ilbm_compute_macro(self.ctx.h, C.byref(b), C.byref(self.params),
+                                             self.f.data_ptr(),
+                                             force.data_ptr() if force is not None else None,
+                                             out.data_ptr(), None, None), "compute_macro")
+        self.ctx.sync()
+        v = self._valid(out, self.gm)[1:4].to(torch.float64)
+        return v.reshape(3, -1).mean(dim=1).cpu().numpy()
+
+    def footprint_bytes(self) -> int:
+        """Device memory this solver holds (fields; IB arrays estimated)."""
+        n = sum(t.numel() * t.element_size()
+                for t in (self.f, self.f_next, self.macro, self.force_cur, self.force_prev))
+        if self.ib is not None:
+            n += ib_footprint(self.case, self.ib_case)
+        return int(n)
 
     def get_force(self) -> np.ndarray:
         """Force F used in the last step ([3, nz, ny, nx])."""
