@@ -264,7 +264,7 @@ def run_served(args, world, device):
     for r, sv in zip(reqs, service):
         done = max(done, r.arrival) + sv
         lat.append(done - r.arrival)
-    plain_mlups = lups / sum(service) / 1e6
+    plain_mlups = lups / done / 1e6  # same arrivals, one request at a time (FIFO)
     sizes = [r.case.cells for r in reqs]
     return {"metric": "served MLUPS, mixed D2Q9/D3Q19 FP32 requests", "value": round(stats["mlups"], 2),
             "unit": "MLUPS", "p50_latency_s": round(stats["p50_latency_s"], 4),
@@ -274,6 +274,8 @@ def run_served(args, world, device):
             "plain_p99_latency_s": round(float(np.percentile(lat, 99)), 4),
             "speedup_vs_plain": round(stats["mlups"] / plain_mlups, 2),
             "requests": n, "arrival_rate_per_s": args.serve_rate, "makespan_s": round(stats["makespan_s"], 3),
+            "plain_makespan_s": round(done, 3), "plain_busy_s": round(sum(service), 3),
+            "server_time_s": stats["time_s"],
             "cells_min_max": [int(min(sizes)), int(max(sizes))],
             "steps_min_max": [args.serve_min_steps, args.serve_max_steps],
             "workload": f"seeded Poisson arrivals; 50% D2Q9 cylinder/airfoil, 25% D3Q19 duct N x N x 4N, "
@@ -290,8 +292,8 @@ def run_b200(args):
     from ilbmrex_b200 import capi, cases
     from ilbmrex_b200.level import LevelSolver
 
-    if args.only_batched:  # profiling aid: the batched workload alone
-        out = run_batched(args, world, device)
+    if args.only_batched or args.only_served:  # profiling aids: one workload alone
+        out = run_batched(args, world, device) if args.only_batched else run_served(args, world, device)
         if rank == 0:
             print(json.dumps(out), flush=True)
         return
@@ -450,13 +452,15 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched workload")
     ap.add_argument("--no-served", action="store_true", help="skip the served workload")
     ap.add_argument("--serve-requests", type=int, default=24)
-    ap.add_argument("--serve-rate", type=float, default=40.0, help="arrivals per second")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="arrivals per second")
     ap.add_argument("--serve-scale", type=float, default=0.5)
     ap.add_argument("--serve-min-steps", type=int, default=300)
     ap.add_argument("--serve-max-steps", type=int, default=1500)
-    ap.add_argument("--serve-chunk", type=int, default=50)
+    ap.add_argument("--serve-chunk", type=int, default=100)
     ap.add_argument("--only-batched", action="store_true",
                     help="run only the batched workload and print its result (profiling aid)")
+    ap.add_argument("--only-served", action="store_true",
+                    help="run only the served workload and print its result (profiling aid)")
     ap.add_argument("--batch-cases", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=40)
     ap.add_argument("--batch-plain-steps", type=int, default=8)

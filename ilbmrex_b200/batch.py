@@ -80,6 +80,17 @@ class Batch:
     def set_tiles(self, tile_w: int, ctas_per_sm: int = 0):
         capi.check(self.L.ilbm_batch_set_tiles(self.h, int(tile_w), int(ctas_per_sm)), "batch_set_tiles")
 
+    def progress(self) -> dict[int, tuple[int, int]]:
+        """case id -> (steps taken in the batch, steps remaining); one sync."""
+        n = C.c_int()
+        capi.check(self.L.ilbm_batch_progress(self.h, 0, None, None, None, C.byref(n)), "batch_progress")
+        m = n.value
+        ids = (C.c_int * max(m, 1))()
+        done = (C.c_int64 * max(m, 1))()
+        left = (C.c_int * max(m, 1))()
+        capi.check(self.L.ilbm_batch_progress(self.h, m, ids, done, left, C.byref(n)), "batch_progress")
+        return {ids[i]: (done[i], left[i]) for i in range(m)}
+
     def size(self):
         n, cells = C.c_int(), C.c_int64()
         capi.check(self.L.ilbm_batch_size(self.h, C.byref(n), C.byref(cells)), "batch_size")

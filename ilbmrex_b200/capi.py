@@ -34,7 +34,7 @@ EXPORTS = [
     "ilbm_force_integrals", "ilbm_force_integrals_noalloc", "ilbm_momentum_exchange",
     "ilbm_batch_create", "ilbm_batch_destroy", "ilbm_batch_add", "ilbm_batch_remove",
     "ilbm_batch_step", "ilbm_batch_case_state", "ilbm_batch_records", "ilbm_batch_set_tiles",
-    "ilbm_batch_tune", "ilbm_batch_size",
+    "ilbm_batch_tune", "ilbm_batch_size", "ilbm_batch_progress",
 ]
 
 
@@ -147,6 +147,7 @@ def lib():
         "ilbm_batch_set_tiles": (I, [P, I, I]),
         "ilbm_batch_tune": (I, [P, I, C.POINTER(I), C.POINTER(I), C.POINTER(C.c_float)]),
         "ilbm_batch_size": (I, [P, C.POINTER(I), C.POINTER(I64)]),
+        "ilbm_batch_progress": (I, [P, I, C.POINTER(I), C.POINTER(I64), C.POINTER(I), C.POINTER(I)]),
         "ilbm_momentum_exchange": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P,
                                        D, D, D, D, dp, dp, I, dp]),
     }

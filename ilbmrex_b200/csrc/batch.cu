@@ -28,7 +28,7 @@ struct ilbm_batch {
     ilbm_ib *ib;
     double dt, time;   // time of the case's next step
     int max_steps;     // steps the caller may still ask for (kinematics table)
-    int parity;        // buffers of the current state: 0 as in box, 1 swapped
+    int parity;        // buffers of the state at the last build: 0 as in box, 1 swapped
     int64_t steps;     // steps taken inside this batch
     int64_t cells;
     std::vector<double> rec;  // 8 doubles per step taken in the batch
@@ -37,11 +37,11 @@ struct ilbm_batch {
   std::vector<Case> cases;
   int next_id = 1;
   int rec_slots = 256;
-  int tile_w = 256, ctas_per_sm = 0;  // 0: as many as fit
+  int tile_w = 128, ctas_per_sm = 0;  // 0: as many as fit
   int sms = 0;
   // built state
   bool built = false;
-  int phase = 0;    // slot of the next step; case state = parity ^ phase
+  int phase = 0;    // slot of the next step (a case's state: parity ^ (its steps & 1))
   int pending = 0;  // steps since the record rings were drained
   StepArgs *d_args = nullptr;  // [2][ncase]
   StepTile *d_tiles = nullptr;
@@ -118,7 +118,7 @@ int settle(ilbm_batch *b) {
     for (int64_t s = 0; s < taken; ++s) k.time += k.dt;  // as the single path accumulates it
     k.steps += taken;
     k.max_steps -= (int)taken;
-    k.parity ^= b->phase;
+    k.parity ^= (int)(taken & 1);  // a case that stopped early keeps its own parity
   }
   b->phase = 0;
   free_built(b);
@@ -160,7 +160,7 @@ int build(ilbm_batch *b) {
       }
       if ((rc = batch_case_args(ctx, x, &p, &args[(size_t)s * nc + c]))) return rc;
     }
-    ibc[c] = IBBatchCase{k.ib, k.dt, k.time, std::max(1, k.max_steps)};
+    ibc[c] = IBBatchCase{k.ib, k.dt, k.time, std::max(1, k.max_steps), std::max(0, k.max_steps)};
   }
   // tile table: every case's ghost-push chunks first (strided, slow), then
   // its row segments
@@ -211,7 +211,8 @@ int step_slot(ilbm_batch *b, int slot) {
   const StepArgs *a = b->d_args + (size_t)slot * nc;
   int rc = ib_batch_forcing(b->ibb, a, b->ctx->stream);
   if (rc) return rc;
-  if ((rc = batch_step_launch(b->ctx, a, b->d_tiles, b->ntiles, b->tile_w, b->blocks, b->ctx->stream)))
+  if ((rc = batch_step_launch(b->ctx, a, b->d_tiles, b->ntiles, b->tile_w, b->blocks,
+                              ib_batch_steps(b->ibb), ib_batch_limits(b->ibb), b->ctx->stream)))
     return rc;
   return ib_batch_record(b->ibb, a, b->ctx->stream);
 }
@@ -326,7 +327,7 @@ int ilbm_batch_add(ilbm_batch *b, const ilbm_box *box, const ilbm_level_params *
   k.ib = ib;
   k.dt = dt;
   k.time = time;
-  k.max_steps = std::max(1, max_steps);
+  k.max_steps = std::max(0, max_steps);
   k.parity = 0;
   k.steps = 0;
   k.cells = 1;
@@ -371,7 +372,7 @@ int ilbm_batch_case_state(ilbm_batch *b, int case_id, int *parity, int64_t *step
   const int64_t taken = (int64_t)k->rec.size() / 8 - k->steps;
   double t = k->time;
   for (int64_t s = 0; s < taken; ++s) t += k->dt;
-  if (parity) *parity = k->parity ^ (b->built ? b->phase : 0);
+  if (parity) *parity = k->parity ^ (int)(taken & 1);
   if (steps_done) *steps_done = k->steps + taken;
   if (time) *time = t;
   return ILBM_OK;
@@ -445,6 +446,26 @@ int ilbm_batch_tune(ilbm_batch *b, int trial_steps, int *tile_w, int *ctas_per_s
   if (tile_w) *tile_w = bw;
   if (ctas_per_sm) *ctas_per_sm = bc;
   if (ms_per_step) *ms_per_step = best;
+  return ILBM_OK;
+}
+
+int ilbm_batch_progress(ilbm_batch *b, int max_cases, int *ids, int64_t *steps_done,
+                        int *remaining, int *ncase) {
+  if (!b || !ncase) {
+    set_error("ilbm_batch_progress: null argument");
+    return ILBM_ERR_ARG;
+  }
+  int rc = drain(b);
+  if (rc) return rc;
+  const int n = std::min((int)b->cases.size(), std::max(0, max_cases));
+  for (int c = 0; c < n; ++c) {
+    const auto &k = b->cases[c];
+    const int64_t taken = (int64_t)k.rec.size() / 8 - k.steps;
+    if (ids) ids[c] = k.id;
+    if (steps_done) steps_done[c] = k.steps + taken;
+    if (remaining) remaining[c] = std::max(0, k.max_steps - (int)taken);
+  }
+  *ncase = (int)b->cases.size();
   return ILBM_OK;
 }
 

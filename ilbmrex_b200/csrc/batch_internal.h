@@ -18,12 +18,14 @@ int batch_case_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_par
                     StepArgs *out);
 // ghost-push chunks of w threads one case needs
 int batch_ghost_chunks(const ilbm_ctx *ctx, const StepArgs &a, int w);
-// k_step_batch over a tile table (w threads per block, `blocks` persistent blocks)
+// k_step_batch over a tile table (w threads per block, `blocks` persistent
+// blocks); cases with steps[c] >= limit[c] are skipped
 int batch_step_launch(ilbm_ctx *ctx, const StepArgs *d_args, const StepTile *d_tiles, int ntiles,
-                      int w, int blocks, cudaStream_t st);
-// band macro of every case's body
+                      int w, int blocks, const int *steps, const int *limit, cudaStream_t st);
+// band macro of every case's body (same skipping)
 int batch_band_macro_launch(ilbm_ctx *ctx, const StepArgs *d_args, const BandDesc *d_bands,
-                            const int64_t *d_off, int ncase, int64_t total, cudaStream_t st);
+                            const int64_t *d_off, int ncase, int64_t total, const int *steps,
+                            const int *limit, cudaStream_t st);
 // resident blocks of w threads per SM of k_step_batch
 int batch_step_occupancy(const ilbm_ctx *ctx, int w, int *per_sm);
 
@@ -34,7 +36,8 @@ struct IBBatchCase {
   ilbm_ib *ib;     // NULL: a case without an immersed body
   double dt;       // time step of the case's level
   double time0;    // time of the case's next step
-  int kin_steps;   // steps the kinematics table covers (moving bodies)
+  int kin_steps;   // length of its kinematics table (>= limit, >= 1)
+  int limit;       // steps the case may take in this batch (it stops there)
 };
 
 // device tables for a set of cases; fails if a body has not taken its first
@@ -52,5 +55,8 @@ int ib_batch_record(IBBatch *b, const StepArgs *d_args, cudaStream_t s);
 int ib_batch_read(IBBatch *b, std::vector<double> &rec, std::vector<int> &steps,
                   std::vector<int> &status, cudaStream_t s);
 int ib_batch_rec_slots(const IBBatch *b);
+// device step counters and limits (one int per case)
+const int *ib_batch_steps(const IBBatch *b);
+const int *ib_batch_limits(const IBBatch *b);
 
 }  // namespace ilbm

@@ -1827,11 +1827,17 @@ struct IBCase {
   double *rec;        // rec_slots x 8: Eulerian force sum (3), marker force sum (3), step, 0
 };
 
+// a case that has taken all the steps it was added for sits out
+__device__ __forceinline__ bool live(const int *steps, const int *limit, int c) {
+  return steps[c] < limit[c];
+}
+
 __global__ void __launch_bounds__(256) k_b_markers(const IBCase *cs, const int64_t *off, int nc,
-                                                   const int *steps) {
+                                                   const int *steps, const int *limit) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < off[nc];
        t += (int64_t)gridDim.x * blockDim.x) {
     const int c = case_of(off, nc, t);
+    if (!live(steps, limit, c)) continue;
     const IBCase &k = cs[c];
     const int m = (int)(t - off[c]);
     if (m == 0) {
@@ -1853,10 +1859,12 @@ __global__ void __launch_bounds__(256) k_b_markers(const IBCase *cs, const int64
   }
 }
 
-__global__ void __launch_bounds__(256) k_b_band(const IBCase *cs, const int64_t *off, int nc, int op) {
+__global__ void __launch_bounds__(256) k_b_band(const IBCase *cs, const int64_t *off, int nc, int op,
+                                                const int *steps, const int *limit) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < off[nc];
        t += (int64_t)gridDim.x * blockDim.x) {
     const int c = case_of(off, nc, t);
+    if (!live(steps, limit, c)) continue;
     const IBCase &k = cs[c];
     const int64_t u = t - off[c];
     if (op == 0) {
@@ -1874,11 +1882,12 @@ __global__ void __launch_bounds__(256) k_b_band(const IBCase *cs, const int64_t 
 // one warp per marker; stage 0 interpolation, 1 explicit force, 2 spreading,
 // 3 CSR row count, 4 CSR row fill
 __global__ void __launch_bounds__(128) k_b_marker_warp(const IBCase *cs, const int64_t *off, int nc,
-                                                       int stage) {
+                                                       int stage, const int *steps, const int *limit) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < off[nc]; w += nw) {
     const int c = case_of(off, nc, w);
+    if (!live(steps, limit, c)) continue;
     const IBCase &k = cs[c];
     const int m = (int)(w - off[c]);
     if (stage == 0) {
@@ -1898,7 +1907,9 @@ __global__ void __launch_bounds__(128) k_b_marker_warp(const IBCase *cs, const i
 }
 
 // one block per CG case: the CSR scan, or the whole solve
-__global__ void __launch_bounds__(1024) k_b_cg(const IBCase *cs, const int *cg_case, int stage) {
+__global__ void __launch_bounds__(1024) k_b_cg(const IBCase *cs, const int *cg_case, int stage,
+                                               const int *steps, const int *limit) {
+  if (!live(steps, limit, cg_case[blockIdx.x])) return;
   const IBCase &k = cs[cg_case[blockIdx.x]];
   if (stage == 0) {
     if (k.rebuild) csr_scan_block(k.a.n, k.rowptr, k.nnz_cap, k.status);
@@ -1910,18 +1921,22 @@ __global__ void __launch_bounds__(1024) k_b_cg(const IBCase *cs, const int *cg_c
 
 // one block per row of every stored inverse
 __global__ void __launch_bounds__(kDenseThreads) k_b_dense(const IBCase *cs, const int *dcase,
-                                                           const int64_t *doff, int nd) {
+                                                           const int64_t *doff, int nd,
+                                                           const int *steps, const int *limit) {
   const int di = case_of(doff, nd, blockIdx.x);
+  if (!live(steps, limit, dcase[di])) return;
   const IBCase &k = cs[dcase[di]];
   dense_row(k.a, k.rhs, k.Ainv, k.ld, k.F, (int)(blockIdx.x - doff[di]));
 }
 
 template <class R>
 __global__ void __launch_bounds__(256) k_b_export(const IBCase *cs, const int64_t *off, int nc,
-                                                  const StepArgs *args) {
+                                                  const StepArgs *args, const int *steps,
+                                                  const int *limit) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < off[nc];
        t += (int64_t)gridDim.x * blockDim.x) {
     const int c = case_of(off, nc, t);
+    if (!live(steps, limit, c)) continue;
     const IBCase &k = cs[c];
     const StepArgs &sa = args[c];
     export_cell<R>(k.a, k.EFI, k.RHO, static_cast<R *>(const_cast<void *>(sa.force)), sa.mgl[0],
@@ -1937,11 +1952,13 @@ constexpr int kRecParts = 8;
 constexpr int kRecThreads = 256;
 template <class R>
 __global__ void __launch_bounds__(kRecThreads) k_b_record(const IBCase *cs, const StepArgs *args,
-                                                          int *steps, int rec_slots, double *part,
+                                                          int *steps, const int *limit,
+                                                          int rec_slots, double *part,
                                                           unsigned *done) {
   __shared__ double sh[33];
   __shared__ bool last;
   const int c = blockIdx.x / kRecParts, pt = blockIdx.x % kRecParts;
+  if (!live(steps, limit, c)) return;  // uniform over the case's blocks
   const IBCase &k = cs[c];
   const StepArgs &sa = args[c];
   if (k.a.n > 0) {
@@ -2014,7 +2031,7 @@ struct IBBatch {
   int *d_dcase = nullptr, *d_cgcase = nullptr;
   int nd = 0, ncg = 0;
   bool any_periodic = false, any_explicit = false, any_rebuild = false;
-  int *d_steps = nullptr;
+  int *d_steps = nullptr, *d_limit = nullptr;
   double *d_rec = nullptr, *d_part = nullptr;
   unsigned *d_done = nullptr;
   int *d_status_copy = nullptr;
@@ -2172,6 +2189,14 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
   cudaMemset(rec, 0, (size_t)b->nc * b->rec_slots * 8 * sizeof(double));
   cudaMemset(b->d_steps, 0, b->nc * sizeof(int));
   cudaMemset(b->d_done, 0, b->nc * sizeof(unsigned));
+  {
+    std::vector<int> lim(b->nc);
+    for (int c = 0; c < b->nc; ++c) lim[c] = std::max(0, cases[c].limit);
+    if ((rc = bupload(b, &b->d_limit, lim))) {
+      ib_batch_destroy(b);
+      return rc;
+    }
+  }
   b->d_rec = rec;
   for (int c = 0; c < b->nc; ++c) hc[c].rec = rec + (size_t)c * b->rec_slots * 8;
   b->total_m = moff.back();
@@ -2198,47 +2223,49 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
 int ib_batch_forcing(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
   ilbm_ctx *ctx = b->ctx;
   if (b->total_m == 0) return ILBM_OK;
-  int rc = batch_band_macro_launch(ctx, d_args, b->d_bands, b->d_boff, b->nc, b->total_b, s);
+  const int *st = b->d_steps, *lm = b->d_limit;
+  int rc = batch_band_macro_launch(ctx, d_args, b->d_bands, b->d_boff, b->nc, b->total_b, st, lm, s);
   if (rc) return rc;
   const int gb = grid_for(b->total_b, 256), gm = grid_for(b->total_m, 256);
   const int gw = grid_for(b->total_m * 32, 128);
   // (the band macro also zeroed EFI)
-  k_b_markers<<<gm, 256, 0, s>>>(b->d_cases, b->d_moff, b->nc, b->d_steps);
+  k_b_markers<<<gm, 256, 0, s>>>(b->d_cases, b->d_moff, b->nc, st, lm);
   ctx->launches += 1;
   if (b->any_periodic) {
-    k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 1);
+    k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 1, st, lm);
     ctx->launches++;
   }
-  k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 0);
+  k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 0, st, lm);
   ctx->launches++;
   if (b->any_rebuild) {
-    k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 3);
-    k_b_cg<<<b->ncg, 1024, 0, s>>>(b->d_cases, b->d_cgcase, 0);
-    k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 4);
+    k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 3, st, lm);
+    k_b_cg<<<b->ncg, 1024, 0, s>>>(b->d_cases, b->d_cgcase, 0, st, lm);
+    k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 4, st, lm);
     ctx->launches += 3;
   }
   if (b->nd > 0) {
-    k_b_dense<<<(unsigned)b->total_drows, kDenseThreads, 0, s>>>(b->d_cases, b->d_dcase, b->d_doff, b->nd);
+    k_b_dense<<<(unsigned)b->total_drows, kDenseThreads, 0, s>>>(b->d_cases, b->d_dcase, b->d_doff,
+                                                                 b->nd, st, lm);
     ctx->launches++;
   }
   if (b->ncg > 0) {
-    k_b_cg<<<b->ncg, 1024, 0, s>>>(b->d_cases, b->d_cgcase, 1);
+    k_b_cg<<<b->ncg, 1024, 0, s>>>(b->d_cases, b->d_cgcase, 1, st, lm);
     ctx->launches++;
   }
   if (b->any_explicit) {
-    k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 1);
+    k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 1, st, lm);
     ctx->launches++;
   }
-  k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 2);
+  k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 2, st, lm);
   ctx->launches++;
   if (b->any_periodic) {
-    k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 2);
+    k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 2, st, lm);
     ctx->launches++;
   }
   if (ctx->storage == ILBM_STORAGE_F64)
-    k_b_export<double><<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, d_args);
+    k_b_export<double><<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, d_args, st, lm);
   else
-    k_b_export<float><<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, d_args);
+    k_b_export<float><<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, d_args, st, lm);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "batched update_forcing");
@@ -2249,11 +2276,11 @@ int ib_batch_record(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
   if (b->nc == 0) return ILBM_OK;
   const unsigned g = (unsigned)b->nc * kRecParts;
   if (b->ctx->storage == ILBM_STORAGE_F64)
-    k_b_record<double><<<g, kRecThreads, 0, s>>>(b->d_cases, d_args, b->d_steps, b->rec_slots,
-                                                 b->d_part, b->d_done);
+    k_b_record<double><<<g, kRecThreads, 0, s>>>(b->d_cases, d_args, b->d_steps, b->d_limit,
+                                                 b->rec_slots, b->d_part, b->d_done);
   else
-    k_b_record<float><<<g, kRecThreads, 0, s>>>(b->d_cases, d_args, b->d_steps, b->rec_slots,
-                                                b->d_part, b->d_done);
+    k_b_record<float><<<g, kRecThreads, 0, s>>>(b->d_cases, d_args, b->d_steps, b->d_limit,
+                                                b->rec_slots, b->d_part, b->d_done);
   b->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "batched force record");
@@ -2276,5 +2303,7 @@ int ib_batch_read(IBBatch *b, std::vector<double> &rec, std::vector<int> &steps,
 }
 
 int ib_batch_rec_slots(const IBBatch *b) { return b->rec_slots; }
+const int *ib_batch_steps(const IBBatch *b) { return b->d_steps; }
+const int *ib_batch_limits(const IBBatch *b) { return b->d_limit; }
 
 }  // namespace ilbm

@@ -452,15 +452,27 @@ struct StepOcc {
 // `edge` selects the checked push plus the completion of ghost-sourced pulls;
 // interior cells take the unchecked path.
 template <class L, int S>
+__device__ __forceinline__ void cell_finish(const StepArgs &a, int i, int j, int k, bool edge,
+                                            typename Store<S>::R *f);
+
+template <class L, int S>
 __device__ __forceinline__ void cell_update(const StepArgs &a, int i, int j, int k, bool edge) {
   using T = typename Store<S>::T;
   using R = typename Store<S>::R;
-  const int64_t base = fidx(a, i, j, k);
-  const T *fin = static_cast<const T *>(a.f_in) + base;
+  const T *fin = static_cast<const T *>(a.f_in) + fidx(a, i, j, k);
   R f[L::Q];
 #pragma unroll
   for (int q = 0; q < L::Q; ++q) f[q] = Store<S>::load(fin + a.loff[q], sfac<L, S>(a, q));
+  cell_finish<L, S>(a, i, j, k, edge, f);
+}
 
+// The rest of a cell update once its populations f^n are in registers.
+template <class L, int S>
+__device__ __forceinline__ void cell_finish(const StepArgs &a, int i, int j, int k, bool edge,
+                                            typename Store<S>::R *f) {
+  using T = typename Store<S>::T;
+  using R = typename Store<S>::R;
+  const int64_t base = fidx(a, i, j, k);
   R Fx, Fy, Fz;
   load_force<L, R>(a, a.force, i, j, k, Fx, Fy, Fz);
 
@@ -600,11 +612,13 @@ __global__ void __launch_bounds__(256, StepOcc<L, S>::value) k_step(const __grid
 // ---------------------------------------------------------------------------
 template <class L, int S>
 __global__ void __launch_bounds__(256, StepOcc<L, S>::value)
-    k_step_batch(const StepArgs *__restrict__ args, const StepTile *__restrict__ tiles, int ntiles) {
+    k_step_batch(const StepArgs *__restrict__ args, const StepTile *__restrict__ tiles, int ntiles,
+                 const int *steps, const int *limit) {
   __shared__ StepArgs sa;
   int cur = -1;  // every thread walks the same tiles, so this stays block-uniform
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const StepTile tl = tiles[t];
+    if (steps[tl.c] >= limit[tl.c]) continue;  // the case has taken all its steps
     if (tl.c != cur) {
       __syncthreads();  // every thread is done with the previous case's arguments
       const int *src = reinterpret_cast<const int *>(args + tl.c);
@@ -798,11 +812,13 @@ __global__ void __launch_bounds__(256) k_band_macro(StepArgs a, int blo0, int bl
 
 template <class L, int S>
 __global__ void __launch_bounds__(256) k_band_macro_batch(const StepArgs *args, const BandDesc *bands,
-                                                          const int64_t *off, int ncase) {
+                                                          const int64_t *off, int ncase,
+                                                          const int *steps, const int *limit) {
   const int64_t total = off[ncase];
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int c = case_of(off, ncase, t);
+    if (steps[c] >= limit[c]) continue;
     const BandDesc &b = bands[c];
     const int64_t u = t - off[c];
     band_macro_cell<L, S>(args[c], b.blo[0], b.blo[1], b.blo[2], b.bn[0], b.bn[1], b.nb, u, b.EV,
@@ -1145,8 +1161,9 @@ int batch_ghost_chunks(const ilbm_ctx *ctx, const StepArgs &a, int w) {
 
 template <class L, int S>
 static int launch_step_batch(ilbm_ctx *ctx, const StepArgs *d_args, const StepTile *d_tiles,
-                             int ntiles, int w, int blocks, cudaStream_t st) {
-  k_step_batch<L, S><<<blocks, w, 0, st>>>(d_args, d_tiles, ntiles);
+                             int ntiles, int w, int blocks, const int *steps, const int *limit,
+                             cudaStream_t st) {
+  k_step_batch<L, S><<<blocks, w, 0, st>>>(d_args, d_tiles, ntiles, steps, limit);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "batched level step launch");
@@ -1154,16 +1171,18 @@ static int launch_step_batch(ilbm_ctx *ctx, const StepArgs *d_args, const StepTi
 }
 
 int batch_step_launch(ilbm_ctx *ctx, const StepArgs *d_args, const StepTile *d_tiles, int ntiles,
-                      int w, int blocks, cudaStream_t st) {
+                      int w, int blocks, const int *steps, const int *limit, cudaStream_t st) {
   if (ntiles <= 0) return ILBM_OK;
-  return ILBM_DISPATCH(ctx, launch_step_batch, ctx, d_args, d_tiles, ntiles, w, blocks, st);
+  return ILBM_DISPATCH(ctx, launch_step_batch, ctx, d_args, d_tiles, ntiles, w, blocks, steps, limit,
+                       st);
 }
 
 template <class L, int S>
 static int launch_band_macro_batch(ilbm_ctx *ctx, const StepArgs *d_args, const BandDesc *d_bands,
-                                   const int64_t *d_off, int ncase, int64_t total, cudaStream_t st) {
+                                   const int64_t *d_off, int ncase, int64_t total,
+                                   const int *steps, const int *limit, cudaStream_t st) {
   const int blocks = (int)std::min<int64_t>((total + 255) / 256, 4096);
-  k_band_macro_batch<L, S><<<blocks, 256, 0, st>>>(d_args, d_bands, d_off, ncase);
+  k_band_macro_batch<L, S><<<blocks, 256, 0, st>>>(d_args, d_bands, d_off, ncase, steps, limit);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "batched band macro launch");
@@ -1171,9 +1190,11 @@ static int launch_band_macro_batch(ilbm_ctx *ctx, const StepArgs *d_args, const 
 }
 
 int batch_band_macro_launch(ilbm_ctx *ctx, const StepArgs *d_args, const BandDesc *d_bands,
-                            const int64_t *d_off, int ncase, int64_t total, cudaStream_t st) {
+                            const int64_t *d_off, int ncase, int64_t total, const int *steps,
+                            const int *limit, cudaStream_t st) {
   if (total <= 0) return ILBM_OK;
-  return ILBM_DISPATCH(ctx, launch_band_macro_batch, ctx, d_args, d_bands, d_off, ncase, total, st);
+  return ILBM_DISPATCH(ctx, launch_band_macro_batch, ctx, d_args, d_bands, d_off, ncase, total, steps,
+                       limit, st);
 }
 
 template <class L, int S>

@@ -98,7 +98,7 @@ class Server:
         self.budget = int(hbm_budget)
         self.used = 0
         self.batches: dict[int, Batch] = {}
-        self.active: dict[int, tuple] = {}   # rid -> (q, cid, request, solver, footprint, left)
+        self.active: dict[int, tuple] = {}   # rid -> (q, cid, request, solver, footprint)
 
     def _batch(self, lattice) -> Batch:
         if lattice.q not in self.batches:
@@ -125,16 +125,16 @@ class Server:
             return False
         B = self._batch(req.case.lattice)
         S = B.solver(req.case, req.ib, req.init)
-        cid = B.add(S, max_steps=req.steps)  # takes the request's first step
+        cid = B.add(S, max_steps=req.steps - 1)  # takes the request's first step itself
         req.admitted = now
         self.used += fp
-        self.active[req.rid] = (req.case.lattice.q, cid, req, S, fp, req.steps - 1)
+        self.active[req.rid] = (req.case.lattice.q, cid, req, S, fp)
         if req.ib is not None:
             S.rec_history = [S.rec.copy()]  # the first step's record
         return True
 
     def _retire(self, rid: int, now: float):
-        q, cid, req, S, fp, left = self.active.pop(rid)
+        q, cid, req, S, fp = self.active.pop(rid)
         self.batches[q].remove(cid)  # hands the state and force records back
         if req.ib is not None:
             req.cd_cl = np.array([r[3:5] for r in S.rec_history])
@@ -149,31 +149,44 @@ class Server:
         pending = sorted(requests, key=lambda r: r.arrival)
         queue: list[Request] = []
         t0 = time.perf_counter()
-        lups = 0
+        lups_done: dict[int, int] = {}
+        spent = {"admit": 0.0, "step": 0.0, "retire": 0.0, "idle": 0.0}
         while pending or queue or self.active:
             now = time.perf_counter() - t0
             while pending and pending[0].arrival <= now:
                 queue.append(pending.pop(0))
+            ta = time.perf_counter()
             while queue and self._admit(queue[0], now):
                 r = queue.pop(0)
-                lups += r.case.cells  # its first step
+                lups_done[r.rid] = r.case.cells  # its first step
+            spent["admit"] += time.perf_counter() - ta
             if not self.active:
                 if pending:
+                    ti = time.perf_counter()
                     time.sleep(max(0.0, min(0.01, pending[0].arrival - now)))
+                    spent["idle"] += time.perf_counter() - ti
                 continue
-            # next chunk: up to the first case that finishes, at most `chunk`
-            k = min(self.chunk, min(v[5] for v in self.active.values()))
-            if k > 0:
-                for q, B in self.batches.items():
-                    if any(v[0] == q for v in self.active.values()):
-                        B.step(k)  # asynchronous: the lattices' batches overlap
-                for B in self.batches.values():
-                    B.ctx.sync()
-                for rid, v in list(self.active.items()):
-                    self.active[rid] = v[:5] + (v[5] - k,)
-                    lups += v[2].case.cells * k
+            ts = time.perf_counter()
+            # next chunk: every batch advances `chunk` steps; a case that
+            # reaches its step count stops there on the device and sits out
+            for q, B in self.batches.items():
+                if any(v[0] == q for v in self.active.values()):
+                    B.step(self.chunk)  # asynchronous: the lattices' batches overlap
+            finished = []
+            for q, B in self.batches.items():
+                if not any(v[0] == q for v in self.active.values()):
+                    continue
+                prog = B.progress()  # synchronises this batch
+                for rid, v in self.active.items():
+                    if v[0] == q:
+                        done, left = prog[v[1]]
+                        if left == 0:
+                            finished.append(rid)
+                        lups_done[rid] = v[2].case.cells * (1 + done)
+            spent["step"] += time.perf_counter() - ts
             now = time.perf_counter() - t0
-            for rid in [rid for rid, v in self.active.items() if v[5] <= 0]:
+            tr = time.perf_counter()
+            for rid in finished:
                 req = self.active[rid][2]
                 if keep_f:
                     S = self.batches[self.active[rid][0]].sync(self.active[rid][1])
@@ -183,13 +196,16 @@ class Server:
                     f_keep = None
                 self._retire(rid, now)
                 req.f_final = f_keep
+            spent["retire"] += time.perf_counter() - tr
         makespan = time.perf_counter() - t0
+        lups = sum(lups_done.values())
         lat = np.array([r.latency for r in requests])
         return {"requests": len(requests), "makespan_s": makespan,
                 "mlups": lups / makespan / 1e6,
                 "p50_latency_s": float(np.percentile(lat, 50)),
                 "p99_latency_s": float(np.percentile(lat, 99)),
-                "lattice_updates": int(lups)}
+                "lattice_updates": int(lups),
+                "time_s": {k: round(v, 4) for k, v in spent.items()}}
 
     def close(self):
         for v in list(self.active.values()):

@@ -310,11 +310,12 @@ int ilbm_batch_destroy(ilbm_batch *b);
 int ilbm_batch_add(ilbm_batch *b, const ilbm_box *box, const ilbm_level_params *p, ilbm_ib *ib,
                    double dt, double time, int max_steps, int *case_id);
 int ilbm_batch_remove(ilbm_batch *b, int case_id);
-/* advances every case by nsteps (asynchronous, except for record read-backs
+/* advances every case by nsteps, each case stopping once it has taken the
+ * max_steps it was added with (asynchronous, except for record read-backs
  * every rec_slots steps) */
 int ilbm_batch_step(ilbm_batch *b, int nsteps);
-/* parity 0: box.f_in (and box.force for F^{n-1}) hold the current state,
- * 1: box.f_out (box.force_prev); synchronises */
+/* parity 0: box.f_in (with box.force_prev holding F^{n-1}) hold the current
+ * state, 1: box.f_out (with box.force); synchronises */
 int ilbm_batch_case_state(ilbm_batch *b, int case_id, int *parity, int64_t *steps_done,
                           double *time);
 /* the case's per-step force records, oldest first, 6 doubles each: Eulerian
@@ -329,6 +330,10 @@ int ilbm_batch_set_tiles(ilbm_batch *b, int tile_w, int ctas_per_sm);
 int ilbm_batch_tune(ilbm_batch *b, int trial_steps, int *tile_w, int *ctas_per_sm,
                     float *ms_per_step);
 int ilbm_batch_size(ilbm_batch *b, int *ncase, int64_t *cells);
+/* ids, steps taken and steps remaining of the first max_cases cases (any of
+ * the arrays may be NULL), *ncase = number of cases; one synchronisation */
+int ilbm_batch_progress(ilbm_batch *b, int max_cases, int *ids, int64_t *steps_done,
+                        int *remaining, int *ncase);
 
 #ifdef __cplusplus
 }

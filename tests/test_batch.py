@@ -119,3 +119,26 @@ def test_batch_tune_keeps_results():
         assert rel_l2(s.get_f(), ref.get_f()) <= 1e-5
         ref.close()
     B.close()
+
+
+def test_case_stops_at_its_step_count():
+    """A case added for 3 steps stops there on the device while the batch
+    runs on; its state equals 1 + 3 steps alone, the other case's 1 + 9."""
+    storage = "f64"
+    (ca, ia, xa), (cb, ib_, xb) = mixed_cases()[1], mixed_cases()[2]
+    B = Batch(D2Q9, storage)
+    ida = B.add(B.solver(ca, ia, xa), max_steps=3)
+    idb = B.add(B.solver(cb, ib_, xb), max_steps=100)
+    B.step(9)
+    prog = B.progress()
+    assert prog[ida] == (3, 0) and prog[idb] == (9, 91)
+    sa, sb = B.sync(ida), B.sync(idb)
+    assert sa.istep == 4 and sb.istep == 10
+    ra, rb = alone(ca, ia, xa, storage, 4), alone(cb, ib_, xb, storage, 10)
+    assert rel_l2(sa.get_f(), ra.get_f()) <= 1e-12
+    assert rel_l2(sb.get_f(), rb.get_f()) <= 1e-12
+    np.testing.assert_allclose(sa.rec[3:5], ra.rec[3:5], rtol=1e-9, atol=1e-12)
+    assert len(B.records(ida)) == 3
+    ra.close()
+    rb.close()
+    B.close()
