@@ -34,6 +34,12 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOAD = dict(nx=256, ny=128, nz=128, D=32.0, center=(64.0, 64.0, 64.0), U=0.04, Re=100.0)
+
+
+def set_workload_size(nx: int, ny: int, nz: int):
+    """Shrinks the sphere workload (tests of the multi-rank logic on CPU);
+    the sphere keeps D = ny / 4 at (nx / 4, ny / 2, nz / 2)."""
+    WORKLOAD.update(nx=nx, ny=ny, nz=nz, D=ny / 4.0, center=(nx / 4.0, ny / 2.0, nz / 2.0))
 METRIC = "MLUPS & % HBM roofline (D3Q19 FP32); batched/served MLUPS, p99 vs plain"
 UNIT = "MLUPS"
 
@@ -113,6 +119,13 @@ def allreduce_max(x: float, world: int, device) -> float:
     t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate_mlups(cells_per_rank: int, steps: int, local_ms: float, world: int, device) -> tuple:
+    """Whole-job MLUPS of `world` replicas from each rank's device time: the
+    cells of all ranks over the slowest rank's time (max over ranks)."""
+    t_max = allreduce_max(local_ms, world, device)
+    return world * cells_per_rank * steps / (t_max * 1e-3) / 1e6, t_max
 
 
 def barrier(world: int):
@@ -357,8 +370,7 @@ def run_b200(args):
         barrier(world)
     launches = ctx.launches() - launches0
     t_ms = ctx.elapsed_ms(0, 1)
-    t_max = allreduce_max(t_ms, world, device)
-    value = world * cells * K / (t_max * 1e-3) / 1e6
+    value, t_max = aggregate_mlups(cells, K, t_ms, world, device)
     clocks = sampler.summary()
 
     # ---- roofline pass: the level step (ghost-shell push + fused collide-
@@ -449,6 +461,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f64", "f32", "f16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nx", type=int, default=0, help="sphere level size override (tests)")
+    ap.add_argument("--ny", type=int, default=0)
+    ap.add_argument("--nz", type=int, default=0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched workload")
     ap.add_argument("--no-served", action="store_true", help="skip the served workload")
     ap.add_argument("--serve-requests", type=int, default=24)
@@ -467,6 +482,8 @@ def main():
     ap.add_argument("--serial", action="store_true",
                     help="run the IB chain and the level step one after the other (no overlap)")
     args = ap.parse_args()
+    if args.nx:
+        set_workload_size(args.nx, args.ny or args.nx // 2, args.nz or args.nx // 2)
     if args.impl == "reference":
         run_reference(args)
     else:
