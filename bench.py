@@ -431,7 +431,7 @@ def run_b200(args):
             "config": workload_config(args),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "kernel": "level step = k_ghost_push + k_step<D3Q19,F32_SHIFT>",
+                         "kernel": "level step = k_step<D3Q19,F32_SHIFT> (ghost-shell push in its leading blocks)",
                          "kernel_ms": round(kern_ms, 4), "bytes_per_cell": B_cell,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_kind == "measured" else "fallback 6650 GB/s"},

@@ -46,11 +46,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return done != 0;
 }
 
-// bounded wait for the phase with the given parity; false if it never came
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait for the phase with the given parity (about two seconds and
+// at most 2^26 polls, whichever ends first; a single poll may itself suspend
+// for a while); false if the phase never came
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); ++it)
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (int it = 0; it < (1 << 26); ++it) {
     if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > 2000000000ull) break;
+  }
   return false;
+}
+
+// a plain arrival (no transaction bytes)
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // orders this thread's earlier generic-proxy shared-memory accesses before

@@ -383,14 +383,40 @@ __device__ double block_sum(double v, double *sh) {
 // work: 4 vectors of 3n doubles (r, z, p, Ap).  F += x on exit.
 // warm: start from the previous solution in X_ (the force changes little
 // from one step to the next), else from zero
+// fixed-order block reduction of NV values per thread; every thread gets the
+// totals in out (sh: kMaxWarps x NV doubles, not shared with a reduction that
+// may still be read)
+constexpr int kMaxWarps = 32;
+constexpr int kCgThreads = 512;  // one-block CG: 128 registers per thread available
+template <int NV>
+__device__ __forceinline__ void block_reduce(const double *v, double (*sh)[NV], double *out) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int c = 0; c < NV; ++c) {
+    double x = v[c];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[wid][c] = x;
+  }
+  __syncthreads();
+  const int nw = (int)(blockDim.x >> 5);
+#pragma unroll
+  for (int c = 0; c < NV; ++c) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += sh[w][c];
+    out[c] = t;
+  }
+}
+
+// Jacobi-preconditioned CG for the three force components at once, one
+// block.  warm: start from the previous solution in X_ (the force changes
+// little from one step to the next), else from zero.  Per iteration two
+// fused reductions (p.Ap; r.z and r.r) keep the block barriers to five.
 __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz, const double *tgt,
                                              const double *uvw, const int *rowptr, const int *col,
                                              const double *val, const double *diag, double *X_,
                                              double *work, double *F, int maxit, double tol,
                                              int *status, int *iters, int warm) {
-  __shared__ double sh[33];
-  __shared__ double s_rz[3], s_alpha[3], s_beta[3], s_bn[3], s_rn[3];
-  __shared__ int s_done;
+  __shared__ double sh3[kMaxWarps][3], sh6[kMaxWarps][6];
   const int n = a.n;
   double *r = work, *z = work + 3 * n, *p = work + 6 * n, *Ap = work + 9 * n;
   // b (kept in Ap until the residual is formed), x0 = 0 or the previous x
@@ -404,7 +430,8 @@ __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz,
     }
   }
   __syncthreads();
-  // r = b - A x0, z = r / diag, p = z
+  // r = b - A x0, z = r / diag, p = z; partial r.z and b.b
+  double part[6] = {0, 0, 0, 0, 0, 0};
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double ax[3] = {0.0, 0.0, 0.0};
     if (warm)
@@ -416,32 +443,26 @@ __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz,
         ax[2] += v * X_[j + 2 * n];
       }
     for (int c = 0; c < 3; ++c) {
-      const double rr = Ap[i + c * n] - ax[c];
+      const double b = Ap[i + c * n];
+      const double rr = b - ax[c];
       r[i + c * n] = rr;
       const double zz = rr / diag[i];
       z[i + c * n] = zz;
       p[i + c * n] = zz;
+      part[c] += rr * zz;
+      part[3 + c] += b * b;
     }
   }
-  __syncthreads();
-  for (int c = 0; c < 3; ++c) {
-    double rz = 0.0, bb = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      rz += r[i + c * n] * z[i + c * n];
-      bb += Ap[i + c * n] * Ap[i + c * n];
-    }
-    rz = block_sum(rz, sh);
-    bb = block_sum(bb, sh);
-    if (threadIdx.x == 0) {
-      s_rz[c] = rz;
-      s_bn[c] = sqrt(bb);
-    }
-  }
-  if (threadIdx.x == 0) s_done = 0;
-  __syncthreads();
+  double tot[6];
+  block_reduce<6>(part, sh6, tot);
+  double rz[3] = {tot[0], tot[1], tot[2]};
+  const double bn[3] = {sqrt(tot[3]), sqrt(tot[4]), sqrt(tot[5])};
+  __syncthreads();  // sh6 is read before the loop reuses it, Ap before it is overwritten
   int it = 0;
+  bool done = false;
   for (; it < maxit; ++it) {
-    // Ap = A p
+    // Ap = A p with the partial p.Ap
+    double pap[3] = {0.0, 0.0, 0.0};
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       double acc[3] = {0.0, 0.0, 0.0};
       for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
@@ -451,63 +472,55 @@ __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz,
         acc[1] += v * p[j + n];
         acc[2] += v * p[j + 2 * n];
       }
-      Ap[i] = acc[0];
-      Ap[i + n] = acc[1];
-      Ap[i + 2 * n] = acc[2];
+      for (int c = 0; c < 3; ++c) {
+        Ap[i + c * n] = acc[c];
+        pap[c] += p[i + c * n] * acc[c];
+      }
     }
-    __syncthreads();
-    for (int c = 0; c < 3; ++c) {
-      double pAp = 0.0;
-      for (int i = threadIdx.x; i < n; i += blockDim.x) pAp += p[i + c * n] * Ap[i + c * n];
-      pAp = block_sum(pAp, sh);
-      if (threadIdx.x == 0) s_alpha[c] = (pAp != 0.0) ? s_rz[c] / pAp : 0.0;
-    }
-    __syncthreads();
+    double pt[3];
+    block_reduce<3>(pap, sh3, pt);
+    double alpha[3];
+    for (int c = 0; c < 3; ++c) alpha[c] = (pt[c] != 0.0) ? rz[c] / pt[c] : 0.0;
+    // x += alpha p, r -= alpha Ap, z = r / diag with the partial r.z, r.r
+    double q6[6] = {0, 0, 0, 0, 0, 0};
     for (int i = threadIdx.x; i < n; i += blockDim.x)
       for (int c = 0; c < 3; ++c) {
-        X_[i + c * n] += s_alpha[c] * p[i + c * n];
-        r[i + c * n] -= s_alpha[c] * Ap[i + c * n];
-        z[i + c * n] = r[i + c * n] / diag[i];
+        X_[i + c * n] += alpha[c] * p[i + c * n];
+        const double rr = r[i + c * n] - alpha[c] * Ap[i + c * n];
+        r[i + c * n] = rr;
+        const double zz = rr / diag[i];
+        z[i + c * n] = zz;
+        q6[c] += rr * zz;
+        q6[3 + c] += rr * rr;
       }
-    __syncthreads();
+    double qt[6];
+    block_reduce<6>(q6, sh6, qt);
+    double beta[3];
+    bool ok = true;
     for (int c = 0; c < 3; ++c) {
-      double rz = 0.0, rr = 0.0;
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        rz += r[i + c * n] * z[i + c * n];
-        rr += r[i + c * n] * r[i + c * n];
-      }
-      rz = block_sum(rz, sh);
-      rr = block_sum(rr, sh);
-      if (threadIdx.x == 0) {
-        s_beta[c] = (s_rz[c] != 0.0) ? rz / s_rz[c] : 0.0;
-        s_rz[c] = rz;
-        s_rn[c] = sqrt(rr);
-      }
+      beta[c] = (rz[c] != 0.0) ? qt[c] / rz[c] : 0.0;
+      rz[c] = qt[c];
+      ok = ok && (sqrt(qt[3 + c]) <= tol * bn[c]);
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      bool ok = true;
-      for (int c = 0; c < 3; ++c) ok = ok && (s_rn[c] <= tol * s_bn[c]);
-      s_done = ok ? 1 : 0;
-    }
-    __syncthreads();
-    if (s_done) {
+    if (ok) {  // every thread holds the same totals: a uniform exit
+      done = true;
       ++it;
       break;
     }
     for (int i = threadIdx.x; i < n; i += blockDim.x)
-      for (int c = 0; c < 3; ++c) p[i + c * n] = z[i + c * n] + s_beta[c] * p[i + c * n];
+      for (int c = 0; c < 3; ++c) p[i + c * n] = z[i + c * n] + beta[c] * p[i + c * n];
     __syncthreads();
   }
   if (threadIdx.x == 0) {
     *iters = it;
-    if (!s_done) atomicOr(status, 4);
+    if (!done) atomicOr(status, 4);
   }
+  __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x)
     for (int c = 0; c < 3; ++c) F[i + c * n] = X::add(F[i + c * n], X_[i + c * n]);
 }
 
-__global__ void __launch_bounds__(1024) k_ivc_cg(IBArgs a, const double *xyz, const double *tgt,
+__global__ void __launch_bounds__(kCgThreads) k_ivc_cg(IBArgs a, const double *xyz, const double *tgt,
                                                  const double *uvw, const int *rowptr,
                                                  const int *col, const double *val,
                                                  const double *diag, double *X_, double *work,
@@ -876,6 +889,122 @@ __global__ void __launch_bounds__(kDenseThreads) k_ivc_dense(IBArgs a, const dou
   dense_row(a, rhs, Ainv, ld, F, blockIdx.x);
 }
 
+// The same solve with A^-1 held in FP32 (the storage forms that keep their
+// populations in 4 or 2 bytes): half the bytes per step, products and sums
+// still in FP64; the rounding of A^-1 (2^-24 relative) is far below the
+// populations' own.
+__device__ __forceinline__ void dense_row32(const IBArgs &a, const double *rhs, const float *Ainv,
+                                            int ld, double *F, int row) {
+  __shared__ double red[kDenseThreads / 32][3];
+  const int n = a.n;
+  const int quarter = ld >> 2;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const float4 *Ar = reinterpret_cast<const float4 *>(Ainv + (size_t)row * ld);
+  const double2 *b0 = reinterpret_cast<const double2 *>(rhs);
+  const double2 *b1 = reinterpret_cast<const double2 *>(rhs + ld);
+  const double2 *b2 = reinterpret_cast<const double2 *>(rhs + 2 * ld);
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll 4
+  for (int h = threadIdx.x; h < quarter; h += kDenseThreads) {
+    const float4 v = __ldcs(Ar + h);
+    const double2 x0 = __ldg(b0 + 2 * h), y0 = __ldg(b0 + 2 * h + 1);
+    const double2 x1 = __ldg(b1 + 2 * h), y1 = __ldg(b1 + 2 * h + 1);
+    const double2 x2 = __ldg(b2 + 2 * h), y2 = __ldg(b2 + 2 * h + 1);
+    s0 += double(v.x) * x0.x + double(v.y) * x0.y + double(v.z) * y0.x + double(v.w) * y0.y;
+    s1 += double(v.x) * x1.x + double(v.y) * x1.y + double(v.z) * y1.x + double(v.w) * y1.y;
+    s2 += double(v.x) * x2.x + double(v.y) * x2.y + double(v.z) * y2.x + double(v.w) * y2.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if (lane == 0) {
+    red[wid][0] = s0;
+    red[wid][1] = s1;
+    red[wid][2] = s2;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double t = 0.0;
+    for (int w = 0; w < kDenseThreads / 32; ++w) t += red[w][threadIdx.x];
+    F[row + threadIdx.x * n] = X::add(F[row + threadIdx.x * n], t);
+  }
+}
+
+__global__ void __launch_bounds__(kDenseThreads) k_ivc_dense32(IBArgs a, const double *rhs,
+                                                               const float *Ainv, int ld, double *F) {
+  dense_row32(a, rhs, Ainv, ld, F, blockIdx.x);
+}
+
+// kDenseRows rows per block: every thread has the loads of all its rows in
+// flight at once and reads the right-hand side once for them, so the solve
+// takes a quarter of the waves of one row per block.  TA: double or float A^-1.
+constexpr int kDenseRows = 4;
+template <class TA>
+__global__ void __launch_bounds__(kDenseThreads) k_ivc_dense_rows(IBArgs a, const double *rhs,
+                                                                  const TA *Ainv, int ld, double *F) {
+  constexpr int V = 16 / (int)sizeof(TA);  // elements per 16-byte load
+  __shared__ double red[kDenseThreads / 32][kDenseRows * 3];
+  const int n = a.n, r0 = blockIdx.x * kDenseRows;
+  const int nr = min(kDenseRows, n - r0);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double acc[kDenseRows][3];
+#pragma unroll
+  for (int r = 0; r < kDenseRows; ++r) acc[r][0] = acc[r][1] = acc[r][2] = 0.0;
+  const int nv = ld / V;
+  for (int h = threadIdx.x; h < nv; h += kDenseThreads) {
+    double av[kDenseRows][V];
+#pragma unroll
+    for (int r = 0; r < kDenseRows; ++r) {
+      const int row = r0 + min(r, nr - 1);  // rows past the end repeat the last one (unused)
+      if (V == 2) {
+        const double2 v = __ldcs(reinterpret_cast<const double2 *>(Ainv + (size_t)row * ld) + h);
+        av[r][0] = v.x;
+        av[r][1] = v.y;
+      } else {
+        const float4 v = __ldcs(reinterpret_cast<const float4 *>(Ainv + (size_t)row * ld) + h);
+        av[r][0] = v.x;
+        av[r][1] = v.y;
+        av[r][V > 2 ? 2 : 0] = v.z;
+        av[r][V > 3 ? 3 : 0] = v.w;
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      const int col = h * V + e;
+      const double x0 = __ldg(rhs + col), x1 = __ldg(rhs + ld + col), x2 = __ldg(rhs + 2 * ld + col);
+#pragma unroll
+      for (int r = 0; r < kDenseRows; ++r) {
+        acc[r][0] += av[r][e] * x0;
+        acc[r][1] += av[r][e] * x1;
+        acc[r][2] += av[r][e] * x2;
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < kDenseRows; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      double x = acc[r][c];
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      if (lane == 0) red[wid][r * 3 + c] = x;
+    }
+  __syncthreads();
+  if ((int)threadIdx.x < nr * 3) {
+    const int r = threadIdx.x / 3, c = threadIdx.x % 3;
+    double t = 0.0;
+    for (int w = 0; w < kDenseThreads / 32; ++w) t += red[w][threadIdx.x];
+    F[r0 + r + c * n] = X::add(F[r0 + r + c * n], t);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_to_f32(const double *src, float *dst, int64_t n) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x)
+    dst[t] = float(src[t]);
+}
+
 // force_spreading_cic, :1331-1448 (dv folded in, 2D spreads x and y only);
 // one warp per marker, lanes over the stencil points, FP64 atomics
 __device__ __forceinline__ void spread_one(const IBArgs &a, int m, int lane, const double *xyz,
@@ -1103,6 +1232,7 @@ struct ilbm_ib {
   bool dense = false, dense_ready = false;
   int ld = 0;
   double *d_Ainv = nullptr, *d_gj = nullptr, *d_rhs = nullptr;
+  float *d_Ainv32 = nullptr;  // FP32 copy of A^-1 for the 4- and 2-byte storage forms
   bool fsum_deferred = false;  // marker force sum still to be launched (ib_finish)
   std::vector<void *> allocs;
 };
@@ -1504,7 +1634,7 @@ static int launch_cg(ilbm_ib *ib, const IBArgs &a_in, cudaStream_t s) {
   // FP32/FP16 populations, whose own rounding is ~1e-7
   const double cg_tol = (ctx->storage == ILBM_STORAGE_F64) ? 1.0e-14 : 1.0e-10;
   if (ib->n <= 1024) {
-    k_ivc_cg<<<1, 1024, 0, s>>>(a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_rowptr, ib->d_col,
+    k_ivc_cg<<<1, kCgThreads, 0, s>>>(a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_rowptr, ib->d_col,
                                 ib->d_val, ib->d_diag, ib->d_X, ib->d_work, ib->d_F, 500, cg_tol,
                                 ib->d_status, ib->d_iters, ib->cg_warm ? 1 : 0);
     ib->cg_warm = true;  // later solves start from this one
@@ -1607,9 +1737,18 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *
             k_gj_update<<<n, 256, 0, s>>>(ib->d_Ainv, n, ld, k, rowk, colk, ib->d_status);
           }
           ctx->launches += 1 + 2 * (int64_t)n;
+          if (ctx->storage != ILBM_STORAGE_F64) {
+            if (!ib->d_Ainv32 && (rc = dmalloc(ib, &ib->d_Ainv32, (size_t)n * ld))) return rc;
+            k_to_f32<<<1024, 256, 0, s>>>(ib->d_Ainv, ib->d_Ainv32, (int64_t)n * ld);
+            ctx->launches++;
+          }
           ib->dense_ready = true;
         }
-        k_ivc_dense<<<ib->n, kDenseThreads, 0, s>>>(a, ib->d_rhs, ib->d_Ainv, ib->ld, ib->d_F);
+        const int db = (ib->n + kDenseRows - 1) / kDenseRows;
+        if (ib->d_Ainv32)
+          k_ivc_dense_rows<float><<<db, kDenseThreads, 0, s>>>(a, ib->d_rhs, ib->d_Ainv32, ib->ld, ib->d_F);
+        else
+          k_ivc_dense_rows<double><<<db, kDenseThreads, 0, s>>>(a, ib->d_rhs, ib->d_Ainv, ib->ld, ib->d_F);
       } else if ((rc = launch_cg(ib, a, s))) {
         return rc;
       }
@@ -1820,6 +1959,7 @@ struct IBCase {
   int nnz_cap;
   double reg, cg_tol;
   const double *Ainv;
+  const float *Ainv32;  // used instead of Ainv when set
   double *rhs;
   int ld;
   const double *kin;  // per step: komega, cos, sin, 0
@@ -1907,7 +2047,7 @@ __global__ void __launch_bounds__(128) k_b_marker_warp(const IBCase *cs, const i
 }
 
 // one block per CG case: the CSR scan, or the whole solve
-__global__ void __launch_bounds__(1024) k_b_cg(const IBCase *cs, const int *cg_case, int stage,
+__global__ void __launch_bounds__(kCgThreads) k_b_cg(const IBCase *cs, const int *cg_case, int stage,
                                                const int *steps, const int *limit) {
   if (!live(steps, limit, cg_case[blockIdx.x])) return;
   const IBCase &k = cs[cg_case[blockIdx.x]];
@@ -1926,7 +2066,10 @@ __global__ void __launch_bounds__(kDenseThreads) k_b_dense(const IBCase *cs, con
   const int di = case_of(doff, nd, blockIdx.x);
   if (!live(steps, limit, dcase[di])) return;
   const IBCase &k = cs[dcase[di]];
-  dense_row(k.a, k.rhs, k.Ainv, k.ld, k.F, (int)(blockIdx.x - doff[di]));
+  if (k.Ainv32)
+    dense_row32(k.a, k.rhs, k.Ainv32, k.ld, k.F, (int)(blockIdx.x - doff[di]));
+  else
+    dense_row(k.a, k.rhs, k.Ainv, k.ld, k.F, (int)(blockIdx.x - doff[di]));
 }
 
 template <class R>
@@ -2134,6 +2277,7 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
     k.reg = ib->p.ivc_diag_reg;
     k.cg_tol = (ctx->storage == ILBM_STORAGE_F64) ? 1.0e-14 : 1.0e-10;
     k.Ainv = ib->d_Ainv;
+    k.Ainv32 = ib->d_Ainv32;
     k.rhs = ib->d_rhs;
     k.ld = ib->ld;
     if (ib->moving) {
@@ -2239,7 +2383,7 @@ int ib_batch_forcing(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
   ctx->launches++;
   if (b->any_rebuild) {
     k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 3, st, lm);
-    k_b_cg<<<b->ncg, 1024, 0, s>>>(b->d_cases, b->d_cgcase, 0, st, lm);
+    k_b_cg<<<b->ncg, kCgThreads, 0, s>>>(b->d_cases, b->d_cgcase, 0, st, lm);
     k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 4, st, lm);
     ctx->launches += 3;
   }
@@ -2249,7 +2393,7 @@ int ib_batch_forcing(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
     ctx->launches++;
   }
   if (b->ncg > 0) {
-    k_b_cg<<<b->ncg, 1024, 0, s>>>(b->d_cases, b->d_cgcase, 1, st, lm);
+    k_b_cg<<<b->ncg, kCgThreads, 0, s>>>(b->d_cases, b->d_cgcase, 1, st, lm);
     ctx->launches++;
   }
   if (b->any_explicit) {

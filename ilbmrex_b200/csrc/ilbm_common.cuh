@@ -185,6 +185,7 @@ struct Store<ILBM_STORAGE_F64> {
   using R = double;
   static constexpr bool shifted = false;
   __device__ static __forceinline__ R load(const T *p, float) { return *p; }
+  __device__ static __forceinline__ R cvt(T v, float) { return v; }
   __device__ static __forceinline__ void store(T *p, R v, float) { *p = v; }
 };
 
@@ -194,6 +195,7 @@ struct Store<ILBM_STORAGE_F32_SHIFT> {
   using R = float;
   static constexpr bool shifted = true;
   __device__ static __forceinline__ R load(const T *p, float) { return __ldg(p); }
+  __device__ static __forceinline__ R cvt(T v, float) { return v; }
   __device__ static __forceinline__ void store(T *p, R v, float) { *p = v; }
 };
 
@@ -204,6 +206,7 @@ struct Store<ILBM_STORAGE_F16_SCALED> {
   static constexpr bool shifted = true;
   // s: per-direction factor w_q / scale
   __device__ static __forceinline__ R load(const T *p, float s) { return __half2float(*p) * s; }
+  __device__ static __forceinline__ R cvt(T v, float s) { return __half2float(v) * s; }
   __device__ static __forceinline__ void store(T *p, R v, float s) { *p = __float2half_rn(v / s); }
 };
 
@@ -244,6 +247,10 @@ struct ilbm_ctx {
   // immersed-boundary chain
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_done = nullptr;
+  // device error word of the level-step kernels (bit 1: a bulk copy never
+  // completed); checked and cleared by ilbm_sync
+  int *d_flag = nullptr;
+  int sms = 0;
 };
 
 // grow ctx scratch to at least n bytes (returns nullptr on failure)

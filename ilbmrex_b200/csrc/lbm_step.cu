@@ -21,10 +21,12 @@
 // Traffic per cell: Q loads + Q stores of the storage type (plus the force
 // band); no scratch copies.
 #include <algorithm>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
 
+#include "bulk_copy.cuh"
 #include "ilbm_common.cuh"
 #include "step_args.cuh"
 
@@ -604,14 +606,145 @@ __global__ void __launch_bounds__(256, StepOcc<L, S>::value) k_step(const __grid
 }
 
 // ---------------------------------------------------------------------------
+// Level step fed by bulk copies (TMA), warp-specialised.  Persistent blocks
+// of W consumer threads plus one producer warp walk row segments of W cells.
+// The producer copies the Q plane-rows of f^n of each segment into a ring of
+// shared-memory stages (one bulk copy per plane, completing on the stage's
+// "full" mbarrier), up to STAGES segments ahead; a consumer waits for its
+// stage, takes its cell's populations from shared memory, arrives on the
+// stage's "empty" mbarrier (freeing the stage for the producer) and runs the
+// same cell_finish as k_step.  The loop has no block-wide barrier.
+// A plane-row copy starts at the 16-byte boundary at or below the segment and
+// ends on the next 16-byte boundary; the elements read beyond the segment
+// (fewer than 16 bytes each side) lie inside the grown box (ngrow_f >= 1).
+// With plane_aligned the plane stride is a multiple of 16 bytes and every
+// plane of a segment shares one offset.  The first `ghost_blocks` blocks
+// push the ghost shell instead.
+// ---------------------------------------------------------------------------
+// resident blocks of W + 32 threads per SM: 3 for the 4- and 2-byte storage
+// forms (<= 72 registers), 1 for FP64
+template <class L, int S>
+struct WsOcc {
+  static constexpr int value = (S != ILBM_STORAGE_F64) ? 3 : 1;
+};
+
+template <class L, int S, int STAGES>
+__global__ void __launch_bounds__(288, WsOcc<L, S>::value)
+    k_step_ws(const __grid_constant__ StepArgs a, int nitems, int nseg, int W, int segE,
+              int ghost_blocks, int plane_aligned, int *flag) {
+  using T = typename Store<S>::T;
+  using R = typename Store<S>::R;
+  constexpr int E = 16 / (int)sizeof(T);  // elements per 16 bytes
+  extern __shared__ __align__(128) unsigned char ws_smem[];
+  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
+  if ((int)blockIdx.x < ghost_blocks) {
+    if ((int)threadIdx.x < W)
+      ghost_push<L, S>(a, (int64_t)blockIdx.x * W + threadIdx.x, (int64_t)ghost_blocks * W);
+    return;
+  }
+  T *sm = reinterpret_cast<T *>(ws_smem);
+  const int pb = blockIdx.x - ghost_blocks, np = gridDim.x - ghost_blocks;
+  const int ny = a.rhi[1] - a.rlo[1] + 1;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], W);
+    }
+    mbar_init_fence();
+  }
+  __syncthreads();
+  auto seg_of = [&](int it, int &i0, int &j, int &k, int &len) {
+    const int sg = it % nseg, row = it / nseg;
+    i0 = a.rlo[0] + sg * W;
+    j = a.rlo[1] + row % ny;
+    k = a.rlo[2] + row / ny;
+    len = min(W, a.rhi[0] - i0 + 1);
+  };
+  if ((int)threadIdx.x >= W) {
+    // producer warp: lane 0 issues the copies, the other lanes are done
+    if ((int)threadIdx.x != W) return;
+    const T *fin = static_cast<const T *>(a.f_in);
+    for (int m = 0;; ++m) {
+      const int it = pb + m * np;
+      if (it >= nitems) break;
+      const int s = m % STAGES;
+      if (m >= STAGES && !mbar_wait_bounded(&empty[s], (uint32_t)(((m / STAGES) - 1) & 1))) {
+        atomicOr(flag, 1);
+        return;
+      }
+      int i0, j, k, len;
+      seg_of(it, i0, j, k, len);
+      T *dst = sm + (size_t)s * L::Q * segE;
+      const int64_t e0 = fidx(a, i0, j, k);
+      uint32_t total = 0;
+#pragma unroll
+      for (int q = 0; q < L::Q; ++q) {
+        const int off = (int)((e0 + a.loff[q]) & (E - 1));
+        total += (uint32_t)(((off + len + E - 1) / E) * E * (int)sizeof(T));
+      }
+      mbar_arrive_expect(&full[s], total);
+#pragma unroll
+      for (int q = 0; q < L::Q; ++q) {
+        const int64_t eq = e0 + a.loff[q];
+        const int off = (int)(eq & (E - 1));
+        bulk_g2s(dst + (size_t)q * segE, fin + (eq - off),
+                 (uint32_t)(((off + len + E - 1) / E) * E * (int)sizeof(T)), &full[s]);
+      }
+    }
+    return;
+  }
+  // consumers
+  const int t = threadIdx.x;
+  for (int m = 0;; ++m) {
+    const int it = pb + m * np;
+    if (it >= nitems) break;
+    const int s = m % STAGES;
+    if (!mbar_wait_bounded(&full[s], (uint32_t)((m / STAGES) & 1))) {
+      if (t == 0) atomicOr(flag, 1);
+      return;
+    }
+    int i0, j, k, len;
+    seg_of(it, i0, j, k, len);
+    const int i = i0 + t;
+    const bool mine = t < len && !(a.use_skip && in_box(a.slo, a.shi, i, j, k));
+    R f[L::Q];
+    if (mine) {
+      const T *src = sm + (size_t)s * L::Q * segE + t;
+      const int64_t e0 = fidx(a, i0, j, k);
+      if (plane_aligned) {
+        const int off = (int)(e0 & (E - 1));
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) f[q] = Store<S>::cvt(src[q * segE + off], sfac<L, S>(a, q));
+      } else {
+#pragma unroll
+        for (int q = 0; q < L::Q; ++q) {
+          const int off = (int)((e0 + a.loff[q]) & (E - 1));
+          f[q] = Store<S>::cvt(src[q * segE + off], sfac<L, S>(a, q));
+        }
+      }
+    }
+    mbar_arrive(&empty[s]);  // this thread is done with the stage
+    if (mine) cell_finish<L, S>(a, i, j, k, needs_fixup<L>(a, i, j, k), f);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Batched level step: many independent cases (each one box = its level
 // domain, self-filled ghosts) in one persistent launch.  Blocks walk a tile
 // table of row segments and ghost-push chunks over all cases; the arguments
 // of a tile's case are copied to shared memory, so the per-direction offsets
 // stay on chip and cannot alias the population stores.
 // ---------------------------------------------------------------------------
+// the batched step's occupancy target: 5 blocks of 256 (48 registers) for
+// D2Q9 in the 4- and 2-byte forms (measured 5% faster on the 64-case D2Q9
+// batch than 4), as k_step otherwise
 template <class L, int S>
-__global__ void __launch_bounds__(256, StepOcc<L, S>::value)
+struct BatchOcc {
+  static constexpr int value = (S != ILBM_STORAGE_F64 && L::Q <= 9) ? 5 : StepOcc<L, S>::value;
+};
+
+template <class L, int S>
+__global__ void __launch_bounds__(256, BatchOcc<L, S>::value)
     k_step_batch(const StepArgs *__restrict__ args, const StepTile *__restrict__ tiles, int ntiles,
                  const int *steps, const int *limit) {
   __shared__ StepArgs sa;
@@ -951,6 +1084,73 @@ static int64_t ghost_work(const StepArgs &a) {
   return n;
 }
 
+// stages of the bulk-copy level step: ILBM_PIPE_STAGES = 0 (default: plain
+// k_step, measured faster on B200 for the D3Q19 FP32 sphere level), 2 or 3
+static int pipe_stages() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = std::getenv("ILBM_PIPE_STAGES");
+    v = e ? std::atoi(e) : 0;
+    if (v != 0 && v != 2 && v != 3) v = 0;
+  }
+  return v;
+}
+
+template <class L, int S, int ST>
+static bool launch_ws_n(ilbm_ctx *ctx, const StepArgs &a, cudaStream_t st, bool with_ghosts) {
+  using T = typename Store<S>::T;
+  constexpr int E = 16 / (int)sizeof(T);
+  const int nx = a.rhi[0] - a.rlo[0] + 1, ny = a.rhi[1] - a.rlo[1] + 1;
+  const int nz = (L::D == 3) ? a.rhi[2] - a.rlo[2] + 1 : 1;
+  const int W = nx >= 256 ? 256 : ((nx + 31) / 32) * 32;
+  const int segE = W + 2 * E;
+  const size_t smem = (size_t)ST * L::Q * segE * sizeof(T);
+  if (smem > 200 * 1024) return false;
+  // the copies reach fewer than E elements beyond either end of a row
+  // segment: inside the grown box as long as a row plus its ghost is longer
+  if (a.fs0 < E) return false;
+  static int attr_set[64] = {0};  // the attribute is per device; setting it twice is harmless
+  const int dev = ctx->device & 63;
+  if (!attr_set[dev]) {
+    if (cudaFuncSetAttribute(k_step_ws<L, S, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             200 * 1024) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    attr_set[dev] = 1;
+  }
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_ws<L, S, ST>, W + 32, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (occ < 1) return false;
+  const int nseg = (nx + W - 1) / W;
+  const int nitems = nseg * ny * nz;
+  int ghost_blocks = 0;
+  if (with_ghosts) {
+    const int64_t w = ghost_work<L>(a);
+    ghost_blocks = (int)std::min<int64_t>(512, (w + W - 1) / W);
+  }
+  const int plane_aligned = (a.fs2 % E) == 0 ? 1 : 0;
+  const int pipes = std::max(1, std::min(nitems, occ * ctx->sms));
+  k_step_ws<L, S, ST><<<ghost_blocks + pipes, W + 32, smem, st>>>(a, nitems, nseg, W, segE, ghost_blocks,
+                                                                    plane_aligned, ctx->d_flag);
+  ctx->launches++;
+  return true;
+}
+
+// the level step of [rlo, rhi] through k_step_ws when it applies (f_in on a
+// 16-byte boundary); false: the caller uses k_step
+template <class L, int S>
+static bool launch_ws(ilbm_ctx *ctx, const StepArgs &a, cudaStream_t st, bool with_ghosts) {
+  if ((reinterpret_cast<uintptr_t>(a.f_in) & 15) != 0) return false;
+  const int ns = pipe_stages();
+  if (ns == 3) return launch_ws_n<L, S, 3>(ctx, a, st, with_ghosts);
+  if (ns == 2) return launch_ws_n<L, S, 2>(ctx, a, st, with_ghosts);
+  return false;
+}
+
 // k_step over [rlo, rhi] (minus the skip box), with the ghost shell push in
 // leading z-slices when with_ghosts is set
 template <class L, int S>
@@ -976,7 +1176,7 @@ static void launch_cells(ilbm_ctx *ctx, const StepArgs &a_in, cudaStream_t st, b
 template <class L, int S>
 static int launch_step(ilbm_ctx *ctx, const StepArgs &a, const ilbm_level_params *p) {
   (void)p;
-  launch_cells<L, S>(ctx, a, ctx->stream, true);
+  if (!launch_ws<L, S>(ctx, a, ctx->stream, true)) launch_cells<L, S>(ctx, a, ctx->stream, true);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "level step launch");
   return ILBM_OK;
@@ -993,7 +1193,7 @@ static int launch_step_split(ilbm_ctx *ctx, const StepArgs &a, const int *blo, c
     outer.slo[d] = blo[d];
     outer.shi[d] = bhi[d];
   }
-  launch_cells<L, S>(ctx, outer, ctx->stream, true);
+  if (!launch_ws<L, S>(ctx, outer, ctx->stream, true)) launch_cells<L, S>(ctx, outer, ctx->stream, true);
   cudaError_t e = cudaStreamWaitEvent(ctx->stream, band_ready, 0);
   if (e != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
   StepArgs inner = a;
@@ -1299,9 +1499,12 @@ int ilbm_create(const ilbm_lattice *lat, int storage, int device, void *cuda_str
     }
   }
   e = cudaMallocHost(&c->host_pinned, 64 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_flag, 16);
+  if (e == cudaSuccess) e = cudaMemset(c->d_flag, 0, 16);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
   if (e != cudaSuccess) {
     ilbm_destroy(c);
-    return cuda_fail(e, "cudaMallocHost");
+    return cuda_fail(e, "ilbm_create");
   }
   *out = c;
   return ILBM_OK;
@@ -1318,6 +1521,7 @@ int ilbm_destroy(ilbm_ctx *ctx) {
   delete[] ctx->xev;
   if (ctx->scratch) cudaFree(ctx->scratch);
   if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
+  if (ctx->d_flag) cudaFree(ctx->d_flag);
   if (ctx->side) {
     cudaStreamSynchronize(ctx->side);
     cudaStreamDestroy(ctx->side);
@@ -1334,6 +1538,14 @@ int ilbm_sync(ilbm_ctx *ctx) {
   if (!ctx) return ILBM_ERR_ARG;
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "stream synchronize");
+  int flag = 0;
+  e = cudaMemcpy(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "level-step status");
+  if (flag) {
+    cudaMemset(ctx->d_flag, 0, sizeof(int));
+    set_error("level step: a bulk copy into shared memory did not complete (step abandoned)");
+    return ILBM_ERR_CUDA;
+  }
   return ILBM_OK;
 }
 
