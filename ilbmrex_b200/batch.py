@@ -43,11 +43,12 @@ class Batch:
         return s
 
     def add(self, s: LevelSolver, max_steps: int) -> int:
-        """Joins a solver to the batch (after its first step, taken here if
-        needed); returns the case id."""
+        """Joins a solver to the batch (after its first step, or its first step
+        since a restart when it has a body, taken here if needed); returns the
+        case id."""
         if s.ctx is not self.ctx:
             raise capi.IlbmError("the solver must be built on the batch's context (Batch.solver)")
-        if s.istep == 0:
+        if s.istep == 0 or (s.ib is not None and not s.ib_ready):
             s.advance_phi_at_level(record_force=s.ib is not None)
         b = s._box(s.f, s.f_next, force=s.force_cur if s.ib is not None else None,
                    force_prev=s.force_prev if s.ib is not None else None)

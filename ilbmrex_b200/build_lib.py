@@ -45,7 +45,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     objdir = LIBDIR / "obj"
     objdir.mkdir(exist_ok=True)
     srcs = sorted(CSRC.glob("*.cu"))
-    deps = sorted(CSRC.glob("*.cuh")) + [INCLUDE / "ilbm_b200.h"]
+    deps = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [INCLUDE / "ilbm_b200.h"]
     dep_mtime = max(p.stat().st_mtime for p in deps)
     jobs = []
     for s in srcs:

@@ -16,6 +16,8 @@ MAXQ = 27
 ILBM_OK = 0
 ILBM_ERR_ARG, ILBM_ERR_CUDA, ILBM_ERR_UNSUPPORTED = -1, -2, -3
 ILBM_ERR_NOMEM, ILBM_ERR_SOLVER, ILBM_ERR_RANGE = -4, -5, -6
+ILBM_ERR_IO = -7
+CKPT_MACRO, CKPT_FORCE, CKPT_BODY = 1, 2, 4
 STORAGE = {"f64": 0, "f32": 1, "f16": 2}
 GHOST_SELF, GHOST_CALLER = 0, 1
 IVC_AUTO, IVC_CG, IVC_DENSE = 0, 1, 2
@@ -35,6 +37,8 @@ EXPORTS = [
     "ilbm_batch_create", "ilbm_batch_destroy", "ilbm_batch_add", "ilbm_batch_remove",
     "ilbm_batch_step", "ilbm_batch_case_state", "ilbm_batch_records", "ilbm_batch_set_tiles",
     "ilbm_batch_tune", "ilbm_batch_size", "ilbm_batch_progress",
+    "ilbm_derived_fields", "ilbm_tag_cells",
+    "ilbm_checkpoint_write", "ilbm_checkpoint_read", "ilbm_plotfile_write",
 ]
 
 
@@ -93,6 +97,18 @@ class IBParams_t(C.Structure):
                 ("pivot_x", C.c_double)]
 
 
+class CheckpointMeta_t(C.Structure):
+    _fields_ = [("istep", C.c_int64), ("time", C.c_double), ("user", C.c_double * 16),
+                ("flags", C.c_int)]
+
+
+class PlotInfo_t(C.Structure):
+    _fields_ = [("prob_lo", C.c_double * 3), ("prob_hi", C.c_double * 3), ("dx", C.c_double * 3),
+                ("time", C.c_double), ("istep", C.c_int), ("levelset", C.c_int),
+                ("ls_center", C.c_double * 3), ("ls_radius", C.c_double),
+                ("body_u", C.c_double * 3)]
+
+
 class IlbmError(RuntimeError):
     pass
 
@@ -147,7 +163,14 @@ def lib():
         "ilbm_batch_set_tiles": (I, [P, I, I]),
         "ilbm_batch_tune": (I, [P, I, C.POINTER(I), C.POINTER(I), C.POINTER(C.c_float)]),
         "ilbm_batch_size": (I, [P, C.POINTER(I), C.POINTER(I64)]),
+        "ilbm_derived_fields": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P, P, dp, P, P, dp]),
+        "ilbm_tag_cells": (I, [P, C.POINTER(Box_t), P, D, I, dp, dp, D, D, dp, dp, dp, dp, P,
+                               C.POINTER(I64)]),
         "ilbm_batch_progress": (I, [P, I, C.POINTER(I), C.POINTER(I64), C.POINTER(I), C.POINTER(I)]),
+        "ilbm_checkpoint_write": (I, [P, C.POINTER(Box_t), P, C.POINTER(CheckpointMeta_t), C.c_char_p]),
+        "ilbm_checkpoint_read": (I, [P, C.POINTER(Box_t), P, C.POINTER(CheckpointMeta_t), C.c_char_p]),
+        "ilbm_plotfile_write": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t),
+                                    C.POINTER(PlotInfo_t), C.c_char_p]),
         "ilbm_momentum_exchange": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P,
                                        D, D, D, D, dp, dp, I, dp]),
     }

@@ -115,6 +115,10 @@ class MarkerIB:
     U0: float = 0.1
     # pitching NACA (Examples/Pitching_airfoil/IBMUserDefinedGeometry.H:14-20)
     airfoil: tuple | None = None  # (chord, thickness, mean, amplitude, frequency, phase, pivot_x)
+    # refinement box around the body in radii (MarkerIBParams.H:86-88; <= 0: R + padding)
+    refine_upstream: float = -1.0
+    refine_downstream: float = -1.0
+    refine_cross: float = -1.0
 
     AIRFOIL_DEFAULT = (20.0, 0.12, 0.0, 0.2617993877991494, 0.0015, 0.0, 0.0)
 

@@ -25,6 +25,7 @@
 #include <cooperative_groups.h>
 
 #include "ilbm_common.cuh"
+#include "state_internal.h"
 
 namespace cgrp = cooperative_groups;
 
@@ -1930,6 +1931,26 @@ int ilbm_ib_markers(ilbm_ib *ib, double *xyz, double *uvw, double *force) {
 }
 
 }  // extern "C"
+
+namespace ilbm {
+
+void ib_state(ilbm_ib *ib, IBState *out) {
+  out->n = ib->n;
+  out->dim = ib->dim;
+  out->geometry = ib->p.geometry_type;
+  out->coupling = ib->p.coupling_method;
+  out->xyz = ib->d_xyz;
+  out->uvw = ib->d_uvw;
+  out->F = ib->d_F;
+  out->fsum = ib->d_fsum;
+  out->X = ib->d_X;
+  out->cg_warm = ib->cg_warm;
+}
+
+void ib_set_cg_warm(ilbm_ib *ib, bool warm) { ib->cg_warm = warm && ib->d_X != nullptr; }
+
+}  // namespace ilbm
+
 
 // ---------------------------------------------------------------------------
 // Batched update_forcing for the batch engine (batch.cu): every stage runs as

@@ -231,6 +231,7 @@ struct ilbm_ctx {
   int q = 0;
   int dim = 0;
   int storage = 0;
+  double w[27] = {};  // lattice weights w_q (wis / wim)
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;

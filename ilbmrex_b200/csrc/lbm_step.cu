@@ -1409,6 +1409,149 @@ int batch_step_occupancy(const ilbm_ctx *ctx, int w, int *per_sm) {
   return ILBM_DISPATCH(ctx, occupancy_step_batch, ctx, w, per_sm);
 }
 
+// ---- derived fields and refinement tags ------------------------------------
+// UpdateDerivedMacroFields / visPara (Source/Core/AmrCoreLBM.cpp:105-168,
+// Source/LBM/visPara.H:10-54): vorticity from central differences of the
+// FillPatched velocity (2D: dv/dx - du/dy; 3D: |curl u|) and pressure
+// (rho - 1)/3 on valid cells; the band macro over the box grown by one gives
+// the ghost values with the FillPatch rules.  Also the level maximum of the
+// vorticity (ErrorEst's vortMax, AmrCoreLBM.cpp:1047) as block partials.
+struct DeriveArgs {
+  int dim;
+  int lo[3], hi[3];
+  int blo[3], bn[3];
+  int64_t nb;
+  int mgl[3];
+  int64_t ms0, ms1;
+  double dx[3];
+};
+
+__device__ __forceinline__ double ev_at(const DeriveArgs &d, const double *EV, int c, int i, int j, int k) {
+  return EV[(int64_t)c * d.nb + (i - d.blo[0]) + (int64_t)(j - d.blo[1]) * d.bn[0] +
+            (int64_t)(k - d.blo[2]) * d.bn[0] * d.bn[1]];
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_derive(DeriveArgs d, const double *EV, const double *RHO,
+                                                R *vor, R *pres, double *bmax) {
+  __shared__ double sh[8];
+  const int nx = d.hi[0] - d.lo[0] + 1, ny = d.hi[1] - d.lo[1] + 1;
+  const int nz = (d.dim == 3) ? d.hi[2] - d.lo[2] + 1 : 1;
+  const int64_t n = (int64_t)nx * ny * nz;
+  double mx = -1.0e300;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = d.lo[0] + (int)(t % nx), j = d.lo[1] + (int)((t / nx) % ny);
+    const int k = (d.dim == 3) ? d.lo[2] + (int)(t / ((int64_t)nx * ny)) : 0;
+    const double dv_dx = X::div(X::sub(ev_at(d, EV, 1, i + 1, j, k), ev_at(d, EV, 1, i - 1, j, k)),
+                                X::mul(2.0, d.dx[0]));
+    const double du_dy = X::div(X::sub(ev_at(d, EV, 0, i, j + 1, k), ev_at(d, EV, 0, i, j - 1, k)),
+                                X::mul(2.0, d.dx[1]));
+    double w;
+    if (d.dim == 3) {
+      const double du_dz = X::div(X::sub(ev_at(d, EV, 0, i, j, k + 1), ev_at(d, EV, 0, i, j, k - 1)),
+                                  X::mul(2.0, d.dx[2]));
+      const double dw_dx = X::div(X::sub(ev_at(d, EV, 2, i + 1, j, k), ev_at(d, EV, 2, i - 1, j, k)),
+                                  X::mul(2.0, d.dx[0]));
+      const double dv_dz = X::div(X::sub(ev_at(d, EV, 1, i, j, k + 1), ev_at(d, EV, 1, i, j, k - 1)),
+                                  X::mul(2.0, d.dx[2]));
+      const double dw_dy = X::div(X::sub(ev_at(d, EV, 2, i, j + 1, k), ev_at(d, EV, 2, i, j - 1, k)),
+                                  X::mul(2.0, d.dx[1]));
+      const double ox = X::sub(dw_dy, dv_dz), oy = X::sub(du_dz, dw_dx), oz = X::sub(dv_dx, du_dy);
+      w = __dsqrt_rn(X::add(X::add(X::mul(ox, ox), X::mul(oy, oy)), X::mul(oz, oz)));
+    } else {
+      w = X::sub(dv_dx, du_dy);
+    }
+    const int64_t m = (int64_t)(i - d.mgl[0]) + (int64_t)(j - d.mgl[1]) * d.ms0 +
+                      (int64_t)(k - d.mgl[2]) * d.ms1;
+    const int64_t b = (i - d.blo[0]) + (int64_t)(j - d.blo[1]) * d.bn[0] +
+                      (int64_t)(k - d.blo[2]) * d.bn[0] * d.bn[1];
+    if (vor) vor[m] = R(w);
+    if (pres) pres[m] = R(X::div(X::sub(RHO[b], 1.0), 3.0));
+    mx = fmax(mx, w);
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = sh[0];
+    for (int w2 = 1; w2 < (int)(blockDim.x >> 5); ++w2) t = fmax(t, sh[w2]);
+    bmax[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_max_final(const double *bmax, int nb, double *out) {
+  if (threadIdx.x == 0) {
+    double t = -1.0e300;
+    for (int b = 0; b < nb; ++b) t = fmax(t, bmax[b]);
+    *out = t;
+  }
+}
+
+// ErrorEst tagging (AmrCoreLBM.cpp:1145-1180, Tagging.H:12-18) on valid
+// cells: cleared inside the no-refine x zones, set where |vorticity| >
+// threshold or inside the body refinement box; tags[i + nx*(j + ny*k)].
+struct TagArgs {
+  int dim;
+  int lo[3], hi[3];
+  int mgl[3];
+  int64_t ms0, ms1;
+  double threshold;
+  int use_box;
+  double box_lo[3], box_hi[3];
+  double nr_lo, nr_hi;
+  double plo[3], phi[3], dx[3];
+  int use_ls;                  // level-set band of a cylinder / sphere body
+  double ls_c[3], ls_r, ls_band;
+};
+
+template <class R>
+__global__ void __launch_bounds__(256) k_tags(TagArgs g, const R *vor, unsigned char *tags,
+                                              unsigned long long *count) {
+  const int nx = g.hi[0] - g.lo[0] + 1, ny = g.hi[1] - g.lo[1] + 1;
+  const int nz = (g.dim == 3) ? g.hi[2] - g.lo[2] + 1 : 1;
+  const int64_t n = (int64_t)nx * ny * nz;
+  unsigned long long mine = 0;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = g.lo[0] + (int)(t % nx), j = g.lo[1] + (int)((t / nx) % ny);
+    const int k = (g.dim == 3) ? g.lo[2] + (int)(t / ((int64_t)nx * ny)) : 0;
+    const double x = X::add(g.plo[0], X::mul(X::add(double(i), 0.5), g.dx[0]));
+    unsigned char tag = 0;
+    bool blocked = false;
+    if (g.nr_lo > 0.0 || g.nr_hi > 0.0)
+      blocked = (x <= X::add(g.plo[0], g.nr_lo)) || (x >= X::sub(g.phi[0], g.nr_hi));
+    if (!blocked) {
+      const int64_t m = (int64_t)(i - g.mgl[0]) + (int64_t)(j - g.mgl[1]) * g.ms0 +
+                        (int64_t)(k - g.mgl[2]) * g.ms1;
+      if (fabs(double(vor[m])) > g.threshold) tag = 1;
+      if (g.use_ls) {
+        // signed distance at the cell centre, as LevelSetManager builds it
+        const double y = X::add(g.plo[1], X::mul(X::add(double(j), 0.5), g.dx[1]));
+        const double ex = X::sub(x, g.ls_c[0]), ey = X::sub(y, g.ls_c[1]);
+        double r2 = X::add(X::mul(ex, ex), X::mul(ey, ey));
+        if (g.dim == 3) {
+          const double z = X::add(g.plo[2], X::mul(X::add(double(k), 0.5), g.dx[2]));
+          const double ez = X::sub(z, g.ls_c[2]);
+          r2 = X::add(r2, X::mul(ez, ez));
+        }
+        if (X::sub(__dsqrt_rn(r2), g.ls_r) < g.ls_band) tag = 1;
+      }
+      if (g.use_box) {
+        const double y = X::add(g.plo[1], X::mul(X::add(double(j), 0.5), g.dx[1]));
+        const double z = (g.dim == 3) ? X::add(g.plo[2], X::mul(X::add(double(k), 0.5), g.dx[2])) : 0.0;
+        if (x >= g.box_lo[0] && x <= g.box_hi[0] && y >= g.box_lo[1] && y <= g.box_hi[1] &&
+            z >= g.box_lo[2] && z <= g.box_hi[2])
+          tag = 1;
+      }
+    }
+    tags[t] = tag;
+    mine += tag;
+  }
+  for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(0xffffffffu, mine, o);
+  if ((threadIdx.x & 31) == 0 && mine) atomicAdd(count, mine);
+}
+
 }  // namespace ilbm
 
 using namespace ilbm;
@@ -1464,6 +1607,7 @@ int ilbm_create(const ilbm_lattice *lat, int storage, int device, void *cuda_str
   if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
   auto *c = new ilbm_ctx();
   c->q = lat->q;
+  for (int q = 0; q < lat->q; ++q) c->w[q] = lat->wis[q] / lat->wim[q];
   c->dim = dim;
   c->storage = storage;
   c->device = device;
@@ -1707,6 +1851,146 @@ int ilbm_init_equilibrium(ilbm_ctx *ctx, const ilbm_box *box) {
   int rc = fill_args(ctx, *box, nullptr, a);
   if (rc) return rc;
   return ILBM_DISPATCH(ctx, launch_init, ctx, a, box->ngrow_f);
+}
+
+
+int ilbm_derived_fields(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
+                        const void *f, const void *force_prev, const double dx[3], void *vor,
+                        void *pres, double *vort_max) {
+  if (!ctx || !box || !p || !f || !dx) {
+    set_error("ilbm_derived_fields: null argument");
+    return ILBM_ERR_ARG;
+  }
+  int rc = check_params(ctx, p);
+  if (rc) return rc;
+  if (p->ghost_mode != ILBM_GHOST_SELF) {
+    set_error("ilbm_derived_fields: needs self-filled ghosts (one box equal to the domain)");
+    return ILBM_ERR_UNSUPPORTED;
+  }
+  for (int d = 0; d < ctx->dim; ++d)
+    if (box->lo[d] != p->domain_lo[d] || box->hi[d] != p->domain_hi[d]) {
+      set_error("ilbm_derived_fields: the box must equal the domain");
+      return ILBM_ERR_ARG;
+    }
+  if ((vor || pres) && (box->mstride[0] <= 0 || box->mstride[1] <= 0)) {
+    set_error("ilbm_derived_fields: macro strides must be positive");
+    return ILBM_ERR_ARG;
+  }
+  ilbm_box b = *box;
+  b.f_in = const_cast<void *>(f);
+  b.f_out = nullptr;
+  b.macro_in = nullptr;
+  b.force_prev = const_cast<void *>(force_prev);
+  DeriveArgs d;
+  std::memset(&d, 0, sizeof(d));
+  d.dim = ctx->dim;
+  int64_t nb = 1, ncell = 1;
+  int blo[3] = {0, 0, 0}, bn[3] = {1, 1, 1};
+  for (int q = 0; q < 3; ++q) {
+    d.lo[q] = (q < ctx->dim) ? box->lo[q] : 0;
+    d.hi[q] = (q < ctx->dim) ? box->hi[q] : 0;
+    d.mgl[q] = (q < ctx->dim) ? box->lo[q] - box->ngrow_m : 0;
+    if (q < ctx->dim) {
+      blo[q] = box->lo[q] - 1;
+      bn[q] = box->hi[q] - box->lo[q] + 3;
+    }
+    d.blo[q] = blo[q];
+    d.bn[q] = bn[q];
+    nb *= bn[q];
+    ncell *= (d.hi[q] - d.lo[q] + 1);
+  }
+  d.nb = nb;
+  d.ms0 = box->mstride[0];
+  d.ms1 = box->mstride[1];
+  for (int q = 0; q < 3; ++q) d.dx[q] = dx[q];  // the level's xCellSize, yCellSize, zCellSize
+  const int blocks = (int)std::min<int64_t>((ncell + 255) / 256, 1184);
+  double *scr = static_cast<double *>(ilbm_ctx_scratch(ctx, (4 * nb + blocks + 8) * sizeof(double)));
+  if (!scr) {
+    set_error("ilbm_derived_fields: scratch allocation failed");
+    return ILBM_ERR_NOMEM;
+  }
+  double *EV = scr, *RHO = scr + 3 * nb, *bmax = scr + 4 * nb, *out = bmax + blocks;
+  if ((rc = band_macro(ctx, b, p, blo, bn, EV, RHO, ctx->stream))) return rc;
+  if (ctx->storage == ILBM_STORAGE_F64)
+    k_derive<double><<<blocks, 256, 0, ctx->stream>>>(d, EV, RHO, static_cast<double *>(vor),
+                                                      static_cast<double *>(pres), bmax);
+  else
+    k_derive<float><<<blocks, 256, 0, ctx->stream>>>(d, EV, RHO, static_cast<float *>(vor),
+                                                     static_cast<float *>(pres), bmax);
+  k_max_final<<<1, 32, 0, ctx->stream>>>(bmax, blocks, out);
+  ctx->launches += 2;
+  double mx = 0.0;
+  cudaMemcpyAsync(&mx, out, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_derived_fields");
+  if (vort_max) *vort_max = mx;
+  return ILBM_OK;
+}
+
+int ilbm_tag_cells(ilbm_ctx *ctx, const ilbm_box *box, const void *vor, double threshold,
+                   int use_box, const double box_lo[3], const double box_hi[3],
+                   double no_refine_xlo, double no_refine_xhi, const double prob_lo[3],
+                   const double prob_hi[3], const double dx[3], const double *levelset,
+                   void *tags, int64_t *ntagged) {
+  if (!ctx || !box || !vor || !tags || !prob_lo || !prob_hi || !dx || (use_box && (!box_lo || !box_hi))) {
+    set_error("ilbm_tag_cells: null argument");
+    return ILBM_ERR_ARG;
+  }
+  TagArgs g;
+  std::memset(&g, 0, sizeof(g));
+  g.dim = ctx->dim;
+  int64_t ncell = 1;
+  for (int q = 0; q < 3; ++q) {
+    g.lo[q] = (q < ctx->dim) ? box->lo[q] : 0;
+    g.hi[q] = (q < ctx->dim) ? box->hi[q] : 0;
+    g.mgl[q] = (q < ctx->dim) ? box->lo[q] - box->ngrow_m : 0;
+    ncell *= (g.hi[q] - g.lo[q] + 1);
+    g.plo[q] = prob_lo[q];
+    g.phi[q] = prob_hi[q];
+    g.dx[q] = dx[q];
+    if (use_box) {
+      g.box_lo[q] = box_lo[q];
+      g.box_hi[q] = box_hi[q];
+    }
+  }
+  g.ms0 = box->mstride[0];
+  g.ms1 = box->mstride[1];
+  g.threshold = threshold;
+  g.use_box = use_box;
+  g.nr_lo = no_refine_xlo;
+  g.nr_hi = no_refine_xhi;
+  if (levelset) {
+    if (!(levelset[4] >= 0.0) || !(levelset[5] > 0.0)) {
+      set_error("ilbm_tag_cells: level-set band cells must be >= 0 and dx_min > 0");
+      return ILBM_ERR_ARG;
+    }
+    g.use_ls = 1;
+    for (int q = 0; q < 3; ++q) g.ls_c[q] = levelset[q];
+    g.ls_r = levelset[3];
+    // (n_cells_band + 0.5) * dx_min
+    g.ls_band = (std::floor(levelset[4]) + 0.5) * levelset[5];
+  }
+  unsigned long long *cnt =
+      static_cast<unsigned long long *>(ilbm_ctx_scratch(ctx, 8 * sizeof(unsigned long long)));
+  if (!cnt) {
+    set_error("ilbm_tag_cells: scratch allocation failed");
+    return ILBM_ERR_NOMEM;
+  }
+  cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), ctx->stream);
+  const int blocks = (int)std::min<int64_t>((ncell + 255) / 256, 1184);
+  if (ctx->storage == ILBM_STORAGE_F64)
+    k_tags<double><<<blocks, 256, 0, ctx->stream>>>(g, static_cast<const double *>(vor),
+                                                    static_cast<unsigned char *>(tags), cnt);
+  else
+    k_tags<float><<<blocks, 256, 0, ctx->stream>>>(g, static_cast<const float *>(vor),
+                                                   static_cast<unsigned char *>(tags), cnt);
+  ctx->launches++;
+  unsigned long long h = 0;
+  cudaMemcpyAsync(&h, cnt, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_tag_cells");
+  if (ntagged) *ntagged = (int64_t)h;
+  return ILBM_OK;
 }
 
 }  // extern "C"

@@ -133,6 +133,39 @@ class Context:
             pass
 
 
+def refinement_region(case: LevelCase, ib: MarkerIB):
+    """The body refinement box of ErrorEst in physical coordinates, or None
+    (immersed_boundary_refinement_region, Source/Core/AmrCoreLBM.cpp:56-100;
+    the pitching-airfoil hook, Examples/Pitching_airfoil/
+    IBMUserDefinedGeometry.H:25-57, with the leading edge moved by pivot_x)."""
+    dx = case.dx
+    pad = max(6.0 * dx, 2.0)
+    if ib.geometry_type == 1:
+        lo = (ib.box_xlo - pad, (ib.box_yhi - pad) if ib.box_lid_only > 0 else (ib.box_ylo - pad),
+              ib.box_zlo - pad)
+        hi = (ib.box_xhi + pad, ib.box_yhi + pad, ib.box_zhi + pad)
+        return lo, hi
+    if ib.geometry_type == 2:
+        if case.dim != 2:
+            return None
+        af = ib.airfoil if ib.airfoil is not None else MarkerIB.AIRFOIL_DEFAULT
+        chord = max(af[0], 1.0e-12)
+        half_t = 0.5 * af[1] * chord
+        y_ext = chord * math.sin(abs(af[3])) + half_t
+        le = ib.x0 - af[6]
+        return (le - pad, ib.y0 - y_ext - pad, ib.z0 - pad), (le + chord + pad, ib.y0 + y_ext + pad, ib.z0 + pad)
+    R = ib.R
+    if R <= 0.0:
+        return None
+    if ib.refine_upstream > 0 and ib.refine_downstream > 0 and ib.refine_cross > 0:
+        return ((ib.x0 - ib.refine_upstream * R - pad, ib.y0 - ib.refine_cross * R - pad,
+                 ib.z0 - ib.refine_cross * R - pad),
+                (ib.x0 + ib.refine_downstream * R + pad, ib.y0 + ib.refine_cross * R + pad,
+                 ib.z0 + ib.refine_cross * R + pad))
+    return ((ib.x0 - R - pad, ib.y0 - R - pad, ib.z0 - R - pad),
+            (ib.x0 + R + pad, ib.y0 + R + pad, ib.z0 + R + pad))
+
+
 def ib_footprint(case: LevelCase, ib: MarkerIB) -> int:
     """Estimated device bytes of an IB object: band arrays (10 doubles per
     cell of the support band), marker arrays and the IVC operator (stored
@@ -200,6 +233,7 @@ class LevelSolver:
         self.have_prev_body = False
         self.prev_body = np.zeros(3)
         self.rec = np.zeros(18)
+        self.ib_ready = False  # the body's IVC operator is built by its first step
 
     # ---- layout helpers ---------------------------------------------------
     def _box(self, f_in, f_out, macro_in=None, macro_out=None, force=None, force_prev=None):
@@ -275,6 +309,7 @@ class LevelSolver:
         self.f, self.f_next = self.f_next, self.f
         self.force_cur, self.force_prev = self.force_prev, self.force_cur
         self.first_step_macro = False
+        self.ib_ready = ib_on
         self.time += self.case.dt
         self.istep += 1
         if record_force and ib_on:
@@ -344,6 +379,110 @@ class LevelSolver:
                                              out.data_ptr(), None, None), "compute_macro")
         self.ctx.sync()
         return self._valid(out, self.gm).to(torch.float64).cpu().numpy()
+
+    # ---- derived fields and refinement tags (UpdateDerivedMacroFields, ErrorEst)
+    def derived_fields(self):
+        """(vorticity, pressure, max vorticity) of the current state on valid
+        cells (device tensors kept in self.vor / self.pres)."""
+        self.vor = torch.zeros_like(self.macro[0])
+        self.pres = torch.zeros_like(self.macro[0])
+        b = self._box(self.f, None)
+        force = self.force_prev if self.ib is not None else None
+        vmax = C.c_double()
+        capi.check(self.L.ilbm_derived_fields(self.ctx.h, C.byref(b), C.byref(self.params),
+                                              self.f.data_ptr(),
+                                              force.data_ptr() if force is not None else None,
+                                              capi.dvec3([self.case.dx] * 3), self.vor.data_ptr(),
+                                              self.pres.data_ptr(), C.byref(vmax)), "derived_fields")
+        to_np = lambda t: self._valid(t, self.gm).to(torch.float64).cpu().numpy()
+        return to_np(self.vor), to_np(self.pres), vmax.value
+
+    def tag_cells(self, threshold_ratio: float = 1.0, refine_box=True, no_refine=(0.0, 0.0),
+                  levelset=True, n_cells_band: int = 5):
+        """ErrorEst tags of the current state: (tags [nz, ny, nx] of 0/1,
+        number tagged, threshold).  refine_box: True for the body's refinement
+        region (when there is a body), a (lo, hi) pair, or False.  levelset:
+        also tag the signed-distance band of a cylinder / sphere body (the
+        reference's cylinder-geometry branch), when there is one."""
+        _, _, vmax = self.derived_fields()
+        ls = None
+        if levelset and self.ib_case is not None and self.ib_case.geometry_type == 0:
+            m = self.ib_case
+            ls = (C.c_double * 6)(m.x0, m.y0, m.z0 if self.dim == 3 else 0.0, m.R,
+                                  float(n_cells_band), self.case.dx)
+        threshold = threshold_ratio * vmax
+        box = None
+        if refine_box is True and self.ib_case is not None:
+            box = refinement_region(self.case, self.ib_case)
+        elif refine_box not in (True, False, None):
+            box = refine_box
+        nx, ny, nz = self.case.n_cell
+        tags = torch.zeros(nx * ny * (nz if self.dim == 3 else 1), dtype=torch.uint8, device=self.dev)
+        b = self._box(self.f, None)
+        cnt = C.c_int64()
+        capi.check(self.L.ilbm_tag_cells(self.ctx.h, C.byref(b), self.vor.data_ptr(), threshold,
+                                         int(box is not None),
+                                         capi.dvec3(box[0]) if box is not None else None,
+                                         capi.dvec3(box[1]) if box is not None else None,
+                                         float(no_refine[0]), float(no_refine[1]),
+                                         capi.dvec3(self.case.prob_lo), capi.dvec3(self.case.prob_hi),
+                                         capi.dvec3([self.case.dx] * 3), ls, tags.data_ptr(),
+                                         C.byref(cnt)), "tag_cells")
+        shape = (nz, ny, nx) if self.dim == 3 else (1, ny, nx)
+        return tags.cpu().numpy().reshape(shape), cnt.value, threshold
+
+    # ---- state I/O (checkpoint / restart, plotfile) ------------------------
+    def save_checkpoint(self, path) -> None:
+        """Checkpoint of the level: f^n, F^{n-1} and the body when there is one,
+        the stored macro fields when the next step still reads them, and this
+        object's step count, time and force-record history (the
+        WriteCheckpointFile the reference leaves as a stub,
+        Source/Core/AmrCoreLBM.cpp:1932-2010)."""
+        b = self._box(self.f, None, macro_in=self.macro if self.first_step_macro else None,
+                      force_prev=self.force_prev if self.ib is not None else None)
+        m = capi.CheckpointMeta_t()
+        m.istep, m.time = self.istep, self.time
+        m.user[0] = 1.0 if self.have_prev_body else 0.0
+        m.user[1], m.user[2], m.user[3] = (float(v) for v in self.prev_body)
+        capi.check(self.L.ilbm_checkpoint_write(self.ctx.h, C.byref(b), self.ib, C.byref(m),
+                                                str(path).encode()), "checkpoint_write")
+
+    def load_checkpoint(self, path) -> None:
+        """Restores a checkpoint written by save_checkpoint on a solver made
+        with the same case, storage and body; the next step continues the saved
+        run bit for bit (ReadCheckpointFile, AmrCoreLBM.cpp:2020-2115)."""
+        b = self._box(self.f, None, macro_in=self.macro,
+                      force_prev=self.force_prev if self.ib is not None else None)
+        m = capi.CheckpointMeta_t()
+        capi.check(self.L.ilbm_checkpoint_read(self.ctx.h, C.byref(b), self.ib, C.byref(m),
+                                               str(path).encode()), "checkpoint_read")
+        self.istep, self.time = int(m.istep), float(m.time)
+        self.first_step_macro = bool(m.flags & capi.CKPT_MACRO)
+        self.have_prev_body = m.user[0] != 0.0
+        self.prev_body = np.array([m.user[1], m.user[2], m.user[3]])
+        self.ib_ready = False
+
+    def write_plotfile(self, path, levelset: bool | None = None) -> None:
+        """AMReX plotfile of the current state (WritePlotFile,
+        AmrCoreLBM.cpp:1908-1930): rho, ux, uy, uz, vor, Pressure,
+        f_new_0..Q-1 and, for a cylinder / sphere body (levelset None picks
+        that), phi with the body's interior masked as PlotFileMF does."""
+        if levelset is None:
+            levelset = self.ib_case is not None and self.ib_case.geometry_type == 0
+        b = self._box(self.f, None, force_prev=self.force_prev if self.ib is not None else None)
+        c = self.case
+        info = capi.PlotInfo_t()
+        for d in range(3):
+            info.prob_lo[d], info.prob_hi[d], info.dx[d] = c.prob_lo[d], c.prob_hi[d], c.dx
+        info.time, info.istep = self.time, self.istep
+        if levelset:
+            m = self.ib_case
+            info.levelset = 1
+            info.ls_center[0], info.ls_center[1], info.ls_center[2] = m.x0, m.y0, m.z0
+            info.ls_radius = m.R
+            info.body_u[0], info.body_u[1], info.body_u[2] = m.ubx, m.uby, m.ubz
+        capi.check(self.L.ilbm_plotfile_write(self.ctx.h, C.byref(b), C.byref(self.params),
+                                              C.byref(info), str(path).encode()), "plotfile_write")
 
     def mean_velocity(self) -> np.ndarray:
         """Domain-mean velocity of the current state (reduced on the device)."""

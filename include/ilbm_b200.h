@@ -288,6 +288,97 @@ int ilbm_momentum_exchange(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_
                            const double prob_lo[3], const double dx[3], int one_sided,
                            double out[3]);
 
+/* ---- derived fields and refinement tags ---------------------------------- */
+/* UpdateDerivedMacroFields / visPara (Source/Core/AmrCoreLBM.cpp:105-168,
+ * Source/LBM/visPara.H:10-54) for a level held in one box with self-filled
+ * ghosts: vorticity (2D: dv/dx - du/dy; 3D: |curl u|) by central differences
+ * of the velocity of f (with the half force of force_prev, which may be
+ * NULL) FillPatched one cell out, and pressure (rho - 1)/3, written on valid
+ * cells into vor / pres (macro-array layout of `box`, real type; either may
+ * be NULL); *vort_max = the largest vorticity of the level (ErrorEst's
+ * vortMax, AmrCoreLBM.cpp:1047).  dx: the level's cell sizes.  Synchronises. */
+int ilbm_derived_fields(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
+                        const void *f, const void *force_prev, const double dx[3], void *vor,
+                        void *pres, double *vort_max);
+/* ErrorEst tags (AmrCoreLBM.cpp:988-1185, Tagging.H:12-18): on every valid
+ * cell, 0 inside the no-refine x zones (within no_refine_xlo of prob_lo[0] or
+ * no_refine_xhi of prob_hi[0], when either is > 0), else 1 where |vor| >
+ * threshold (the caller's thresholdRatio * vortMax) or, with use_box, where the
+ * cell centre lies in [box_lo, box_hi] (the body refinement region), else 0.
+ * levelset: NULL, or {x0, y0, z0, R, n_cells_band, dx_min} of a cylinder /
+ * sphere body (the cylinder-geometry branch, AmrCoreLBM.cpp:1073-1132 with
+ * levelset_tagging, Tagging.H:27-35): a cell is also tagged where the signed
+ * distance |x - x0| - R of its centre is below (n_cells_band + 0.5) * dx_min,
+ * which takes in the body's interior.  The reference uses n_cells_band = 5.
+ * tags: device array of one byte per valid cell, i fastest; *ntagged = count.
+ * Synchronises. */
+int ilbm_tag_cells(ilbm_ctx *ctx, const ilbm_box *box, const void *vor, double threshold,
+                   int use_box, const double box_lo[3], const double box_hi[3],
+                   double no_refine_xlo, double no_refine_xhi, const double prob_lo[3],
+                   const double prob_hi[3], const double dx[3], const double *levelset,
+                   void *tags, int64_t *ntagged);
+
+/* ---- state I/O ----------------------------------------------------------
+ * Checkpoint and restart of one level box (and its immersed body): the
+ * checkpoint the reference declares but leaves as commented-out stubs
+ * (AmrCoreLBM::WriteCheckpointFile / ReadCheckpointFile,
+ * Source/Core/AmrCoreLBM.cpp:1932-2115), in a format of this library: a
+ * header, then sections of valid-cell data (component-major, i fastest) in
+ * the storage's own bits, each closed by a 64-bit word hash.  A restart from
+ * it continues bit for bit where the saved run left off.
+ *   box->f_in          f^n (saved / restored, storage type)
+ *   box->macro_in      rho,u,v,w when the next step still reads the stored
+ *                      macro fields (the first step after initialisation),
+ *                      else NULL; on restore it may be given for a file
+ *                      without them (flags then says so)
+ *   box->force_prev    F^{n-1} (3 comps) of a level with a body, else NULL
+ *   ib                 the body (marker positions, velocities and forces,
+ *                      last force sum, the CG start vector), or NULL; on
+ *                      restore it must have been created with the same
+ *                      parameters on the same level
+ *   f16 storage keeps its raw half bits: restore with the same f16_scale.
+ * Both synchronise the context's stream.  Errors: ILBM_ERR_IO (file, short
+ * read, hash mismatch), ILBM_ERR_ARG (the file does not match the lattice,
+ * storage, box, body or the sections asked for). */
+#define ILBM_ERR_IO (-7)
+#define ILBM_CKPT_MACRO 1 /* flags: the file holds stored macro fields */
+#define ILBM_CKPT_FORCE 2 /*        F^{n-1} */
+#define ILBM_CKPT_BODY 4  /*        an immersed body */
+typedef struct {
+  int64_t istep;     /* steps taken by the level */
+  double time;       /* time of the next step */
+  double user[16];   /* caller state carried with the checkpoint */
+  int flags;         /* read: ILBM_CKPT_* of the file (ignored on write) */
+} ilbm_checkpoint_meta;
+int ilbm_checkpoint_write(ilbm_ctx *ctx, const ilbm_box *box, ilbm_ib *ib,
+                          const ilbm_checkpoint_meta *meta, const char *path);
+int ilbm_checkpoint_read(ilbm_ctx *ctx, const ilbm_box *box, ilbm_ib *ib,
+                         ilbm_checkpoint_meta *meta, const char *path);
+
+/* AMReX plotfile of one level held in one box (AmrCoreLBM::WritePlotFile,
+ * PlotFileMF and PlotFileVarNames, Source/Core/AmrCoreLBM.cpp:1756-1930, which
+ * call AMReX's WriteMultiLevelPlotfile): the directory `dir` gets Header,
+ * Level_0/Cell_H and Level_0/Cell_D_00000 ("HyperCLaw-V1.1", one FAB of
+ * little-endian doubles), readable by AMReX-based tools.  Components: rho,
+ * ux, uy, uz, vor, Pressure (macro of f^n with the half force of F^{n-1},
+ * vorticity and pressure as ilbm_derived_fields), f_new_0 .. f_new_{Q-1}
+ * (unshifted populations), and with `levelset` set, phi = |x - c| - R of a
+ * cylinder / sphere body, whose interior (phi < 0) then shows the body
+ * velocity and zero vorticity (PlotFileMF's masking).  Self-filled ghosts,
+ * box equal to the domain; uses box->f_in and box->force_prev.
+ * Synchronises. */
+typedef struct {
+  double prob_lo[3], prob_hi[3], dx[3];
+  double time;
+  int istep;
+  int levelset;          /* 1: append phi and mask the body interior */
+  double ls_center[3];
+  double ls_radius;
+  double body_u[3];      /* ubx, uby, ubz */
+} ilbm_plot_info;
+int ilbm_plotfile_write(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
+                        const ilbm_plot_info *info, const char *dir);
+
 /* ---- batch engine (no counterpart in the reference) ---------------------
  * Many independent single-level cases of the context's lattice and storage
  * form, advanced together: per step one launch per immersed-boundary stage

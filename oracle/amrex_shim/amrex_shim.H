@@ -338,6 +338,14 @@ struct BoxArray {
   const Box &operator[](int i) const { return boxes[i]; }
 };
 struct DistributionMapping {};
+inline bool operator!=(const BoxArray &a, const BoxArray &b) {
+  if (a.size() != b.size()) return true;
+  for (int n = 0; n < a.size(); ++n)
+    for (int d = 0; d < AMREX_SPACEDIM; ++d)
+      if (a[n].smallEnd(d) != b[n].smallEnd(d) || a[n].bigEnd(d) != b[n].bigEnd(d)) return true;
+  return false;
+}
+inline bool operator!=(const DistributionMapping &, const DistributionMapping &) { return false; }
 
 struct FArrayBox {
   Box gbox;

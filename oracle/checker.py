@@ -161,6 +161,10 @@ def _load(backend: str, dim: int, fp32: bool = False):
                 ("ref_delta_function", C.c_double, [C.c_double] * 3 + [C.c_int]),
                 ("ref_overlap_1d", C.c_double, [C.c_double] * 3 + [C.c_int, C.c_double, C.c_int, C.c_int]),
                 ("ref_feq", C.c_double, [C.c_double] * 8),
+                ("ref_derived", C.c_int, [C.c_void_p] + [C.POINTER(C.c_double)] * 3),
+                ("ref_tags", C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.c_double, C.c_int,
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                                       C.c_double, C.POINTER(C.c_double), C.c_char_p]),
             ]:
                 fn = getattr(lib, name)
                 fn.restype, fn.argtypes = res, args
@@ -304,5 +308,89 @@ class CpuLevel:
             self.lib.ref_ib_marker_state(self.h, self.time, _dp(out), n)
         return out.reshape(n, 6)
 
+    def ref_derived(self):
+        """(vorticity, pressure, vortMax) from the reference build's visPara on
+        its FillPatched macro_new (valid cells, [nz, ny, nx])."""
+        vor, pres, vm = np.zeros(self.ncell), np.zeros(self.ncell), C.c_double()
+        self._chk(self.lib.ref_derived(self.h, _dp(vor), _dp(pres), C.byref(vm)), "derived")
+        return vor.reshape(self.shape), pres.reshape(self.shape), vm.value
+
+    def ref_tags(self, vor, threshold, box=None, no_refine=(0.0, 0.0), levelset=None):
+        """ErrorEst tags from the reference build's Tagging.H functions."""
+        v = np.ascontiguousarray(vor, dtype=np.float64).reshape(-1)
+        out = C.create_string_buffer(self.ncell)
+        dv = lambda a: (C.c_double * len(a))(*a)
+        rc = self.lib.ref_tags(self.h, _dp(v), float(threshold), int(box is not None),
+                               dv(box[0]) if box is not None else None,
+                               dv(box[1]) if box is not None else None,
+                               float(no_refine[0]), float(no_refine[1]),
+                               dv(levelset) if levelset is not None else None, out)
+        self._chk(rc, "tags")
+        return np.frombuffer(out.raw, dtype=np.uint8).reshape(self.shape).copy()
+
     def marker_dv(self) -> float:
         return float(self.lib.orc_ib_dv(self.h))
+
+
+# ---------------------------------------------------------------------------
+# Derived fields and refinement tags, restated for checking (numpy, FP64, the
+# reference's operation order; every operation is one IEEE rounding)
+# ---------------------------------------------------------------------------
+def vorticity_pressure(mg, ng: int, dim: int, dx: float, dy: float, dz: float):
+    """vorticityDiagnostic / visPara (Source/LBM/visPara.H:10-54) on the valid
+    cells of a FillPatched macro array mg[comp, k, j, i] (comps rho, u, v, w,
+    ...; ng ghost layers, none in z for 2D): (vorticity, pressure), each
+    [nz, ny, nx]."""
+    rho, u, v, w = mg[0], mg[1], mg[2], mg[3]
+    kz = slice(ng, -ng) if dim == 3 else slice(0, 1)
+
+    def sh(a, di=0, dj=0, dk=0):
+        gz, gy, gx = a.shape
+        ks = slice(ng + dk, gz - ng + dk) if dim == 3 else slice(0, 1)
+        return a[ks, ng + dj:gy - ng + dj, ng + di:gx - ng + di]
+
+    dv_dx = (sh(v, 1) - sh(v, -1)) / (2.0 * dx)
+    du_dy = (sh(u, 0, 1) - sh(u, 0, -1)) / (2.0 * dy)
+    if dim == 3:
+        du_dz = (sh(u, 0, 0, 1) - sh(u, 0, 0, -1)) / (2.0 * dz)
+        dw_dx = (sh(w, 1) - sh(w, -1)) / (2.0 * dx)
+        dv_dz = (sh(v, 0, 0, 1) - sh(v, 0, 0, -1)) / (2.0 * dz)
+        dw_dy = (sh(w, 0, 1) - sh(w, 0, -1)) / (2.0 * dy)
+        ox, oy, oz = dw_dy - dv_dz, du_dz - dw_dx, dv_dx - du_dy
+        vor = np.sqrt(ox * ox + oy * oy + oz * oz)
+    else:
+        vor = dv_dx - du_dy
+    pres = (sh(rho) - 1.0) / 3.0
+    return vor, pres
+
+
+def error_est_tags(vor, threshold: float, prob_lo, prob_hi, dx, box=None, no_refine=(0.0, 0.0),
+                   levelset=None):
+    """ErrorEst's tagging (Source/Core/AmrCoreLBM.cpp:1073-1180 with
+    vorticity_tagging and levelset_tagging, Source/Tagging.H:12-35) of
+    vor[nz, ny, nx]: 0/1 tags.  levelset: None or (x0, y0, z0, R,
+    n_cells_band, dx_min) of the cylinder-geometry branch, whose phi is
+    LevelSetManager::build_from_cylinder (Source/LevelSet/LevelSet.cpp:36-74)."""
+    nz, ny, nx = vor.shape
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    x = prob_lo[0] + (i + 0.5) * dx[0]
+    tags = (np.abs(vor) > threshold)
+    if levelset is not None:
+        x0, y0, z0, R, nband, dx_min = levelset
+        y = prob_lo[1] + (j + 0.5) * dx[1]
+        r2 = (x - x0) * (x - x0) + (y - y0) * (y - y0)
+        if nz > 1:
+            z = prob_lo[2] + (k + 0.5) * dx[2]
+            r2 = r2 + (z - z0) * (z - z0)
+        phi = np.sqrt(r2) - R
+        tags = tags | (phi < (float(int(nband)) + 0.5) * dx_min)
+    if box is not None:
+        y = prob_lo[1] + (j + 0.5) * dx[1]
+        z = prob_lo[2] + (k + 0.5) * dx[2] if nz > 1 else np.zeros_like(x)
+        inb = ((x >= box[0][0]) & (x <= box[1][0]) & (y >= box[0][1]) & (y <= box[1][1])
+               & (z >= box[0][2]) & (z <= box[1][2]))
+        tags = tags | inb
+    if no_refine[0] > 0.0 or no_refine[1] > 0.0:
+        blocked = (x <= prob_lo[0] + no_refine[0]) | (x >= prob_hi[0] - no_refine[1])
+        tags = tags & ~blocked
+    return tags.astype(np.uint8)

@@ -38,6 +38,9 @@
 #include "BC/bc_val.cpp"
 #include "IBM/IBMarkerDF.cpp"
 #include "IBM/IBForceEval.cpp"
+#include "LevelSet/LevelSet.cpp"
+#include <visPara.H>
+#include <Tagging.H>
 
 #include "oracle_case.h"
 
@@ -712,6 +715,100 @@ int ref_momentum_exchange(void *h, double x0, double y0, double z0, double R, in
     auto F = IBForceEval::ComputeMomentumExchangeBodyForce(L->f_new, L->geom, L->dirx, L->diry,
                                                            L->dirz, L->ndir, par, one_sided != 0);
     for (int n = 0; n < 3; ++n) out3[n] = (double)F[n];
+  });
+}
+
+// ErrorEst's field step (Source/Core/AmrCoreLBM.cpp:1020-1047): rho, u, v, w
+// of macro_new FillPatched one cell out, then the reference's visPara
+// (Source/LBM/visPara.H:39-54: vorticityDiagnostic and the pressure) on the
+// valid cells; *vmax = vortMax.  vor / pres: valid cells, i fastest.
+int ref_derived(void *h, double *vor, double *pres, double *vmax) {
+  auto *L = static_cast<RefLevel *>(h);
+  return guard([&] {
+    MultiFab mt(L->ba, L->dm, 4, 1);
+    fill_patch(*L, mt, L->macro_new, 4, L->bcsMacro, macroBcFill{L->bcval});
+    MultiFab vo(L->ba, L->dm, 1, 0), pr(L->ba, L->dm, 1, 0);
+    const auto dxa = L->geom.CellSizeArray();
+#if (AMREX_SPACEDIM == 3)
+    const Real dz = dxa[2];
+#else
+    const Real dz = Real(0.0);
+#endif
+    auto rho = mt[0].const_array(0), u = mt[0].const_array(1), v = mt[0].const_array(2),
+         w = mt[0].const_array(3);
+    auto va = vo[0].array(), pa = pr[0].array();
+    const Box vb = L->ba[0];
+    for_box(vb, [&](int i, int j, int k) {
+      visPara(i, j, k, rho, u, v, w, va, pa, dxa[0], dxa[1], dz, Real(0.0));
+    });
+    copy_out(vo, 0, 1, vor, vb);
+    copy_out(pr, 0, 1, pres, vb);
+    double m = -1e300;
+    MultiFab::forBox(vb, [&](const IntVect &iv) { m = std::max(m, (double)va(iv, 0)); });
+    *vmax = m;
+  });
+}
+
+// ErrorEst's tag loop (AmrCoreLBM.cpp:1073-1180, restated glue) around the
+// reference's vorticity_tagging / levelset_tagging (Source/Tagging.H:12-35),
+// with phi from the reference's LevelSetManager::build_from_cylinder
+// (Source/LevelSet/LevelSet.cpp:36-74).  ls6: NULL or {x0, y0, z0, R,
+// n_cells_band, dx_min}.  tags: valid cells, i fastest, 0/1.
+int ref_tags(void *h, const double *vor, double threshold, int use_box, const double *box_lo,
+             const double *box_hi, double nr_lo, double nr_hi, const double *ls6,
+             unsigned char *tags) {
+  auto *L = static_cast<RefLevel *>(h);
+  return guard([&] {
+    const Box vb = L->ba[0];
+    MultiFab vo(L->ba, L->dm, 1, 0);
+    copy_in(vo, 0, 1, vor, vb);
+    LevelSetManager lsm;
+    int nband = 0;
+    Real dx_min = 0;
+    if (ls6) {
+      LevelSetParams par;
+      par.x0 = Real(ls6[0]);
+      par.y0 = Real(ls6[1]);
+      par.z0 = Real(ls6[2]);
+      par.R = Real(ls6[3]);
+      nband = (int)ls6[4];
+      dx_min = Real(ls6[5]);
+      lsm.define_level(0, L->ba, L->dm, L->nghost);
+      lsm.build_from_cylinder(0, L->geom, par);
+    }
+    std::vector<char> tb((size_t)vb.numPts(), 0);
+    Array4<char> tg(tb.data(), vb, 1);
+    auto vort = vo[0].const_array(0);
+    const auto problo = L->geom.ProbLoArray();
+    const auto probhi = L->geom.ProbHiArray();
+    const auto dx = L->geom.CellSizeArray();
+    const char tagval = 1, clearval = 0;
+    for_box(vb, [&](int i, int j, int k) {
+      const Real x = problo[0] + (Real(i) + Real(0.5)) * dx[0];
+      if (nr_lo > 0.0 || nr_hi > 0.0) {
+        if (x <= problo[0] + Real(nr_lo) || x >= probhi[0] - Real(nr_hi)) {
+          tg(i, j, k) = clearval;
+          return;
+        }
+      }
+      vorticity_tagging(i, j, k, tg, vort, Real(threshold), tagval);
+      if (ls6) {
+        Array4<const Real> phi = lsm.phi_at(0)[0].const_array(0);
+        levelset_tagging(i, j, k, tg, phi, dx_min, nband, tagval);
+      }
+      if (use_box) {
+        const Real y = problo[1] + (Real(j) + Real(0.5)) * dx[1];
+#if (AMREX_SPACEDIM == 3)
+        const Real z = problo[2] + (Real(k) + Real(0.5)) * dx[2];
+#else
+        const Real z = Real(0.0);
+#endif
+        if (x >= box_lo[0] && x <= box_hi[0] && y >= box_lo[1] && y <= box_hi[1] &&
+            z >= box_lo[2] && z <= box_hi[2])
+          tg(i, j, k) = tagval;
+      }
+    });
+    for (size_t n = 0; n < tb.size(); ++n) tags[n] = (unsigned char)tb[n];
   });
 }
 

@@ -74,3 +74,35 @@ def test_delta_kernel_matches_reference_and_partitions_unity():
         for x in np.linspace(-2.5, 2.5, 101):
             for kt in (0, 1):
                 assert ref.ref_delta_function(x, 0.1, 1.0, kt) == lib.orc_delta_function(x, 0.1, 1.0, kt)
+
+
+@pytest.mark.parametrize("name", ["cylinder96x64_ivc", "sphere40x24x24_d3q19_ivc",
+                                  "channel16x12_bounceback", "duct12_d3q19_user2",
+                                  "couette24_extdir_foextrap"])
+def test_derived_and_tags_match_reference_build(name):
+    """The numpy restatements of visPara and ErrorEst's tagging (which check
+    the device kernels) against the reference's own visPara.H, Tagging.H and
+    LevelSet.cpp compiled in place, on the oracle's FillPatched macro."""
+    from ilbmrex_b200.level import refinement_region
+    case, init, ib = GOLDEN_CASES[name][0]()
+    if not checker.available("ref", case.dim):
+        pytest.skip("reference build (oracle/_ref/libref*.so) not present")
+    a, b = _run("oracle", name), _run("ref", name)
+    ng = case.nghost
+    nx, ny, nz = case.n_cell
+    gz = nz + 2 * ng if case.dim == 3 else 1
+    mg = a.fill_patch_macro().reshape(6, gz, ny + 2 * ng, nx + 2 * ng)
+    vor, pres = checker.vorticity_pressure(mg, ng, case.dim, case.dx, case.dx, case.dx)
+    rv, rp, rmax = b.ref_derived()
+    np.testing.assert_array_equal(vor, rv)
+    np.testing.assert_array_equal(pres, rp)
+    assert vor.max() == rmax
+    box = refinement_region(case, ib) if ib is not None else None
+    ls = (ib.x0, ib.y0, ib.z0 if case.dim == 3 else 0.0, ib.R, 5, case.dx) if ib is not None else None
+    for ratio, nr, bx, l6 in ((0.3, (0.0, 0.0), box, ls), (0.05, (4.0, 6.0), box, ls),
+                              (0.3, (0.0, 0.0), None, ls), (0.1, (0.0, 0.0), box, None)):
+        mine = checker.error_est_tags(vor, ratio * rmax, case.prob_lo, case.prob_hi, [case.dx] * 3,
+                                      bx, nr, l6)
+        ref = b.ref_tags(rv, ratio * rmax, bx, nr, l6)
+        np.testing.assert_array_equal(mine, ref)
+        assert ref.sum() > 0 or nr != (0.0, 0.0)
