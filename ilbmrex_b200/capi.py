@@ -39,6 +39,7 @@ EXPORTS = [
     "ilbm_batch_tune", "ilbm_batch_size", "ilbm_batch_progress",
     "ilbm_derived_fields", "ilbm_tag_cells",
     "ilbm_checkpoint_write", "ilbm_checkpoint_read", "ilbm_plotfile_write",
+    "ilbm_advance_two_level", "ilbm_average_down",
 ]
 
 
@@ -167,6 +168,10 @@ def lib():
         "ilbm_tag_cells": (I, [P, C.POINTER(Box_t), P, D, I, dp, dp, D, D, dp, dp, dp, dp, P,
                                C.POINTER(I64)]),
         "ilbm_batch_progress": (I, [P, I, C.POINTER(I), C.POINTER(I64), C.POINTER(I), C.POINTER(I)]),
+        "ilbm_advance_two_level": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), C.POINTER(Box_t),
+                                       C.POINTER(LevelParams_t), P, D, D]),
+        "ilbm_average_down": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), C.POINTER(Box_t),
+                                  C.POINTER(LevelParams_t)]),
         "ilbm_checkpoint_write": (I, [P, C.POINTER(Box_t), P, C.POINTER(CheckpointMeta_t), C.c_char_p]),
         "ilbm_checkpoint_read": (I, [P, C.POINTER(Box_t), P, C.POINTER(CheckpointMeta_t), C.c_char_p]),
         "ilbm_plotfile_write": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t),

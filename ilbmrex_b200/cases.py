@@ -277,3 +277,108 @@ def batch_mix(n_cases: int = 64, seed: int = 20261203, U: float = 0.05):
         case.name = f"{case.name}#{c}"
         out.append((case, ib, init))
     return out
+
+
+# ---------------------------------------------------------------------------
+# static two-level hierarchies (amr.max_level = 1, amr.ref_ratio = 2)
+# ---------------------------------------------------------------------------
+@dataclass
+class TwoLevelCase:
+    """A coarse level equal to the domain and one fixed fine box of
+    refinement ratio 2 (fine-domain cell indices, lo even, hi odd, at least
+    two coarse cells inside every face of the domain).  The fine level is
+    stepped twice per coarse step (timeStepWithSubcycling,
+    Source/Core/AmrCoreLBM.cpp:1690-1755); a body lives on it (the finest
+    level, AdvanceLBMAtLevel.cpp:30, 73-93)."""
+    coarse: LevelCase
+    fine_lo: tuple
+    fine_hi: tuple
+    name: str = "two_level"
+
+    def __post_init__(self):
+        d = self.coarse.dim
+        lo = tuple(int(v) for v in self.fine_lo) + (0,) * (3 - len(self.fine_lo))
+        hi = tuple(int(v) for v in self.fine_hi) + (0,) * (3 - len(self.fine_hi))
+        self.fine_lo, self.fine_hi = lo[:3], hi[:3]
+        for a in range(d):
+            if self.fine_lo[a] % 2 or self.fine_hi[a] % 2 == 0 or self.fine_hi[a] < self.fine_lo[a]:
+                raise ValueError("fine box must cover whole coarse cells (lo even, hi odd)")
+            if self.fine_lo[a] // 2 < 2 or self.fine_hi[a] // 2 > self.coarse.n_cell[a] - 3:
+                raise ValueError("fine box must lie two coarse cells inside the domain")
+
+    @property
+    def dim(self) -> int:
+        return self.coarse.dim
+
+    @property
+    def fine_n_cell(self) -> tuple:
+        return tuple((self.fine_hi[a] - self.fine_lo[a] + 1) if a < self.dim else 1 for a in range(3))
+
+    def fine_level(self) -> LevelCase:
+        """The fine level's domain (twice the coarse cells, same geometry)."""
+        c = self.coarse
+        n = tuple(2 * c.n_cell[a] if a < c.dim else 1 for a in range(3))
+        return replace(c, n_cell=n, name=c.name + "_fine")
+
+    def fine_box(self) -> LevelCase:
+        """The fine box as a level of its own (its cells and physical extent),
+        for initial fields evaluated at its cell centres."""
+        c = self.coarse
+        dxf = c.dx / 2.0
+        lo = tuple(c.prob_lo[a] + dxf * self.fine_lo[a] if a < c.dim else c.prob_lo[a] for a in range(3))
+        hi = tuple(c.prob_lo[a] + dxf * (self.fine_hi[a] + 1) if a < c.dim else c.prob_hi[a]
+                   for a in range(3))
+        return replace(c, n_cell=self.fine_n_cell, prob_lo=lo, prob_hi=hi, periodic=(False,) * 3,
+                       name=c.name + "_finebox")
+
+
+def field_init(case: LevelCase, fn):
+    """Initial (rho, u, v, w) of fn(x, y, z) at the cell centres of a level."""
+    def init():
+        nz, ny, nx = case.shape
+        dx = case.dx
+        x = case.prob_lo[0] + (np.arange(nx) + 0.5) * dx
+        y = case.prob_lo[1] + (np.arange(ny) + 0.5) * dx
+        z = case.prob_lo[2] + (np.arange(nz) + 0.5) * dx if case.dim == 3 else np.zeros(1)
+        Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+        return tuple(np.asarray(v, dtype=np.float64) * np.ones(case.shape) for v in fn(X, Y, Z))
+    return init
+
+
+def shear_layer_two_level(n=64, U0=0.02, nu=0.01, fine=(24, 48), lattice: Lattice = D2Q9):
+    """Periodic box with a perturbed double shear layer and a centred fine
+    patch covering fine cells [fine[0], fine[1]) in every direction (no body):
+    velocity gradients cross the coarse-fine boundary."""
+    periodic = (True, True, True)
+    dims = (n, n, n if lattice.dim == 3 else 1)
+    coarse = LevelCase(lattice, dims, periodic=periodic, nu=nu, name=f"shear{n}")
+    lo = (fine[0],) * lattice.dim
+    hi = (fine[1] - 1,) * lattice.dim
+    tl = TwoLevelCase(coarse, lo, hi, name=f"shear{n}_2lev")
+    L = float(n)
+
+    def fn(X, Y, Z):
+        u = U0 * np.tanh(30.0 * (np.abs(Y / L - 0.5) - 0.25))
+        v = 0.05 * U0 * np.sin(2.0 * np.pi * X / L)
+        w = 0.02 * U0 * np.sin(2.0 * np.pi * Z / L) if lattice.dim == 3 else 0.0 * X
+        return 1.0 + 0.0 * X, u, v, w
+
+    return tl, field_init(coarse, fn), field_init(tl.fine_box(), fn)
+
+
+def cylinder_two_level(nx=256, ny=128, D=24.0, center=(64.3, 63.7), U=0.05, Re=100.0,
+                       upstream=1.0, downstream=4.0, cross=1.5):
+    """The reference's 2D cylinder deck on two levels (Examples/Cylinder_flow/
+    inputs: max_level 1, ref_ratio 2): coarse level as ``cylinder``, a fine box
+    around the body and its near wake (upstream / downstream / cross extents
+    in diameters from the centre) on which the marker IBM runs, with the
+    body's cells at twice the resolution."""
+    case, ib, init_c = cylinder(nx=nx, ny=ny, D=D, center=center, U=U, Re=Re)
+    lo = [int(math.floor((center[0] - upstream * D))) * 2, int(math.floor((center[1] - cross * D))) * 2]
+    hi = [int(math.ceil((center[0] + downstream * D))) * 2 - 1,
+          int(math.ceil((center[1] + cross * D))) * 2 - 1]
+    lo = [max(lo[a], 4) for a in range(2)]
+    hi = [min(hi[a], 2 * (case.n_cell[a] - 2) - 1) for a in range(2)]
+    tl = TwoLevelCase(case, tuple(lo), tuple(hi), name=f"cylinder{nx}x{ny}_2lev")
+    init_f = uniform_init(tl.fine_box(), 1.0, (U, 0.0, 0.0))
+    return tl, ib, init_c, init_f

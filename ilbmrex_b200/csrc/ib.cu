@@ -1673,11 +1673,19 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *
     return ILBM_ERR_ARG;
   }
   ilbm_ctx *ctx = ib->ctx;
-  for (int d = 0; d < ib->dim; ++d)
-    if (box->lo[d] != 0 || box->hi[d] != ib->g.n_cell[d] - 1) {
-      set_error("ilbm_ib_update_forcing: the box must cover the level domain (one box per level)");
-      return ILBM_ERR_ARG;
-    }
+  // one box per level: the whole domain, or (a fine box of a two-level
+  // hierarchy) a box whose valid cells hold the body's whole support band,
+  // so every band cell the IB reads or writes lies inside the box's arrays
+  bool whole = true, holds_band = true;
+  for (int d = 0; d < ib->dim; ++d) {
+    whole = whole && box->lo[d] == 0 && box->hi[d] == ib->g.n_cell[d] - 1;
+    holds_band = holds_band && ib->blo[d] >= box->lo[d] && ib->blo[d] + ib->bn[d] - 1 <= box->hi[d];
+  }
+  if (!whole && !holds_band) {
+    set_error("ilbm_ib_update_forcing: the box must cover the level domain, or hold the body's "
+              "whole support band in its valid cells");
+    return ILBM_ERR_ARG;
+  }
   if (box->macro_in && box->ngrow_m < 2) {
     set_error("ilbm_ib_update_forcing: macro_in needs at least two filled ghost layers");
     return ILBM_ERR_ARG;

@@ -210,6 +210,19 @@ struct Store<ILBM_STORAGE_F16_SCALED> {
   __device__ static __forceinline__ void store(T *p, R v, float s) { *p = __float2half_rn(v / s); }
 };
 
+// shifted equilibrium: f_eq - w_q
+__device__ __forceinline__ float feqsv(float cx, float cy, float cz, float wq, float drho, float u,
+                                       float v, float w) {
+  const float cu = cx * u + cy * v + cz * w;
+  const float uu = u * u + v * v + w * w;
+  const float P = 3.0f * cu + 4.5f * cu * cu - 1.5f * uu;
+  return wq * (drho + (1.0f + drho) * P);
+}
+template <class L>
+__device__ __forceinline__ float feqs(int q, float drho, float u, float v, float w) {
+  return feqsv(float(L::cx(q)), float(L::cy(q)), float(L::cz(q)), float(L::w(q)), drho, u, v, w);
+}
+
 // ---------------------------------------------------------------------------
 // Launch helpers
 // ---------------------------------------------------------------------------
@@ -224,6 +237,24 @@ __host__ __device__ __forceinline__ bool in_box(const int *lo, const int *hi, in
 
 void set_error(const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
+
+// calls FN<Lat<Q>, storage>(...) for the context's lattice and storage form
+#define ILBM_DISPATCH(ctx, FN, ...)                                                        \
+  [&]() -> int {                                                                           \
+    switch ((ctx)->q * 4 + (ctx)->storage) {                                               \
+      case 9 * 4 + ILBM_STORAGE_F64: return FN<Lat<9>, ILBM_STORAGE_F64>(__VA_ARGS__);     \
+      case 9 * 4 + ILBM_STORAGE_F32_SHIFT: return FN<Lat<9>, ILBM_STORAGE_F32_SHIFT>(__VA_ARGS__); \
+      case 9 * 4 + ILBM_STORAGE_F16_SCALED: return FN<Lat<9>, ILBM_STORAGE_F16_SCALED>(__VA_ARGS__); \
+      case 19 * 4 + ILBM_STORAGE_F64: return FN<Lat<19>, ILBM_STORAGE_F64>(__VA_ARGS__);   \
+      case 19 * 4 + ILBM_STORAGE_F32_SHIFT: return FN<Lat<19>, ILBM_STORAGE_F32_SHIFT>(__VA_ARGS__); \
+      case 19 * 4 + ILBM_STORAGE_F16_SCALED: return FN<Lat<19>, ILBM_STORAGE_F16_SCALED>(__VA_ARGS__); \
+      case 27 * 4 + ILBM_STORAGE_F64: return FN<Lat<27>, ILBM_STORAGE_F64>(__VA_ARGS__);   \
+      case 27 * 4 + ILBM_STORAGE_F32_SHIFT: return FN<Lat<27>, ILBM_STORAGE_F32_SHIFT>(__VA_ARGS__); \
+      case 27 * 4 + ILBM_STORAGE_F16_SCALED: return FN<Lat<27>, ILBM_STORAGE_F16_SCALED>(__VA_ARGS__); \
+      default: set_error("unsupported lattice/storage"); return ILBM_ERR_UNSUPPORTED;      \
+    }                                                                                      \
+  }()
+
 
 }  // namespace ilbm
 

@@ -142,19 +142,6 @@ __device__ __forceinline__ void moments32(const float *g, float Fx, float Fy, fl
   w = (m3 + 0.5f * Fz) * inv;
 }
 
-// shifted equilibrium: f_eq - w_q
-__device__ __forceinline__ float feqsv(float cx, float cy, float cz, float wq, float drho, float u,
-                                       float v, float w) {
-  const float cu = cx * u + cy * v + cz * w;
-  const float uu = u * u + v * v + w * w;
-  const float P = 3.0f * cu + 4.5f * cu * cu - 1.5f * uu;
-  return wq * (drho + (1.0f + drho) * P);
-}
-template <class L>
-__device__ __forceinline__ float feqs(int q, float drho, float u, float v, float w) {
-  return feqsv(float(L::cx(q)), float(L::cy(q)), float(L::cz(q)), float(L::w(q)), drho, u, v, w);
-}
-
 template <int D>
 __device__ __forceinline__ float guo32v(float cx, float cy, float cz, float wq, float omh, float u,
                                         float v, float w, float Fx, float Fy, float Fz) {
@@ -1236,21 +1223,6 @@ static int launch_init(ilbm_ctx *ctx, const StepArgs &a, int ng) {
   return ILBM_OK;
 }
 
-#define ILBM_DISPATCH(ctx, FN, ...)                                                        \
-  [&]() -> int {                                                                           \
-    switch ((ctx)->q * 4 + (ctx)->storage) {                                               \
-      case 9 * 4 + ILBM_STORAGE_F64: return FN<Lat<9>, ILBM_STORAGE_F64>(__VA_ARGS__);     \
-      case 9 * 4 + ILBM_STORAGE_F32_SHIFT: return FN<Lat<9>, ILBM_STORAGE_F32_SHIFT>(__VA_ARGS__); \
-      case 9 * 4 + ILBM_STORAGE_F16_SCALED: return FN<Lat<9>, ILBM_STORAGE_F16_SCALED>(__VA_ARGS__); \
-      case 19 * 4 + ILBM_STORAGE_F64: return FN<Lat<19>, ILBM_STORAGE_F64>(__VA_ARGS__);   \
-      case 19 * 4 + ILBM_STORAGE_F32_SHIFT: return FN<Lat<19>, ILBM_STORAGE_F32_SHIFT>(__VA_ARGS__); \
-      case 19 * 4 + ILBM_STORAGE_F16_SCALED: return FN<Lat<19>, ILBM_STORAGE_F16_SCALED>(__VA_ARGS__); \
-      case 27 * 4 + ILBM_STORAGE_F64: return FN<Lat<27>, ILBM_STORAGE_F64>(__VA_ARGS__);   \
-      case 27 * 4 + ILBM_STORAGE_F32_SHIFT: return FN<Lat<27>, ILBM_STORAGE_F32_SHIFT>(__VA_ARGS__); \
-      case 27 * 4 + ILBM_STORAGE_F16_SCALED: return FN<Lat<27>, ILBM_STORAGE_F16_SCALED>(__VA_ARGS__); \
-      default: set_error("unsupported lattice/storage"); return ILBM_ERR_UNSUPPORTED;      \
-    }                                                                                      \
-  }()
 
 static int check_box(const ilbm_ctx *ctx, const ilbm_box &b, bool need_out) {
   if (!b.f_in || (need_out && !b.f_out)) {

@@ -1,0 +1,196 @@
+"""A static two-level hierarchy on the GPU through the C ABI.
+
+``TwoLevelSolver`` holds a coarse level equal to the domain and one fixed
+fine box of refinement ratio 2 (``cases.TwoLevelCase``) in device memory and
+advances them with ``ilbm_advance_two_level``: one coarse step, two fine
+substeps whose ghost cells come from the coarse macro fields on the device,
+then average-down (AmrCoreLBM::timeStepWithSubcycling,
+Source/Core/AmrCoreLBM.cpp:1690-1755, for max_level = 1 without regrid).  A
+marker body lives on the fine level, the finest one
+(Source/Core/AdvanceLBMAtLevel.cpp:30, 73-93).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import capi
+from .cases import MarkerIB, TwoLevelCase
+from .level import (_REAL_DT, _TORCH_DT, Context, LevelSolver, ib_params, level_geom,
+                    level_params)
+
+
+class _Level:
+    """Device buffers of one level box: populations and stored macro fields
+    in pairs, forces in a pair (fine level with a body)."""
+
+    def __init__(self, q, dim, n_cell, lo, storage, dev, with_force):
+        self.dim, self.lo = dim, tuple(lo)
+        self.n_cell = tuple(n_cell)
+        self.gf, self.gm = 1, 2
+        nx, ny, nz = n_cell
+        gz_f = nz + 2 * self.gf if dim == 3 else 1
+        gz_m = nz + 2 * self.gm if dim == 3 else 1
+        fdt, rdt = _TORCH_DT[storage], _REAL_DT[storage]
+        fsh = (q, gz_f, ny + 2 * self.gf, nx + 2 * self.gf)
+        msh = (gz_m, ny + 2 * self.gm, nx + 2 * self.gm)
+        self.f = torch.zeros(fsh, dtype=fdt, device=dev)
+        self.f_next = torch.zeros(fsh, dtype=fdt, device=dev)
+        self.m = torch.zeros((4,) + msh, dtype=rdt, device=dev)
+        self.m_next = torch.zeros((4,) + msh, dtype=rdt, device=dev)
+        self.fa = torch.zeros((3,) + msh, dtype=rdt, device=dev) if with_force else None
+        self.fb = torch.zeros((3,) + msh, dtype=rdt, device=dev) if with_force else None
+
+    def box(self, f_in=None, f_out=None, m_in=None, m_out=None, force=None, force_prev=None):
+        b = capi.Box_t()
+        for d in range(3):
+            b.lo[d] = self.lo[d] if d < self.dim else 0
+            b.hi[d] = self.lo[d] + self.n_cell[d] - 1 if d < self.dim else 0
+        b.ngrow_f, b.ngrow_m = self.gf, self.gm
+        fs, ms = self.f.stride(), self.m.stride()
+        b.fstride[0], b.fstride[1], b.fstride[2] = fs[2], fs[1], fs[0]
+        b.mstride[0], b.mstride[1], b.mstride[2] = ms[2], ms[1], ms[0]
+        ptr = lambda t: t.data_ptr() if t is not None else None
+        b.f_in, b.f_out = ptr(f_in), ptr(f_out)
+        b.macro_in, b.macro_out = ptr(m_in), ptr(m_out)
+        b.force, b.force_prev = ptr(force), ptr(force_prev)
+        return b
+
+    def valid(self, t, g):
+        nx, ny, nz = self.n_cell
+        if self.dim == 3:
+            return t[..., g:g + nz, g:g + ny, g:g + nx]
+        return t[..., :, g:g + ny, g:g + nx]
+
+
+class TwoLevelSolver:
+    """Coarse level + one fine box (ratio 2) stepped on the GPU."""
+
+    def __init__(self, tl: TwoLevelCase, storage: str = "f64", ib: MarkerIB | None = None,
+                 device: int = 0, f16_scale: float = 1024.0):
+        if not torch.cuda.is_available():
+            raise capi.IlbmError("TwoLevelSolver needs a CUDA device")
+        self.tl = tl
+        self.storage = storage
+        self.dev = torch.device("cuda", device)
+        c = tl.coarse
+        self.case = tl.fine_level()          # the finest level (force record, body)
+        self.ib_case = ib
+        self.dim = c.dim
+        self.ctx = Context(c.lattice, storage, device)
+        self.L = self.ctx.L
+        q = c.lattice.q
+        self.C = _Level(q, c.dim, c.n_cell, (0, 0, 0), storage, self.dev, False)
+        self.F = _Level(q, c.dim, tl.fine_n_cell, tl.fine_lo, storage, self.dev, ib is not None)
+        self.pc = level_params(c, uniform_force=True, f16_scale=f16_scale)
+        self.pf = level_params(self.case, uniform_force=ib is None, f16_scale=f16_scale)
+        self.pf.ghost_mode = capi.GHOST_CALLER
+        self._fine_boxes = (C.c_int * 6)(*tl.fine_lo, *tl.fine_hi)
+        self.pf.level_boxes = C.cast(self._fine_boxes, C.POINTER(C.c_int))
+        self.pf.nlevel_boxes = 1
+        self.ib = None
+        if ib is not None:
+            self._geom = level_geom(self.case)
+            self._ibp = ib_params(ib, self.dim)
+            h = C.c_void_p()
+            capi.check(self.L.ilbm_ib_create(self.ctx.h, C.byref(self._ibp), C.byref(self._geom),
+                                             C.byref(h)), "ilbm_ib_create")
+            self.ib = h
+            lo, hi = (C.c_int * 3)(), (C.c_int * 3)()
+            capi.check(self.L.ilbm_ib_force_region(self.ib, lo, hi), "ib_force_region")
+            self.force_region = (tuple(lo), tuple(hi))
+        self.time = 0.0
+        self.istep = 0
+        self.have_prev_body = False
+        self.prev_body = np.zeros(3)
+        self.rec = np.zeros(18)
+
+    # ---- initialisation (MakeNewLevelFromScratch per level + InitData) ----
+    def set_macro(self, init_coarse, init_fine):
+        """Initial (rho, u, v, w) of each level on its valid cells; each
+        level's populations become their equilibrium, then the fine level is
+        averaged down onto the coarse one (InitData, AmrCoreLBM.cpp:704-722)."""
+        for lvl, vals in ((self.C, init_coarse), (self.F, init_fine)):
+            v = lvl.valid(lvl.m, lvl.gm)
+            for n in range(4 if self.dim == 3 else 3):
+                v[n].copy_(torch.as_tensor(np.asarray(vals[n]), dtype=lvl.m.dtype))
+            torch.cuda.synchronize(self.dev)
+            b = lvl.box(lvl.f, lvl.f_next, m_in=lvl.m)
+            capi.check(self.L.ilbm_init_equilibrium(self.ctx.h, C.byref(b)), "init_equilibrium")
+        bc = self.C.box(self.C.f, None, m_in=self.C.m)
+        bf = self.F.box(self.F.f, None, m_in=self.F.m)
+        capi.check(self.L.ilbm_average_down(self.ctx.h, C.byref(bc), C.byref(self.pc), C.byref(bf),
+                                            C.byref(self.pf)), "average_down")
+        self.ctx.sync()
+        self.time, self.istep = 0.0, 0
+
+    # ---- one coarse step ---------------------------------------------------
+    def advance(self, record_force: bool = False):
+        Cl, Fl = self.C, self.F
+        bc = Cl.box(Cl.f, Cl.f_next, m_in=Cl.m, m_out=Cl.m_next)
+        bf = Fl.box(Fl.f, Fl.f_next, m_in=Fl.m, m_out=Fl.m_next, force=Fl.fa, force_prev=Fl.fb)
+        capi.check(self.L.ilbm_advance_two_level(self.ctx.h, C.byref(bc), C.byref(self.pc),
+                                                 C.byref(bf), C.byref(self.pf), self.ib,
+                                                 self.tl.coarse.dt, self.time), "advance_two_level")
+        Cl.f, Cl.f_next = Cl.f_next, Cl.f
+        Cl.m, Cl.m_next = Cl.m_next, Cl.m
+        self.time += self.tl.coarse.dt
+        self.istep += 1
+        if record_force and self.ib is not None:
+            self.compute_ib_force()
+
+    def step(self, n: int = 1, record_force: bool = False):
+        for _ in range(n):
+            self.advance(record_force=record_force)
+
+    def compute_ib_force(self):
+        """ComputeIBForce on the finest level (AmrCoreLBM.cpp:456-631) with
+        the force of the last fine substep."""
+        lo, hi = self.force_region
+        b = self.F.box(self.F.f, None)
+        s = (C.c_double * 3)()
+        capi.check(self.L.ilbm_force_integrals(self.ctx.h, C.byref(b), self.F.fb.data_ptr(),
+                                               capi.ivec3(lo), capi.ivec3(hi), s), "force_integrals")
+        m = (C.c_double * 3)()
+        capi.check(self.L.ilbm_ib_last_marker_force_sum(self.ib, m), "marker_force_sum")
+        self.rec = LevelSolver.force_record(self, np.array([s[0], s[1], s[2]]),
+                                            np.array([m[0], m[1], m[2]]))
+        return self.rec
+
+    # ---- read-back ---------------------------------------------------------
+    def _lvl(self, lev):
+        return self.F if lev else self.C
+
+    def get_f(self, lev: int) -> np.ndarray:
+        self.ctx.sync()
+        lvl = self._lvl(lev)
+        v = lvl.valid(lvl.f, lvl.gf).to(torch.float64)
+        if self.storage != "f64":
+            w = torch.tensor(self.tl.coarse.lattice.w, dtype=torch.float64, device=self.dev).view(-1, 1, 1, 1)
+            if self.storage == "f16":
+                v = v * (w / self.pc.f16_scale)
+            v = v + w
+        return v.cpu().numpy()
+
+    def get_macro(self, lev: int) -> np.ndarray:
+        """The stored rho, u, v, w of a level (valid cells)."""
+        self.ctx.sync()
+        lvl = self._lvl(lev)
+        return lvl.valid(lvl.m, lvl.gm).to(torch.float64).cpu().numpy()
+
+    def get_force(self) -> np.ndarray:
+        self.ctx.sync()
+        return self.F.valid(self.F.fb, self.F.gm).to(torch.float64).cpu().numpy()
+
+    def marker_force_sum(self) -> np.ndarray:
+        m = (C.c_double * 3)()
+        capi.check(self.L.ilbm_ib_last_marker_force_sum(self.ib, m), "marker_force_sum")
+        return np.array([m[0], m[1], m[2]])
+
+    def close(self):
+        if self.ib is not None:
+            self.L.ilbm_ib_destroy(self.ib)
+            self.ib = None
+        self.ctx.close()

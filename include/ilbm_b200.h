@@ -318,6 +318,39 @@ int ilbm_tag_cells(ilbm_ctx *ctx, const ilbm_box *box, const void *vor, double t
                    const double prob_hi[3], const double dx[3], const double *levelset,
                    void *tags, int64_t *ntagged);
 
+/* ---- static two-level hierarchy ------------------------------------------
+ * A coarse level equal to its domain (ILBM_GHOST_SELF) and one fine box of
+ * refinement ratio 2 (ILBM_GHOST_CALLER, fine domain = the coarse domain
+ * refined by 2, box lo even and hi odd in fine indices, at least two coarse
+ * cells inside every face of the domain), advanced as
+ * AmrCoreLBM::timeStepWithSubcycling does for max_level = 1
+ * (Source/Core/AmrCoreLBM.cpp:1690-1755):
+ *   1. the coarse level steps by dt (coarse->f_in, macro_in -> f_out,
+ *      macro_out; stored macro fields on both levels, since after
+ *      average-down they are no longer those of the coarse populations);
+ *   2. the fine level steps twice by dt/2 at t and t + dt/2; before each
+ *      substep every fine ghost cell gets the coarse macro fields at the
+ *      substep's time (old, new, or their linear time interpolation,
+ *      GetDataMacro :2239-2269), interpolated by cell-conservative linear
+ *      interpolation with monotonised-central limited slopes (AMReX's
+ *      cell_cons_interp in FillPatchMacro :2166-2198), and ghost populations
+ *      equal to the equilibrium of that state (FillPatchMesoscopic's
+ *      coarse-fine overwrite, :1566-1626).  The body `ib` (or NULL) lives
+ *      on the fine level (AdvanceLBMAtLevel.cpp:30, 73-93);
+ *   3. average-down of ratio 2 (AverageDownTo :1519-1527) of the fine
+ *      populations and macro fields onto coarse->f_out / macro_out.
+ * Buffers: the fine level's f_in / macro_in hold the new fine state on
+ * return (two substeps swap them twice), force / force_prev hold the first /
+ * second substep's forces; the caller swaps the coarse in / out pairs.
+ * Asynchronous on the context's stream. */
+int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_params *pc,
+                           const ilbm_box *fine, const ilbm_level_params *pf, ilbm_ib *ib,
+                           double dt, double time);
+/* average-down alone (InitData's AverageDown after the levels are made,
+ * AmrCoreLBM.cpp:710-720): fine f_in / macro_in onto coarse f_in / macro_in */
+int ilbm_average_down(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_params *pc,
+                      const ilbm_box *fine, const ilbm_level_params *pf);
+
 /* ---- state I/O ----------------------------------------------------------
  * Checkpoint and restart of one level box (and its immersed body): the
  * checkpoint the reference declares but leaves as commented-out stubs

@@ -332,6 +332,88 @@ class CpuLevel:
         return float(self.lib.orc_ib_dv(self.h))
 
 
+class CpuTwoLevel:
+    """A static two-level hierarchy advanced by the oracle (orc2_*): coarse
+    level = the domain, one fine box of ratio 2, two fine substeps per coarse
+    step with coarse-fine ghosts from the coarse macro fields, average-down."""
+
+    def __init__(self, tl):
+        self.tl = tl
+        self.lib = _load("oracle", tl.dim)
+        lib = self.lib
+        P, I, dp = C.c_void_p, C.c_int, C.POINTER(C.c_double)
+        ip = C.POINTER(C.c_int)
+        for name, res, args in [("orc2_create", P, [C.POINTER(IlbmCase), ip, ip]),
+                                ("orc2_destroy", None, [P]), ("orc2_level", P, [P, I]),
+                                ("orc2_step", I, [P, I]), ("orc2_init_equilibrium", I, [P])]:
+            fn = getattr(lib, name)
+            fn.restype, fn.argtypes = res, args
+        self._case = to_case(tl.coarse)
+        lo = (C.c_int * 3)(*tl.fine_lo)
+        hi = (C.c_int * 3)(*tl.fine_hi)
+        self.h = lib.orc2_create(C.byref(self._case), lo, hi)
+        if not self.h:
+            raise RuntimeError("orc2_create refused the fine box")
+        self.q = tl.coarse.lattice.q
+        self.shapes = (tl.coarse.shape, tl.fine_box().shape)
+
+    def level(self, lev: int):
+        return self.lib.orc2_level(self.h, lev)
+
+    def close(self):
+        if self.h:
+            self.lib.orc2_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_macro(self, lev, rho, ux, uy, uz=None):
+        m = np.zeros((4,) + self.shapes[lev])
+        m[0], m[1], m[2] = rho, ux, uy
+        if uz is not None:
+            m[3] = uz
+        m = np.ascontiguousarray(m)
+        self.lib.orc_set_macro(self.level(lev), _dp(m))
+
+    def init_equilibrium(self):
+        self.lib.orc2_init_equilibrium(self.h)
+
+    def ib_create(self, ib):
+        if getattr(ib, "airfoil", None) is not None:
+            p = np.ascontiguousarray(np.asarray(ib.airfoil, dtype=np.float64))
+            self.lib.orc_set_airfoil(_dp(p))
+        self._ib = to_ib_case(ib)
+        if self.lib.orc_ib_create(self.level(1), C.byref(self._ib)) != 0:
+            raise RuntimeError("oracle: ib_create failed")
+
+    def step(self, n: int = 1):
+        self.lib.orc2_step(self.h, int(n))
+
+    def get_f(self, lev):
+        out = np.zeros((self.q,) + self.shapes[lev])
+        self.lib.orc_get_f(self.level(lev), _dp(out))
+        return out
+
+    def get_macro(self, lev):
+        out = np.zeros((4,) + self.shapes[lev])
+        self.lib.orc_get_macro(self.level(lev), _dp(out))
+        return out
+
+    def force_record(self):
+        out = np.zeros(FORCE_REC)
+        self.lib.orc_force_record(self.level(1), _dp(out))
+        return out
+
+    def marker_force_sum(self):
+        out = np.zeros(3)
+        self.lib.orc_ib_marker_force_sum(self.level(1), _dp(out))
+        return out
+
+
 # ---------------------------------------------------------------------------
 # Derived fields and refinement tags, restated for checking (numpy, FP64, the
 # reference's operation order; every operation is one IEEE rounding)

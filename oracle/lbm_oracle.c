@@ -44,7 +44,7 @@ typedef struct {
   double chord, thick, pitch_mean, pitch_amp, pitch_freq, pitch_phase, pivot_x;
 } orc_ib;
 
-typedef struct {
+typedef struct orc_level_s {
   ilbm_case c;
   int dim, Q, ng, ngz;
   int n[3], gn[3];
@@ -64,6 +64,13 @@ typedef struct {
   double rec[ILBM_FORCE_REC];
   int have_prev;
   double prev[3];
+  /* fine level of a two-level hierarchy: its coarse level, the fine-domain
+   * index of its cell 0, and the time weights of the coarse macro fields
+   * for the substep being taken (mode 0 old, 1 new, 2 a*old + b*new) */
+  struct orc_level_s *cf;
+  int cflo[3];
+  int cf_mode;
+  double cf_a, cf_b;
 } orc_level;
 
 /* ------------------------------------------------------------------------ */
@@ -281,8 +288,101 @@ static void fill_boundary(const orc_level *L, double *a, int nc) {
       }
 }
 
+/* ---- coarse-fine ghosts of a fine level (static two-level hierarchy) ---- */
+
+/* coarse macro component n at coarse cell (i,j,k) at the substep's time:
+ * GetDataMacro's choice of old / new / both (AmrCoreLBM.cpp:2239-2269) and,
+ * for both, FillPatchSingleLevel's linear time interpolation (AMReX
+ * MultiFab::LinComb, a*old + b*new) */
+static double cf_coarse(const orc_level *F, int n, int i, int j, int k) {
+  const orc_level *C = F->cf;
+  const long e = IX(C, i, j, k) + (long)n * C->gcells;
+  if (F->cf_mode == 0) return C->mac_old[e];
+  if (F->cf_mode == 1) return C->mac_new[e];
+  return F->cf_a * C->mac_old[e] + F->cf_b * C->mac_new[e];
+}
+
+/* monotonised-central limited slope of AMReX's cell-conservative linear
+ * interpolation (cell_cons_interp), from the coarse cell and its two
+ * neighbours in one direction */
+static double mc_slope(double cl, double c, double cr) {
+  const double dc = 0.5 * (cr - cl), dl = c - cl, dr = cr - c;
+  if (dl * dr <= 0.0) return 0.0;
+  double m = fabs(dc);
+  m = dmin(m, 2.0 * fabs(dl));
+  m = dmin(m, 2.0 * fabs(dr));
+  return (dc < 0.0) ? -m : m;
+}
+
+static int floor_half(int v) { return (v >= 0) ? v / 2 : -((1 - v) / 2); }
+
+/* FillPatchTwoLevels of the macro fields into fine cell (i,j,k) (fine-level
+ * local index) from the coarse level, ratio 2: the coarse cell under it, its
+ * limited slopes, and the fine cell centre's offset of -1/4 or +1/4 coarse
+ * cell per direction (AmrCoreLBM::FillPatchMacro, AmrCoreLBM.cpp:2166-2198) */
+static void cf_macro(const orc_level *F, int i, int j, int k, double *m, int nc) {
+  const int fi[3] = {i + F->cflo[0], j + F->cflo[1], (F->dim == 3) ? k + F->cflo[2] : 0};
+  int ic[3] = {0, 0, 0};
+  double off[3] = {0.0, 0.0, 0.0};
+  for (int d = 0; d < F->dim; ++d) {
+    ic[d] = floor_half(fi[d]);
+    off[d] = (fi[d] - 2 * ic[d] == 0) ? -0.25 : 0.25;
+  }
+  for (int n = 0; n < nc; ++n) {
+    const double c = cf_coarse(F, n, ic[0], ic[1], ic[2]);
+    double v = c;
+    for (int d = 0; d < F->dim; ++d) {
+      int lo[3] = {ic[0], ic[1], ic[2]}, hi[3] = {ic[0], ic[1], ic[2]};
+      lo[d] -= 1;
+      hi[d] += 1;
+      const double cl = cf_coarse(F, n, lo[0], lo[1], lo[2]);
+      const double cr = cf_coarse(F, n, hi[0], hi[1], hi[2]);
+      v = v + mc_slope(cl, c, cr) * off[d];
+    }
+    m[n] = v;
+  }
+}
+
+/* the equilibrium FillPatchMesoscopic writes into a fine level's ghosts
+ * (AmrCoreLBM.cpp:1566-1626) */
+static double cf_feq(double wi, double cx, double cy, double cz, double rho, double u0, double v0,
+                     double w0) {
+  const double r = dmax(rho, 1.e-12);
+  const double u2 = u0 * u0 + v0 * v0 + w0 * w0;
+  const double cu = cx * u0 + cy * v0 + cz * w0;
+  return wi * r * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * u2);
+}
+
+/* a fine level's FillPatch: valid cells copied, every ghost cell (all of them
+ * lie on the coarse-fine boundary: the fine box is inside the domain) from
+ * the coarse macro fields -- the macro itself, or its equilibrium */
+static void fill_patch_fine(const orc_level *L, double *dst, const double *src, int nc, int meso) {
+  const int kz0 = (L->dim == 3) ? -L->ng : 0, kz1 = (L->dim == 3) ? L->n[2] + L->ng : 1;
+  for (int k = kz0; k < kz1; ++k)
+    for (int j = -L->ng; j < L->n[1] + L->ng; ++j)
+      for (int i = -L->ng; i < L->n[0] + L->ng; ++i) {
+        const long gi = IX(L, i, j, k);
+        if (in_domain(L, i, j, k)) {
+          for (int n = 0; n < nc; ++n) dst[gi + n * L->gcells] = src[gi + n * L->gcells];
+          continue;
+        }
+        double m[6];
+        cf_macro(L, i, j, k, m, 6);
+        if (meso) {
+          for (int q = 0; q < nc; ++q)
+            dst[gi + q * L->gcells] = cf_feq(L->w[q], L->cx[q], L->cy[q], L->cz[q], m[0], m[1], m[2], m[3]);
+        } else {
+          for (int n = 0; n < nc; ++n) dst[gi + n * L->gcells] = m[n];
+        }
+      }
+}
+
 /* FillPatchSingleLevel(dst <- src) + PhysBCFunct (faces, then edges, then corners) */
 static void fill_patch(const orc_level *L, double *dst, const double *src, int nc, int meso) {
+  if (L->cf) {
+    fill_patch_fine(L, dst, src, nc, meso);
+    return;
+  }
   const int kz0 = (L->dim == 3) ? -L->ng : 0, kz1 = (L->dim == 3) ? L->n[2] + L->ng : 1;
   for (int n = 0; n < nc; ++n)
     for (int k = kz0; k < kz1; ++k)
@@ -1357,4 +1457,123 @@ int orc_momentum_exchange(void *h, double x0, double y0, double z0, double R, in
 double orc_delta_function(double xf, double xp, double h, int type) { return orc_delta(xf, xp, h, type); }
 double orc_overlap(double xa, double xb, double h, int type, double plo, int ilo, int ihi) {
   return orc_overlap_1d(xa, xb, h, type, plo, ilo, ihi);
+}
+
+/* ------------------------------------------------------------------------ */
+/* static two-level hierarchy: AmrCoreLBM::timeStepWithSubcycling           */
+/* (Source/Core/AmrCoreLBM.cpp:1690-1755) for a coarse level equal to the   */
+/* domain and one fine box of ratio 2 inside it, fixed (no regrid)          */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  orc_level *C, *F;
+  int flo[3], fhi[3]; /* fine box in fine-domain index space */
+} orc_two;
+
+/* amrex::average_down of ratio 2 (AverageDownTo, AmrCoreLBM.cpp:1519-1527):
+ * each covered coarse cell gets the mean of its fine cells, summed k, j, i
+ * inner and scaled by the volume fraction */
+static void average_down(const orc_two *T, const double *fine, double *crse, int nc) {
+  const orc_level *C = T->C, *F = T->F;
+  const int kr = (C->dim == 3) ? 2 : 1;
+  const double volfrac = (C->dim == 3) ? 0.125 : 0.25;
+  const int ck0 = (C->dim == 3) ? T->flo[2] / 2 : 0, ck1 = (C->dim == 3) ? T->fhi[2] / 2 : 0;
+  for (int n = 0; n < nc; ++n)
+    for (int kc = ck0; kc <= ck1; ++kc)
+      for (int jc = T->flo[1] / 2; jc <= T->fhi[1] / 2; ++jc)
+        for (int ic = T->flo[0] / 2; ic <= T->fhi[0] / 2; ++ic) {
+          double c = 0.0;
+          for (int kk = 0; kk < kr; ++kk)
+            for (int jj = 0; jj < 2; ++jj)
+              for (int ii = 0; ii < 2; ++ii) {
+                const int fi = 2 * ic + ii - T->flo[0], fj = 2 * jc + jj - T->flo[1];
+                const int fk = (C->dim == 3) ? 2 * kc + kk - T->flo[2] : 0;
+                c += fine[IX(F, fi, fj, fk) + (long)n * F->gcells];
+              }
+          crse[IX(C, ic, jc, kc) + (long)n * C->gcells] = volfrac * c;
+        }
+}
+
+/* coarse case c, fine box [flo, fhi] (fine-domain indices, even lo, odd hi,
+ * at least two coarse cells away from every face of the domain) */
+void *orc2_create(const ilbm_case *c, const int *flo, const int *fhi) {
+  for (int d = 0; d < c->dim; ++d) {
+    if ((flo[d] & 1) || !(fhi[d] & 1) || fhi[d] < flo[d]) return NULL;
+    if (flo[d] / 2 < 2 || fhi[d] / 2 > c->n_cell[d] - 3) return NULL;
+  }
+  orc_two *T = (orc_two *)calloc(1, sizeof(orc_two));
+  T->C = (orc_level *)orc_create(c);
+  ilbm_case fc = *c;
+  const double dxf = (c->prob_hi[0] - c->prob_lo[0]) / (double)c->n_cell[0] / 2.0;
+  for (int d = 0; d < 3; ++d) {
+    T->flo[d] = (d < c->dim) ? flo[d] : 0;
+    T->fhi[d] = (d < c->dim) ? fhi[d] : 0;
+    if (d < c->dim) {
+      fc.n_cell[d] = fhi[d] - flo[d] + 1;
+      fc.prob_lo[d] = c->prob_lo[d] + dxf * (double)flo[d];
+      fc.prob_hi[d] = c->prob_lo[d] + dxf * (double)(fhi[d] + 1);
+    }
+    fc.periodic[d] = 0;
+    fc.bc_lo[d] = fc.bc_hi[d] = BC_FOEXTRAP; /* unused: every ghost is coarse-fine */
+  }
+  T->F = (orc_level *)orc_create(&fc);
+  if (!T->C || !T->F) return NULL;
+  T->F->cf = T->C;
+  for (int d = 0; d < 3; ++d) T->F->cflo[d] = T->flo[d];
+  return T;
+}
+
+void orc2_destroy(void *h) {
+  orc_two *T = (orc_two *)h;
+  orc_destroy(T->C);
+  orc_destroy(T->F);
+  free(T);
+}
+
+void *orc2_level(void *h, int lev) { orc_two *T = (orc_two *)h; return lev ? T->F : T->C; }
+
+/* one coarse step: the coarse level, two fine substeps with their coarse-fine
+ * ghosts at times t and t + dt/2, average-down; the force record of the fine
+ * level once per coarse step (Evolve, AmrCoreLBM.cpp:361-420) */
+int orc2_step(void *h, int nsteps) {
+  orc_two *T = (orc_two *)h;
+  orc_level *C = T->C, *F = T->F;
+  for (int s = 0; s < nsteps; ++s) {
+    const double t_old = C->time, t_new = C->time + C->dt;
+    level_step(C);
+    C->time = t_new;
+    C->step += 1;
+    for (int sub = 0; sub < 2; ++sub) {
+      const double t = t_old + (double)sub * F->dt;
+      /* GetDataMacro(0, t): within teps of t_new / t_old, else both */
+      const double teps = dmax(1.e-12, fabs(t_new - t_old) * 1.e-3);
+      if (t >= t_new - teps && t <= t_new + teps) F->cf_mode = 1;
+      else if (t >= t_old - teps && t <= t_old + teps) F->cf_mode = 0;
+      else {
+        F->cf_mode = 2;
+        F->cf_a = (t_new - t) / (t_new - t_old);
+        F->cf_b = (t - t_old) / (t_new - t_old);
+      }
+      F->time = t;
+      level_step(F);
+      F->step += 1;
+    }
+    F->time = t_new;
+    average_down(T, F->f_new, C->f_new, C->Q);
+    average_down(T, F->mac_new, C->mac_new, 6);
+    compute_ib_force(F);
+  }
+  return 0;
+}
+
+/* InitData for two levels (AmrCoreLBM.cpp:704-722): each level's equilibrium
+ * from its own macro fields, then AverageDown and macro_old = macro_new */
+int orc2_init_equilibrium(void *h) {
+  orc_two *T = (orc_two *)h;
+  orc_init_equilibrium(T->C);
+  orc_init_equilibrium(T->F);
+  average_down(T, T->F->f_new, T->C->f_new, T->C->Q);
+  average_down(T, T->F->mac_new, T->C->mac_new, 6);
+  memcpy(T->C->mac_old, T->C->mac_new, sizeof(double) * 6 * T->C->gcells);
+  memcpy(T->C->f_old, T->C->f_new, sizeof(double) * T->C->Q * T->C->gcells);
+  return 0;
 }

@@ -106,3 +106,31 @@ def test_derived_and_tags_match_reference_build(name):
         ref = b.ref_tags(rv, ratio * rmax, bx, nr, l6)
         np.testing.assert_array_equal(mine, ref)
         assert ref.sum() > 0 or nr != (0.0, 0.0)
+
+
+def test_two_level_oracle_invariants():
+    """The oracle's two-level driver: a uniform state stays uniform across the
+    coarse-fine boundary, and after a step every covered coarse cell holds the
+    mean of its four fine cells (average-down)."""
+    from ilbmrex_b200 import cases
+    from oracle.checker import CpuTwoLevel
+    c = cases.LevelCase(cases.D2Q9, (24, 24, 1), nu=0.02)
+    tl = cases.TwoLevelCase(c, (12, 12), (35, 35))
+    T = CpuTwoLevel(tl)
+    T.set_macro(0, *cases.uniform_init(c, 1.0, (0.03, -0.01, 0.0))())
+    T.set_macro(1, *cases.uniform_init(tl.fine_box(), 1.0, (0.03, -0.01, 0.0))())
+    T.init_equilibrium()
+    T.step(4)
+    for lev in (0, 1):
+        m = T.get_macro(lev)
+        assert np.abs(m[1] - 0.03).max() < 1e-14 and np.abs(m[2] + 0.01).max() < 1e-14
+    tl2, ic, if_ = cases.shear_layer_two_level(n=32, fine=(16, 48))
+    T2 = CpuTwoLevel(tl2)
+    T2.set_macro(0, *ic())
+    T2.set_macro(1, *if_())
+    T2.init_equilibrium()
+    T2.step(3)
+    fc, ff = T2.get_f(0), T2.get_f(1)
+    sub = ff[:, 0]
+    mean = 0.25 * (((sub[:, 0::2, 0::2] + sub[:, 0::2, 1::2]) + sub[:, 1::2, 0::2]) + sub[:, 1::2, 1::2])
+    np.testing.assert_array_equal(fc[:, 0, 8:24, 8:24], mean)

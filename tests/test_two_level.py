@@ -1,0 +1,101 @@
+"""Static two-level hierarchy on the GPU (ilbm_advance_two_level) against the
+oracle's two-level driver (oracle/lbm_oracle.c, orc2_*), same seeded fields.
+
+FP64 storage without a body: both levels' populations and stored macro
+fields bit for bit (the coarse-fine fill, the subcycled steps and the
+average-down keep the oracle's operation order).  With a body on the fine
+level the marker forces are spread with FP64 atomics: relative L2 <= 1e-12
+and force coefficients to 1e-9.  FP32 / FP16 storage: the velocity fields
+within the bounds of the single-level storage tests.
+"""
+import numpy as np
+import pytest
+
+from ilbmrex_b200 import cases
+from oracle.checker import CpuTwoLevel
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+from ilbmrex_b200.hierarchy import TwoLevelSolver  # noqa: E402
+
+
+def rel_l2(a, b):
+    return float(np.sqrt(np.sum((a - b) ** 2) / max(np.sum(b ** 2), 1e-300)))
+
+
+def _pair(tl, ic, if_, ib, storage, steps):
+    cpu = CpuTwoLevel(tl)
+    cpu.set_macro(0, *ic())
+    cpu.set_macro(1, *if_())
+    cpu.init_equilibrium()
+    if ib is not None:
+        cpu.ib_create(ib)
+    gpu = TwoLevelSolver(tl, storage, ib=ib)
+    gpu.set_macro(ic(), if_())
+    for lev in (0, 1):
+        if storage == "f64":
+            np.testing.assert_array_equal(gpu.get_f(lev), cpu.get_f(lev))
+    cpu.step(steps)
+    gpu.step(steps, record_force=ib is not None)
+    return cpu, gpu
+
+
+@pytest.mark.parametrize("lattice", ["d2q9", "d3q19"])
+def test_shear_layer_bit_exact(lattice):
+    if lattice == "d2q9":
+        tl, ic, if_ = cases.shear_layer_two_level(n=48, fine=(24, 72))
+        steps = 12
+    else:
+        tl, ic, if_ = cases.shear_layer_two_level(n=20, fine=(12, 28), lattice=cases.D3Q19)
+        steps = 5
+    cpu, gpu = _pair(tl, ic, if_, None, "f64", steps)
+    for lev in (0, 1):
+        np.testing.assert_array_equal(gpu.get_f(lev), cpu.get_f(lev))
+        np.testing.assert_array_equal(gpu.get_macro(lev), cpu.get_macro(lev))
+    # the fine level carries structure the coarse one does not resolve alone
+    assert np.abs(gpu.get_macro(1)[1]).max() > 0.0
+    gpu.close()
+
+
+def test_cylinder_body_on_fine_level():
+    tl, ib, ic, if_ = cases.cylinder_two_level(nx=96, ny=64, D=12.0, center=(32.3, 31.7), U=0.05,
+                                               Re=40.0, upstream=1.0, downstream=2.0, cross=1.2)
+    cpu, gpu = _pair(tl, ic, if_, ib, "f64", 6)
+    for lev in (0, 1):
+        assert rel_l2(gpu.get_f(lev), cpu.get_f(lev)) <= 1e-12
+    np.testing.assert_allclose(gpu.rec[3:5], cpu.force_record()[3:5], rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(gpu.marker_force_sum(), cpu.marker_force_sum(), rtol=1e-9, atol=1e-14)
+    gpu.close()
+
+
+@pytest.mark.parametrize("storage,tol", [("f32", 2e-5), ("f16", 5e-3)])
+def test_shear_layer_storage_forms(storage, tol):
+    tl, ic, if_ = cases.shear_layer_two_level(n=48, fine=(24, 72))
+    cpu, gpu = _pair(tl, ic, if_, None, storage, 12)
+    for lev in (0, 1):
+        g, c = gpu.get_macro(lev), cpu.get_macro(lev)
+        scale = np.abs(c[1:3]).max()  # the flow's velocity scale
+        for n in (1, 2):
+            assert np.abs(g[n] - c[n]).max() <= tol * scale, (lev, n)
+    gpu.close()
+
+
+def test_uniform_flow_stays_uniform():
+    """A uniform state is a fixed point of the coarse-fine fill, the
+    subcycling and the average-down."""
+    c = cases.LevelCase(cases.D2Q9, (32, 32, 1), nu=0.02)
+    tl = cases.TwoLevelCase(c, (16, 16), (47, 47))
+    ic = cases.uniform_init(c, 1.0, (0.03, -0.01, 0.0))
+    if_ = cases.uniform_init(tl.fine_box(), 1.0, (0.03, -0.01, 0.0))
+    gpu = TwoLevelSolver(tl, "f64")
+    gpu.set_macro(ic(), if_())
+    gpu.step(6)
+    for lev in (0, 1):
+        m = gpu.get_macro(lev)
+        assert np.abs(m[1] - 0.03).max() < 1e-14 and np.abs(m[2] + 0.01).max() < 1e-14
+        assert np.abs(m[0] - 1.0).max() < 1e-14
+    gpu.close()
