@@ -18,6 +18,7 @@ ILBM_ERR_ARG, ILBM_ERR_CUDA, ILBM_ERR_UNSUPPORTED = -1, -2, -3
 ILBM_ERR_NOMEM, ILBM_ERR_SOLVER, ILBM_ERR_RANGE = -4, -5, -6
 ILBM_ERR_IO = -7
 CKPT_MACRO, CKPT_FORCE, CKPT_BODY = 1, 2, 4
+TWO_LEVEL_FIRST_STEP = 1
 STORAGE = {"f64": 0, "f32": 1, "f16": 2}
 GHOST_SELF, GHOST_CALLER = 0, 1
 IVC_AUTO, IVC_CG, IVC_DENSE = 0, 1, 2
@@ -169,7 +170,7 @@ def lib():
                                C.POINTER(I64)]),
         "ilbm_batch_progress": (I, [P, I, C.POINTER(I), C.POINTER(I64), C.POINTER(I), C.POINTER(I)]),
         "ilbm_advance_two_level": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), C.POINTER(Box_t),
-                                       C.POINTER(LevelParams_t), P, D, D]),
+                                       C.POINTER(LevelParams_t), P, D, D, I]),
         "ilbm_average_down": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), C.POINTER(Box_t),
                                   C.POINTER(LevelParams_t)]),
         "ilbm_checkpoint_write": (I, [P, C.POINTER(Box_t), P, C.POINTER(CheckpointMeta_t), C.c_char_p]),

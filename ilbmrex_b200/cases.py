@@ -382,3 +382,18 @@ def cylinder_two_level(nx=256, ny=128, D=24.0, center=(64.3, 63.7), U=0.05, Re=1
     tl = TwoLevelCase(case, tuple(lo), tuple(hi), name=f"cylinder{nx}x{ny}_2lev")
     init_f = uniform_init(tl.fine_box(), 1.0, (U, 0.0, 0.0))
     return tl, ib, init_c, init_f
+
+
+def sphere_two_level(nx=256, ny=128, nz=128, D=32.0, center=(64.0, 64.0, 64.0), U=0.04, Re=100.0,
+                     box_lo=(32, 32, 32), box_hi=(128, 96, 96), lattice: Lattice = D3Q19):
+    """The D3Q19 sphere on two levels: base grid as ``sphere`` plus one
+    refined level (ratio 2) over the base-cell box [box_lo, box_hi) around
+    the sphere, on which the marker IBM runs with markers about one fine cell
+    apart (golden-spiral lattice, IBMarkerDF.cpp:385-421: ~4 pi R^2 / dx_f^2
+    points, 12.9k for D = 32 base cells)."""
+    case, ib, init_c = sphere(nx, ny, nz, D=D, center=center, U=U, Re=Re, lattice=lattice)
+    lo = tuple(2 * int(v) for v in box_lo)
+    hi = tuple(2 * int(v) - 1 for v in box_hi)
+    tl = TwoLevelCase(case, lo, hi, name=f"sphere{nx}x{ny}x{nz}_2lev")
+    init_f = uniform_init(tl.fine_box(), 1.0, (U, 0.0, 0.0))
+    return tl, ib, init_c, init_f

@@ -13,6 +13,10 @@ struct ilbm_ib;
 namespace ilbm {
 
 // ---- lbm_step.cu --------------------------------------------------------
+// the level step with a stored-macro box (the two-level hierarchy's coarse
+// level); mlo / mhi NULL: ilbm_level_step
+int level_step_impl(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const ilbm_level_params *p,
+                    const int *mlo, const int *mhi);
 // StepArgs of one batched case (self-filled ghosts, one box = domain)
 int batch_case_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p,
                     StepArgs *out);
@@ -30,6 +34,19 @@ int batch_band_macro_launch(ilbm_ctx *ctx, const StepArgs *d_args, const BandDes
 int batch_step_occupancy(const ilbm_ctx *ctx, int w, int *per_sm);
 
 // ---- ib.cu ----------------------------------------------------------------
+// ilbm_advance_level in two halves: begin starts the body's update_forcing
+// (on the side stream, after the work queued so far on the main stream, when
+// it may overlap), end runs the level step of the cells outside the body's
+// band and then the band.  Work the caller queues in between on the main
+// stream overlaps the body's forcing.
+struct AdvanceSplit {
+  ilbm_level_params q;  // the level's parameters with the body's force region
+  int lo[3], hi[3];     // the body's band
+  bool serial;          // no overlap: forcing first, then the whole step
+};
+int advance_begin(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p, ilbm_ib *ib,
+                  double dt, double time, AdvanceSplit *sp);
+int advance_end(ilbm_ctx *ctx, const ilbm_box *box, const AdvanceSplit *sp);
 struct IBBatch;
 
 struct IBBatchCase {

@@ -19,11 +19,13 @@
 // the reference's operation order.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include <cooperative_groups.h>
 
+#include "batch_internal.h"
 #include "ilbm_common.cuh"
 #include "state_internal.h"
 
@@ -1572,13 +1574,19 @@ int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom
       ilbm_ib_destroy(ib);
       return rc;
     }
-    // grid-wide CG: as many co-resident blocks as the device holds, at most 2 per SM
+    // grid-wide CG: as many co-resident blocks as the device holds, at most 2
+    // per SM (fastest beside the level step it overlaps; ILBM_CG_BLOCKS_PER_SM
+    // overrides it, up to the co-resident maximum)
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ivc_cg_grid, 256, 0);
     ib->cg_blocks = std::max(1, std::min(2, per_sm) * sms);
-    if ((rc = dmalloc(ib, &ib->d_partial, 8 * (size_t)std::max(ib->cg_blocks, 16)))) {
+    if (const char *e = std::getenv("ILBM_CG_BLOCKS_PER_SM")) {
+      const int b = std::atoi(e);
+      if (b >= 1) ib->cg_blocks = std::max(1, std::min(b, per_sm) * sms);
+    }
+    if ((rc = dmalloc(ib, &ib->d_partial, 8 * (size_t)std::max(per_sm * sms, 16)))) {
       ilbm_ib_destroy(ib);
       return rc;
     }
@@ -1808,6 +1816,62 @@ static int ib_finish(ilbm_ib *ib, cudaStream_t s) {
   return ILBM_OK;
 }
 
+namespace ilbm {
+
+int advance_begin(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p, ilbm_ib *ib,
+                  double dt, double time, AdvanceSplit *sp) {
+  if (ib->ctx != ctx) {
+    set_error("ilbm_advance_level: the IB object belongs to another context");
+    return ILBM_ERR_ARG;
+  }
+  sp->q = *p;
+  ilbm_ib_force_region(ib, sp->lo, sp->hi);
+  for (int d = 0; d < 3; ++d) {
+    sp->q.force_lo[d] = sp->lo[d];
+    sp->q.force_hi[d] = sp->hi[d];
+  }
+  // caller-filled ghosts covered by other boxes of the level may carry their
+  // IB forces, so those levels run serially; one box that holds the whole
+  // band (the fine box of a two-level hierarchy) overlaps like self-fill
+  bool band_inside = p->nlevel_boxes <= 1 && box->f_in != box->f_out;
+  for (int d = 0; d < ctx->dim; ++d)
+    band_inside = band_inside && sp->lo[d] >= box->lo[d] && sp->hi[d] <= box->hi[d];
+  sp->serial = (p->ghost_mode != ILBM_GHOST_SELF && !band_inside);
+  if (sp->serial) return ib_update(ib, box, &sp->q, dt, time, ctx->stream, false);
+  // validate like ilbm_level_step does before anything is launched
+  if ((p->ghost_mode == ILBM_GHOST_SELF && box->lo[0] != p->domain_lo[0]) || box->f_in == box->f_out) {
+    set_error("ilbm_advance_level: self-fill needs one box equal to the domain, f_in != f_out");
+    return ILBM_ERR_ARG;
+  }
+  // the IB chain runs on the side stream, after what the main stream holds so
+  // far, while the main stream goes on with other work
+  cudaError_t e = cudaEventRecord(ctx->ev_fork, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level fork");
+  int rc = ib_update(ib, box, &sp->q, dt, time, ctx->side, true);
+  if (rc) return rc;
+  e = cudaEventRecord(ctx->ev_join, ctx->side);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level join");
+  // the marker force sum runs beside the band's collide-stream
+  if ((rc = ib_finish(ib, ctx->side))) return rc;
+  e = cudaEventRecord(ctx->ev_done, ctx->side);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level done");
+  return ILBM_OK;
+}
+
+int advance_end(ilbm_ctx *ctx, const ilbm_box *box, const AdvanceSplit *sp) {
+  if (sp->serial) return ilbm_level_step(ctx, box, 1, &sp->q);
+  // the collide-stream of every cell outside the band, then the band once
+  // the body's forcing is in
+  int rc = level_step_split(ctx, *box, &sp->q, sp->lo, sp->hi, ctx->ev_join);
+  if (rc) return rc;
+  cudaError_t e = cudaStreamWaitEvent(ctx->stream, ctx->ev_done, 0);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level wait");
+  return ILBM_OK;
+}
+
+}  // namespace ilbm
+
 extern "C" {
 
 int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *lp,
@@ -1826,45 +1890,10 @@ int ilbm_advance_level(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_para
     return ILBM_ERR_ARG;
   }
   if (!ib) return ilbm_level_step(ctx, box, 1, p);
-  if (ib->ctx != ctx) {
-    set_error("ilbm_advance_level: the IB object belongs to another context");
-    return ILBM_ERR_ARG;
-  }
-  ilbm_level_params q = *p;
-  int lo[3], hi[3];
-  ilbm_ib_force_region(ib, lo, hi);
-  for (int d = 0; d < 3; ++d) {
-    q.force_lo[d] = lo[d];
-    q.force_hi[d] = hi[d];
-  }
-  if (p->ghost_mode != ILBM_GHOST_SELF) {
-    // caller-filled ghosts may carry IB forces of neighbouring boxes: serial
-    int rc = ib_update(ib, box, &q, dt, time, ctx->stream, false);
-    if (rc) return rc;
-    return ilbm_level_step(ctx, box, 1, &q);
-  }
-  // the IB chain runs on the side stream while the collide-stream of every
-  // cell outside its band runs on the main stream; the band waits for it
-  cudaError_t e = cudaEventRecord(ctx->ev_fork, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0);
-  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level fork");
-  // validate like ilbm_level_step does before anything is launched
-  if (box->lo[0] != p->domain_lo[0] || box->f_in == box->f_out) {
-    set_error("ilbm_advance_level: self-fill needs one box equal to the domain, f_in != f_out");
-    return ILBM_ERR_ARG;
-  }
-  int rc = ib_update(ib, box, &q, dt, time, ctx->side, true);
+  AdvanceSplit sp;
+  int rc = advance_begin(ctx, box, p, ib, dt, time, &sp);
   if (rc) return rc;
-  e = cudaEventRecord(ctx->ev_join, ctx->side);
-  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level join");
-  // the marker force sum runs beside the band's collide-stream
-  if ((rc = ib_finish(ib, ctx->side))) return rc;
-  e = cudaEventRecord(ctx->ev_done, ctx->side);
-  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level done");
-  if ((rc = level_step_split(ctx, *box, &q, lo, hi, ctx->ev_join))) return rc;
-  e = cudaStreamWaitEvent(ctx->stream, ctx->ev_done, 0);
-  if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level wait");
-  return ILBM_OK;
+  return advance_end(ctx, box, &sp);
 }
 
 int ilbm_ib_last_marker_force_sum(ilbm_ib *ib, double out[3]) {
@@ -1970,7 +1999,6 @@ void ib_set_cg_warm(ilbm_ib *ib, bool warm) { ib->cg_warm = warm && ib->d_X != n
 // kinematics from a per-step table filled on the host with the same
 // arithmetic as make_args.
 // ---------------------------------------------------------------------------
-#include "batch_internal.h"
 
 namespace {
 

@@ -210,6 +210,44 @@ struct Store<ILBM_STORAGE_F16_SCALED> {
   __device__ static __forceinline__ void store(T *p, R v, float s) { *p = __float2half_rn(v / s); }
 };
 
+// rho, u of a cell from its populations and the previous force
+// (calculateMacroForcing.H:155-166, exact order in FP64)
+template <class L>
+__device__ __forceinline__ void moments64(const double *f, double Fx, double Fy, double Fz,
+                                          double &rho, double &u, double &v, double &w) {
+  double r = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    r = X::add(r, f[q]);
+    m1 = X::add(m1, X::mul(double(L::cx(q)), f[q]));
+    m2 = X::add(m2, X::mul(double(L::cy(q)), f[q]));
+    m3 = X::add(m3, X::mul(double(L::cz(q)), f[q]));
+  }
+  rho = r;
+  u = X::div(X::add(m1, X::mul(0.5, Fx)), r);
+  v = X::div(X::add(m2, X::mul(0.5, Fy)), r);
+  w = X::div(X::add(m3, X::mul(0.5, Fz)), r);
+}
+
+// shifted form (g = f - w): drho = rho - 1
+template <class L>
+__device__ __forceinline__ void moments32(const float *g, float Fx, float Fy, float Fz,
+                                          float &drho, float &u, float &v, float &w) {
+  float r = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f;
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) {
+    r += g[q];
+    if (L::cx(q)) m1 += float(L::cx(q)) * g[q];
+    if (L::cy(q)) m2 += float(L::cy(q)) * g[q];
+    if (L::cz(q)) m3 += float(L::cz(q)) * g[q];
+  }
+  drho = r;
+  const float inv = 1.0f / (1.0f + r);
+  u = (m1 + 0.5f * Fx) * inv;
+  v = (m2 + 0.5f * Fy) * inv;
+  w = (m3 + 0.5f * Fz) * inv;
+}
+
 // shifted equilibrium: f_eq - w_q
 __device__ __forceinline__ float feqsv(float cx, float cy, float cz, float wq, float drho, float u,
                                        float v, float w) {

@@ -104,44 +104,6 @@ __device__ __forceinline__ void load_force(const StepArgs &a, const void *F, int
 // Per-cell physics in the two arithmetic forms
 // ---------------------------------------------------------------------------
 
-// rho, u of a cell from its populations and the previous force
-// (calculateMacroForcing.H:155-166, exact order in FP64)
-template <class L>
-__device__ __forceinline__ void moments64(const double *f, double Fx, double Fy, double Fz,
-                                          double &rho, double &u, double &v, double &w) {
-  double r = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
-#pragma unroll
-  for (int q = 0; q < L::Q; ++q) {
-    r = X::add(r, f[q]);
-    m1 = X::add(m1, X::mul(double(L::cx(q)), f[q]));
-    m2 = X::add(m2, X::mul(double(L::cy(q)), f[q]));
-    m3 = X::add(m3, X::mul(double(L::cz(q)), f[q]));
-  }
-  rho = r;
-  u = X::div(X::add(m1, X::mul(0.5, Fx)), r);
-  v = X::div(X::add(m2, X::mul(0.5, Fy)), r);
-  w = X::div(X::add(m3, X::mul(0.5, Fz)), r);
-}
-
-// shifted form (g = f - w): drho = rho - 1
-template <class L>
-__device__ __forceinline__ void moments32(const float *g, float Fx, float Fy, float Fz,
-                                          float &drho, float &u, float &v, float &w) {
-  float r = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f;
-#pragma unroll
-  for (int q = 0; q < L::Q; ++q) {
-    r += g[q];
-    if (L::cx(q)) m1 += float(L::cx(q)) * g[q];
-    if (L::cy(q)) m2 += float(L::cy(q)) * g[q];
-    if (L::cz(q)) m3 += float(L::cz(q)) * g[q];
-  }
-  drho = r;
-  const float inv = 1.0f / (1.0f + r);
-  u = (m1 + 0.5f * Fx) * inv;
-  v = (m2 + 0.5f * Fy) * inv;
-  w = (m3 + 0.5f * Fz) * inv;
-}
-
 template <int D>
 __device__ __forceinline__ float guo32v(float cx, float cy, float cz, float wq, float omh, float u,
                                         float v, float w, float Fx, float Fy, float Fz) {
@@ -367,7 +329,7 @@ __device__ __noinline__ void ghost_push(const StepArgs &a, int64_t gid, int64_t 
     } else if (mode == 2) {
       load_force<L, R>(a, a.force, g[0], g[1], gk, gFx, gFy, gFz);
       ghf = !(gFx == R(0) && gFy == R(0) && gFz == R(0));
-      if (a.macro_in) {
+      if (stored_macro_at(a, g[0], g[1], gk)) {
         const int64_t m = midx(a, g[0], g[1], gk);
         if (S == ILBM_STORAGE_F64) {
           r64 = ldm<double>(a.macro_in, m);
@@ -468,8 +430,9 @@ __device__ __forceinline__ void cell_finish(const StepArgs &a, int i, int j, int
   // per-cell collision state: rho^n, u^n (stored or recovered) and F^n
   double rho64 = 0, u64 = 0, v64 = 0, w64 = 0;
   float drho32 = 0, u32 = 0, v32 = 0, w32 = 0;
+  const bool stored = stored_macro_at(a, i, j, k);
   if (S == ILBM_STORAGE_F64) {
-    if (a.macro_in) {
+    if (stored) {
       const int64_t m = midx(a, i, j, k);
       rho64 = ldm<double>(a.macro_in, m);
       u64 = ldm<double>(a.macro_in, m + a.ms2);
@@ -482,7 +445,7 @@ __device__ __forceinline__ void cell_finish(const StepArgs &a, int i, int j, int
       if (L::D != 3) w64 = 0.0;
     }
   } else {
-    if (a.macro_in) {
+    if (stored) {
       const int64_t m = midx(a, i, j, k);
       drho32 = ldm<float>(a.macro_in, m) - 1.0f;
       u32 = ldm<float>(a.macro_in, m + a.ms2);
@@ -844,7 +807,7 @@ __global__ void __launch_bounds__(256) k_init_eq(StepArgs a, int ng) {
 // ---------------------------------------------------------------------------
 template <class L, int S>
 __device__ void macro_at(const StepArgs &a, int i, int j, int k, double *m4) {
-  if (a.macro_in) {
+  if (stored_macro_at(a, i, j, k)) {
     const int64_t m = midx(a, i, j, k);
     if (S == ILBM_STORAGE_F64) {
       m4[0] = ldm<double>(a.macro_in, m);
@@ -1524,6 +1487,85 @@ __global__ void __launch_bounds__(256) k_tags(TagArgs g, const R *vor, unsigned 
   if ((threadIdx.x & 31) == 0 && mine) atomicAdd(count, mine);
 }
 
+// one level step; with mlo / mhi the boxes' macro_in holds stored values
+// only on [mlo, mhi] (elsewhere rho, u are recovered from f^n and F^{n-1}),
+// and macro_out is written there only
+int level_step_impl(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const ilbm_level_params *p,
+                    const int *mlo, const int *mhi) {
+  if (!ctx || !boxes || nbox <= 0) {
+    set_error("level step: null argument");
+    return ILBM_ERR_ARG;
+  }
+  int rc = check_params(ctx, p);
+  if (rc) return rc;
+  for (int n = 0; n < nbox; ++n)
+    if (boxes[n].ngrow_f < 1) {
+      set_error("f arrays need at least one ghost layer (edge cells push into it as scratch)");
+      return ILBM_ERR_ARG;
+    }
+  if (p->ghost_mode == ILBM_GHOST_SELF) {
+    if (nbox != 1) {
+      set_error("self-fill ghost mode needs exactly one box covering the domain");
+      return ILBM_ERR_ARG;
+    }
+    for (int d = 0; d < ctx->dim; ++d)
+      if (boxes[0].lo[d] != p->domain_lo[d] || boxes[0].hi[d] != p->domain_hi[d]) {
+        set_error("self-fill ghost mode: the box must equal the domain");
+        return ILBM_ERR_ARG;
+      }
+
+  } else if (p->ghost_mode != ILBM_GHOST_CALLER) {
+    set_error("unknown ghost mode");
+    return ILBM_ERR_ARG;
+  }
+  for (int n = 0; n < nbox; ++n) {
+    const ilbm_box &b = boxes[n];
+    if ((rc = check_box(ctx, b, true))) return rc;
+    if (p->ghost_mode == ILBM_GHOST_CALLER && b.ngrow_f < 1) {
+      set_error("caller ghost mode needs ngrow_f >= 1");
+      return ILBM_ERR_ARG;
+    }
+    if (p->ghost_mode == ILBM_GHOST_CALLER && (b.macro_in || b.force || b.force_prev) &&
+        b.ngrow_m < 1) {
+      set_error("caller ghost mode reads macro/force ghosts: needs ngrow_m >= 1");
+      return ILBM_ERR_ARG;
+    }
+    if ((b.macro_in || b.macro_out || b.force || b.force_prev) &&
+        (b.mstride[0] <= 0 || b.mstride[1] <= 0 || b.mstride[2] <= 0)) {
+      set_error("box: macro/force strides must be positive");
+      return ILBM_ERR_ARG;
+    }
+    if (b.f_in == b.f_out) {
+      set_error("f_in and f_out must be distinct (two-lattice scheme)");
+      return ILBM_ERR_ARG;
+    }
+    StepArgs a;
+    if ((rc = fill_args(ctx, b, p, a))) return rc;
+    if (mlo && mhi) {
+      a.use_mbox = 1;
+      for (int d = 0; d < 3; ++d) {
+        a.mblo[d] = (d < ctx->dim) ? mlo[d] : 0;
+        a.mbhi[d] = (d < ctx->dim) ? mhi[d] : 0;
+      }
+    }
+    rc = ILBM_DISPATCH(ctx, launch_step, ctx, a, p);
+    if (rc) return rc;
+    if (b.macro_out) {
+      StepArgs am = a;
+      am.f_in = b.f_out;
+      int rlo[3] = {a.lo[0], a.lo[1], a.lo[2]}, rhi[3] = {a.hi[0], a.hi[1], a.hi[2]};
+      if (a.use_mbox)  // stored values are kept on the macro box only
+        for (int d = 0; d < ctx->dim; ++d) {
+          rlo[d] = std::max(rlo[d], a.mblo[d]);
+          rhi[d] = std::min(rhi[d], a.mbhi[d]);
+        }
+      rc = ILBM_DISPATCH(ctx, launch_macro, ctx, am, rlo, rhi, b.macro_out);
+      if (rc) return rc;
+    }
+  }
+  return ILBM_OK;
+}
+
 }  // namespace ilbm
 
 using namespace ilbm;
@@ -1721,66 +1763,7 @@ int ilbm_storage_bytes(const ilbm_ctx *ctx, int *sb, int *rb) {
 }
 
 int ilbm_level_step(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const ilbm_level_params *p) {
-  if (!ctx || !boxes || nbox <= 0) {
-    set_error("ilbm_level_step: null argument");
-    return ILBM_ERR_ARG;
-  }
-  int rc = check_params(ctx, p);
-  if (rc) return rc;
-  for (int n = 0; n < nbox; ++n)
-    if (boxes[n].ngrow_f < 1) {
-      set_error("f arrays need at least one ghost layer (edge cells push into it as scratch)");
-      return ILBM_ERR_ARG;
-    }
-  if (p->ghost_mode == ILBM_GHOST_SELF) {
-    if (nbox != 1) {
-      set_error("self-fill ghost mode needs exactly one box covering the domain");
-      return ILBM_ERR_ARG;
-    }
-    for (int d = 0; d < ctx->dim; ++d)
-      if (boxes[0].lo[d] != p->domain_lo[d] || boxes[0].hi[d] != p->domain_hi[d]) {
-        set_error("self-fill ghost mode: the box must equal the domain");
-        return ILBM_ERR_ARG;
-      }
-
-  } else if (p->ghost_mode != ILBM_GHOST_CALLER) {
-    set_error("unknown ghost mode");
-    return ILBM_ERR_ARG;
-  }
-  for (int n = 0; n < nbox; ++n) {
-    const ilbm_box &b = boxes[n];
-    if ((rc = check_box(ctx, b, true))) return rc;
-    if (p->ghost_mode == ILBM_GHOST_CALLER && b.ngrow_f < 1) {
-      set_error("caller ghost mode needs ngrow_f >= 1");
-      return ILBM_ERR_ARG;
-    }
-    if (p->ghost_mode == ILBM_GHOST_CALLER && (b.macro_in || b.force || b.force_prev) &&
-        b.ngrow_m < 1) {
-      set_error("caller ghost mode reads macro/force ghosts: needs ngrow_m >= 1");
-      return ILBM_ERR_ARG;
-    }
-    if ((b.macro_in || b.macro_out || b.force || b.force_prev) &&
-        (b.mstride[0] <= 0 || b.mstride[1] <= 0 || b.mstride[2] <= 0)) {
-      set_error("box: macro/force strides must be positive");
-      return ILBM_ERR_ARG;
-    }
-    if (b.f_in == b.f_out) {
-      set_error("f_in and f_out must be distinct (two-lattice scheme)");
-      return ILBM_ERR_ARG;
-    }
-    StepArgs a;
-    if ((rc = fill_args(ctx, b, p, a))) return rc;
-    rc = ILBM_DISPATCH(ctx, launch_step, ctx, a, p);
-    if (rc) return rc;
-    if (b.macro_out) {
-      StepArgs am = a;
-      am.f_in = b.f_out;
-      int rlo[3] = {a.lo[0], a.lo[1], a.lo[2]}, rhi[3] = {a.hi[0], a.hi[1], a.hi[2]};
-      rc = ILBM_DISPATCH(ctx, launch_macro, ctx, am, rlo, rhi, b.macro_out);
-      if (rc) return rc;
-    }
-  }
-  return ILBM_OK;
+  return level_step_impl(ctx, boxes, nbox, p, nullptr, nullptr);
 }
 
 int ilbm_compute_macro(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,

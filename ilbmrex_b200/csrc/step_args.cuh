@@ -44,7 +44,19 @@ struct StepArgs {
   int act_lo[3], act_hi[3];  // face returns outgoing populations (wrap / reflect)
   int nlb;
   int lb[kMaxLevelBoxes][6];
+  // with use_mbox, macro_in holds stored values only on [mblo, mbhi]; cells
+  // outside recover rho, u from f^n and F^{n-1}
+  int use_mbox;
+  int mblo[3], mbhi[3];
 };
+
+// the cell's rho, u come from macro_in (else from its populations)
+__device__ __forceinline__ bool stored_macro_at(const StepArgs &a, int i, int j, int k) {
+  if (!a.macro_in) return false;
+  if (!a.use_mbox) return true;
+  return i >= a.mblo[0] && i <= a.mbhi[0] && j >= a.mblo[1] && j <= a.mbhi[1] && k >= a.mblo[2] &&
+         k <= a.mbhi[2];
+}
 
 // One work item of the batched level step (k_step_batch): a row segment of
 // blockDim.x cells of case c starting at (i0, j, k), or, when i0 < 0, chunk

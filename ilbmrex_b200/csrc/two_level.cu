@@ -12,13 +12,15 @@
 //                     cell_cons_interp, FillPatchMacro :2166-2198); the ghost
 //                     populations are the equilibrium of that macro state
 //                     (FillPatchMesoscopic's coarse-fine overwrite,
-//                     :1566-1626).  One thread per cell of the grown fine box;
-//                     valid cells return at once.
+//                     :1566-1626).  One thread per cell of the ghost shell.
 //   k_avg_down<L,S>   amrex::average_down of ratio 2 (AverageDownTo,
 //                     :1519-1527) of the fine populations and macro fields
 //                     onto the covered coarse cells, one thread per coarse
 //                     cell: the sum of the 2^d fine cells (k, j, i inner)
-//                     times the volume fraction.
+//                     times the volume fraction.  The fine macro fields are
+//                     those of the fine populations with the last substep's
+//                     force (calculateMacroForcing), computed from the
+//                     populations the kernel loads anyway.
 // Both are HBM-bound gathers; FP64 storage reproduces the oracle's
 // arithmetic bit for bit (separately rounded products and sums).
 
@@ -26,6 +28,8 @@
 #include <cmath>
 #include <cstring>
 
+#include "batch_internal.h"
+#include "ilbm_b200.h"
 #include "ilbm_common.cuh"
 
 namespace ilbm {
@@ -37,7 +41,7 @@ struct CFArgs {
   int64_t fs0, fs1, fs2;   // fine f strides
   int64_t ms0, ms1, ms2;   // fine macro strides
   void *f;                 // fine f_in (storage type)
-  void *m;                 // fine macro_in (real type, rho u v w)
+  void *m;                 // fine macro_in (real type, rho u v w) or NULL
   const void *cold, *cnew; // coarse macro at the coarse step's start / end
   int clo[3], cgm;         // coarse box lo and macro ghost width
   int64_t cs0, cs1, cs2;   // coarse macro strides
@@ -67,24 +71,65 @@ __device__ __forceinline__ double mc_slope(double cl, double c, double cr) {
 
 __device__ __forceinline__ int floor_half(int v) { return (v >= 0) ? v / 2 : -((1 - v) / 2); }
 
+// The ghost shell of width w around the fine box, as one slab per
+// dimension: slab d holds the cells outside the box in dimension d and inside
+// it in every dimension below d (grown range in the dimensions above), so
+// every shell cell is counted once.
+template <int D>
+struct Shell {
+  int lo[3], n[3], w;  // box lo, box extents, shell width
+  int64_t off[4];      // first shell index of each slab, and the total
+  __host__ __device__ void init(const int *blo, const int *bhi, int width) {
+    w = width;
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = blo[d];
+      n[d] = (d < D) ? bhi[d] - blo[d] + 1 : 1;
+    }
+    off[0] = 0;
+    for (int d = 0; d < 3; ++d) {
+      int64_t c = 0;
+      if (d < D) {
+        c = 2 * w;
+        for (int e = 0; e < D; ++e)
+          if (e != d) c *= (e < d) ? n[e] : n[e] + 2 * w;
+      }
+      off[d + 1] = off[d] + c;
+    }
+  }
+  __host__ __device__ int64_t total() const { return off[3]; }
+  // cell t of the shell (fine-domain indices)
+  __device__ void cell(int64_t t, int *g) const {
+    const int d = (t >= off[1]) + (t >= off[2]);
+    int64_t r = t - (d == 0 ? off[0] : (d == 1 ? off[1] : off[2]));
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      if (e >= D) {
+        g[e] = 0;
+        continue;
+      }
+      const int ext = (e == d) ? 2 * w : ((e < d) ? n[e] : n[e] + 2 * w);
+      const int c = (int)(r % ext);
+      r /= ext;
+      if (e == d) g[e] = (c < w) ? lo[e] - w + c : lo[e] + n[e] + (c - w);
+      else if (e < d) g[e] = lo[e] + c;
+      else g[e] = lo[e] - w + c;
+    }
+  }
+};
+
 template <class L, int S>
-__global__ void __launch_bounds__(256) k_cf_fill(CFArgs g) {
+__global__ void __launch_bounds__(256) k_cf_fill(CFArgs g, Shell<L::D> sh) {
   using T = typename Store<S>::T;
   using R = typename Store<S>::R;
-  const int nx = g.hi[0] - g.lo[0] + 1 + 2 * g.gm, ny = g.hi[1] - g.lo[1] + 1 + 2 * g.gm;
-  const int nz = (L::D == 3) ? g.hi[2] - g.lo[2] + 1 + 2 * g.gm : 1;
-  const int64_t n = (int64_t)nx * ny * nz;
+  const int64_t n = sh.total();
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x) {
     int fi[3];
-    fi[0] = g.lo[0] - g.gm + (int)(t % nx);
-    fi[1] = g.lo[1] - g.gm + (int)((t / nx) % ny);
-    fi[2] = (L::D == 3) ? g.lo[2] - g.gm + (int)(t / ((int64_t)nx * ny)) : 0;
+    sh.cell(t, fi);
     int layer = 0;  // Chebyshev distance outside the box
 #pragma unroll
     for (int d = 0; d < L::D; ++d)
       layer = max(layer, max(g.lo[d] - fi[d], fi[d] - g.hi[d]));
-    if (layer <= 0) continue;
     int ic[3] = {0, 0, 0};
     double off[3] = {0.0, 0.0, 0.0};
 #pragma unroll
@@ -112,11 +157,13 @@ __global__ void __launch_bounds__(256) k_cf_fill(CFArgs g) {
       }
       mv[c] = v;
     }
-    const int64_t mi = (int64_t)(fi[0] - g.lo[0] + g.gm) + (int64_t)(fi[1] - g.lo[1] + g.gm) * g.ms0 +
-                       ((L::D == 3) ? (int64_t)(fi[2] - g.lo[2] + g.gm) * g.ms1 : 0);
-    R *m = static_cast<R *>(g.m);
+    if (g.m) {
+      const int64_t mi = (int64_t)(fi[0] - g.lo[0] + g.gm) + (int64_t)(fi[1] - g.lo[1] + g.gm) * g.ms0 +
+                         ((L::D == 3) ? (int64_t)(fi[2] - g.lo[2] + g.gm) * g.ms1 : 0);
+      R *m = static_cast<R *>(g.m);
 #pragma unroll
-    for (int c = 0; c < 4; ++c) m[mi + c * g.ms2] = R(mv[c]);
+      for (int c = 0; c < 4; ++c) m[mi + c * g.ms2] = R(mv[c]);
+    }
     if (layer > g.gf) continue;
     const int64_t bi = (int64_t)(fi[0] - g.lo[0] + g.gf) + (int64_t)(fi[1] - g.lo[1] + g.gf) * g.fs0 +
                        ((L::D == 3) ? (int64_t)(fi[2] - g.lo[2] + g.gf) * g.fs1 : 0);
@@ -146,11 +193,62 @@ struct AvgArgs {
   int64_t ffs0, ffs1, ffs2, fms0, fms1, fms2;  // fine strides (f, macro)
   int64_t cfs0, cfs1, cfs2, cms0, cms1, cms2;  // coarse strides
   int cblo[3];             // coarse box lo
-  const void *ff, *fm;     // fine f, macro
+  const void *ff, *fm;     // fine f, fine stored macro (NULL: from f and F)
   void *cf, *cm;           // coarse f, macro
+  const void *fF;          // fine force of the last substep (NULL: uniform or zero)
+  int rlo[3], rhi[3];      // the fine force array's region (zero outside)
+  int use_uniform;
+  double uf[3];
   float f16_scale;
 };
 
+// rho, u, v, w of a fine cell from its populations (already loaded) and the
+// force of the substep that produced them (calculateMacroForcing), or its
+// stored value
+template <class L, int S>
+__device__ __forceinline__ void fine_macro(const AvgArgs &g, const typename Store<S>::R *f, int64_t fmi,
+                                           int fi, int fj, int fk, double *m4) {
+  using R = typename Store<S>::R;
+  if (g.fm) {
+    const R *fm = static_cast<const R *>(g.fm);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) m4[c] = (L::D == 2 && c == 3) ? 0.0 : double(fm[fmi + c * g.fms2]);
+    return;
+  }
+  const int gi[3] = {fi + g.flo[0], fj + g.flo[1], fk + g.flo[2]};
+  double F3[3] = {0.0, 0.0, 0.0};
+  if (g.fF) {
+    bool in = true;
+#pragma unroll
+    for (int d = 0; d < L::D; ++d) in = in && gi[d] >= g.rlo[d] && gi[d] <= g.rhi[d];
+    if (in) {
+      const R *F = static_cast<const R *>(g.fF);
+      F3[0] = double(F[fmi]);
+      F3[1] = double(F[fmi + g.fms2]);
+      F3[2] = (L::D == 3) ? double(F[fmi + 2 * g.fms2]) : 0.0;
+    }
+  } else if (g.use_uniform) {
+    F3[0] = g.uf[0];
+    F3[1] = g.uf[1];
+    F3[2] = (L::D == 3) ? g.uf[2] : 0.0;
+  }
+  if (S == ILBM_STORAGE_F64) {
+    moments64<L>(reinterpret_cast<const double *>(f), F3[0], F3[1], F3[2], m4[0], m4[1], m4[2], m4[3]);
+    if (L::D != 3) m4[3] = 0.0;
+  } else {
+    float dr, u, v, w;
+    moments32<L>(reinterpret_cast<const float *>(f), float(F3[0]), float(F3[1]), float(F3[2]), dr, u,
+                 v, w);
+    m4[0] = 1.0 + double(dr);
+    m4[1] = u;
+    m4[2] = v;
+    m4[3] = (L::D == 3) ? double(w) : 0.0;
+  }
+}
+
+// one coarse cell per thread, its 2^d fine cells visited once each (k, j, i
+// inner): populations summed per direction, macro fields summed, both scaled
+// by the volume fraction
 template <class L, int S>
 __global__ void __launch_bounds__(256) k_avg_down(AvgArgs g) {
   using T = typename Store<S>::T;
@@ -158,54 +256,62 @@ __global__ void __launch_bounds__(256) k_avg_down(AvgArgs g) {
   const int nx = g.chi_box[0] - g.clo_box[0] + 1, ny = g.chi_box[1] - g.clo_box[1] + 1;
   const int nz = (L::D == 3) ? g.chi_box[2] - g.clo_box[2] + 1 : 1;
   const int64_t n = (int64_t)nx * ny * nz;
-  const int kr = (L::D == 3) ? 2 : 1;
+  constexpr int kr = (L::D == 3) ? 2 : 1;
+  const T *ff = static_cast<const T *>(g.ff);
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += (int64_t)gridDim.x * blockDim.x) {
     const int ic = g.clo_box[0] + (int)(t % nx), jc = g.clo_box[1] + (int)((t / nx) % ny);
     const int kc = (L::D == 3) ? g.clo_box[2] + (int)(t / ((int64_t)nx * ny)) : 0;
+    R acc[L::Q];
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) acc[q] = R(0);
+    double accm[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int kk = 0; kk < kr; ++kk)
+#pragma unroll
+      for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+        for (int ii = 0; ii < 2; ++ii) {
+          const int fi = 2 * ic + ii - g.flo[0], fj = 2 * jc + jj - g.flo[1];
+          const int fk = (L::D == 3) ? 2 * kc + kk - g.flo[2] : 0;
+          const int64_t fb = (int64_t)(fi + g.fgf) + (int64_t)(fj + g.fgf) * g.ffs0 +
+                             ((L::D == 3) ? (int64_t)(fk + g.fgf) * g.ffs1 : 0);
+          const int64_t fmi = (int64_t)(fi + g.fgm) + (int64_t)(fj + g.fgm) * g.fms0 +
+                              ((L::D == 3) ? (int64_t)(fk + g.fgm) * g.fms1 : 0);
+          R f[L::Q];
+#pragma unroll
+          for (int q = 0; q < L::Q; ++q) {
+            const float sc = (S == ILBM_STORAGE_F16_SCALED) ? float(L::w(q)) / g.f16_scale : 1.0f;
+            f[q] = Store<S>::cvt(ff[fb + q * g.ffs2], sc);
+          }
+#pragma unroll
+          for (int q = 0; q < L::Q; ++q) {
+            if (S == ILBM_STORAGE_F64)
+              acc[q] = R(X::add(double(acc[q]), double(f[q])));
+            else
+              acc[q] += f[q];
+          }
+          double m4[4];
+          fine_macro<L, S>(g, f, fmi, fi, fj, fk, m4);
+#pragma unroll
+          for (int c = 0; c < 4; ++c) accm[c] = X::add(accm[c], m4[c]);
+        }
     const int64_t cb = (int64_t)(ic - g.cblo[0] + g.cgf) + (int64_t)(jc - g.cblo[1] + g.cgf) * g.cfs0 +
                        ((L::D == 3) ? (int64_t)(kc - g.cblo[2] + g.cgf) * g.cfs1 : 0);
     const int64_t cmi = (int64_t)(ic - g.cblo[0] + g.cgm) + (int64_t)(jc - g.cblo[1] + g.cgm) * g.cms0 +
                         ((L::D == 3) ? (int64_t)(kc - g.cblo[2] + g.cgm) * g.cms1 : 0);
-    int64_t fb[8], fmi[8];
-    int nf = 0;
-    for (int kk = 0; kk < kr; ++kk)
-      for (int jj = 0; jj < 2; ++jj)
-        for (int ii = 0; ii < 2; ++ii) {
-          const int fi = 2 * ic + ii - g.flo[0], fj = 2 * jc + jj - g.flo[1];
-          const int fk = (L::D == 3) ? 2 * kc + kk - g.flo[2] : 0;
-          fb[nf] = (int64_t)(fi + g.fgf) + (int64_t)(fj + g.fgf) * g.ffs0 +
-                   ((L::D == 3) ? (int64_t)(fk + g.fgf) * g.ffs1 : 0);
-          fmi[nf] = (int64_t)(fi + g.fgm) + (int64_t)(fj + g.fgm) * g.fms0 +
-                    ((L::D == 3) ? (int64_t)(fk + g.fgm) * g.fms1 : 0);
-          ++nf;
-        }
-    const T *ff = static_cast<const T *>(g.ff);
     T *cf = static_cast<T *>(g.cf);
-    if (S == ILBM_STORAGE_F64) {
-      const double vf = (L::D == 3) ? 0.125 : 0.25;
-      for (int q = 0; q < L::Q; ++q) {
-        double c = 0.0;
-        for (int e = 0; e < nf; ++e) c = X::add(c, double(ff[fb[e] + q * g.ffs2]));
-        reinterpret_cast<double *>(cf)[cb + q * g.cfs2] = X::mul(vf, c);
-      }
-    } else {
-      const float vf = (L::D == 3) ? 0.125f : 0.25f;
-      for (int q = 0; q < L::Q; ++q) {
-        const float s = (S == ILBM_STORAGE_F16_SCALED) ? float(L::w(q)) / g.f16_scale : 1.0f;
-        float c = 0.0f;
-        for (int e = 0; e < nf; ++e) c += Store<S>::cvt(ff[fb[e] + q * g.ffs2], s);
-        Store<S>::store(cf + cb + q * g.cfs2, vf * c, s);
-      }
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q) {
+      const float sc = (S == ILBM_STORAGE_F16_SCALED) ? float(L::w(q)) / g.f16_scale : 1.0f;
+      if (S == ILBM_STORAGE_F64)
+        reinterpret_cast<double *>(cf)[cb + q * g.cfs2] = X::mul((L::D == 3) ? 0.125 : 0.25, double(acc[q]));
+      else
+        Store<S>::store(cf + cb + q * g.cfs2, ((L::D == 3) ? 0.125f : 0.25f) * float(acc[q]), sc);
     }
-    const R *fm = static_cast<const R *>(g.fm);
     R *cm = static_cast<R *>(g.cm);
     const int ncm = (L::D == 3) ? 4 : 3;
-    for (int c4 = 0; c4 < ncm; ++c4) {
-      double c = 0.0;
-      for (int e = 0; e < nf; ++e) c = X::add(c, double(fm[fmi[e] + c4 * g.fms2]));
-      cm[cmi + c4 * g.cms2] = R(X::mul((L::D == 3) ? 0.125 : 0.25, c));
-    }
+    for (int c4 = 0; c4 < ncm; ++c4) cm[cmi + c4 * g.cms2] = R(X::mul((L::D == 3) ? 0.125 : 0.25, accm[c4]));
   }
 }
 
@@ -216,9 +322,10 @@ int grid_of(const ilbm_ctx *ctx, int64_t n) {
 
 template <class L, int S>
 int launch_cf_fill(ilbm_ctx *ctx, const CFArgs &g) {
-  int64_t n = 1;
-  for (int d = 0; d < L::D; ++d) n *= (int64_t)(g.hi[d] - g.lo[d] + 1 + 2 * g.gm);
-  k_cf_fill<L, S><<<grid_of(ctx, n), 256, 0, ctx->stream>>>(g);
+  // macro ghosts (width gm) only when the substep reads stored macro fields
+  Shell<L::D> sh;
+  sh.init(g.lo, g.hi, g.m ? g.gm : g.gf);
+  k_cf_fill<L, S><<<grid_of(ctx, sh.total()), 256, 0, ctx->stream>>>(g, sh);
   ctx->launches++;
   return ILBM_OK;
 }
@@ -256,8 +363,8 @@ int check_two_level(const ilbm_ctx *ctx, const ilbm_box *c, const ilbm_level_par
       return fail("the fine box must lie two coarse cells inside the domain");
   }
   if (f->ngrow_f < 1 || f->ngrow_m < 1 || c->ngrow_m < 1) return fail("ghost widths must be at least 1");
-  if (!c->macro_in || !c->macro_out || !f->macro_in || !f->macro_out)
-    return fail("both levels carry stored macro fields (macro_in and macro_out)");
+  if (!c->macro_in || !c->macro_out)
+    return fail("the coarse level carries stored macro fields (macro_in and macro_out)");
   return ILBM_OK;
 }
 
@@ -285,6 +392,10 @@ AvgArgs avg_args(const ilbm_ctx *ctx, const ilbm_box *c, const ilbm_box *f, cons
   g.cf = cf;
   g.cm = cm;
   g.f16_scale = (float)f16_scale_of(p);
+  if (p->use_uniform_force) {
+    g.use_uniform = 1;
+    for (int d = 0; d < 3; ++d) g.uf[d] = p->uniform_force[d];
+  }
   return g;
 }
 
@@ -304,7 +415,6 @@ int ilbm_average_down(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_pa
   }
   ilbm_box c = *coarse, f = *fine;
   c.macro_out = c.macro_in;
-  f.macro_out = f.macro_in;
   int rc = check_two_level(ctx, &c, pc, &f, pf);
   if (rc) return rc;
   const AvgArgs g = avg_args(ctx, &c, &f, f.f_in, f.macro_in, c.f_in, c.macro_in, pf);
@@ -313,7 +423,7 @@ int ilbm_average_down(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_pa
 
 int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_params *pc,
                            const ilbm_box *fine, const ilbm_level_params *pf, ilbm_ib *ib,
-                           double dt, double time) {
+                           double dt, double time, int flags) {
   if (!ctx || !coarse || !pc || !fine || !pf) {
     set_error("ilbm_advance_two_level: null argument");
     return ILBM_ERR_ARG;
@@ -328,9 +438,30 @@ int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_lev
     set_error("ilbm_advance_two_level: a body needs the fine level's force and force_prev");
     return ILBM_ERR_ARG;
   }
-  // coarse step (no body: the body lives on the finest level)
-  if ((rc = ilbm_advance_level(ctx, coarse, pc, nullptr, dt, time))) return rc;
+  const bool first = (flags & ILBM_TWO_LEVEL_FIRST_STEP) != 0;
+  if (first && !fine->macro_in) {
+    set_error("ilbm_advance_two_level: the first step reads the fine level's stored macro_in");
+    return ILBM_ERR_ARG;
+  }
   const double t_old = time, t_new = time + dt, dtf = 0.5 * dt;
+  // the first substep's body forcing needs only the fine state at t: it
+  // starts before the coarse step and overlaps it
+  ilbm_box b0 = *fine;
+  b0.macro_in = first ? fine->macro_in : nullptr;
+  b0.macro_out = nullptr;
+  AdvanceSplit sp0;
+  if (ib && (rc = advance_begin(ctx, &b0, pf, ib, dtf, t_old, &sp0))) return rc;
+  // coarse step (no body: the body lives on the finest level).  Its stored
+  // macro fields are kept on the covered cells grown by two coarse cells --
+  // what average-down writes and the fine ghost fill reads; elsewhere they
+  // equal the populations' own and are recovered from them
+  int mlo[3] = {0, 0, 0}, mhi[3] = {0, 0, 0};
+  for (int d = 0; d < ctx->dim; ++d) {
+    mlo[d] = fine->lo[d] / 2 - 2;
+    mhi[d] = fine->hi[d] / 2 + 2;
+  }
+  if ((rc = level_step_impl(ctx, coarse, 1, pc, first ? nullptr : mlo, first ? nullptr : mhi)))
+    return rc;
   CFArgs g;
   std::memset(&g, 0, sizeof(g));
   for (int d = 0; d < 3; ++d) {
@@ -349,10 +480,13 @@ int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_lev
   g.cnew = coarse->macro_out;
   g.f16_scale = (float)f16_scale_of(pf);
   for (int sub = 0; sub < 2; ++sub) {
-    ilbm_box b = *fine;
+    // stored fine macro fields only for a first step after initialisation;
+    // afterwards rho, u are recovered from f and F^{n-1}
+    ilbm_box b = (sub == 0) ? b0 : *fine;
     if (sub == 1) {
+      b.macro_in = nullptr;
+      b.macro_out = nullptr;
       std::swap(b.f_in, b.f_out);
-      std::swap(b.macro_in, b.macro_out);
       std::swap(b.force, b.force_prev);
     }
     const double t = t_old + (double)sub * dtf;
@@ -370,11 +504,29 @@ int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_lev
     g.f = b.f_in;
     g.m = b.macro_in;
     if ((rc = ILBM_DISPATCH(ctx, launch_cf_fill, ctx, g))) return rc;
-    if ((rc = ilbm_advance_level(ctx, &b, pf, ib, dtf, t))) return rc;
+    if (!ib) {
+      if ((rc = ilbm_level_step(ctx, &b, 1, pf))) return rc;
+    } else if (sub == 0) {
+      if ((rc = advance_end(ctx, &b, &sp0))) return rc;
+    } else {
+      AdvanceSplit sp1;
+      if ((rc = advance_begin(ctx, &b, pf, ib, dtf, t, &sp1))) return rc;
+      if ((rc = advance_end(ctx, &b, &sp1))) return rc;
+    }
   }
-  // the fine state is back in fine->f_in / fine->macro_in after two substeps
-  const AvgArgs a = avg_args(ctx, coarse, fine, fine->f_in, fine->macro_in, coarse->f_out,
-                             coarse->macro_out, pf);
+  // the fine state is back in fine->f_in after two substeps, the force of
+  // the second substep in fine->force_prev
+  AvgArgs a = avg_args(ctx, coarse, fine, fine->f_in, nullptr, coarse->f_out, coarse->macro_out, pf);
+  if (ib) {
+    a.fF = fine->force_prev;
+    a.use_uniform = 0;
+    int lo[3], hi[3];
+    ilbm_ib_force_region(ib, lo, hi);
+    for (int d = 0; d < 3; ++d) {
+      a.rlo[d] = lo[d];
+      a.rhi[d] = hi[d];
+    }
+  }
   return ILBM_DISPATCH(ctx, launch_avg_down, ctx, a);
 }
 

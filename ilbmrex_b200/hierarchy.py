@@ -101,8 +101,11 @@ class TwoLevelSolver:
             lo, hi = (C.c_int * 3)(), (C.c_int * 3)()
             capi.check(self.L.ilbm_ib_force_region(self.ib, lo, hi), "ib_force_region")
             self.force_region = (tuple(lo), tuple(hi))
+            for d in range(3):
+                self.pf.force_lo[d], self.pf.force_hi[d] = lo[d], hi[d]
         self.time = 0.0
         self.istep = 0
+        self.first_step = True
         self.have_prev_body = False
         self.prev_body = np.zeros(3)
         self.rec = np.zeros(18)
@@ -125,17 +128,22 @@ class TwoLevelSolver:
                                             C.byref(self.pf)), "average_down")
         self.ctx.sync()
         self.time, self.istep = 0.0, 0
+        self.first_step = True
 
     # ---- one coarse step ---------------------------------------------------
     def advance(self, record_force: bool = False):
         Cl, Fl = self.C, self.F
         bc = Cl.box(Cl.f, Cl.f_next, m_in=Cl.m, m_out=Cl.m_next)
-        bf = Fl.box(Fl.f, Fl.f_next, m_in=Fl.m, m_out=Fl.m_next, force=Fl.fa, force_prev=Fl.fb)
+        bf = Fl.box(Fl.f, Fl.f_next, m_in=Fl.m if self.first_step else None,
+                    force=Fl.fa, force_prev=Fl.fb)
+        flags = capi.TWO_LEVEL_FIRST_STEP if self.first_step else 0
         capi.check(self.L.ilbm_advance_two_level(self.ctx.h, C.byref(bc), C.byref(self.pc),
                                                  C.byref(bf), C.byref(self.pf), self.ib,
-                                                 self.tl.coarse.dt, self.time), "advance_two_level")
+                                                 self.tl.coarse.dt, self.time, flags),
+                   "advance_two_level")
         Cl.f, Cl.f_next = Cl.f_next, Cl.f
         Cl.m, Cl.m_next = Cl.m_next, Cl.m
+        self.first_step = False
         self.time += self.tl.coarse.dt
         self.istep += 1
         if record_force and self.ib is not None:
@@ -175,10 +183,32 @@ class TwoLevelSolver:
         return v.cpu().numpy()
 
     def get_macro(self, lev: int) -> np.ndarray:
-        """The stored rho, u, v, w of a level (valid cells)."""
+        """rho, u, v, w of a level (valid cells): those of its populations
+        (calculateMacroForcing with the force of its last step), and on the
+        coarse cells under the fine box the averaged-down values."""
         self.ctx.sync()
         lvl = self._lvl(lev)
-        return lvl.valid(lvl.m, lvl.gm).to(torch.float64).cpu().numpy()
+        if self.first_step:
+            return lvl.valid(lvl.m, lvl.gm).to(torch.float64).cpu().numpy()
+        out = torch.zeros_like(lvl.m)
+        b = lvl.box(lvl.f, None)
+        force = self.F.fb if (lev == 1 and self.ib is not None) else None
+        p = self.pf if lev == 1 else self.pc
+        capi.check(self.L.ilbm_compute_macro(self.ctx.h, C.byref(b), C.byref(p), lvl.f.data_ptr(),
+                                             force.data_ptr() if force is not None else None,
+                                             out.data_ptr(), None, None), "compute_macro")
+        self.ctx.sync()
+        m = lvl.valid(out, lvl.gm).to(torch.float64).cpu().numpy()
+        if lev == 0:
+            st = lvl.valid(lvl.m, lvl.gm).to(torch.float64).cpu().numpy()
+            lo = [v // 2 for v in self.tl.fine_lo]
+            hi = [v // 2 + 1 for v in self.tl.fine_hi]
+            if self.dim == 3:
+                sl = (slice(None), slice(lo[2], hi[2]), slice(lo[1], hi[1]), slice(lo[0], hi[0]))
+            else:
+                sl = (slice(None), slice(None), slice(lo[1], hi[1]), slice(lo[0], hi[0]))
+            m[sl] = st[sl]
+        return m
 
     def get_force(self) -> np.ndarray:
         self.ctx.sync()

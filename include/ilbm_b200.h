@@ -326,8 +326,7 @@ int ilbm_tag_cells(ilbm_ctx *ctx, const ilbm_box *box, const void *vor, double t
  * AmrCoreLBM::timeStepWithSubcycling does for max_level = 1
  * (Source/Core/AmrCoreLBM.cpp:1690-1755):
  *   1. the coarse level steps by dt (coarse->f_in, macro_in -> f_out,
- *      macro_out; stored macro fields on both levels, since after
- *      average-down they are no longer those of the coarse populations);
+ *      macro_out);
  *   2. the fine level steps twice by dt/2 at t and t + dt/2; before each
  *      substep every fine ghost cell gets the coarse macro fields at the
  *      substep's time (old, new, or their linear time interpolation,
@@ -339,13 +338,22 @@ int ilbm_tag_cells(ilbm_ctx *ctx, const ilbm_box *box, const void *vor, double t
  *      on the fine level (AdvanceLBMAtLevel.cpp:30, 73-93);
  *   3. average-down of ratio 2 (AverageDownTo :1519-1527) of the fine
  *      populations and macro fields onto coarse->f_out / macro_out.
- * Buffers: the fine level's f_in / macro_in hold the new fine state on
- * return (two substeps swap them twice), force / force_prev hold the first /
+ * Stored macro fields: the coarse level's macro_in / macro_out hold them on
+ * the covered cells grown by two coarse cells (what average-down writes and
+ * the fine ghost fill reads); elsewhere, and on the fine level, rho and u are
+ * recovered from f^n and F^{n-1}, which equals the stored value.  The first
+ * step after initialisation (flags ILBM_TWO_LEVEL_FIRST_STEP) instead reads
+ * both levels' initial macro fields everywhere (coarse->macro_in,
+ * fine->macro_in).  With a body, its forcing for the first substep overlaps
+ * the coarse step.
+ * Buffers: the fine level's f_in holds the new fine state on return (two
+ * substeps swap f_in / f_out twice), force / force_prev hold the first /
  * second substep's forces; the caller swaps the coarse in / out pairs.
  * Asynchronous on the context's stream. */
+#define ILBM_TWO_LEVEL_FIRST_STEP 1
 int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_params *pc,
                            const ilbm_box *fine, const ilbm_level_params *pf, ilbm_ib *ib,
-                           double dt, double time);
+                           double dt, double time, int flags);
 /* average-down alone (InitData's AverageDown after the levels are made,
  * AmrCoreLBM.cpp:710-720): fine f_in / macro_in onto coarse f_in / macro_in */
 int ilbm_average_down(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_params *pc,
