@@ -20,6 +20,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -40,6 +41,28 @@ def set_workload_size(nx: int, ny: int, nz: int):
     """Shrinks the sphere workload (tests of the multi-rank logic on CPU);
     the sphere keeps D = ny / 4 at (nx / 4, ny / 2, nz / 2)."""
     WORKLOAD.update(nx=nx, ny=ny, nz=nz, D=ny / 4.0, center=(nx / 4.0, ny / 2.0, nz / 2.0))
+
+
+def refined_box():
+    """Base-cell box [lo, hi) of the refined level around the sphere: one
+    diameter upstream and across, two downstream (32..128 x 32..96 x 32..96
+    for the 256 x 128 x 128 grid), kept two base cells inside the domain."""
+    w = WORKLOAD
+    n = (w["nx"], w["ny"], w["nz"])
+    c, D = w["center"], w["D"]
+    lo = [int(math.floor(c[0] - D)), int(math.floor(c[1] - D)), int(math.floor(c[2] - D))]
+    hi = [int(math.ceil(c[0] + 2 * D)), int(math.ceil(c[1] + D)), int(math.ceil(c[2] + D))]
+    lo = [max(lo[a], 2) for a in range(3)]
+    hi = [min(hi[a], n[a] - 2) for a in range(3)]
+    return tuple(lo), tuple(hi)
+
+
+def sphere_hierarchy():
+    from ilbmrex_b200 import cases
+    w = WORKLOAD
+    lo, hi = refined_box()
+    return cases.sphere_two_level(w["nx"], w["ny"], w["nz"], D=w["D"], center=w["center"], U=w["U"],
+                                  Re=w["Re"], box_lo=lo, box_hi=hi)
 METRIC = "MLUPS & % HBM roofline (D3Q19 FP32); batched/served MLUPS, p99 vs plain"
 UNIT = "MLUPS"
 
@@ -135,34 +158,42 @@ def barrier(world: int):
 
 
 def cpu_reference_steps(steps: int, warmup: int, threads: int | None = None):
-    """Times the reference's own CPU path (oracle/_ref, FP32 3D build) on the
-    same workload; returns (MLUPS, seconds per step, threads, sample text)."""
+    """Times the reference's own CPU level step (oracle/_ref: Source/LBM,
+    Source/BC compiled in place, FP32 3D build, OpenMP) on the levels of the
+    same hierarchy: the coarse level and the fine box each advanced as a
+    level; MLUPS = updates of one coarse step (coarse + 2 x fine cells) over
+    (coarse step time + 2 x fine step time).  Returns (MLUPS, seconds per
+    coarse step, threads, kind, sample text)."""
     from ilbmrex_b200 import cases
     from oracle import checker
     from oracle.checker import CpuLevel
-    w = WORKLOAD
-    case, ib, init = cases.sphere(w["nx"], w["ny"], w["nz"], D=w["D"], center=w["center"],
-                                  U=w["U"], Re=w["Re"])
+    tl, ib, ic, if_ = sphere_hierarchy()
     kind = "reference" if checker.available("ref", 3, fp32=True) else "port"
     threads = threads or os.cpu_count() or 1
-    if kind == "reference":
-        L = CpuLevel(case, "ref", fp32=True, threads=threads)
-    else:
-        L = CpuLevel(case, "oracle")
-        threads = 1
-    L.set_macro(*init())
-    L.init_equilibrium()
-    L.ib_create(ib)
-    L.step(max(1, warmup))  # includes the one-time dense LU of the IVC operator
-    t0 = time.perf_counter()
-    L.step(steps)
-    dt = (time.perf_counter() - t0) / steps
-    sample = (f"{steps} full level steps of the {w['nx']}x{w['ny']}x{w['nz']} D3Q19 sphere "
-              f"(after {max(1, warmup)} warm-up steps incl. the one-time IVC LU); "
-              + ("reference sources (Source/LBM, Source/BC, Source/IBM) compiled in place, "
-                 "float, restated AdvancePhiAtLevel pass structure, OpenMP"
-                 if kind == "reference" else "plain-C oracle port, FP64, 1 thread"))
-    return case.cells / dt / 1e6, dt, threads, kind, sample
+    t = []
+    for case, init in ((tl.coarse, ic), (tl.fine_box(), if_)):
+        if kind == "reference":
+            L = CpuLevel(case, "ref", fp32=True, threads=threads)
+        else:
+            L = CpuLevel(case, "oracle")
+            threads = 1
+        L.set_macro(*init())
+        L.init_equilibrium()
+        L.step(max(1, warmup))
+        t0 = time.perf_counter()
+        L.step(steps)
+        t.append((time.perf_counter() - t0) / steps)
+        L.close()
+    dt = t[0] + 2.0 * t[1]
+    updates = tl.coarse.cells + 2 * int(np.prod(tl.fine_n_cell))
+    sample = (f"{steps} level steps each of the coarse level ({tl.coarse.cells} cells) and of the fine box "
+              f"({int(np.prod(tl.fine_n_cell))} cells) after {max(1, warmup)} warm-up step(s), timed as "
+              "coarse + 2 x fine per coarse step; the body's forcing (12.9k-marker IVC, whose dense LU "
+              "alone runs for minutes on the host) and the coarse-fine fill are not included; "
+              + ("reference sources (Source/LBM, Source/BC) compiled in place, float, restated "
+                 "AdvancePhiAtLevel pass structure, OpenMP" if kind == "reference"
+                 else "plain-C oracle port, FP64, 1 thread"))
+    return updates / dt / 1e6, dt, threads, kind, sample
 
 
 def run_reference(args):
@@ -185,12 +216,46 @@ def run_reference(args):
 
 def workload_config(args):
     w = WORKLOAD
-    return {"workload": f"D3Q19 IB-LBM sphere, single level {w['nx']}x{w['ny']}x{w['nz']}, "
-                        f"D={w['D']:g}, U={w['U']}, Re={w['Re']:g}, IVC marker IB, FP32 shifted storage",
-            "lattice": "D3Q19", "cells": w["nx"] * w["ny"] * w["nz"], "storage": args.storage,
-            "levels": 1, "parallelism": f"replicas{args.gpus}",
-            "ib_overlap": not getattr(args, "serial", False),
-            "l2_policy": "working set 637 MB > 126 MB L2 (no flush needed)"}
+    lo, hi = refined_box()
+    nf = [2 * (hi[a] - lo[a]) for a in range(3)]
+    cells_c = w["nx"] * w["ny"] * w["nz"]
+    cells_f = nf[0] * nf[1] * nf[2]
+    return {"workload": f"D3Q19 IB-LBM sphere, base grid {w['nx']}x{w['ny']}x{w['nz']} plus 1 refined "
+                        f"level (ratio 2) over base cells [{lo[0]},{hi[0]})x[{lo[1]},{hi[1]})x[{lo[2]},{hi[2]}) "
+                        f"({nf[0]}x{nf[1]}x{nf[2]} fine cells), D={w['D']:g} base cells, U={w['U']}, "
+                        f"Re={w['Re']:g}, golden-spiral markers ~1 fine dx apart, IVC marker IB on the fine "
+                        f"level, subcycled (2 fine steps per coarse step), FP32 shifted storage",
+            "lattice": "D3Q19", "levels": 2, "coarse_cells": cells_c, "fine_cells": cells_f,
+            "updates_per_coarse_step": cells_c + 2 * cells_f, "storage": args.storage,
+            "parallelism": f"replicas{args.gpus}",
+            "l2_policy": "working set > 1 GB of populations >> 126 MB L2 (no flush needed)"}
+
+
+def run_single_level(args, world, device):
+    """The sphere on its base grid alone (one level, 3,218 markers, stored
+    IVC inverse), through ilbm_advance_level with the IB chain overlapped."""
+    from ilbmrex_b200 import cases
+    from ilbmrex_b200.level import LevelSolver
+    w = WORKLOAD
+    case, ib, init = cases.sphere(w["nx"], w["ny"], w["nz"], D=w["D"], center=w["center"],
+                                  U=w["U"], Re=w["Re"])
+    S = LevelSolver(case, args.storage, ib=ib, device=device.index or 0)
+    S.set_macro(*init())
+    S.step(max(3, args.warmup))
+    S.ctx.sync()
+    barrier(world)
+    K = args.steps
+    S.ctx.record(10)
+    S.step(K)
+    S.ctx.record(11)
+    S.ctx.sync()
+    t = allreduce_max(S.ctx.elapsed_ms(10, 11), world, device)
+    out = {"metric": "MLUPS, the same sphere on its base grid alone (one level)",
+           "value": round(world * case.cells * K / (t * 1e-3) / 1e6, 2), "unit": "MLUPS",
+           "ms_per_step": round(t / K, 4), "cells": case.cells, "ib_markers": S.num_markers(),
+           "steps": K}
+    S.close()
+    return out
 
 
 def run_batched(args, world, device):
@@ -249,6 +314,64 @@ def run_batched(args, world, device):
                         "each case steps through its own IB (stored IVC inverse or CG)"}
 
 
+def run_two_level(args, world, device):
+    """The reference's 2D cylinder deck (Examples/Cylinder_flow/inputs:
+    512 x 256, D = 32, Re = 100, U0 = 0.03, max_level 1, ref_ratio 2) as a
+    static two-level hierarchy: a fixed fine box over the body and its near
+    wake (1.5 D upstream, 6 D downstream, 1.5 D across) carrying the marker
+    IBM, FP32 storage.  Cell updates per coarse step: coarse cells + 2 x fine
+    cells.  Beside it, the oracle's two-level driver (plain C, FP64, one
+    thread) on one coarse step of the same hierarchy."""
+    from ilbmrex_b200 import cases
+    from ilbmrex_b200.hierarchy import TwoLevelSolver
+    tl, ib, ic, if_ = cases.cylinder_two_level(nx=512, ny=256, D=32.0, center=(96.0, 127.9), U=0.03,
+                                               Re=100.0, upstream=1.5, downstream=6.0, cross=1.5)
+    nc = tl.coarse.cells
+    nf = int(np.prod(tl.fine_n_cell[: tl.dim]))
+    updates = nc + 2 * nf
+    S = TwoLevelSolver(tl, "f32", ib=ib, device=device.index or 0)
+    S.set_macro(ic(), if_())
+    S.step(3)
+    S.ctx.sync()
+    barrier(world)
+    K = args.two_level_steps
+    l0 = S.ctx.launches()
+    S.ctx.record(8)
+    S.step(K)
+    S.ctx.record(9)
+    S.ctx.sync()
+    launches = S.ctx.launches() - l0
+    t = allreduce_max(S.ctx.elapsed_ms(8, 9), world, device)
+    mlups = world * updates * K / (t * 1e-3) / 1e6
+    S.step(1, record_force=True)
+    cd = float(S.rec[3])
+    S.close()
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle.checker import CpuTwoLevel
+            T = CpuTwoLevel(tl)
+            T.set_macro(0, *ic())
+            T.set_macro(1, *if_())
+            T.init_equilibrium()
+            T.ib_create(ib)
+            T.step(1)  # includes the one-time dense LU of the IVC operator
+            t0 = time.perf_counter()
+            T.step(2)
+            dt = (time.perf_counter() - t0) / 2
+            cpu = {"value": round(updates / dt / 1e6, 3), "unit": "MLUPS", "cores": 1, "kind": "port",
+                   "sample": "two coarse steps of the same hierarchy (coarse step + 2 fine substeps "
+                             "+ average-down) after one warm-up step, oracle two-level driver, FP64"}
+            T.close()
+        except Exception as e:  # the checker is optional at run time
+            cpu = {"value": None, "unit": "MLUPS", "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
+    return {"metric": "two-level MLUPS (cylinder deck, max_level 1, D2Q9 FP32)",
+            "value": round(mlups, 2), "unit": "MLUPS", "ms_per_coarse_step": round(t / K, 4),
+            "coarse_cells": nc, "fine_cells": nf, "fine_box": [list(tl.fine_lo[:2]), list(tl.fine_hi[:2])],
+            "updates_per_coarse_step": updates, "steps": K, "gpu_launches": int(launches),
+            "cd_after": round(cd, 5), "cpu_baseline": cpu}
+
+
 def run_served(args, world, device):
     """Served mixed workload: Poisson arrivals (seeded) of D2Q9 cylinder /
     airfoil, D3Q19 duct and D3Q19 sphere requests through the continuous-
@@ -305,97 +428,91 @@ def run_b200(args):
     from ilbmrex_b200 import capi, cases
     from ilbmrex_b200.level import LevelSolver
 
-    if args.only_batched or args.only_served:  # profiling aids: one workload alone
-        out = run_batched(args, world, device) if args.only_batched else run_served(args, world, device)
+    if args.only_batched or args.only_served or args.only_two_level:  # profiling aids: one workload alone
+        if args.only_two_level:
+            out = run_two_level(args, world, device)
+        else:
+            out = run_batched(args, world, device) if args.only_batched else run_served(args, world, device)
         if rank == 0:
             print(json.dumps(out), flush=True)
         return
 
-    w = WORKLOAD
-    case, ib, init = cases.sphere(w["nx"], w["ny"], w["nz"], D=w["D"], center=w["center"],
-                                  U=w["U"], Re=w["Re"])
-    S = LevelSolver(case, args.storage, ib=ib, device=local)
-    S.set_macro(*init())
+    from ilbmrex_b200.hierarchy import TwoLevelSolver
+    tl, ib, init_c, init_f = sphere_hierarchy()
+    S = TwoLevelSolver(tl, args.storage, ib=ib, device=local)
+    S.set_macro(init_c(), init_f())
     ctx = S.ctx
-    cells = case.cells
-    q = case.lattice.q
+    cells_c = tl.coarse.cells
+    cells_f = int(np.prod(tl.fine_n_cell))
+    updates = cells_c + 2 * cells_f
+    q = tl.coarse.lattice.q
     sbytes = {"f64": 8, "f32": 4, "f16": 2}[args.storage]
     B_cell = 2 * q * sbytes
 
-    # ---- device-resident timed region -----------------------------------
+    # ---- device-resident timed region: K coarse steps --------------------
     K = args.steps
-
-    def one_step(s_idx=None, serial=False):
-        use_macro = S.macro if S.first_step_macro else None
-        b = S._box(S.f, S.f_next, macro_in=use_macro, force=S.force_cur, force_prev=S.force_prev)
-        if serial:
-            capi.check(S.L.ilbm_ib_update_forcing(S.ib, C.byref(b), C.byref(S.params), case.dt,
-                                                  S.time), "ib")
-            if s_idx is not None:
-                ctx.record(16 + 2 * s_idx)
-            capi.check(S.L.ilbm_level_step(ctx.h, C.byref(b), 1, C.byref(S.params)), "step")
-            if s_idx is not None:
-                ctx.record(17 + 2 * s_idx)
-        else:
-            capi.check(S.L.ilbm_advance_level(ctx.h, C.byref(b), C.byref(S.params), S.ib,
-                                              case.dt, S.time), "advance_level")
-        S.f, S.f_next = S.f_next, S.f
-        S.force_cur, S.force_prev = S.force_prev, S.force_cur
-        S.first_step_macro = False
-        S.time += case.dt
-        S.istep += 1
-
-    # first step: includes the one-time IVC operator set-up (stored inverse)
     ctx.sync()
     ctx.record(2)
-    one_step(serial=args.serial)
+    S.advance()  # includes the one-time CSR build of the IVC operator
     ctx.record(3)
     ctx.sync()
     first_step_ms = ctx.elapsed_ms(2, 3)
     for _ in range(max(3, args.warmup) - 1):
-        one_step(serial=args.serial)
+        S.advance()
     ctx.sync()
     torch.cuda.synchronize(device)
-
     launches0 = ctx.launches()
     sampler = ClockSampler(local)
     with sampler:
         barrier(world)
         ctx.sync()
         ctx.record(0)
-        for s in range(K):
-            one_step(serial=args.serial)
+        for _ in range(K):
+            S.advance()
         ctx.record(1)
         ctx.sync()
         barrier(world)
     launches = ctx.launches() - launches0
     t_ms = ctx.elapsed_ms(0, 1)
-    value, t_max = aggregate_mlups(cells, K, t_ms, world, device)
+    value, t_max = aggregate_mlups(updates, K, t_ms, world, device)
     clocks = sampler.summary()
 
-    # ---- roofline pass: the level step (ghost-shell push + fused collide-
-    # stream) bracketed by events, IB chain outside the brackets ------------
+    # ---- roofline pass: the dominant kernel, the level step k_step
+    # <D3Q19, storage> with its ghost-shell push, on the coarse level
+    # (4,194,304 cells), from the current state into the scratch buffer (the
+    # hierarchy's state is left as it was) ------------------------------------
+    Cl = S.C
+    bk = Cl.box(Cl.f, Cl.f_next)
     Kr = max(3, min(K, 20))
-    for s in range(Kr):
-        one_step(s, serial=True)
+    for r in range(Kr + 2):
+        if r >= 2:
+            ctx.record(16 + 2 * (r - 2))
+        capi.check(S.L.ilbm_level_step(ctx.h, C.byref(bk), 1, C.byref(S.pc)), "level step")
+        if r >= 2:
+            ctx.record(17 + 2 * (r - 2))
     ctx.sync()
-    step_ms = [ctx.elapsed_ms(16 + 2 * s, 17 + 2 * s) for s in range(Kr)]
-    kern_ms = float(np.mean(step_ms))
+    kern_ms = float(np.mean([ctx.elapsed_ms(16 + 2 * r, 17 + 2 * r) for r in range(Kr)]))
     peak, peak_kind = peaks()
-    achieved = B_cell * cells / (kern_ms * 1e-3) / 1e9
+    achieved = B_cell * cells_c / (kern_ms * 1e-3) / 1e9
 
-    # ---- end-to-end through the public API --------------------------------
+    # ---- end-to-end through the public call: per coarse step the host
+    # parameter structs go down and the force record (Cd / Cl) comes back ----
     Ke = max(3, min(K, 20))
     ctx.sync()
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(Ke):
-        S.advance_phi_at_level(record_force=True)  # reads Cd/Cl back every step
+        S.advance(record_force=True)
     ctx.sync()
     e2e_s = allreduce_max(time.perf_counter() - t0, world, device)
-    e2e = world * cells * Ke / e2e_s / 1e6
-    h2d = C.sizeof(capi.LevelParams_t) + C.sizeof(capi.Box_t) + 16
-    d2h = 3 * 8 + 3 * 8 + 4
+    e2e = world * updates * Ke / e2e_s / 1e6
+    h2d = 2 * C.sizeof(capi.LevelParams_t) + 2 * C.sizeof(capi.Box_t) + 24
+    d2h = 3 * 8 + 3 * 8 + 8
+    cd, cl = float(S.rec[3]), float(S.rec[4])
+    n_mark = C.c_int64()
+    S.L.ilbm_ib_num_markers(S.ib, C.byref(n_mark))
+    cg_it = C.c_int()
+    S.L.ilbm_ib_solver_stats(S.ib, C.byref(cg_it))
 
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
@@ -404,6 +521,7 @@ def run_b200(args):
             traffic = json.loads(tf.read_text()).get("k_step_d3q19_f32_bytes_per_launch")
         except Exception:
             traffic = None
+    S.close()
 
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -415,12 +533,16 @@ def run_b200(args):
             cpu_base = {"value": None, "unit": UNIT, "cores": 0, "kind": "port",
                         "sample": f"unavailable: {e}"}
 
+    single = None if args.no_single_level else run_single_level(args, world, device)
     batched = None
     if not args.no_batched:
         batched = run_batched(args, world, device)
     served = None
     if not args.no_served:
         served = run_served(args, world, device)
+    two_level = None
+    if not args.no_two_level:
+        two_level = run_two_level(args, world, device)
 
     if rank == 0:
         line = {
@@ -431,7 +553,8 @@ def run_b200(args):
             "config": workload_config(args),
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
                          "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "kernel": "level step = k_step<D3Q19,F32_SHIFT> (ghost-shell push in its leading blocks)",
+                         "kernel": "level step = k_step<D3Q19,F32_SHIFT> (ghost-shell push in its "
+                                   "leading blocks), timed alone on the 256x128x128 coarse level",
                          "kernel_ms": round(kern_ms, 4), "bytes_per_cell": B_cell,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
                          if peak_kind == "measured" else "fallback 6650 GB/s"},
@@ -440,14 +563,16 @@ def run_b200(args):
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
             "clocks": clocks,
-            "ib_markers": S.num_markers(),
-            "ivc_cg_iterations": S.cg_iterations(),
+            "ib_markers": int(n_mark.value),
+            "ivc_cg_iterations": int(cg_it.value),
+            "cd_cl_after": [round(cd, 5), round(cl, 6)],
             "first_step_ms_incl_ivc_setup": round(first_step_ms, 2),
+            "single_level": single,
             "batched": batched,
             "served": served,
+            "two_level": two_level,
         }
         print(json.dumps(line), flush=True)
-    S.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -465,7 +590,12 @@ def main():
     ap.add_argument("--ny", type=int, default=0)
     ap.add_argument("--nz", type=int, default=0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched workload")
+    ap.add_argument("--no-single-level", action="store_true", help="skip the single-level sphere")
     ap.add_argument("--no-served", action="store_true", help="skip the served workload")
+    ap.add_argument("--no-two-level", action="store_true", help="skip the two-level cylinder workload")
+    ap.add_argument("--two-level-steps", type=int, default=100)
+    ap.add_argument("--only-two-level", action="store_true",
+                    help="run only the two-level cylinder workload and print its result (profiling aid)")
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-rate", type=float, default=200.0, help="arrivals per second")
     ap.add_argument("--serve-scale", type=float, default=0.5)
@@ -479,8 +609,6 @@ def main():
     ap.add_argument("--batch-cases", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=40)
     ap.add_argument("--batch-plain-steps", type=int, default=8)
-    ap.add_argument("--serial", action="store_true",
-                    help="run the IB chain and the level step one after the other (no overlap)")
     args = ap.parse_args()
     if args.nx:
         set_workload_size(args.nx, args.ny or args.nx // 2, args.nz or args.nx // 2)
