@@ -660,22 +660,43 @@ __device__ __forceinline__ void block_partials(const double *v, int nval, double
   __syncthreads();
 }
 
+// Grid-wide preconditioned CG (Jacobi) for the three right-hand sides of the
+// IVC system, one cooperative launch.  Two grid barriers per iteration: the
+// search direction p = z + beta p_old is formed on the fly by every row that
+// reads it (z and p_old are frozen between barriers), the owner storing it in
+// the other of two p buffers; block partial sums alternate between two
+// buffers, so a block that runs ahead never overwrites partials another
+// block is still reducing.  Start: x0 = 0 (warm 0), the previous solution
+// (warm 1), or its linear extrapolation 2 x_n - x_{n-1} from the last two
+// solutions (warm 2; Xh keeps the history).
 __global__ void __launch_bounds__(256) k_ivc_cg_grid(IBArgs a, const double *xyz, const double *tgt,
                                                      const double *uvw, const int *rowptr,
                                                      const int *col, const double *val,
-                                                     const double *diag, double *X_, double *work,
-                                                     double *F, double *partial, int maxit,
-                                                     double tol, int warm, int *status,
+                                                     const double *diag, double *X_, double *Xh,
+                                                     double *work, double *F, double *partial,
+                                                     int maxit, double tol, int warm, int *status,
                                                      int *iters) {
   cgrp::grid_group grid = cgrp::this_grid();
   __shared__ double sh[8][8];
   __shared__ double red[8];
   const int n = a.n;
-  double *r = work, *z = work + 3 * n, *p = work + 6 * n, *Ap = work + 9 * n;
+  double *r = work, *z = work + 3 * n, *Ap = work + 9 * n;
+  double *P[2] = {work + 6 * n, work + 12 * n};
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
   const int lane = threadIdx.x & 31, nw = gsz >> 5, gw = gtid >> 5;
-  // warm start: x0 = previous solution (the force changes little per step);
-  // r0 = b - A x0, one warp per row
+  double *pbuf[2] = {partial, partial + 8 * gridDim.x};
+  int k = 0;  // reductions so far (selects the partials buffer)
+  if (warm >= 2) {
+    for (int i = gtid; i < 3 * n; i += gsz) {
+      const double xc = X_[i];
+      X_[i] = X::sub(X::mul(2.0, xc), Xh[i]);
+      Xh[i] = xc;
+    }
+    grid.sync();
+  } else if (warm == 1) {
+    for (int i = gtid; i < 3 * n; i += gsz) Xh[i] = X_[i];
+  }
+  // r0 = b - A x0, z0 = r0 / diag; one warp per row
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (int row = gw; row < n; row += nw) {
     double s0 = 0, s1 = 0, s2 = 0;
@@ -705,32 +726,36 @@ __global__ void __launch_bounds__(256) k_ivc_cg_grid(IBArgs a, const double *xyz
         const double zz = rr / diag[row];
         r[row + c * n] = rr;
         z[row + c * n] = zz;
-        p[row + c * n] = zz;
         acc[c] += rr * zz;
         acc[3 + c] += b * b;
       }
     }
   }
-  block_partials(acc, 6, sh, partial);
+  block_partials(acc, 6, sh, pbuf[k & 1]);
   grid.sync();
-  reduce_partials(partial, gridDim.x, 6, red);
+  reduce_partials(pbuf[k & 1], gridDim.x, 6, red);
+  ++k;
   double rz[3] = {red[0], red[1], red[2]};
   const double bn[3] = {sqrt(red[3]), sqrt(red[4]), sqrt(red[5])};
+  double beta[3] = {0.0, 0.0, 0.0};
   __syncthreads();
-  int it = 0;
+  int it = 0, cur = 0;  // P[cur]: the previous search direction
   bool done = false;
-  if (warm) grid.sync();  // X_ reads of the residual pass are complete before updates
   for (; it < maxit; ++it) {
-    // Ap = A p, one warp per row; partial p.Ap
+    double *pold = P[cur], *pnew = P[cur ^ 1];
+    // p = z + beta p_old, formed by every reader; Ap = A p; partial p.Ap
     double pap[3] = {0, 0, 0};
     for (int row = gw; row < n; row += nw) {
       double s0 = 0, s1 = 0, s2 = 0;
       for (int e = rowptr[row] + lane; e < rowptr[row + 1]; e += 32) {
         const double v = val[e];
         const int j = col[e];
-        s0 += v * p[j];
-        s1 += v * p[j + n];
-        s2 += v * p[j + 2 * n];
+        const double p0 = it ? __fma_rn(beta[0], pold[j], z[j]) : z[j];
+        const double p1 = it ? __fma_rn(beta[1], pold[j + n], z[j + n]) : z[j + n];
+        const double p2 = it ? __fma_rn(beta[2], pold[j + 2 * n], z[j + 2 * n]) : z[j + 2 * n];
+        s0 += v * p0;
+        s1 += v * p1;
+        s2 += v * p2;
       }
       for (int o = 16; o > 0; o >>= 1) {
         s0 += __shfl_xor_sync(0xffffffffu, s0, o);
@@ -738,24 +763,27 @@ __global__ void __launch_bounds__(256) k_ivc_cg_grid(IBArgs a, const double *xyz
         s2 += __shfl_xor_sync(0xffffffffu, s2, o);
       }
       if (lane == 0) {
-        Ap[row] = s0;
-        Ap[row + n] = s1;
-        Ap[row + 2 * n] = s2;
-        pap[0] += p[row] * s0;
-        pap[1] += p[row + n] * s1;
-        pap[2] += p[row + 2 * n] * s2;
+        const double s3[3] = {s0, s1, s2};
+        for (int c = 0; c < 3; ++c) {
+          const int ii = row + c * n;
+          const double pv = it ? __fma_rn(beta[c], pold[ii], z[ii]) : z[ii];
+          pnew[ii] = pv;
+          Ap[ii] = s3[c];
+          pap[c] += pv * s3[c];
+        }
       }
     }
-    block_partials(pap, 3, sh, partial);
+    block_partials(pap, 3, sh, pbuf[k & 1]);
     grid.sync();
-    reduce_partials(partial, gridDim.x, 3, red);
+    reduce_partials(pbuf[k & 1], gridDim.x, 3, red);
+    ++k;
     double alpha[3];
     for (int c = 0; c < 3; ++c) alpha[c] = (red[c] != 0.0) ? rz[c] / red[c] : 0.0;
     __syncthreads();
     double ac[6] = {0, 0, 0, 0, 0, 0};
     for (int i = gtid; i < n; i += gsz)
       for (int c = 0; c < 3; ++c) {
-        X_[i + c * n] += alpha[c] * p[i + c * n];
+        X_[i + c * n] += alpha[c] * pnew[i + c * n];
         const double rr = r[i + c * n] - alpha[c] * Ap[i + c * n];
         r[i + c * n] = rr;
         const double zz = rr / diag[i];
@@ -763,10 +791,10 @@ __global__ void __launch_bounds__(256) k_ivc_cg_grid(IBArgs a, const double *xyz
         ac[c] += rr * zz;
         ac[3 + c] += rr * rr;
       }
-    block_partials(ac, 6, sh, partial);
+    block_partials(ac, 6, sh, pbuf[k & 1]);
     grid.sync();
-    reduce_partials(partial, gridDim.x, 6, red);
-    double beta[3];
+    reduce_partials(pbuf[k & 1], gridDim.x, 6, red);
+    ++k;
     bool ok = true;
     for (int c = 0; c < 3; ++c) {
       beta[c] = (rz[c] != 0.0) ? red[c] / rz[c] : 0.0;
@@ -774,14 +802,12 @@ __global__ void __launch_bounds__(256) k_ivc_cg_grid(IBArgs a, const double *xyz
       ok = ok && (sqrt(red[3 + c]) <= tol * bn[c]);
     }
     __syncthreads();
+    cur ^= 1;
     if (ok) {
       done = true;
       ++it;
       break;
     }
-    for (int i = gtid; i < n; i += gsz)
-      for (int c = 0; c < 3; ++c) p[i + c * n] = z[i + c * n] + beta[c] * p[i + c * n];
-    grid.sync();
   }
   if (gtid == 0) {
     *iters = it;
@@ -1230,6 +1256,8 @@ struct ilbm_ib {
   double *d_partial = nullptr;  // CG block partials
   int cg_blocks = 0;
   bool cg_warm = false;  // previous IVC solution available as the CG start
+  bool cg_hist2 = false; // and the one before it (d_Xh), for the extrapolated start
+  double *d_Xh = nullptr;
   // fixed operator solved through its stored inverse (k_ivc_dense)
   int ivc_solver = ILBM_IVC_AUTO;
   bool dense = false, dense_ready = false;
@@ -1570,7 +1598,8 @@ int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom
     ib->nnz_cap = (int)std::min<int64_t>((int64_t)n * per_row, (int64_t)n * n);
     if ((rc = dmalloc(ib, &ib->d_rowptr, (size_t)n + 1)) || (rc = dmalloc(ib, &ib->d_col, (size_t)ib->nnz_cap)) ||
         (rc = dmalloc(ib, &ib->d_val, (size_t)ib->nnz_cap)) || (rc = dmalloc(ib, &ib->d_diag, (size_t)n)) ||
-        (rc = dmalloc(ib, &ib->d_X, 3 * (size_t)n)) || (rc = dmalloc(ib, &ib->d_work, 12 * (size_t)n))) {
+        (rc = dmalloc(ib, &ib->d_X, 3 * (size_t)n)) || (rc = dmalloc(ib, &ib->d_Xh, 3 * (size_t)n)) ||
+        (rc = dmalloc(ib, &ib->d_work, 15 * (size_t)n))) {
       ilbm_ib_destroy(ib);
       return rc;
     }
@@ -1586,7 +1615,7 @@ int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom
       const int b = std::atoi(e);
       if (b >= 1) ib->cg_blocks = std::max(1, std::min(b, per_sm) * sms);
     }
-    if ((rc = dmalloc(ib, &ib->d_partial, 8 * (size_t)std::max(per_sm * sms, 16)))) {
+    if ((rc = dmalloc(ib, &ib->d_partial, 16 * (size_t)std::max(per_sm * sms, 16)))) {
       ilbm_ib_destroy(ib);
       return rc;
     }
@@ -1652,18 +1681,19 @@ static int launch_cg(ilbm_ib *ib, const IBArgs &a_in, cudaStream_t s) {
   const double *xyz = ib->d_xyz, *tgt = ib->d_tgt, *uvw = ib->d_uvw, *val = ib->d_val,
                *diag = ib->d_diag;
   const int *rowptr = ib->d_rowptr, *col = ib->d_col;
-  double *Xv = ib->d_X, *work = ib->d_work, *Fm = ib->d_F, *partial = ib->d_partial;
+  double *Xv = ib->d_X, *Xh = ib->d_Xh, *work = ib->d_work, *Fm = ib->d_F, *partial = ib->d_partial;
   int maxit = 500;
   double tol = cg_tol;
-  int warm = ib->cg_warm ? 1 : 0;
+  int warm = ib->cg_warm ? (ib->cg_hist2 ? 2 : 1) : 0;
   int *status = ib->d_status, *iters = ib->d_iters;
-  void *args[] = {&a, &xyz, &tgt, &uvw, &rowptr, &col, &val, &diag, &Xv, &work, &Fm,
+  void *args[] = {&a, &xyz, &tgt, &uvw, &rowptr, &col, &val, &diag, &Xv, &Xh, &work, &Fm,
                   &partial, &maxit, &tol, &warm, &status, &iters};
   // one warp per ~2 rows keeps the SpMV latency-tolerant; more blocks than
   // that only make the grid barriers dearer
   const int blocks = std::max(8, std::min(ib->cg_blocks, (ib->n + 15) / 16));
   cudaError_t ce = cudaLaunchCooperativeKernel((const void *)k_ivc_cg_grid, dim3(blocks), dim3(256),
                                                args, 0, s);
+  ib->cg_hist2 = ib->cg_warm;  // Xh now holds the previous solution
   ib->cg_warm = true;  // the next solve starts from this one (an initial guess only)
   if (ce != cudaSuccess) return cuda_fail(ce, "cooperative CG launch");
   return ILBM_OK;
@@ -1952,6 +1982,7 @@ int ilbm_ib_set_ivc_solver(ilbm_ib *ib, int solver) {
   }
   ib->ivc_solver = solver;
   ib->cg_warm = false;
+  ib->cg_hist2 = false;
   return ILBM_OK;
 }
 
@@ -1981,10 +2012,15 @@ void ib_state(ilbm_ib *ib, IBState *out) {
   out->F = ib->d_F;
   out->fsum = ib->d_fsum;
   out->X = ib->d_X;
+  out->Xh = ib->d_Xh;
   out->cg_warm = ib->cg_warm;
+  out->cg_hist2 = ib->cg_hist2;
 }
 
-void ib_set_cg_warm(ilbm_ib *ib, bool warm) { ib->cg_warm = warm && ib->d_X != nullptr; }
+void ib_set_cg_warm(ilbm_ib *ib, bool warm, bool hist2) {
+  ib->cg_warm = warm && ib->d_X != nullptr;
+  ib->cg_hist2 = ib->cg_warm && hist2 && ib->d_Xh != nullptr;
+}
 
 }  // namespace ilbm
 

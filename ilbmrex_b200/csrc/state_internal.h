@@ -19,9 +19,11 @@ struct IBState {
   double *xyz = nullptr, *uvw = nullptr, *F = nullptr;  // 3n each
   double *fsum = nullptr;  // 3: last marker force sum
   double *X = nullptr;     // 3n: CG start of the next solve, or NULL
+  double *Xh = nullptr;    // 3n: the solution before it (extrapolated start), or NULL
   bool cg_warm = false;
+  bool cg_hist2 = false;
 };
 
 void ib_state(ilbm_ib *ib, IBState *out);
-void ib_set_cg_warm(ilbm_ib *ib, bool warm);
+void ib_set_cg_warm(ilbm_ib *ib, bool warm, bool hist2);
 }  // namespace ilbm

@@ -465,9 +465,10 @@ int ilbm_checkpoint_write(ilbm_ctx *ctx, const ilbm_box *box, ilbm_ib *ib,
   }
   hd.flags = (box->macro_in ? ILBM_CKPT_MACRO : 0) | (box->force_prev ? ILBM_CKPT_FORCE : 0) |
              (ib ? ILBM_CKPT_BODY : 0);
-  hd.nsec = 1 + (box->macro_in ? 1 : 0) + (box->force_prev ? 1 : 0) + (ib ? 4 + (bs.X ? 1 : 0) : 0);
+  hd.nsec = 1 + (box->macro_in ? 1 : 0) + (box->force_prev ? 1 : 0) +
+            (ib ? 4 + (bs.X ? 1 : 0) + (bs.Xh ? 1 : 0) : 0);
   hd.n_markers = ib ? bs.n : 0;
-  hd.cg_warm = (ib && bs.cg_warm) ? 1 : 0;
+  hd.cg_warm = (ib && bs.cg_warm) ? (bs.cg_hist2 ? 3 : 1) : 0;  // bit 1: CG history
   hd.istep = meta->istep;
   hd.time = meta->time;
   std::memcpy(hd.user, meta->user, sizeof(hd.user));
@@ -497,6 +498,7 @@ int ilbm_checkpoint_write(ilbm_ctx *ctx, const ilbm_box *box, ilbm_ib *ib,
           (rc = write_small(ctx, fp, "MFRC", bs.F, n3)) || (rc = write_small(ctx, fp, "MSUM", bs.fsum, 3)))
         return rc;
       if (bs.X && (rc = write_small(ctx, fp, "MCGX", bs.X, n3))) return rc;
+      if (bs.Xh && (rc = write_small(ctx, fp, "MCGH", bs.Xh, n3))) return rc;
     }
     if (std::fflush(fp) != 0) return io_fail("checkpoint write");
     fc.fp = nullptr;
@@ -551,7 +553,7 @@ int ilbm_checkpoint_read(ilbm_ctx *ctx, const ilbm_box *box, ilbm_ib *ib, ilbm_c
   if ((rc = st.init((size_t)pf.cells() * 8))) return rc;
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "ilbm_checkpoint_read");
-  bool got_cgx = false;
+  bool got_cgx = false, got_cgh = false;
   for (int s = 0; s < hd.nsec; ++s) {
     SecHeader sh;
     if (std::fread(&sh, sizeof(sh), 1, fp) != 1) return io_fail("checkpoint read: short file");
@@ -568,22 +570,24 @@ int ilbm_checkpoint_read(ilbm_ctx *ctx, const ilbm_box *box, ilbm_ib *ib, ilbm_c
       if (!want(3, pm.cells(), real_bytes(ctx))) return mismatch("force section shape");
       if ((rc = read_planes(ctx, fp, sh, box->force_prev, box->mstride[2], pm, st))) return rc;
     } else if (ib && (tag_is(sh, "MXYZ") || tag_is(sh, "MUVW") || tag_is(sh, "MFRC") ||
-                      tag_is(sh, "MSUM") || tag_is(sh, "MCGX"))) {
+                      tag_is(sh, "MSUM") || tag_is(sh, "MCGX") || tag_is(sh, "MCGH"))) {
       const bool sum = tag_is(sh, "MSUM");
       if (!want(1, sum ? 3 : 3 * (uint64_t)bs.n, 8)) return mismatch("body section shape");
       double *dst = tag_is(sh, "MXYZ") ? bs.xyz
                     : tag_is(sh, "MUVW") ? bs.uvw
                     : tag_is(sh, "MFRC") ? bs.F
                     : sum                ? bs.fsum
-                                         : bs.X;
+                    : tag_is(sh, "MCGX") ? bs.X
+                                         : bs.Xh;
       if (!dst) return mismatch("the file holds a CG start vector this body does not use");
       if ((rc = read_small(ctx, fp, sh, dst))) return rc;
       got_cgx = got_cgx || tag_is(sh, "MCGX");
+      got_cgh = got_cgh || tag_is(sh, "MCGH");
     } else {
       return mismatch(std::string("unknown section ") + std::string(sh.tag, 4));
     }
   }
-  if (ib) ib_set_cg_warm(ib, hd.cg_warm != 0 && got_cgx);
+  if (ib) ib_set_cg_warm(ib, (hd.cg_warm & 1) && got_cgx, (hd.cg_warm & 2) && got_cgh);
   meta->istep = hd.istep;
   meta->time = hd.time;
   meta->flags = hd.flags;
