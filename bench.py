@@ -315,16 +315,17 @@ def run_batched(args, world, device):
 
 
 def run_two_level(args, world, device):
-    """The reference's 2D cylinder deck (Examples/Cylinder_flow/inputs:
-    512 x 256, D = 32, Re = 100, U0 = 0.03, max_level 1, ref_ratio 2) as a
-    static two-level hierarchy: a fixed fine box over the body and its near
-    wake (1.5 D upstream, 6 D downstream, 1.5 D across) carrying the marker
-    IBM, FP32 storage.  Cell updates per coarse step: coarse cells + 2 x fine
-    cells.  Beside it, the oracle's two-level driver (plain C, FP64, one
-    thread) on one coarse step of the same hierarchy."""
+    """The D2Q9 cylinder wake on two levels: base grid 1024 x 512, D = 40
+    base cells centred at (256, 256), inflow U = 0.05, Re = 100, one refined
+    level (ratio 2) over a fixed box around the body and its near wake
+    (1.5 D upstream, 6 D downstream, 1.5 D across) carrying the marker IBM
+    with markers ~1 fine dx apart, FP32 storage.  Cell updates per coarse
+    step: coarse cells + 2 x fine cells.  Beside it, the oracle's two-level
+    driver (plain C, FP64, one thread) on coarse steps of the same
+    hierarchy."""
     from ilbmrex_b200 import cases
     from ilbmrex_b200.hierarchy import TwoLevelSolver
-    tl, ib, ic, if_ = cases.cylinder_two_level(nx=512, ny=256, D=32.0, center=(96.0, 127.9), U=0.03,
+    tl, ib, ic, if_ = cases.cylinder_two_level(nx=1024, ny=512, D=40.0, center=(256.0, 256.0), U=0.05,
                                                Re=100.0, upstream=1.5, downstream=6.0, cross=1.5)
     nc = tl.coarse.cells
     nf = int(np.prod(tl.fine_n_cell[: tl.dim]))
@@ -365,7 +366,7 @@ def run_two_level(args, world, device):
             T.close()
         except Exception as e:  # the checker is optional at run time
             cpu = {"value": None, "unit": "MLUPS", "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
-    return {"metric": "two-level MLUPS (cylinder deck, max_level 1, D2Q9 FP32)",
+    return {"metric": "two-level MLUPS (D2Q9 cylinder wake 1024x512 + 1 refined level, FP32)",
             "value": round(mlups, 2), "unit": "MLUPS", "ms_per_coarse_step": round(t / K, 4),
             "coarse_cells": nc, "fine_cells": nf, "fine_box": [list(tl.fine_lo[:2]), list(tl.fine_hi[:2])],
             "updates_per_coarse_step": updates, "steps": K, "gpu_launches": int(launches),

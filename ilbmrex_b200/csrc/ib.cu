@@ -1136,13 +1136,28 @@ __global__ void k_sum_boundary(IBArgs a, double *EFI) {
 }
 
 // marker force sum (:1781-1819), deterministic single-CTA reduction
+// Fixed-order sum of the marker forces times dv: each thread takes markers
+// t, t + B, t + 2B, ... in two interleaved chains (even and odd multiples of
+// B), the three components together, then one block reduction per component.
 __device__ __forceinline__ void marker_sum_block(const IBArgs &a, const double *F, double *fsum) {
   __shared__ double sh[33];
+  double s0[3] = {0.0, 0.0, 0.0}, s1[3] = {0.0, 0.0, 0.0};
+  const int B = blockDim.x;
+  int m = threadIdx.x;
+  for (; m + B < a.n; m += 2 * B) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      s0[c] = X::add(s0[c], X::mul(F[m + c * a.n], a.dv));
+      s1[c] = X::add(s1[c], X::mul(F[m + B + c * a.n], a.dv));
+    }
+  }
+  if (m < a.n) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) s0[c] = X::add(s0[c], X::mul(F[m + c * a.n], a.dv));
+  }
   for (int c = 0; c < 3; ++c) {
-    double s = 0.0;
-    for (int m = threadIdx.x; m < a.n; m += blockDim.x) s += X::mul(F[m + c * a.n], a.dv);
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0) fsum[c] = X::add(fsum[c], s);
+    const double t = block_sum(X::add(s0[c], s1[c]), sh);
+    if (threadIdx.x == 0) fsum[c] = X::add(fsum[c], t);
   }
 }
 
@@ -1668,9 +1683,10 @@ static int launch_cg(ilbm_ib *ib, const IBArgs &a_in, cudaStream_t s) {
   ilbm_ctx *ctx = ib->ctx;
   IBArgs a = a_in;
   // stopping tolerance (relative residual): 1e-14 with FP64 populations, where
-  // results are compared with the reference's dense LU at 1e-12; 1e-10 with
-  // FP32/FP16 populations, whose own rounding is ~1e-7
-  const double cg_tol = (ctx->storage == ILBM_STORAGE_F64) ? 1.0e-14 : 1.0e-10;
+  // results are compared with the reference's dense LU at 1e-12; 1e-8 with
+  // FP32/FP16 populations, below their own rounding (~1e-7) and the FP32
+  // force arrays the solution is exported to
+  const double cg_tol = (ctx->storage == ILBM_STORAGE_F64) ? 1.0e-14 : 1.0e-8;
   if (ib->n <= 1024) {
     k_ivc_cg<<<1, kCgThreads, 0, s>>>(a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_rowptr, ib->d_col,
                                 ib->d_val, ib->d_diag, ib->d_X, ib->d_work, ib->d_F, 500, cg_tol,
@@ -2368,7 +2384,7 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
     k.work = ib->d_work;
     k.nnz_cap = ib->nnz_cap;
     k.reg = ib->p.ivc_diag_reg;
-    k.cg_tol = (ctx->storage == ILBM_STORAGE_F64) ? 1.0e-14 : 1.0e-10;
+    k.cg_tol = (ctx->storage == ILBM_STORAGE_F64) ? 1.0e-14 : 1.0e-8;  // as launch_cg
     k.Ainv = ib->d_Ainv;
     k.Ainv32 = ib->d_Ainv32;
     k.rhs = ib->d_rhs;
