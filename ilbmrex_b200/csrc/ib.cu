@@ -216,6 +216,9 @@ __device__ __forceinline__ void interp_one(const IBArgs &a, int m, int lane, con
       continue;
     }
     const double dvl = (a.dim == 3) ? X::mul(X::mul(tU, tV), tW) : X::mul(tU, tV);
+    // points outside the kernel's support add signed zeros: skipping their
+    // loads leaves every sum bit for bit as it was
+    if (dvl == 0.0) continue;
     const int64_t e = bidx(a, ip, jp, kp);
     part = X::add(part, X::mul(dvl, d));
     u = X::add(u, X::mul(X::mul(dvl, EV[e]), d));
@@ -1083,6 +1086,9 @@ __device__ __forceinline__ void spread_one(const IBArgs &a, int m, int lane, con
       continue;
     }
     const double t3 = (a.dim == 3) ? X::mul(X::mul(tU, tV), tW) : X::mul(tU, tV);
+    // points outside the kernel's support would add signed zeros to a band
+    // that starts at +0: skipping their atomics changes no value
+    if (t3 == 0.0) continue;
     const double dvl = X::mul(t3, scale);
     const int64_t e = bidx(a, ip, jp, kp);
     atomicAdd(&EFI[e], X::mul(dvl, fx));
