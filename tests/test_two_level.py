@@ -99,3 +99,21 @@ def test_uniform_flow_stays_uniform():
         assert np.abs(m[1] - 0.03).max() < 1e-14 and np.abs(m[2] + 0.01).max() < 1e-14
         assert np.abs(m[0] - 1.0).max() < 1e-14
     gpu.close()
+
+
+def test_sphere_body_on_fine_level_3d():
+    """The headline's machinery at test size: D3Q19, two levels, a sphere on
+    the fine level with more than 1024 markers (grid CG, extrapolated starts),
+    its forcing overlapped with the level steps; FP64 against the oracle's
+    two-level driver with dense LU (relative L2 <= 1e-12)."""
+    tl, ib, ic, if_ = cases.sphere_two_level(nx=32, ny=24, nz=24, D=10.0, center=(12.3, 11.8, 12.1),
+                                             U=0.04, Re=30.0, box_lo=(4, 4, 4), box_hi=(22, 20, 20))
+    cpu, gpu = _pair(tl, ic, if_, ib, "f64", 4)
+    n = __import__("ctypes").c_int64()
+    gpu.L.ilbm_ib_num_markers(gpu.ib, __import__("ctypes").byref(n))
+    assert n.value > 1024
+    for lev in (0, 1):
+        assert rel_l2(gpu.get_f(lev), cpu.get_f(lev)) <= 1e-12
+        assert rel_l2(gpu.get_macro(lev), cpu.get_macro(lev)) <= 1e-12
+    np.testing.assert_allclose(gpu.rec[3:5], cpu.force_record()[3:5], rtol=1e-9, atol=1e-12)
+    gpu.close()
