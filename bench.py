@@ -258,6 +258,43 @@ def run_single_level(args, world, device):
     return out
 
 
+def run_precision(args, world, device):
+    """The storage forms of the headline hierarchy against its FP64 run: the
+    two-level sphere advanced the same number of coarse steps from the same
+    state with FP64, FP32-shifted and FP16-scaled populations; per form its
+    ms per coarse step, Cd / Cl and their relative difference to FP64, and
+    the relative L2 difference of the fine level's velocity."""
+    from ilbmrex_b200.hierarchy import TwoLevelSolver
+    tl, ib, init_c, init_f = sphere_hierarchy()
+    n = args.precision_steps
+    out, ref = {}, None
+    for st in ("f64", "f32", "f16"):
+        S = TwoLevelSolver(tl, st, ib=ib, device=device.index or 0)
+        S.set_macro(init_c(), init_f())
+        S.step(n - 1)
+        S.ctx.sync()
+        S.ctx.record(12)
+        S.advance(record_force=True)
+        S.ctx.record(13)
+        S.ctx.sync()
+        ms = S.ctx.elapsed_ms(12, 13)
+        u = S.get_macro(1)[1:4]
+        cd, cl = float(S.rec[3]), float(S.rec[4])
+        S.close()
+        if ref is None:
+            ref = (u, cd, cl)
+            out[st] = {"cd": round(cd, 6), "cl": round(cl, 8), "ms_last_step": round(ms, 3)}
+            continue
+        du = float(np.sqrt(np.sum((u - ref[0]) ** 2) / np.sum(ref[0] ** 2)))
+        out[st] = {"cd": round(cd, 6), "cl": round(cl, 8), "ms_last_step": round(ms, 3),
+                   "cd_rel_err_vs_f64": float(f"{abs(cd - ref[1]) / abs(ref[1]):.3e}"),
+                   "cl_abs_err_vs_f64": float(f"{abs(cl - ref[2]):.3e}"),
+                   "fine_u_rel_l2_vs_f64": float(f"{du:.3e}")}
+    return {"what": f"the two-level sphere after {n} coarse steps in each storage form, "
+                    "errors against the FP64 run of the same steps (Cl ~ 0 by symmetry: absolute)",
+            "steps": n, **out}
+
+
 def run_batched(args, world, device):
     """Batched D2Q9 FP32 workload (64 seeded cylinder / pitching-airfoil cases)
     through the batch engine, against the same cases run one after another
@@ -271,8 +308,7 @@ def run_batched(args, world, device):
     cells = sum(c.cells for c, _, _ in mix)
     K = args.batch_steps
     B = Batch(D2Q9, "f32", device=device.index or 0, rec_slots=512)
-    for c, ib, init in mix:
-        B.add(B.solver(c, ib, init), max_steps=K + 200)
+    ids = [B.add(B.solver(c, ib, init), max_steps=K + 200) for c, ib, init in mix]
     tile_w, cps, _ = B.tune(trial_steps=4)
     B.step(4)
     B.ctx.sync()
@@ -285,6 +321,21 @@ def run_batched(args, world, device):
     launches = B.ctx.launches() - launches0
     t_b = allreduce_max(B.ctx.elapsed_ms(4, 5), world, device)
     batched = world * cells * K / (t_b * 1e-3) / 1e6
+    # FP32 batched cases against the same cases run alone in FP64 for the
+    # same steps: Cd / Cl of the last step
+    errs = []
+    for idx in range(min(args.batch_check_cases, len(mix))):
+        c, ib, init = mix[idx]
+        s32 = B.sync(ids[idx])
+        cd32, cl32, nsteps = float(s32.rec[3]), float(s32.rec[4]), s32.istep
+        R = LevelSolver(c, "f64", ib=ib, device=device.index or 0)
+        R.set_macro(*init())
+        R.step(nsteps, record_force=True)
+        cd64, cl64 = float(R.rec[3]), float(R.rec[4])
+        R.close()
+        errs.append({"case": c.name, "steps": nsteps, "cd_f32": round(cd32, 6), "cd_f64": round(cd64, 6),
+                     "cd_rel_err": float(f"{abs(cd32 - cd64) / max(abs(cd64), 1e-30):.3e}"),
+                     "cl_abs_err": float(f"{abs(cl32 - cl64):.3e}")})
     B.close()
     # plain: case by case through the single-case call
     Kp = args.batch_plain_steps
@@ -309,6 +360,7 @@ def run_batched(args, world, device):
             "cases": len(mix), "cells": cells,
             "steps": K, "plain_steps_per_case": Kp, "ms_per_step": round(t_b / K, 4),
             "tile_w": tile_w, "ctas_per_sm": cps, "gpu_launches": int(launches),
+            "vs_f64_alone": errs,
             "workload": "seeded mix: grids 256x128..1024x512, cylinders D 16-48 Re 20-200, "
                         "NACA0012 pitching (chord 64-128, 2-15 deg, k 0.05-0.3), FP32 storage; "
                         "each case steps through its own IB (stored IVC inverse or CG)"}
@@ -317,16 +369,19 @@ def run_batched(args, world, device):
 def run_two_level(args, world, device):
     """The D2Q9 cylinder wake on two levels: base grid 1024 x 512, D = 40
     base cells centred at (256, 256), inflow U = 0.05, Re = 100, one refined
-    level (ratio 2) over a fixed box around the body and its near wake
-    (1.5 D upstream, 6 D downstream, 1.5 D across) carrying the marker IBM
-    with markers ~1 fine dx apart, FP32 storage.  Cell updates per coarse
-    step: coarse cells + 2 x fine cells.  Beside it, the oracle's two-level
-    driver (plain C, FP64, one thread) on coarse steps of the same
-    hierarchy."""
+    level (ratio 2, max_level 1) over the fixed body-and-wake box of the
+    reference's refinement rule (1 R upstream, 4 R downstream, 2 R across,
+    plus a 6-cell pad) carrying the marker IBM with markers ~1 fine dx apart,
+    FP32 storage.  Cell updates per coarse step: coarse cells + 2 x fine
+    cells.  Beside it, the oracle's two-level driver (plain C, FP64, one
+    thread) on coarse steps of the same hierarchy."""
     from ilbmrex_b200 import cases
     from ilbmrex_b200.hierarchy import TwoLevelSolver
-    tl, ib, ic, if_ = cases.cylinder_two_level(nx=1024, ny=512, D=40.0, center=(256.0, 256.0), U=0.05,
-                                               Re=100.0, upstream=1.5, downstream=6.0, cross=1.5)
+    R, pad = 20.0, 6.0
+    tl, ib, ic, if_ = cases.cylinder_two_level(nx=1024, ny=512, D=2 * R, center=(256.0, 256.0), U=0.05,
+                                               Re=100.0, upstream=(R + pad) / (2 * R),
+                                               downstream=(4 * R + pad) / (2 * R),
+                                               cross=(2 * R + pad) / (2 * R))
     nc = tl.coarse.cells
     nf = int(np.prod(tl.fine_n_cell[: tl.dim]))
     updates = nc + 2 * nf
@@ -535,6 +590,7 @@ def run_b200(args):
                         "sample": f"unavailable: {e}"}
 
     single = None if args.no_single_level else run_single_level(args, world, device)
+    precision = None if args.no_precision else run_precision(args, world, device)
     batched = None
     if not args.no_batched:
         batched = run_batched(args, world, device)
@@ -568,6 +624,7 @@ def run_b200(args):
             "ivc_cg_iterations": int(cg_it.value),
             "cd_cl_after": [round(cd, 5), round(cl, 6)],
             "first_step_ms_incl_ivc_setup": round(first_step_ms, 2),
+            "precision": precision,
             "single_level": single,
             "batched": batched,
             "served": served,
@@ -592,6 +649,8 @@ def main():
     ap.add_argument("--nz", type=int, default=0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched workload")
     ap.add_argument("--no-single-level", action="store_true", help="skip the single-level sphere")
+    ap.add_argument("--no-precision", action="store_true", help="skip the storage-form error check")
+    ap.add_argument("--precision-steps", type=int, default=200)
     ap.add_argument("--no-served", action="store_true", help="skip the served workload")
     ap.add_argument("--no-two-level", action="store_true", help="skip the two-level cylinder workload")
     ap.add_argument("--two-level-steps", type=int, default=100)
@@ -610,6 +669,7 @@ def main():
     ap.add_argument("--batch-cases", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=40)
     ap.add_argument("--batch-plain-steps", type=int, default=8)
+    ap.add_argument("--batch-check-cases", type=int, default=4)
     args = ap.parse_args()
     if args.nx:
         set_workload_size(args.nx, args.ny or args.nx // 2, args.nz or args.nx // 2)
