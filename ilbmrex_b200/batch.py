@@ -120,10 +120,12 @@ class Batch:
         if new > 0:
             if s.ib is not None:
                 hist = getattr(s, "rec_history", None)
-                for r in self.records(cid)[self._taken[cid]:steps.value]:
-                    s.rec = s.force_record(r[0:3], r[3:6])
+                raw = np.asarray(self.records(cid)[self._taken[cid]:steps.value], dtype=np.float64)
+                if len(raw):
+                    recs = s.force_records(raw[:, 0:3], raw[:, 3:6])
+                    s.rec = recs[-1].copy()
                     if hist is not None:
-                        hist.append(s.rec.copy())
+                        hist.extend(recs)
             s.istep += new
             self._taken[cid] = steps.value
         # parity 0: the state is in the buffers as added; 1: roles swapped

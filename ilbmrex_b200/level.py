@@ -357,6 +357,39 @@ class LevelSolver:
                 rec[5] = Ftc[2] / denom
         return rec
 
+    def force_records(self, eul_sums: np.ndarray, marker_sums: np.ndarray) -> np.ndarray:
+        """force_record for a run of consecutive steps at once: rows of
+        Eulerian and marker force sums in, rows of the 18-value record out
+        (the same elementwise arithmetic, so the same values), with the
+        previous-step state carried through and left at the last step."""
+        case, ib = self.case, self.ib_case
+        n = len(eul_sums)
+        if n == 0:
+            return np.zeros((0, 18))
+        Fs = np.array(eul_sums, dtype=np.float64).reshape(n, 3).copy()
+        if self.dim != 3:
+            Fs[:, 2] = 0.0
+        dV = case.dx ** self.dim
+        Feul = -(Fs * dV) / case.dt
+        Fm = -np.asarray(marker_sums, dtype=np.float64).reshape(n, 3)
+        Fme = Feul.copy()
+        Fb = {0: Fme, 1: Feul, 2: Fm}.get(ib.force_eval_method, Feul)
+        prev = np.vstack([self.prev_body[None, :], Fb[:-1]])
+        Ftc = 0.5 * (prev + Fb)
+        if not self.have_prev_body:
+            Ftc[0] = Fb[0]
+        self.prev_body = Fb[-1].copy()
+        self.have_prev_body = True
+        U = ib.U0
+        denom = (0.5 * 1.0 * U * U * (math.pi * ib.R * ib.R)) if self.dim == 3 else (0.5 * 1.0 * U * U * (2.0 * ib.R))
+        rec = np.zeros((n, 18))
+        rec[:, 0:3], rec[:, 6:9], rec[:, 9:12], rec[:, 12:15], rec[:, 15:18] = Ftc, Fb, Feul, Fm, Fme
+        if denom > 0:
+            rec[:, 3], rec[:, 4] = Ftc[:, 0] / denom, Ftc[:, 1] / denom
+            if self.dim == 3:
+                rec[:, 5] = Ftc[:, 2] / denom
+        return rec
+
     # ---- read-back ---------------------------------------------------------
     def get_f(self) -> np.ndarray:
         self.ctx.sync()
