@@ -60,8 +60,8 @@ void free_built(ilbm_batch *b) {
       cudaGraphExecDestroy(b->gexec[i]);
       b->gexec[i] = nullptr;
     }
-  if (b->d_args) cudaFree(b->d_args);
-  if (b->d_tiles) cudaFree(b->d_tiles);
+  ilbm_ctx_free(b->ctx, b->d_args);  // stream-ordered: after the steps that read them
+  ilbm_ctx_free(b->ctx, b->d_tiles);
   b->d_args = nullptr;
   b->d_tiles = nullptr;
   ib_batch_destroy(b->ibb);
@@ -185,12 +185,15 @@ int build(ilbm_batch *b) {
   }
   const int use = (b->ctas_per_sm > 0) ? std::min(b->ctas_per_sm, per_sm) : per_sm;
   b->blocks = std::max(1, std::min(b->ntiles, use * b->sms));
-  cudaError_t e = cudaMalloc(&b->d_args, args.size() * sizeof(StepArgs));
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_tiles, tiles.size() * sizeof(StepTile));
+  // stream-ordered tables (pageable sources are staged before the copies return)
+  cudaError_t e = ilbm_ctx_malloc(ctx, (void **)&b->d_args, args.size() * sizeof(StepArgs));
+  if (e == cudaSuccess) e = ilbm_ctx_malloc(ctx, (void **)&b->d_tiles, tiles.size() * sizeof(StepTile));
   if (e == cudaSuccess)
-    e = cudaMemcpy(b->d_args, args.data(), args.size() * sizeof(StepArgs), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(b->d_args, args.data(), args.size() * sizeof(StepArgs), cudaMemcpyHostToDevice,
+                        ctx->stream);
   if (e == cudaSuccess)
-    e = cudaMemcpy(b->d_tiles, tiles.data(), tiles.size() * sizeof(StepTile), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(b->d_tiles, tiles.data(), tiles.size() * sizeof(StepTile), cudaMemcpyHostToDevice,
+                        ctx->stream);
   if (e != cudaSuccess) {
     free_built(b);
     return cuda_fail(e, "batch tables");

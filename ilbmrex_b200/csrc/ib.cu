@@ -1294,8 +1294,8 @@ namespace {
 template <class T>
 int dmalloc(ilbm_ib *ib, T **p, size_t count) {
   void *q = nullptr;
-  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
-  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc (IB)");
+  cudaError_t e = ilbm_ctx_malloc(ib->ctx, &q, count * sizeof(T));
+  if (e != cudaSuccess) return cuda_fail(e, "device allocation (IB)");
   ib->allocs.push_back(q);
   *p = static_cast<T *>(q);
   return ILBM_OK;
@@ -1547,7 +1547,7 @@ int enable_dense(ilbm_ib *ib) {
       (rc = dmalloc(ib, &ib->d_rhs, 3 * (size_t)ld)))
     return rc;
   // the padding of the right-hand side meets zero columns of A^-1: keep it finite
-  cudaError_t e = cudaMemset(ib->d_rhs, 0, 3 * (size_t)ld * sizeof(double));
+  cudaError_t e = cudaMemsetAsync(ib->d_rhs, 0, 3 * (size_t)ld * sizeof(double), ib->ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "enable_dense");
   ib->ld = ld;
   ib->dense = true;
@@ -1601,17 +1601,18 @@ int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom
     h[i + n] = ib->hy[i];
     h[i + 2 * n] = ib->hz[i];
   }
-  cudaMemcpy(ib->d_xyz, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
+  // stream-ordered like the allocations (pageable source: staged before return)
+  cudaMemcpyAsync(ib->d_xyz, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
   if (!ib->xref.empty()) {
     for (int i = 0; i < n; ++i) {
       h[i] = ib->xref[i + 1];
       h[i + n] = ib->yref[i + 1];
       h[i + 2 * n] = ib->zref[i + 1];
     }
-    cudaMemcpy(ib->d_ref, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice);
+    cudaMemcpyAsync(ib->d_ref, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
   }
-  cudaMemset(ib->d_status, 0, 2 * sizeof(int));
-  cudaMemset(ib->d_fsum, 0, 4 * sizeof(double));
+  cudaMemsetAsync(ib->d_status, 0, 2 * sizeof(int), ctx->stream);
+  cudaMemsetAsync(ib->d_fsum, 0, 4 * sizeof(double), ctx->stream);
   if (p->coupling_method == 1) {
     // neighbours per row: at most (9 cells)^d of markers within +-4 cells;
     // keep a generous cap and report overflow through the status word
@@ -1657,11 +1658,14 @@ int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom
 
 int ilbm_ib_destroy(ilbm_ib *ib) {
   if (!ib) return ILBM_OK;
-  if (ib->ctx) {
-    cudaSetDevice(ib->ctx->device);
-    cudaStreamSynchronize(ib->ctx->stream);
-  }
-  for (void *q : ib->allocs) cudaFree(q);
+  ilbm_ctx *ctx = ib->ctx;
+  cudaSetDevice(ctx->device);
+  // stream-ordered frees after the work queued on the context's streams
+  // (the side stream's last immersed-boundary stage included): no
+  // device-wide synchronisation, the memory returns to the context's pool
+  cudaEventRecord(ctx->ev_fork, ctx->side);
+  cudaStreamWaitEvent(ctx->stream, ctx->ev_fork, 0);
+  for (void *q : ib->allocs) ilbm_ctx_free(ctx, q);
   delete ib;
   return ILBM_OK;
 }
@@ -2299,8 +2303,8 @@ struct IBBatch {
 template <class T>
 static int bmalloc(IBBatch *b, T **p, size_t count) {
   void *q = nullptr;
-  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
-  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc (IB batch)");
+  cudaError_t e = ilbm_ctx_malloc(b->ctx, &q, count * sizeof(T));
+  if (e != cudaSuccess) return cuda_fail(e, "device allocation (IB batch)");
   b->allocs.push_back(q);
   *p = static_cast<T *>(q);
   return ILBM_OK;
@@ -2310,7 +2314,8 @@ static int bupload(IBBatch *b, T **p, const std::vector<T> &h) {
   int rc = bmalloc(b, p, h.size());
   if (rc) return rc;
   if (!h.empty()) {
-    cudaError_t e = cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+    cudaError_t e = cudaMemcpyAsync(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice,
+                                    b->ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "IB batch upload");
   }
   return ILBM_OK;
@@ -2321,7 +2326,7 @@ static int grid_for(int64_t items, int threads) {
 
 void ib_batch_destroy(IBBatch *b) {
   if (!b) return;
-  for (void *q : b->allocs) cudaFree(q);
+  for (void *q : b->allocs) ilbm_ctx_free(b->ctx, q);
   delete b;
 }
 
@@ -2445,9 +2450,9 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
     ib_batch_destroy(b);
     return rc;
   }
-  cudaMemset(rec, 0, (size_t)b->nc * b->rec_slots * 8 * sizeof(double));
-  cudaMemset(b->d_steps, 0, b->nc * sizeof(int));
-  cudaMemset(b->d_done, 0, b->nc * sizeof(unsigned));
+  cudaMemsetAsync(rec, 0, (size_t)b->nc * b->rec_slots * 8 * sizeof(double), ctx->stream);
+  cudaMemsetAsync(b->d_steps, 0, b->nc * sizeof(int), ctx->stream);
+  cudaMemsetAsync(b->d_done, 0, b->nc * sizeof(unsigned), ctx->stream);
   {
     std::vector<int> lim(b->nc);
     for (int c = 0; c < b->nc; ++c) lim[c] = std::max(0, cases[c].limit);

@@ -321,7 +321,16 @@ struct ilbm_ctx {
   // completed); checked and cleared by ilbm_sync
   int *d_flag = nullptr;
   int sms = 0;
+  // the context's own memory pool for stream-ordered allocations (IB arrays,
+  // batch tables): freed memory stays in the pool for the next request
+  // instead of a device-wide synchronising cudaFree
+  cudaMemPool_t pool = nullptr;
 };
 
 // grow ctx scratch to at least n bytes (returns nullptr on failure)
 void *ilbm_ctx_scratch(ilbm_ctx *ctx, size_t n);
+// stream-ordered allocation from the context's pool, on ctx->stream: usable by
+// work queued on that stream (or ordered after it by an event) once it returns
+cudaError_t ilbm_ctx_malloc(ilbm_ctx *ctx, void **p, size_t bytes);
+// stream-ordered free on ctx->stream: after the work queued before it
+void ilbm_ctx_free(ilbm_ctx *ctx, void *p);

@@ -1580,6 +1580,14 @@ void *ilbm_ctx_scratch(ilbm_ctx *ctx, size_t n) {
   return ctx->scratch;
 }
 
+cudaError_t ilbm_ctx_malloc(ilbm_ctx *ctx, void **p, size_t bytes) {
+  return cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 1), ctx->pool, ctx->stream);
+}
+
+void ilbm_ctx_free(ilbm_ctx *ctx, void *p) {
+  if (p) cudaFreeAsync(p, ctx->stream);
+}
+
 extern "C" {
 
 const char *ilbm_last_error(void) { return ilbm::get_error(); }
@@ -1660,6 +1668,15 @@ int ilbm_create(const ilbm_lattice *lat, int storage, int device, void *cuda_str
   if (e == cudaSuccess) e = cudaMalloc(&c->d_flag, 16);
   if (e == cudaSuccess) e = cudaMemset(c->d_flag, 0, 16);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) {
+    cudaMemPoolProps pp = {};
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = device;
+    e = cudaMemPoolCreate(&c->pool, &pp);
+    uint64_t keep = UINT64_MAX;  // never trim at synchronisation points
+    if (e == cudaSuccess) e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   if (e != cudaSuccess) {
     ilbm_destroy(c);
     return cuda_fail(e, "ilbm_create");
@@ -1687,6 +1704,8 @@ int ilbm_destroy(ilbm_ctx *ctx) {
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->ev_done) cudaEventDestroy(ctx->ev_done);
+  // a pool with allocations outstanding is released once they are freed
+  if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return ILBM_OK;
