@@ -443,9 +443,18 @@ def run_served(args, world, device):
     for r, t in zip(reqs, arr):
         r.arrival = float(t)
     lups = sum(r.case.cells * r.steps for r in reqs)
+    # warm-up (untimed), through the same long-lived server and the plain call:
+    # a few short requests of every kind load the kernels and fill the
+    # server's memory pools
+    wrng = np.random.default_rng(7)
+    warm = [make_request(1000 + i, k, wrng, 20, scale=args.serve_scale)
+            for i, k in enumerate(["cylinder"] * 4 + ["duct"] * 2 + ["sphere"] * 2)]
     srv = Server("f32", device=device.index or 0, chunk=args.serve_chunk)
+    srv.run(warm)
     stats = srv.run(reqs)
     srv.close()
+    for r in warm:
+        run_alone(r, "f32", device=device.index or 0)
     # plain: one request at a time through the single-case call
     service = []
     for r in reqs:
@@ -468,6 +477,7 @@ def run_served(args, world, device):
             "requests": n, "arrival_rate_per_s": args.serve_rate, "makespan_s": round(stats["makespan_s"], 3),
             "plain_makespan_s": round(done, 3), "plain_busy_s": round(sum(service), 3),
             "server_time_s": stats["time_s"],
+            "warmup": f"{len(warm)} requests of 20 steps through the same server and the plain call, untimed",
             "cells_min_max": [int(min(sizes)), int(max(sizes))],
             "steps_min_max": [args.serve_min_steps, args.serve_max_steps],
             "workload": f"seeded Poisson arrivals; 50% D2Q9 cylinder/airfoil, 25% D3Q19 duct N x N x 4N, "

@@ -413,6 +413,41 @@ __device__ __forceinline__ void block_reduce(const double *v, double (*sh)[NV], 
   }
 }
 
+// One CSR row times three vectors (entries j, j + n, j + 2n of v3), one
+// thread: the index and value loads of four entries are issued before their
+// gathers, and the gathers before the multiply-adds, which run in entry
+// order as the straight loop's do (same partial sums, fewer dependent
+// round trips per row).
+__device__ __forceinline__ void thread_row_dot3(const int *col, const double *val, int e0, int e1,
+                                                const double *v3, int n, double (&acc)[3]) {
+  for (int e = e0; e < e1; e += 4) {
+    int j[4];
+    double v[4], q[4][3];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      j[u] = (e + u < e1) ? col[e + u] : 0;
+      v[u] = (e + u < e1) ? val[e + u] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (e + u < e1) {
+        q[u][0] = v3[j[u]];
+        q[u][1] = v3[j[u] + n];
+        q[u][2] = v3[j[u] + 2 * n];
+      }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (e + u < e1) {
+        acc[0] += v[u] * q[u][0];
+        acc[1] += v[u] * q[u][1];
+        acc[2] += v[u] * q[u][2];
+      }
+  }
+}
+
+// systems up to this size keep the search direction in shared memory
+constexpr int kCgSharedN = 1024;
+
 // Jacobi-preconditioned CG for the three force components at once, one
 // block.  warm: start from the previous solution in X_ (the force changes
 // little from one step to the next), else from zero.  Per iteration two
@@ -423,8 +458,10 @@ __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz,
                                              double *work, double *F, int maxit, double tol,
                                              int *status, int *iters, int warm) {
   __shared__ double sh3[kMaxWarps][3], sh6[kMaxWarps][6];
+  __shared__ double p_sh[3 * kCgSharedN];
   const int n = a.n;
-  double *r = work, *z = work + 3 * n, *p = work + 6 * n, *Ap = work + 9 * n;
+  double *r = work, *z = work + 3 * n, *Ap = work + 9 * n;
+  double *p = (n <= kCgSharedN) ? p_sh : work + 6 * n;
   // b (kept in Ap until the residual is formed), x0 = 0 or the previous x
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double Ux, Uy, Uz;
@@ -440,14 +477,7 @@ __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz,
   double part[6] = {0, 0, 0, 0, 0, 0};
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double ax[3] = {0.0, 0.0, 0.0};
-    if (warm)
-      for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
-        const double v = val[e];
-        const int j = col[e];
-        ax[0] += v * X_[j];
-        ax[1] += v * X_[j + n];
-        ax[2] += v * X_[j + 2 * n];
-      }
+    if (warm) thread_row_dot3(col, val, rowptr[i], rowptr[i + 1], X_, n, ax);
     for (int c = 0; c < 3; ++c) {
       const double b = Ap[i + c * n];
       const double rr = b - ax[c];
@@ -471,13 +501,7 @@ __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz,
     double pap[3] = {0.0, 0.0, 0.0};
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       double acc[3] = {0.0, 0.0, 0.0};
-      for (int e = rowptr[i]; e < rowptr[i + 1]; ++e) {
-        const double v = val[e];
-        const int j = col[e];
-        acc[0] += v * p[j];
-        acc[1] += v * p[j + n];
-        acc[2] += v * p[j + 2 * n];
-      }
+      thread_row_dot3(col, val, rowptr[i], rowptr[i + 1], p, n, acc);
       for (int c = 0; c < 3; ++c) {
         Ap[i + c * n] = acc[c];
         pap[c] += p[i + c * n] * acc[c];
