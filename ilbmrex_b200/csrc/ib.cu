@@ -661,8 +661,17 @@ __device__ __forceinline__ void reduce_partials(const double *partial, int nbloc
                                                 double *out_sh) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (wid < nval) {
+    // eight loads in flight per lane before the adds, which keep the order
+    // b = lane, lane + 32, ... (one L2 round trip per eight partials)
     double s = 0.0;
-    for (int b = lane; b < nblocks; b += 32) s += partial[b * 8 + wid];
+    for (int b0 = lane; b0 < nblocks; b0 += 256) {
+      double t[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) t[u] = (b0 + 32 * u < nblocks) ? partial[(b0 + 32 * u) * 8 + wid] : 0.0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (b0 + 32 * u < nblocks) s += t[u];
+    }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) out_sh[wid] = s;
   }
@@ -771,8 +780,16 @@ __global__ void __launch_bounds__(256) k_ivc_cg_grid(IBArgs a, const double *xyz
   for (; it < maxit; ++it) {
     double *pold = P[cur], *pnew = P[cur ^ 1];
     // p = z + beta p_old, formed by every reader; Ap = A p; partial p.Ap
-    double pap[3] = {0, 0, 0};
+    // (lane c < 3 owns component c of the row: its p entries are loaded
+    // before the row's products)
+    double pap_c = 0.0;
+    const double beta_c = (lane == 0) ? beta[0] : ((lane == 1) ? beta[1] : beta[2]);
     for (int row = gw; row < n; row += nw) {
+      double zc = 0.0, pc = 0.0;
+      if (lane < 3) {
+        zc = z[row + lane * n];
+        if (it) pc = pold[row + lane * n];
+      }
       double s0 = 0, s1 = 0, s2 = 0;
       for (int e = rowptr[row] + lane; e < rowptr[row + 1]; e += 32) {
         const double v = val[e];
@@ -789,17 +806,17 @@ __global__ void __launch_bounds__(256) k_ivc_cg_grid(IBArgs a, const double *xyz
         s1 += __shfl_xor_sync(0xffffffffu, s1, o);
         s2 += __shfl_xor_sync(0xffffffffu, s2, o);
       }
-      if (lane == 0) {
-        const double s3[3] = {s0, s1, s2};
-        for (int c = 0; c < 3; ++c) {
-          const int ii = row + c * n;
-          const double pv = it ? __fma_rn(beta[c], pold[ii], z[ii]) : z[ii];
-          pnew[ii] = pv;
-          Ap[ii] = s3[c];
-          pap[c] += pv * s3[c];
-        }
+      if (lane < 3) {
+        const int ii = row + lane * n;
+        const double sc = (lane == 0) ? s0 : ((lane == 1) ? s1 : s2);
+        const double pv = it ? __fma_rn(beta_c, pc, zc) : zc;
+        pnew[ii] = pv;
+        Ap[ii] = sc;
+        pap_c += pv * sc;
       }
     }
+    double pap[3];
+    for (int c = 0; c < 3; ++c) pap[c] = (lane == c) ? pap_c : 0.0;
     block_partials(pap, 3, sh, pbuf[k & 1]);
     grid.sync();
     reduce_partials(pbuf[k & 1], gridDim.x, 3, red);
