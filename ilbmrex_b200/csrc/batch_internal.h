@@ -14,9 +14,11 @@ namespace ilbm {
 
 // ---- lbm_step.cu --------------------------------------------------------
 // the level step with a stored-macro box (the two-level hierarchy's coarse
-// level); mlo / mhi NULL: ilbm_level_step
+// level); mlo / mhi NULL: ilbm_level_step.  part 0: the whole step; 1 / 2:
+// its two halves along the box's last dimension (one box; the ghost push
+// runs with the first, macro_out after the second)
 int level_step_impl(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const ilbm_level_params *p,
-                    const int *mlo, const int *mhi);
+                    const int *mlo, const int *mhi, int part);
 // StepArgs of one batched case (self-filled ghosts, one box = domain)
 int batch_case_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p,
                     StepArgs *out);

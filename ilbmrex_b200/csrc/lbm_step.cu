@@ -1132,6 +1132,15 @@ static int launch_step(ilbm_ctx *ctx, const StepArgs &a, const ilbm_level_params
   return ILBM_OK;
 }
 
+// the cells [a.rlo, a.rhi] of a level step, with the ghost-shell push or not
+template <class L, int S>
+static int launch_step_part(ilbm_ctx *ctx, const StepArgs &a, bool with_ghosts) {
+  launch_cells<L, S>(ctx, a, ctx->stream, with_ghosts);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "level step launch");
+  return ILBM_OK;
+}
+
 // Level step whose band [blo,bhi] waits for `band_ready` (recorded on another
 // stream): ghost push and every cell outside the band run first, then the band.
 template <class L, int S>
@@ -1489,10 +1498,14 @@ __global__ void __launch_bounds__(256) k_tags(TagArgs g, const R *vor, unsigned 
 
 // one level step; with mlo / mhi the boxes' macro_in holds stored values
 // only on [mlo, mhi] (elsewhere rho, u are recovered from f^n and F^{n-1}),
-// and macro_out is written there only
+// and macro_out is written there only.  part (one box only): 0 = the whole
+// step; 1 = the ghost-shell push and the cells of the first half of the box
+// along its last dimension; 2 = the cells of the second half, then
+// macro_out.  Every (cell, direction) slot of f_out is written by exactly one
+// cell or ghost push, so the two halves may run at different times
 int level_step_impl(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const ilbm_level_params *p,
-                    const int *mlo, const int *mhi) {
-  if (!ctx || !boxes || nbox <= 0) {
+                    const int *mlo, const int *mhi, int part) {
+  if (!ctx || !boxes || nbox <= 0 || part < 0 || part > 2 || (part && nbox != 1)) {
     set_error("level step: null argument");
     return ILBM_ERR_ARG;
   }
@@ -1548,8 +1561,22 @@ int level_step_impl(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const ilbm_l
         a.mbhi[d] = (d < ctx->dim) ? mhi[d] : 0;
       }
     }
-    rc = ILBM_DISPATCH(ctx, launch_step, ctx, a, p);
+    if (part == 0) {
+      rc = ILBM_DISPATCH(ctx, launch_step, ctx, a, p);
+    } else if (a.hi[ctx->dim - 1] == a.lo[ctx->dim - 1]) {
+      // one cell along the split dimension: the first part takes it all
+      if (part == 1) rc = ILBM_DISPATCH(ctx, launch_step_part, ctx, a, true);
+    } else {
+      const int e = ctx->dim - 1;  // split along the last dimension
+      const int mid = a.lo[e] + (a.hi[e] - a.lo[e] + 1) / 2 - 1;
+      if (part == 1)
+        a.rhi[e] = mid;
+      else
+        a.rlo[e] = mid + 1;
+      rc = ILBM_DISPATCH(ctx, launch_step_part, ctx, a, part == 1);
+    }
     if (rc) return rc;
+    if (part == 1) continue;  // macro_out once both halves have run
     if (b.macro_out) {
       StepArgs am = a;
       am.f_in = b.f_out;
@@ -1782,7 +1809,7 @@ int ilbm_storage_bytes(const ilbm_ctx *ctx, int *sb, int *rb) {
 }
 
 int ilbm_level_step(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const ilbm_level_params *p) {
-  return level_step_impl(ctx, boxes, nbox, p, nullptr, nullptr);
+  return level_step_impl(ctx, boxes, nbox, p, nullptr, nullptr, 0);
 }
 
 int ilbm_compute_macro(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,

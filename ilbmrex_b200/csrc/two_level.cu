@@ -444,8 +444,14 @@ int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_lev
     return ILBM_ERR_ARG;
   }
   const double t_old = time, t_new = time + dt, dtf = 0.5 * dt;
-  // the first substep's body forcing needs only the fine state at t: it
-  // starts before the coarse step and overlaps it
+  // Schedule.  The first substep reads the coarse data at t_old only, so the
+  // coarse step need not precede it; the second substep's ghosts need the
+  // coarse step's result.  With a body, each substep's forcing chain runs on
+  // the side stream beside work of the main stream: the first substep's
+  // beside the first half of the coarse step and the substep's cells outside
+  // the body's band, the second substep's (which needs the first substep's
+  // band) beside the second half of the coarse step and the second
+  // substep's outer cells.
   ilbm_box b0 = *fine;
   b0.macro_in = first ? fine->macro_in : nullptr;
   b0.macro_out = nullptr;
@@ -460,8 +466,8 @@ int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_lev
     mlo[d] = fine->lo[d] / 2 - 2;
     mhi[d] = fine->hi[d] / 2 + 2;
   }
-  if ((rc = level_step_impl(ctx, coarse, 1, pc, first ? nullptr : mlo, first ? nullptr : mhi)))
-    return rc;
+  const int *cmlo = first ? nullptr : mlo, *cmhi = first ? nullptr : mhi;
+  if ((rc = level_step_impl(ctx, coarse, 1, pc, cmlo, cmhi, ib ? 1 : 0))) return rc;
   CFArgs g;
   std::memset(&g, 0, sizeof(g));
   for (int d = 0; d < 3; ++d) {
@@ -479,6 +485,7 @@ int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_lev
   g.cold = coarse->macro_in;
   g.cnew = coarse->macro_out;
   g.f16_scale = (float)f16_scale_of(pf);
+  AdvanceSplit sp1;
   for (int sub = 0; sub < 2; ++sub) {
     // stored fine macro fields only for a first step after initialisation;
     // afterwards rho, u are recovered from f and F^{n-1}
@@ -509,9 +516,19 @@ int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_lev
     } else if (sub == 0) {
       if ((rc = advance_end(ctx, &b, &sp0))) return rc;
     } else {
-      AdvanceSplit sp1;
-      if ((rc = advance_begin(ctx, &b, pf, ib, dtf, t, &sp1))) return rc;
       if ((rc = advance_end(ctx, &b, &sp1))) return rc;
+    }
+    if (ib && sub == 0) {
+      // the second substep's forcing (after the first substep's band), then
+      // the rest of the coarse step with its stored macro fields, which the
+      // second substep's ghost fill reads
+      ilbm_box b1 = *fine;
+      b1.macro_in = nullptr;
+      b1.macro_out = nullptr;
+      std::swap(b1.f_in, b1.f_out);
+      std::swap(b1.force, b1.force_prev);
+      if ((rc = advance_begin(ctx, &b1, pf, ib, dtf, t_old + dtf, &sp1))) return rc;
+      if ((rc = level_step_impl(ctx, coarse, 1, pc, cmlo, cmhi, 2))) return rc;
     }
   }
   // the fine state is back in fine->f_in after two substeps, the force of

@@ -93,6 +93,32 @@ def test_checkpoint_restart(which, storage, tmp_path):
     b.close()
 
 
+def test_checkpoint_restart_grid_cg(tmp_path):
+    """A body solved every step by the grid-wide CG (more than 1024 markers)
+    restarts with its CG start vectors (the last solution and the one before
+    it, for the extrapolated start) and continues the saved run."""
+    c, ib, init = cases.sphere(64, 48, 48, D=24.0, center=(24.3, 23.8, 24.1), U=0.04, Re=40.0)
+    a = LevelSolver(c, "f64", ib=ib)
+    a.set_ivc_solver(capi.IVC_CG)
+    a.set_macro(*init())
+    assert a.num_markers() > 1024
+    a.step(6, record_force=True)
+    path = tmp_path / "chk_cg"
+    a.save_checkpoint(path)
+    b = LevelSolver(c, "f64", ib=cases.sphere(64, 48, 48, D=24.0, center=(24.3, 23.8, 24.1), U=0.04,
+                                              Re=40.0)[1])
+    b.set_ivc_solver(capi.IVC_CG)
+    b.load_checkpoint(path)
+    assert b.istep == 6
+    a.step(5, record_force=True)
+    b.step(5, record_force=True)
+    assert a.cg_iterations() > 0 and b.cg_iterations() > 0
+    assert rel_l2(b.get_f(), a.get_f()) <= 1e-12
+    np.testing.assert_allclose(b.rec[3:5], a.rec[3:5], rtol=1e-9, atol=1e-12)
+    a.close()
+    b.close()
+
+
 def test_checkpoint_before_the_first_step(tmp_path):
     """A level saved right after initialisation carries its stored macro
     fields (the first step reads them): the restart takes the same first step."""
