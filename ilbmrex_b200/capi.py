@@ -34,7 +34,8 @@ EXPORTS = [
     "ilbm_ib_update_forcing", "ilbm_advance_level", "ilbm_ib_last_marker_force_sum",
     "ilbm_ib_solver_stats", "ilbm_ib_set_ivc_solver",
     "ilbm_ib_markers",
-    "ilbm_force_integrals", "ilbm_force_integrals_noalloc", "ilbm_momentum_exchange",
+    "ilbm_force_integrals", "ilbm_force_integrals_noalloc", "ilbm_force_record_async",
+    "ilbm_momentum_exchange",
     "ilbm_batch_create", "ilbm_batch_destroy", "ilbm_batch_add", "ilbm_batch_remove",
     "ilbm_batch_step", "ilbm_batch_case_state", "ilbm_batch_records", "ilbm_batch_set_tiles",
     "ilbm_batch_tune", "ilbm_batch_size", "ilbm_batch_progress",
@@ -154,6 +155,7 @@ def lib():
         "ilbm_ib_markers": (I, [P, dp, dp, dp]),
         "ilbm_force_integrals": (I, [P, C.POINTER(Box_t), P, ip3, ip3, dp]),
         "ilbm_force_integrals_noalloc": (I, [P, C.POINTER(Box_t), P, ip3, ip3, dp]),
+        "ilbm_force_record_async": (I, [P, C.POINTER(Box_t), P, P, ip3, ip3, P]),
         "ilbm_batch_create": (I, [P, I, C.POINTER(P)]),
         "ilbm_batch_destroy": (I, [P]),
         "ilbm_batch_add": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P, D, D, I,

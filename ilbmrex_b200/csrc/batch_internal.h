@@ -35,6 +35,13 @@ int batch_band_macro_launch(ilbm_ctx *ctx, const StepArgs *d_args, const BandDes
 // resident blocks of w threads per SM of k_step_batch
 int batch_step_occupancy(const ilbm_ctx *ctx, int w, int *per_sm);
 
+// ---- forces.cu ------------------------------------------------------------
+// the Eulerian force sum of ilbm_force_integrals enqueued on ctx->stream; the
+// three sums land at *d_sum (context scratch, with 8 spare doubles after
+// them) when the stream gets there
+int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *box, const void *force, const int lo[3],
+                      const int hi[3], double **d_sum);
+
 // ---- ib.cu ----------------------------------------------------------------
 // ilbm_advance_level in two halves: begin starts the body's update_forcing
 // (on the side stream, after the work queued so far on the main stream, when

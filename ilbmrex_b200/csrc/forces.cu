@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 
+#include "batch_internal.h"
 #include "ilbm_common.cuh"
 
 using namespace ilbm;
@@ -171,6 +172,22 @@ int ilbm_force_integrals(ilbm_ctx *ctx, const ilbm_box *box, const void *force, 
     set_error("ilbm_force_integrals: null argument");
     return ILBM_ERR_ARG;
   }
+  double *d_sum = nullptr;
+  int rc = force_sum_enqueue(ctx, box, force, lo, hi, &d_sum);
+  if (rc) return rc;
+  cudaMemcpyAsync(ctx->host_pinned, d_sum, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals");
+  for (int c = 0; c < 3; ++c) out_sum[c] = ctx->host_pinned[c];
+  return ILBM_OK;
+}
+
+}  // extern "C"
+
+namespace ilbm {
+
+int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *box, const void *force, const int lo[3],
+                      const int hi[3], double **d_sum) {
   RegionArgs a;
   std::memset(&a, 0, sizeof(a));
   a.dim = ctx->dim;
@@ -190,28 +207,31 @@ int ilbm_force_integrals(ilbm_ctx *ctx, const ilbm_box *box, const void *force, 
   a.ms0 = box->mstride[0];
   a.ms1 = box->mstride[1];
   a.ms2 = box->mstride[2];
-  double *scr = static_cast<double *>(ilbm_ctx_scratch(ctx, (kRedBlocks * 3 + 8) * sizeof(double)));
+  double *scr = static_cast<double *>(ilbm_ctx_scratch(ctx, (kRedBlocks * 3 + 16) * sizeof(double)));
   if (!scr) {
     set_error("ilbm_force_integrals: scratch allocation failed");
     return ILBM_ERR_NOMEM;
   }
+  *d_sum = scr + kRedBlocks * 3;
   if ((int64_t)a.n[0] * a.n[1] * a.n[2] == 0) {
-    out_sum[0] = out_sum[1] = out_sum[2] = 0.0;
+    cudaError_t e = cudaMemsetAsync(*d_sum, 0, 3 * sizeof(double), ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals");
     return ILBM_OK;
   }
   if (ctx->storage == ILBM_STORAGE_F64)
     k_force_partial<double><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(a, static_cast<const double *>(force), scr);
   else
     k_force_partial<float><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(a, static_cast<const float *>(force), scr);
-  k_final_sum<<<1, 32, 0, ctx->stream>>>(scr, kRedBlocks, scr + kRedBlocks * 3);
+  k_final_sum<<<1, 32, 0, ctx->stream>>>(scr, kRedBlocks, *d_sum);
   ctx->launches += 2;
-  cudaMemcpyAsync(ctx->host_pinned, scr + kRedBlocks * 3, 3 * sizeof(double),
-                  cudaMemcpyDeviceToHost, ctx->stream);
-  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals");
-  for (int c = 0; c < 3; ++c) out_sum[c] = ctx->host_pinned[c];
   return ILBM_OK;
 }
+
+}  // namespace ilbm
+
+extern "C" {
 
 int ilbm_momentum_exchange(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
                            const void *f, double x0, double y0, double z0, double R,

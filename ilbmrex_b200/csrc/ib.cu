@@ -1729,6 +1729,19 @@ int ilbm_ib_force_region(const ilbm_ib *ib, int lo[3], int hi[3]) {
 
 }  // extern "C"
 
+// one force record: Eulerian sum (3), last marker force sum (3), the body's
+// two status words as doubles
+__global__ void k_record_pack(const double *sum3, const double *fsum, const int *status,
+                              double *rec) {
+  if (threadIdx.x != 0) return;
+  for (int c = 0; c < 3; ++c) {
+    rec[c] = sum3[c];
+    rec[3 + c] = fsum[c];
+  }
+  rec[6] = (double)status[0];
+  rec[7] = (double)status[1];
+}
+
 // Stopping tolerance of the IVC conjugate gradient (relative residual).  FP64
 // populations: 1e-14, so results meet the reference's dense LU at 1e-12.
 // FP32 populations: 1e-7, the relative precision of the right-hand side,
@@ -2026,6 +2039,27 @@ int ilbm_ib_last_marker_force_sum(ilbm_ib *ib, double out[3]) {
     set_error("IVC operator has a non-positive pivot (not positive definite); its inverse is invalid");
     return ILBM_ERR_SOLVER;
   }
+  return ILBM_OK;
+}
+
+int ilbm_force_record_async(ilbm_ctx *ctx, const ilbm_box *box, const void *force, ilbm_ib *ib,
+                            const int lo[3], const int hi[3], double *out) {
+  if (!ctx || !box || !force || !ib || !out) {
+    set_error("ilbm_force_record_async: null argument");
+    return ILBM_ERR_ARG;
+  }
+  if (ib->ctx != ctx) {
+    set_error("ilbm_force_record_async: the IB object belongs to another context");
+    return ILBM_ERR_ARG;
+  }
+  double *d_sum = nullptr;
+  int rc = force_sum_enqueue(ctx, box, force, lo, hi, &d_sum);
+  if (rc) return rc;
+  double *d_rec = d_sum + 8;  // spare scratch after the sums
+  k_record_pack<<<1, 32, 0, ctx->stream>>>(d_sum, ib->d_fsum, ib->d_status, d_rec);
+  ctx->launches++;
+  cudaError_t e = cudaMemcpyAsync(out, d_rec, 8 * sizeof(double), cudaMemcpyDefault, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_record_async");
   return ILBM_OK;
 }
 

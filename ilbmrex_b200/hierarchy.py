@@ -109,6 +109,10 @@ class TwoLevelSolver:
         self.have_prev_body = False
         self.prev_body = np.zeros(3)
         self.rec = np.zeros(18)
+        # pipelined force records: two pinned host slots, the pending one
+        self._rec_bufs = None
+        self._rec_slot = 0
+        self._pending = None
 
     # ---- initialisation (MakeNewLevelFromScratch per level + InitData) ----
     def set_macro(self, init_coarse, init_fine):
@@ -131,7 +135,11 @@ class TwoLevelSolver:
         self.first_step = True
 
     # ---- one coarse step ---------------------------------------------------
-    def advance(self, record_force: bool = False):
+    def advance(self, record_force: bool = False, pipelined: bool = False):
+        """One coarse step.  record_force: the force record (self.rec) of the
+        step; pipelined: its sums are copied to the host without waiting, and
+        the record of the previous step is taken instead (flush_records takes
+        the last one), so the next step is queued before the host waits."""
         Cl, Fl = self.C, self.F
         bc = Cl.box(Cl.f, Cl.f_next, m_in=Cl.m, m_out=Cl.m_next)
         bf = Fl.box(Fl.f, Fl.f_next, m_in=Fl.m if self.first_step else None,
@@ -147,11 +155,53 @@ class TwoLevelSolver:
         self.time += self.tl.coarse.dt
         self.istep += 1
         if record_force and self.ib is not None:
-            self.compute_ib_force()
+            if pipelined:
+                self._record_async()
+            else:
+                self.flush_records()
+                self.compute_ib_force()
 
-    def step(self, n: int = 1, record_force: bool = False):
+    def step(self, n: int = 1, record_force: bool = False, pipelined: bool = False):
         for _ in range(n):
-            self.advance(record_force=record_force)
+            self.advance(record_force=record_force, pipelined=pipelined)
+        self.flush_records()
+
+    def _record_async(self):
+        if self._rec_bufs is None:
+            self._rec_bufs = [torch.empty(8, dtype=torch.float64, pin_memory=True) for _ in range(2)]
+            self._stream = torch.cuda.ExternalStream(self.L.ilbm_stream(self.ctx.h), device=self.dev)
+        lo, hi = self.force_region
+        b = self.F.box(self.F.f, None)
+        buf = self._rec_bufs[self._rec_slot]
+        self._rec_slot ^= 1
+        capi.check(self.L.ilbm_force_record_async(self.ctx.h, C.byref(b), self.F.fb.data_ptr(), self.ib,
+                                                  capi.ivec3(lo), capi.ivec3(hi), buf.data_ptr()),
+                   "force_record_async")
+        ev = torch.cuda.Event()
+        ev.record(self._stream)
+        prev, self._pending = self._pending, (buf, ev)
+        if prev is not None:
+            self._take_record(*prev)
+
+    def flush_records(self):
+        """Takes the force record still in flight (pipelined steps)."""
+        if self._pending is not None:
+            prev, self._pending = self._pending, None
+            self._take_record(*prev)
+
+    _STATUS = ((0, 1, "IB stencil left the support band (marker outside its envelope)"),
+               (0, 2, "IVC operator exceeded its nonzero capacity"),
+               (0, 4, "IVC conjugate gradient did not converge"),
+               (1, 8, "IVC operator has a non-positive pivot (not positive definite)"))
+
+    def _take_record(self, buf, ev):
+        ev.synchronize()
+        r = buf.numpy().copy()
+        words = (int(r[6]), int(r[7]))
+        for w, bit, msg in self._STATUS:
+            if words[w] & bit:
+                raise capi.IlbmError(f"force_record_async: {msg}")
+        self.rec = LevelSolver.force_record(self, r[0:3], r[3:6])
 
     def compute_ib_force(self):
         """ComputeIBForce on the finest level (AmrCoreLBM.cpp:456-631) with

@@ -282,6 +282,22 @@ int ilbm_force_integrals(ilbm_ctx *ctx, const ilbm_box *box, const void *force,
  *     region return identical bits. */
 int ilbm_force_integrals_noalloc(ilbm_ctx *ctx, const ilbm_box *box, const void *force,
                                  const int lo[3], const int hi[3], double out_sum[3]);
+/* The force record of a step, without synchronising (no counterpart in the
+ * reference, whose ComputeIBForce returns the sums at once,
+ * Source/Core/AmrCoreLBM.cpp:456-631): enqueues on the context's stream the
+ * Eulerian sum of ilbm_force_integrals over [lo, hi] and copies it, the
+ * body's last marker force sum (ilbm_ib_last_marker_force_sum) and the body's
+ * two status words into out[8] = {Eulerian sum (3), marker sum (3),
+ * status word 0, status word 1}.  out should be pinned host memory (or device
+ * memory); the values are there once the stream passes this point (an event
+ * recorded after the call, or ilbm_sync), so a host can issue the next step
+ * before it reads this one's record.  Status bits as reported by
+ * ilbm_ib_last_marker_force_sum: word 0 bit 0 a stencil left the band, bit 1
+ * the IVC operator's nonzero capacity, bit 2 CG not converged; word 1 bit 3 a
+ * non-positive pivot of the stored inverse.  The next call on the context
+ * reuses the record's device slot after this copy, in stream order. */
+int ilbm_force_record_async(ilbm_ctx *ctx, const ilbm_box *box, const void *force, ilbm_ib *ib,
+                            const int lo[3], const int hi[3], double *out);
 /* link-wise momentum exchange on f (IBForceEval); out = body force (3) */
 int ilbm_momentum_exchange(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
                            const void *f, double x0, double y0, double z0, double R,

@@ -117,3 +117,27 @@ def test_sphere_body_on_fine_level_3d():
         assert rel_l2(gpu.get_macro(lev), cpu.get_macro(lev)) <= 1e-12
     np.testing.assert_allclose(gpu.rec[3:5], cpu.force_record()[3:5], rtol=1e-9, atol=1e-12)
     gpu.close()
+
+
+def test_pipelined_force_records():
+    """ilbm_force_record_async: with pipelined records each step's record is
+    taken once the next step is queued (one step behind during the loop,
+    flush_records takes the last) and equals the synchronous record."""
+    tl, ib, ic, if_ = cases.cylinder_two_level(nx=96, ny=64, D=12.0, center=(32.3, 31.7), U=0.05,
+                                               Re=40.0, upstream=1.0, downstream=2.0, cross=1.2)
+    a = TwoLevelSolver(tl, "f64", ib=ib)
+    b = TwoLevelSolver(tl, "f64", ib=ib)
+    for s in (a, b):
+        s.set_macro(ic(), if_())
+    recs = []
+    for k in range(5):
+        a.advance(record_force=True)
+        recs.append(a.rec.copy())
+        b.advance(record_force=True, pipelined=True)
+        if k >= 1:
+            np.testing.assert_allclose(b.rec, recs[k - 1], rtol=1e-9, atol=1e-14)
+    b.flush_records()
+    np.testing.assert_allclose(b.rec, recs[-1], rtol=1e-9, atol=1e-14)
+    assert abs(recs[-1][3]) > 0.0
+    a.close()
+    b.close()
