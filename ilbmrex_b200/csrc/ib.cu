@@ -705,7 +705,11 @@ __device__ __forceinline__ void block_partials(const double *v, int nval, double
 // block is still reducing.  Start: x0 = 0 (warm 0), the previous solution
 // (warm 1), or its linear extrapolation 2 x_n - x_{n-1} from the last two
 // solutions (warm 2; Xh keeps the history).
-__global__ void __launch_bounds__(256) k_ivc_cg_grid(IBArgs a, const double *xyz, const double *tgt,
+// (64 registers: the two resident blocks per SM leave half the register file
+// to the level step that runs beside the solve; 96 registers left it one
+// block per SM, 0.782-0.788 against 0.762-0.771 ms per coarse step of the
+// two-level sphere)
+__global__ void __launch_bounds__(256, 4) k_ivc_cg_grid(IBArgs a, const double *xyz, const double *tgt,
                                                      const double *uvw, const int *rowptr,
                                                      const int *col, const double *val,
                                                      const double *diag, double *X_, double *Xh,
