@@ -203,9 +203,10 @@ def run_reference(args):
     if rank != 0:
         return
     steps = max(1, min(args.steps, 3))
-    mlups, dt, threads, kind, sample = cpu_reference_steps(steps, 1)
+    warm = max(3, min(args.warmup, 5))  # at least three, at most five host steps
+    mlups, dt, threads, kind, sample = cpu_reference_steps(steps, warm)
     line = {"metric": METRIC, "value": round(mlups, 3), "unit": UNIT, "n_gpus": args.gpus,
-            "steps": steps, "warmup": 1, "ms_per_step": round(dt * 1e3, 3),
+            "steps": steps, "warmup": warm, "ms_per_step": round(dt * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
             "config": workload_config(args),
@@ -597,7 +598,7 @@ def run_b200(args):
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            mlups, dt, threads, kind, sample = cpu_reference_steps(2, 1)
+            mlups, dt, threads, kind, sample = cpu_reference_steps(2, 3)
             cpu_base = {"value": round(mlups, 3), "unit": UNIT, "cores": threads, "kind": kind,
                         "sample": sample}
         except Exception as e:  # the checker is optional at run time
