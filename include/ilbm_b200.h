@@ -143,6 +143,9 @@ typedef struct {
 } ilbm_level_params;
 
 /* ---- context ------------------------------------------------------------ */
+/* The context owns a stream (or uses cuda_stream), a high-priority side
+ * stream for the immersed-boundary chain, and a device memory pool from which
+ * IB objects and batches allocate in stream order. */
 int ilbm_create(const ilbm_lattice *lat, int storage, int device, void *cuda_stream,
                 ilbm_ctx **out);
 int ilbm_destroy(ilbm_ctx *ctx);
@@ -212,6 +215,10 @@ typedef struct {
 
 int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom *g,
                    ilbm_ib **out);
+/* Frees the body's device arrays in stream order on its context's stream
+ * (after the work queued there and on the side stream); it does not
+ * synchronise the device.  Destroy IB objects and batches before their
+ * context. */
 int ilbm_ib_destroy(ilbm_ib *ib);
 int ilbm_ib_num_markers(const ilbm_ib *ib, int64_t *n);
 /* Lower/upper corner (inclusive) of the cells whose force the IB may write. */
