@@ -4,6 +4,7 @@
 // (Source/IBM/IBForceEval.cpp:28-191).  Both are two-stage reductions with a
 // fixed summation order, so repeated calls return identical bits.
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 
@@ -324,15 +325,22 @@ constexpr int kNoAllocMaxDevices = 64;
 
 __device__ __align__(256) double g_noalloc_scratch[kNoAllocChunks * 3 + 3];
 
-// device address of g_noalloc_scratch, looked up once per device
-double *g_noalloc_ptr[kNoAllocMaxDevices] = {};
+// Device address of g_noalloc_scratch, looked up once per device.  Two host
+// threads that make their first call on a device at the same time may both
+// look it up; they store the same address, and the atomics make the store
+// and the later loads well defined.  The address belongs to the device's
+// primary context: after cudaDeviceReset every context of this library on
+// that device is gone anyway, and the cache must not be used again (the
+// header says so).
+std::atomic<double *> g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
 int noalloc_scratch(int device, double **out) {
   if (device < 0 || device >= kNoAllocMaxDevices) {
     set_error("ilbm_force_integrals_noalloc: device ordinal out of range");
     return ILBM_ERR_ARG;
   }
-  if (!g_noalloc_ptr[device]) {
+  double *cached = g_noalloc_ptr[device].load(std::memory_order_acquire);
+  if (!cached) {
     int prev = 0;
     cudaError_t e = cudaGetDevice(&prev);
     if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals_noalloc: cudaGetDevice");
@@ -344,9 +352,10 @@ int noalloc_scratch(int device, double **out) {
     if (e != cudaSuccess || !ptr)
       return cuda_fail(e != cudaSuccess ? e : cudaErrorInvalidSymbol,
                        "ilbm_force_integrals_noalloc: cudaGetSymbolAddress");
-    g_noalloc_ptr[device] = static_cast<double *>(ptr);
+    cached = static_cast<double *>(ptr);
+    g_noalloc_ptr[device].store(cached, std::memory_order_release);
   }
-  *out = g_noalloc_ptr[device];
+  *out = cached;
   return ILBM_OK;
 }
 
@@ -405,10 +414,16 @@ int ilbm_force_integrals_noalloc(ilbm_ctx *ctx, const ilbm_box *box, const void 
     k_force_partial<float><<<nchunks, kRedThreads, 0, ctx->stream>>>(a, static_cast<const float *>(force), scr);
   k_final_sum<<<1, 32, 0, ctx->stream>>>(scr, nchunks, scr + kNoAllocChunks * 3);
   ctx->launches += 2;
+  // a launch that failed without poisoning the context (bad configuration,
+  // missing kernel image) is not reported by the synchronisation below; the
+  // result slot would then still hold the previous call's sum
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals_noalloc: launch");
   double res[3] = {0.0, 0.0, 0.0};
-  cudaMemcpyAsync(res, scr + kNoAllocChunks * 3, 3 * sizeof(double), cudaMemcpyDeviceToHost,
-                  ctx->stream);
-  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  e = cudaMemcpyAsync(res, scr + kNoAllocChunks * 3, 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                      ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals_noalloc: copy");
+  e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals_noalloc");
   for (int c = 0; c < 3; ++c) out_sum[c] = res[c];
   return ILBM_OK;

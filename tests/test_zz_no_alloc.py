@@ -82,3 +82,64 @@ def test_noalloc_size_limit():
     assert rc == capi.ILBM_ERR_RANGE
     assert b"8388608" in L.ilbm_last_error()
     ctx.close()
+
+
+def _offset_box(nx, ny, lo=(5, 7), ng=2, seed=20261203):
+    """A 2D box whose valid region starts at `lo` (not the origin) inside a
+    force array grown by `ng` ghost cells; the ghosts hold large values that a
+    wrong offset would pick up."""
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    gx, gy = nx + 2 * ng, ny + 2 * ng
+    F = torch.full((3, gy, gx), 1.0e6, device=dev, dtype=torch.float64)
+    F[:, ng:ng + ny, ng:ng + nx] = torch.rand((3, ny, nx), generator=g, device=dev,
+                                              dtype=torch.float64) - 0.5
+    torch.cuda.synchronize()
+    b = capi.Box_t()
+    b.lo[0], b.lo[1], b.lo[2] = lo[0], lo[1], 0
+    b.hi[0], b.hi[1], b.hi[2] = lo[0] + nx - 1, lo[1] + ny - 1, 0
+    b.ngrow_f, b.ngrow_m = ng, ng
+    b.mstride[0], b.mstride[1], b.mstride[2] = gx, gx * gy, gx * gy
+    return F, b
+
+
+def test_noalloc_offset_box_ragged_chunks():
+    """A region of 241 x 32 = 7,712 cells (two chunks, the last one ragged) on
+    a box whose lo is (5, 7) with two ghost layers: equal to
+    ilbm_force_integrals and to a float64 sum of the same cells."""
+    ctx = Context(cases.D2Q9, "f64")
+    L = ctx.L
+    nx, ny, lo = 300, 50, (5, 7)
+    F, b = _offset_box(nx, ny, lo)
+    rlo, rhi = (lo[0] + 10, lo[1] + 9, 0), (lo[0] + 250, lo[1] + 40, 0)
+    rc, ref = _sum(L, "ilbm_force_integrals", ctx.h, b, F.data_ptr(), rlo, rhi)
+    assert rc == 0
+    ng = 2
+    i0, i1 = rlo[0] - lo[0] + ng, rhi[0] - lo[0] + ng + 1
+    j0, j1 = rlo[1] - lo[1] + ng, rhi[1] - lo[1] + ng + 1
+    host = F[:, j0:j1, i0:i1].sum(dim=(1, 2)).cpu().numpy()
+    for _ in range(2):
+        rc, s = _sum(L, "ilbm_force_integrals_noalloc", ctx.h, b, F.data_ptr(), rlo, rhi)
+        assert rc == 0, L.ilbm_last_error()
+        np.testing.assert_allclose(s, ref, rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(s[:2], host[:2], rtol=1e-12, atol=1e-12)
+    ctx.close()
+
+
+def test_noalloc_empty_region():
+    """A region that clips to nothing returns ILBM_OK and zeros, like
+    ilbm_force_integrals, after a call that left a nonzero sum behind."""
+    ctx = Context(cases.D2Q9, "f64")
+    L = ctx.L
+    F, b = _offset_box(64, 40)
+    rc, s = _sum(L, "ilbm_force_integrals_noalloc", ctx.h, b, F.data_ptr(), (5, 7, 0), (68, 46, 0))
+    assert rc == 0 and np.abs(s).max() > 0.0
+    for rlo, rhi in (((200, 7, 0), (300, 46, 0)), ((30, 20, 0), (29, 30, 0))):
+        rc, ref = _sum(L, "ilbm_force_integrals", ctx.h, b, F.data_ptr(), rlo, rhi)
+        assert rc == 0
+        rc, s = _sum(L, "ilbm_force_integrals_noalloc", ctx.h, b, F.data_ptr(), rlo, rhi)
+        assert rc == 0, L.ilbm_last_error()
+        np.testing.assert_array_equal(s, np.zeros(3))
+        np.testing.assert_array_equal(ref, np.zeros(3))
+    ctx.close()
