@@ -149,6 +149,7 @@ def _load(backend: str, dim: int, fp32: bool = False):
                 ("orc_set_airfoil", None, [C.POINTER(C.c_double)]),
                 ("orc_delta_function", C.c_double, [C.c_double] * 3 + [C.c_int]),
                 ("orc_overlap", C.c_double, [C.c_double] * 3 + [C.c_int, C.c_double, C.c_int, C.c_int]),
+                ("orc_set_spread_order", None, [C.c_int]),
             ]:
                 fn = getattr(lib, name)
                 fn.restype, fn.argtypes = res, args
@@ -170,6 +171,15 @@ def _load(backend: str, dim: int, fp32: bool = False):
                 fn.restype, fn.argtypes = res, args
         _LIBS[key] = lib
     return _LIBS[key]
+
+
+def set_spread_order(reverse: bool) -> None:
+    """Marker order of the oracle's force spreading for every level of the
+    process: False = marker order (the reference's), True = reversed.  Used
+    to measure how much the reference's result depends on the summation
+    order of spreading alone."""
+    for dim in (2, 3):
+        _load("oracle", dim).orc_set_spread_order(1 if reverse else 0)
 
 
 def available(backend: str = "oracle", dim: int = 2, fp32: bool = False) -> bool:

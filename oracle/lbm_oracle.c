@@ -897,6 +897,14 @@ static void force_ivc(orc_level *L, double dt, double t) {
   free(xg); free(yg); free(zg); free(bx); free(by); free(bz); free(sx); free(sy); free(sz);
 }
 
+/* Order in which markers are spread (test aid, process-wide): 0 = marker
+ * order, as the reference's loop over particles; 1 = reversed.  The FP64
+ * atomic spreading of the device path sums in an unspecified order, so its
+ * parity tests measure how far the reference's own result moves when only
+ * this order changes and allow the device that much. */
+static int g_spread_reverse = 0;
+void orc_set_spread_order(int reverse) { g_spread_reverse = reverse ? 1 : 0; }
+
 /* force_spreading_cic + force_spreading, IBMarkerDF.cpp:1331-1512 (E: grown array) */
 static void spread(orc_level *L, double *E, clipbox cb) {
   orc_ib *B = &L->ib;
@@ -906,7 +914,8 @@ static void spread(orc_level *L, double *E, clipbox cb) {
   const long s = L->gcells;
   const double d = (L->dim == 3) ? dx[0] * dx[1] * dx[2] : dx[0] * dx[1];
   const double z0 = (L->dim == 3) ? B->p.z0 : 0.0;
-  for (int m = 0; m < B->n; ++m) {
+  for (int mm = 0; mm < B->n; ++mm) {
+    const int m = g_spread_reverse ? B->n - 1 - mm : mm;
     const double fx = B->fx[m] * B->dv, fy = B->fy[m] * B->dv, fz = B->fz[m] * B->dv;
     const double px = B->x[m], py = B->y[m], pz = (L->dim == 3) ? B->z[m] : 0.0;
     const double rx = px - B->p.x0, ry = py - B->p.y0, rz = (L->dim == 3) ? pz - z0 : 0.0;

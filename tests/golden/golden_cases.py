@@ -58,6 +58,49 @@ def _airfoil():
     return case, cases.uniform_init(case, 1.0, (0.05, 0.0, 0.0)), ib
 
 
+def _cylinder_delta3():
+    # 3-point kernel (IBMarkerDF.cpp:86-96) with IVC coupling
+    c, ib, init = cases.cylinder(nx=96, ny=64, D=16, center=(32.3, 31.7), U=0.05, Re=40)
+    ib.delta_type = 3
+    return c, init, ib
+
+
+def _cylinder_explicit_diag():
+    # explicit_diag coupling (IBMarkerDF.cpp:745-865): (U_d - U) / (dt * M_kk)
+    c, ib, init = cases.cylinder(nx=96, ny=64, D=16, center=(32.3, 31.7), U=0.05, Re=40,
+                                 coupling=2)
+    ib.loop_ns = 2
+    return c, init, ib
+
+
+def _cylinder_ivc_renorm():
+    # renormalize_delta with IVC: spreading renormalised, interpolation not
+    # (IBMarkerDF.cpp:541-542, 727-728, 1484).  No stencil is clipped in these
+    # renorm cases, so each weight is divided by a partition of one up to
+    # rounding: the fixtures pin that arithmetic bit for bit.
+    c, ib, init = cases.cylinder(nx=96, ny=64, D=16, center=(32.3, 31.7), U=0.05, Re=40)
+    ib.renormalize_delta = 1
+    return c, init, ib
+
+
+def _cavity_lid_renorm():
+    # renormalize_delta with explicit coupling: interpolation and spreading
+    # renormalised, 3-point kernel, lid markers along the cavity's top
+    c, ib, init = cases.cavity_lid(32)
+    ib.renormalize_delta = 1
+    ib.delta_type = 3
+    return c, init, ib
+
+
+def _sphere_delta3_diag():
+    # 3D: 3-point kernel with explicit_diag coupling, two MDF iterations
+    c, ib, init = cases.sphere(nx=40, ny=24, nz=24, D=8, center=(12.2, 11.7, 12.4), U=0.04, Re=20,
+                               coupling=2)
+    ib.delta_type = 3
+    ib.loop_ns = 2
+    return c, init, ib
+
+
 GOLDEN_CASES = {
     "tgv32_d2q9": (_tgv, 20),
     "couette24_extdir_foextrap": (_couette, 20),
@@ -68,4 +111,9 @@ GOLDEN_CASES = {
     "sphere40x24x24_d3q19_ivc": (_sphere_ivc, 4),
     "cavity32_lid_box": (_cavity_lid, 8),
     "airfoil96x64_pitching_ivc": (_airfoil, 6),
+    "cylinder96x64_delta3_ivc": (_cylinder_delta3, 8),
+    "cylinder96x64_explicit_diag_mdf2": (_cylinder_explicit_diag, 8),
+    "cylinder96x64_ivc_renorm": (_cylinder_ivc_renorm, 8),
+    "cavity32_lid_renorm_delta3": (_cavity_lid_renorm, 8),
+    "sphere40x24x24_delta3_diag": (_sphere_delta3_diag, 4),
 }

@@ -1,7 +1,8 @@
 """Generates the golden fixtures in this directory from the reference's own
 code (oracle/_ref: Source/LBM, Source/BC, Source/IBM compiled in place against
-oracle/amrex_shim).  Run from the repository root, where /root/reference is
-mounted:  python tests/golden/make_golden.py
+oracle/amrex_shim by ``make -C oracle ref REF=<reference tree>``).  Run from
+the repository root:  python tests/golden/make_golden.py [name ...]
+(no names: every case of golden_cases.GOLDEN_CASES).
 
 Each fixture stores the step count and the reference's macro fields, force
 field, per-direction population sums, the populations themselves for the
@@ -24,7 +25,9 @@ from tests.golden.golden_cases import GOLDEN_CASES  # noqa: E402
 
 def main():
     out = Path(__file__).resolve().parent
-    for name, (builder, steps) in GOLDEN_CASES.items():
+    names = sys.argv[1:] or list(GOLDEN_CASES)
+    for name in names:
+        builder, steps = GOLDEN_CASES[name]
         case, init, ib = builder()
         L = CpuLevel(case, "ref")
         L.set_macro(*init())

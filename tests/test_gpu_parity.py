@@ -59,19 +59,54 @@ def test_fp64_bit_exact(name):
     gpu.close()
 
 
+def _order_sensitivity(name):
+    """How far the oracle's own result moves when only the marker order of
+    its force spreading is reversed: relative L2 of f, rho, u and the force
+    field, and the largest relative change of Cd / Cl."""
+    from oracle import checker
+    builder, steps = GOLDEN_CASES[name]
+    out = []
+    for rev in (False, True):
+        checker.set_spread_order(rev)
+        try:
+            case, init, ib = builder()
+            c = CpuLevel(case, "oracle")
+            c.set_macro(*init())
+            c.init_equilibrium()
+            c.ib_create(ib)
+            c.step(steps)
+            out.append((c.get_f(), c.get_macro(), c.get_force(), c.force_record()))
+        finally:
+            checker.set_spread_order(False)
+    (fa, ma, Fa, ra), (fb, mb, Fb, rb) = out
+    return {"f": rel_l2(fb, fa), "rho": rel_l2(mb[0], ma[0]), "u": rel_l2(mb[1:3], ma[1:3]),
+            "force": rel_l2(Fb, Fa), "cdcl": float(np.max(np.abs(rb[3:5] - ra[3:5]) / np.abs(ra[3])))}
+
+
 @pytest.mark.parametrize("name", WITH_IB)
 def test_fp64_ib_parity(name):
+    """relative L2 <= 1e-12 (force field 1e-11, Cd / Cl 1e-9), or four times
+    the change the oracle itself shows when only its spreading order is
+    reversed, where that is larger: the explicit_diag coupling divides the
+    velocity defect by the small diagonal of the interpolation-spreading
+    operator, which amplifies summation-order rounding (1e-10 relative for
+    the reference's own cylinder case), and the device spreads with FP64
+    atomics in an unspecified order."""
     cpu, gpu, ib = _pair(name)
+    sens = _order_sensitivity(name)
+    tol = lambda base, key: max(base, 4.0 * sens[key])
     assert gpu.num_markers() == cpu.num_markers()
-    assert rel_l2(gpu.get_f(), cpu.get_f()) <= 1e-12
+    assert rel_l2(gpu.get_f(), cpu.get_f()) <= tol(1e-12, "f")
     mg, mc = gpu.get_macro(), cpu.get_macro()
-    assert rel_l2(mg[0], mc[0]) <= 1e-12
-    assert rel_l2(mg[1:3], mc[1:3]) <= 1e-12
-    assert rel_l2(gpu.get_force(), cpu.get_force()) <= 1e-11
+    assert rel_l2(mg[0], mc[0]) <= tol(1e-12, "rho")
+    assert rel_l2(mg[1:3], mc[1:3]) <= tol(1e-12, "u")
+    assert rel_l2(gpu.get_force(), cpu.get_force()) <= tol(1e-11, "force")
     rg, rc = gpu.rec, cpu.force_record()
-    np.testing.assert_allclose(rg[3:5], rc[3:5], rtol=1e-9, atol=1e-12)
-    np.testing.assert_allclose(gpu.marker_force_sum(), cpu.marker_force_sum(), rtol=1e-9, atol=1e-14)
+    np.testing.assert_allclose(rg[3:5], rc[3:5], rtol=tol(1e-9, "cdcl"), atol=1e-12)
+    np.testing.assert_allclose(gpu.marker_force_sum(), cpu.marker_force_sum(), rtol=tol(1e-9, "cdcl"),
+                               atol=1e-14)
     gpu.close()
+
 
 
 def test_fp64_against_golden_fixture():
