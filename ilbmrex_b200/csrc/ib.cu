@@ -1671,17 +1671,12 @@ int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom
       return rc;
     }
     // grid-wide CG: as many co-resident blocks as the device holds, at most 2
-    // per SM (fastest beside the level step it overlaps; ILBM_CG_BLOCKS_PER_SM
-    // overrides it, up to the co-resident maximum)
+    // per SM (measured fastest beside the level step it overlaps)
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ivc_cg_grid, 256, 0);
     ib->cg_blocks = std::max(1, std::min(2, per_sm) * sms);
-    if (const char *e = std::getenv("ILBM_CG_BLOCKS_PER_SM")) {
-      const int b = std::atoi(e);
-      if (b >= 1) ib->cg_blocks = std::max(1, std::min(b, per_sm) * sms);
-    }
     if ((rc = dmalloc(ib, &ib->d_partial, 16 * (size_t)std::max(per_sm * sms, 16)))) {
       ilbm_ib_destroy(ib);
       return rc;

@@ -229,23 +229,25 @@ __device__ __forceinline__ void moments64(const double *f, double Fx, double Fy,
   w = X::div(X::add(m3, X::mul(0.5, Fz)), r);
 }
 
-// shifted form (g = f - w): drho = rho - 1
+// shifted form (g = f - w): drho = rho - 1.  Every operation is an explicit
+// round-to-nearest intrinsic, so the result is the same in every kernel that
+// inlines it (no context-dependent contraction into FMA).
 template <class L>
 __device__ __forceinline__ void moments32(const float *g, float Fx, float Fy, float Fz,
                                           float &drho, float &u, float &v, float &w) {
   float r = 0.f, m1 = 0.f, m2 = 0.f, m3 = 0.f;
 #pragma unroll
   for (int q = 0; q < L::Q; ++q) {
-    r += g[q];
-    if (L::cx(q)) m1 += float(L::cx(q)) * g[q];
-    if (L::cy(q)) m2 += float(L::cy(q)) * g[q];
-    if (L::cz(q)) m3 += float(L::cz(q)) * g[q];
+    r = __fadd_rn(r, g[q]);
+    if (L::cx(q)) m1 = (L::cx(q) > 0) ? __fadd_rn(m1, g[q]) : __fsub_rn(m1, g[q]);
+    if (L::cy(q)) m2 = (L::cy(q) > 0) ? __fadd_rn(m2, g[q]) : __fsub_rn(m2, g[q]);
+    if (L::cz(q)) m3 = (L::cz(q) > 0) ? __fadd_rn(m3, g[q]) : __fsub_rn(m3, g[q]);
   }
   drho = r;
-  const float inv = 1.0f / (1.0f + r);
-  u = (m1 + 0.5f * Fx) * inv;
-  v = (m2 + 0.5f * Fy) * inv;
-  w = (m3 + 0.5f * Fz) * inv;
+  const float inv = __fdiv_rn(1.0f, __fadd_rn(1.0f, r));
+  u = __fmul_rn(__fmaf_rn(0.5f, Fx, m1), inv);
+  v = __fmul_rn(__fmaf_rn(0.5f, Fy, m2), inv);
+  w = __fmul_rn(__fmaf_rn(0.5f, Fz, m3), inv);
 }
 
 // shifted equilibrium: f_eq - w_q
@@ -259,6 +261,92 @@ __device__ __forceinline__ float feqsv(float cx, float cy, float cz, float wq, f
 template <class L>
 __device__ __forceinline__ float feqs(int q, float drho, float u, float v, float w) {
   return feqsv(float(L::cx(q)), float(L::cy(q)), float(L::cz(q)), float(L::w(q)), drho, u, v, w);
+}
+
+// ---------------------------------------------------------------------------
+// FP32 BGK relaxation with the Guo increment in the shifted form
+// (collide.H:48-55, collide_forced.H:81-108 in float), arranged so that a
+// direction and its opposite share their arithmetic.  Write c_q = s c' with
+// c' the member of the pair whose first nonzero component is +1 (s = +-1):
+//   om (feq_q - w_q) = om w drho + om w (1 + drho) (4.5 (c'.u)^2 - 1.5 u.u)
+//                      + s 3 om w (1 + drho) (c'.u)
+//   Guo increment    = w omh (9 (c'.u)(c'.F) - 3 u.F) + s 3 w omh (c'.F)
+//   g*_q             = (1 - om) g_q + [the two lines above]
+// Both members of a pair evaluate the same expressions on the same inputs
+// (products with s are exact sign flips), so the compiler forms them once:
+// about two instructions per direction plus four per pair.
+// ---------------------------------------------------------------------------
+struct Col32 {
+  float u, v, w;      // velocity u^n
+  float m15uu;        // -1.5 u.u
+  float omd, omr;     // om * drho, om * (1 + drho)
+  float omm;          // 1 - om
+  float omh;          // 1 - 1 / (2 tau)
+  float Fx, Fy, Fz;   // F^n
+  float m3uF;         // -3 u.F
+  bool hf;            // F^n != 0 (the Guo increment is skipped otherwise, collide_forced.H:81-83)
+};
+
+template <class L>
+__device__ __forceinline__ Col32 col32_setup(float drho, float u, float v, float w, float om,
+                                             float omh, float Fx, float Fy, float Fz) {
+  Col32 c;
+  c.u = u;
+  c.v = v;
+  c.w = (L::D == 3) ? w : 0.0f;
+  c.m15uu = __fmul_rn(-1.5f, __fmaf_rn(c.w, c.w, __fmaf_rn(v, v, __fmul_rn(u, u))));
+  c.omd = __fmul_rn(om, drho);
+  c.omr = __fmul_rn(om, __fadd_rn(1.0f, drho));
+  c.omm = __fsub_rn(1.0f, om);
+  c.omh = omh;
+  c.Fx = Fx;
+  c.Fy = Fy;
+  c.Fz = (L::D == 3) ? Fz : 0.0f;
+  c.hf = !(Fx == 0.0f && Fy == 0.0f && c.Fz == 0.0f);
+  c.m3uF = __fmul_rn(-3.0f, __fmaf_rn(c.w, c.Fz, __fmaf_rn(v, Fy, __fmul_rn(u, Fx))));
+  return c;
+}
+
+// sign of the first nonzero component of c_q (1 for the rest direction)
+template <class L>
+__host__ __device__ constexpr int pair_sign(int q) {
+  return L::cx(q) != 0 ? L::cx(q) : (L::cy(q) != 0 ? L::cy(q) : (L::cz(q) != 0 ? L::cz(q) : 1));
+}
+
+// c'.x for the canonical member of q's pair (compile-time signs, no products)
+template <class L>
+__device__ __forceinline__ float canon_dot(int q, float x, float y, float z) {
+  const int s = pair_sign<L>(q);
+  const int a = s * L::cx(q), b = s * L::cy(q), c = s * L::cz(q);
+  float r = 0.0f;
+  bool first = true;
+  if (a != 0) { r = (a > 0) ? x : -x; first = false; }
+  if (b != 0) { r = first ? ((b > 0) ? y : -y) : ((b > 0) ? __fadd_rn(r, y) : __fsub_rn(r, y)); first = false; }
+  if (c != 0) { r = first ? ((c > 0) ? z : -z) : ((c > 0) ? __fadd_rn(r, z) : __fsub_rn(r, z)); }
+  return r;
+}
+
+template <class L>
+__device__ __forceinline__ float post32(int q, float g, const Col32 &c) {
+  const float wq = float(L::w(q));
+  const bool rest = (L::cx(q) == 0 && L::cy(q) == 0 && L::cz(q) == 0);
+  const float omrw = __fmul_rn(c.omr, wq), omdw = __fmul_rn(c.omd, wq);
+  if (rest) {
+    float b = __fmaf_rn(omrw, c.m15uu, omdw);
+    if (c.hf) b = __fmaf_rn(__fmul_rn(wq, c.omh), c.m3uF, b);
+    return __fmaf_rn(c.omm, g, b);
+  }
+  const float cu = canon_dot<L>(q, c.u, c.v, c.w);
+  const float t = __fmaf_rn(__fmul_rn(4.5f, cu), cu, c.m15uu);
+  float b = __fmaf_rn(omrw, t, omdw);
+  float p = __fmul_rn(__fmul_rn(3.0f, omrw), cu);
+  if (c.hf) {
+    const float cF = canon_dot<L>(q, c.Fx, c.Fy, c.Fz);
+    const float woh = __fmul_rn(wq, c.omh);
+    b = __fmaf_rn(woh, __fmaf_rn(__fmul_rn(9.0f, cu), cF, c.m3uF), b);
+    p = __fmaf_rn(__fmul_rn(3.0f, woh), cF, p);
+  }
+  return __fmaf_rn(c.omm, g, (pair_sign<L>(q) > 0) ? __fadd_rn(b, p) : __fsub_rn(b, p));
 }
 
 // ---------------------------------------------------------------------------
@@ -317,9 +405,6 @@ struct ilbm_ctx {
   // immersed-boundary chain
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_done = nullptr;
-  // device error word of the level-step kernels (bit 1: a bulk copy never
-  // completed); checked and cleared by ilbm_sync
-  int *d_flag = nullptr;
   int sms = 0;
   // the context's own memory pool for stream-ordered allocations (IB arrays,
   // batch tables): freed memory stays in the pool for the next request

@@ -26,7 +26,6 @@
 #include <cstring>
 #include <string>
 
-#include "bulk_copy.cuh"
 #include "ilbm_common.cuh"
 #include "step_args.cuh"
 
@@ -98,26 +97,6 @@ __device__ __forceinline__ void load_force(const StepArgs &a, const void *F, int
   fx = ldm<R>(F, m);
   fy = ldm<R>(F, m + a.ms2);
   fz = (L::D == 3) ? ldm<R>(F, m + 2 * a.ms2) : R(0);
-}
-
-// ---------------------------------------------------------------------------
-// Per-cell physics in the two arithmetic forms
-// ---------------------------------------------------------------------------
-
-template <int D>
-__device__ __forceinline__ float guo32v(float cx, float cy, float cz, float wq, float omh, float u,
-                                        float v, float w, float Fx, float Fy, float Fz) {
-  const float cu = cx * u + cy * v + cz * w;
-  const float tx = 3.0f * (cx - u) + 9.0f * cu * cx;
-  const float ty = 3.0f * (cy - v) + 9.0f * cu * cy;
-  const float tz = (D == 3) ? 3.0f * (cz - w) + 9.0f * cu * cz : 0.0f;
-  return wq * omh * (tx * Fx + ty * Fy + tz * Fz);
-}
-template <class L>
-__device__ __forceinline__ float guo32(int q, float omh, float u, float v, float w, float Fx,
-                                       float Fy, float Fz) {
-  return guo32v<L::D>(float(L::cx(q)), float(L::cy(q)), float(L::cz(q)), float(L::w(q)), omh, u,
-                      v, w, Fx, Fy, Fz);
 }
 
 // ---------------------------------------------------------------------------
@@ -219,7 +198,6 @@ __device__ __noinline__ void ghost_push(const StepArgs &a, int64_t gid, int64_t 
   ext[d] = 1;
   base[d] = side ? a.hi[d] + 1 : a.lo[d] - 1;
   const int64_t n = (int64_t)ext[0] * ext[1] * ext[2];
-  const T *fin = static_cast<const T *>(a.f_in);
   T *fo = static_cast<T *>(a.f_out);
   for (int64_t t = gid; t < n; t += gstride) {
     int g[3];
@@ -377,11 +355,9 @@ __device__ __noinline__ void ghost_push(const StepArgs &a, int64_t gid, int64_t 
         if (S == ILBM_STORAGE_F64)
           val = R(collide64_one<L>(q, double(fq), feq64<L>(q, r64, u64, v64, w64), a.tau, u64, v64,
                                    w64, double(gFx), double(gFy), double(gFz), ghf));
-        else {
-          float gv = float(fq) + a.om32 * (feqs<L>(q, dr32, u32, v32, w32) - float(fq));
-          if (ghf) gv += guo32<L>(q, a.omh32, u32, v32, w32, float(gFx), float(gFy), float(gFz));
-          val = R(gv);
-        }
+        else
+          val = R(post32<L>(q, float(fq), col32_setup<L>(dr32, u32, v32, w32, a.om32, a.omh32,
+                                                         float(gFx), float(gFy), float(gFz))));
       }
       Store<S>::store(fo + fidx(a, di, dj, dk) + q * a.fs2, val, sfac<L, S>(a, q));
     }
@@ -459,18 +435,15 @@ __device__ __forceinline__ void cell_finish(const StepArgs &a, int i, int j, int
   }
   // the Guo increment is skipped where F == 0 (collide_forced.H:81-83)
   const bool hf = !(Fx == R(0) && Fy == R(0) && Fz == R(0));
-  const float om = a.om32;
-  const float omh = a.omh32;
+  const Col32 c32 = col32_setup<L>(drho32, u32, v32, w32, a.om32, a.omh32, float(Fx), float(Fy),
+                                   float(Fz));
   auto post_v = [&](int q, R fq) -> R {
     if (S == ILBM_STORAGE_F64) {
       const double fe = feq64<L>(q, rho64, u64, v64, w64);
       return R(collide64_one<L>(q, double(fq), fe, a.tau, u64, v64, w64, double(Fx),
                                 double(Fy), double(Fz), hf));
     } else {
-      const float ge = feqs<L>(q, drho32, u32, v32, w32);
-      float val = float(fq) + om * (ge - float(fq));
-      if (hf) val += guo32<L>(q, omh, u32, v32, w32, float(Fx), float(Fy), float(Fz));
-      return R(val);
+      return R(post32<L>(q, float(fq), c32));
     }
   };
 
@@ -537,6 +510,94 @@ __device__ __forceinline__ bool needs_fixup(const StepArgs &a, int i, int j, int
          (L::D == 3 && ((k == a.lo[2] && a.act_lo[2]) || (k == a.hi[2] && a.act_hi[2])));
 }
 
+// Row segments that need none of the per-cell tests of cell_update take a
+// lean path: no face of the segment returns outgoing populations (wrap /
+// reflect), no cell reads stored macro fields, none lies in the skip box,
+// and the force is of one kind over the whole segment.  The kind is the same
+// for every thread of a block (one block = one row segment), so the branch
+// does not diverge.
+enum SegKind { SEG_GENERAL = 0, SEG_SKIP = 1, SEG_ZERO = 2, SEG_UNIFORM = 3, SEG_ARRAYS = 4 };
+
+template <class L>
+__device__ __forceinline__ int seg_kind(const StepArgs &a, int i0, int i1, int j, int k) {
+  if (a.use_skip && j >= a.slo[1] && j <= a.shi[1] &&
+      (L::D == 2 || (k >= a.slo[2] && k <= a.shi[2]))) {
+    if (i0 >= a.slo[0] && i1 <= a.shi[0]) return SEG_SKIP;
+    if (!(i1 < a.slo[0] || i0 > a.shi[0])) return SEG_GENERAL;
+  }
+  if ((j == a.lo[1] && a.act_lo[1]) || (j == a.hi[1] && a.act_hi[1])) return SEG_GENERAL;
+  if (L::D == 3 && ((k == a.lo[2] && a.act_lo[2]) || (k == a.hi[2] && a.act_hi[2])))
+    return SEG_GENERAL;
+  if ((i0 == a.lo[0] && a.act_lo[0]) || (i1 == a.hi[0] && a.act_hi[0])) return SEG_GENERAL;
+  if (a.macro_in) {
+    if (!a.use_mbox) return SEG_GENERAL;
+    if (j >= a.mblo[1] && j <= a.mbhi[1] && k >= a.mblo[2] && k <= a.mbhi[2] &&
+        !(i1 < a.mblo[0] || i0 > a.mbhi[0]))
+      return SEG_GENERAL;
+  }
+  if (a.force == nullptr || a.force_prev == nullptr) {
+    if (a.force != nullptr || a.force_prev != nullptr) return SEG_GENERAL;
+    return a.use_uniform ? SEG_UNIFORM : SEG_ZERO;
+  }
+  // force arrays: zero outside [flo, fhi] (F^n and F^{n-1} alike)
+  if (j < a.flo[1] || j > a.fhi[1] || (L::D == 3 && (k < a.flo[2] || k > a.fhi[2])) ||
+      i1 < a.flo[0] || i0 > a.fhi[0])
+    return SEG_ZERO;
+  if (i0 >= a.flo[0] && i1 <= a.fhi[0]) return SEG_ARRAYS;
+  return SEG_GENERAL;
+}
+
+// One cell of a lean row segment: the same arithmetic as cell_update with
+// edge = false on rho^n, u^n recovered from f^n and F^{n-1}.
+template <class L, int S, int K>
+__device__ __forceinline__ void cell_fast(const StepArgs &a, int i, int j, int k) {
+  using T = typename Store<S>::T;
+  using R = typename Store<S>::R;
+  const int64_t base = fidx(a, i, j, k);
+  const T *fin = static_cast<const T *>(a.f_in) + base;
+  R f[L::Q];
+#pragma unroll
+  for (int q = 0; q < L::Q; ++q) f[q] = Store<S>::load(fin + a.loff[q], sfac<L, S>(a, q));
+  R Fx = R(0), Fy = R(0), Fz = R(0), px = R(0), py = R(0), pz = R(0);
+  if (K == SEG_ARRAYS) {
+    const int64_t m = midx(a, i, j, k);
+    const R *F = static_cast<const R *>(a.force);
+    const R *P = static_cast<const R *>(a.force_prev);
+    Fx = F[m];
+    Fy = F[m + a.ms2];
+    px = P[m];
+    py = P[m + a.ms2];
+    if (L::D == 3) {
+      Fz = F[m + 2 * a.ms2];
+      pz = P[m + 2 * a.ms2];
+    }
+  } else if (K == SEG_UNIFORM) {
+    Fx = px = R(a.uf[0]);
+    Fy = py = R(a.uf[1]);
+    Fz = pz = R(a.uf[2]);
+  }
+  T *fob = static_cast<T *>(a.f_out) + base;
+  if (S == ILBM_STORAGE_F64) {
+    double rho, u, v, w;
+    moments64<L>(reinterpret_cast<double *>(f), double(px), double(py), double(pz), rho, u, v, w);
+    if (L::D != 3) w = 0.0;
+    const bool hf = !(Fx == R(0) && Fy == R(0) && Fz == R(0));
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q)
+      Store<S>::store(fob + a.doff[q],
+                      R(collide64_one<L>(q, double(f[q]), feq64<L>(q, rho, u, v, w), a.tau, u, v, w,
+                                         double(Fx), double(Fy), double(Fz), hf)),
+                      sfac<L, S>(a, q));
+  } else {
+    float drho, u, v, w;
+    moments32<L>(reinterpret_cast<float *>(f), float(px), float(py), float(pz), drho, u, v, w);
+    const Col32 c = col32_setup<L>(drho, u, v, w, a.om32, a.omh32, float(Fx), float(Fy), float(Fz));
+#pragma unroll
+    for (int q = 0; q < L::Q; ++q)
+      Store<S>::store(fob + a.doff[q], R(post32<L>(q, float(f[q]), c)), sfac<L, S>(a, q));
+  }
+}
+
 // The first `ghost_slices` z-slices of the grid push the ghost shell's
 // populations (ghost_push); the rest run one cell per thread.
 template <class L, int S>
@@ -547,134 +608,21 @@ __global__ void __launch_bounds__(256, StepOcc<L, S>::value) k_step(const __grid
                      (int64_t)a.ghost_slices * gridDim.x * gridDim.y * blockDim.x);
     return;
   }
-  const int i = a.rlo[0] + blockIdx.x * blockDim.x + threadIdx.x;
+  const int i0 = a.rlo[0] + blockIdx.x * blockDim.x;
+  const int i = i0 + threadIdx.x;
   const int j = a.rlo[1] + blockIdx.y;
   const int k = a.rlo[2] + (int)blockIdx.z - a.ghost_slices;
-  if (i > a.rhi[0]) return;
-  if (a.use_skip && in_box(a.slo, a.shi, i, j, k)) return;
-  cell_update<L, S>(a, i, j, k, needs_fixup<L>(a, i, j, k));
-}
-
-// ---------------------------------------------------------------------------
-// Level step fed by bulk copies (TMA), warp-specialised.  Persistent blocks
-// of W consumer threads plus one producer warp walk row segments of W cells.
-// The producer copies the Q plane-rows of f^n of each segment into a ring of
-// shared-memory stages (one bulk copy per plane, completing on the stage's
-// "full" mbarrier), up to STAGES segments ahead; a consumer waits for its
-// stage, takes its cell's populations from shared memory, arrives on the
-// stage's "empty" mbarrier (freeing the stage for the producer) and runs the
-// same cell_finish as k_step.  The loop has no block-wide barrier.
-// A plane-row copy starts at the 16-byte boundary at or below the segment and
-// ends on the next 16-byte boundary; the elements read beyond the segment
-// (fewer than 16 bytes each side) lie inside the grown box (ngrow_f >= 1).
-// With plane_aligned the plane stride is a multiple of 16 bytes and every
-// plane of a segment shares one offset.  The first `ghost_blocks` blocks
-// push the ghost shell instead.
-// ---------------------------------------------------------------------------
-// resident blocks of W + 32 threads per SM: 3 for the 4- and 2-byte storage
-// forms (<= 72 registers), 1 for FP64
-template <class L, int S>
-struct WsOcc {
-  static constexpr int value = (S != ILBM_STORAGE_F64) ? 3 : 1;
-};
-
-template <class L, int S, int STAGES>
-__global__ void __launch_bounds__(288, WsOcc<L, S>::value)
-    k_step_ws(const __grid_constant__ StepArgs a, int nitems, int nseg, int W, int segE,
-              int ghost_blocks, int plane_aligned, int *flag) {
-  using T = typename Store<S>::T;
-  using R = typename Store<S>::R;
-  constexpr int E = 16 / (int)sizeof(T);  // elements per 16 bytes
-  extern __shared__ __align__(128) unsigned char ws_smem[];
-  __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES];
-  if ((int)blockIdx.x < ghost_blocks) {
-    if ((int)threadIdx.x < W)
-      ghost_push<L, S>(a, (int64_t)blockIdx.x * W + threadIdx.x, (int64_t)ghost_blocks * W);
-    return;
-  }
-  T *sm = reinterpret_cast<T *>(ws_smem);
-  const int pb = blockIdx.x - ghost_blocks, np = gridDim.x - ghost_blocks;
-  const int ny = a.rhi[1] - a.rlo[1] + 1;
-  if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
-      mbar_init(&full[s], 1);
-      mbar_init(&empty[s], W);
-    }
-    mbar_init_fence();
-  }
-  __syncthreads();
-  auto seg_of = [&](int it, int &i0, int &j, int &k, int &len) {
-    const int sg = it % nseg, row = it / nseg;
-    i0 = a.rlo[0] + sg * W;
-    j = a.rlo[1] + row % ny;
-    k = a.rlo[2] + row / ny;
-    len = min(W, a.rhi[0] - i0 + 1);
-  };
-  if ((int)threadIdx.x >= W) {
-    // producer warp: lane 0 issues the copies, the other lanes are done
-    if ((int)threadIdx.x != W) return;
-    const T *fin = static_cast<const T *>(a.f_in);
-    for (int m = 0;; ++m) {
-      const int it = pb + m * np;
-      if (it >= nitems) break;
-      const int s = m % STAGES;
-      if (m >= STAGES && !mbar_wait_bounded(&empty[s], (uint32_t)(((m / STAGES) - 1) & 1))) {
-        atomicOr(flag, 1);
-        return;
-      }
-      int i0, j, k, len;
-      seg_of(it, i0, j, k, len);
-      T *dst = sm + (size_t)s * L::Q * segE;
-      const int64_t e0 = fidx(a, i0, j, k);
-      uint32_t total = 0;
-#pragma unroll
-      for (int q = 0; q < L::Q; ++q) {
-        const int off = (int)((e0 + a.loff[q]) & (E - 1));
-        total += (uint32_t)(((off + len + E - 1) / E) * E * (int)sizeof(T));
-      }
-      mbar_arrive_expect(&full[s], total);
-#pragma unroll
-      for (int q = 0; q < L::Q; ++q) {
-        const int64_t eq = e0 + a.loff[q];
-        const int off = (int)(eq & (E - 1));
-        bulk_g2s(dst + (size_t)q * segE, fin + (eq - off),
-                 (uint32_t)(((off + len + E - 1) / E) * E * (int)sizeof(T)), &full[s]);
-      }
-    }
-    return;
-  }
-  // consumers
-  const int t = threadIdx.x;
-  for (int m = 0;; ++m) {
-    const int it = pb + m * np;
-    if (it >= nitems) break;
-    const int s = m % STAGES;
-    if (!mbar_wait_bounded(&full[s], (uint32_t)((m / STAGES) & 1))) {
-      if (t == 0) atomicOr(flag, 1);
-      return;
-    }
-    int i0, j, k, len;
-    seg_of(it, i0, j, k, len);
-    const int i = i0 + t;
-    const bool mine = t < len && !(a.use_skip && in_box(a.slo, a.shi, i, j, k));
-    R f[L::Q];
-    if (mine) {
-      const T *src = sm + (size_t)s * L::Q * segE + t;
-      const int64_t e0 = fidx(a, i0, j, k);
-      if (plane_aligned) {
-        const int off = (int)(e0 & (E - 1));
-#pragma unroll
-        for (int q = 0; q < L::Q; ++q) f[q] = Store<S>::cvt(src[q * segE + off], sfac<L, S>(a, q));
-      } else {
-#pragma unroll
-        for (int q = 0; q < L::Q; ++q) {
-          const int off = (int)((e0 + a.loff[q]) & (E - 1));
-          f[q] = Store<S>::cvt(src[q * segE + off], sfac<L, S>(a, q));
-        }
-      }
-    }
-    mbar_arrive(&empty[s]);  // this thread is done with the stage
-    if (mine) cell_finish<L, S>(a, i, j, k, needs_fixup<L>(a, i, j, k), f);
+  const int kind = seg_kind<L>(a, i0, min(i0 + (int)blockDim.x - 1, a.rhi[0]), j, k);
+  if (i > a.rhi[0] || kind == SEG_SKIP) return;
+  if (kind == SEG_ZERO) {
+    cell_fast<L, S, SEG_ZERO>(a, i, j, k);
+  } else if (kind == SEG_UNIFORM) {
+    cell_fast<L, S, SEG_UNIFORM>(a, i, j, k);
+  } else if (kind == SEG_ARRAYS) {
+    cell_fast<L, S, SEG_ARRAYS>(a, i, j, k);
+  } else {
+    if (a.use_skip && in_box(a.slo, a.shi, i, j, k)) return;
+    cell_update<L, S>(a, i, j, k, needs_fixup<L>(a, i, j, k));
   }
 }
 
@@ -1034,73 +982,6 @@ static int64_t ghost_work(const StepArgs &a) {
   return n;
 }
 
-// stages of the bulk-copy level step: ILBM_PIPE_STAGES = 0 (default: plain
-// k_step, measured faster on B200 for the D3Q19 FP32 sphere level), 2 or 3
-static int pipe_stages() {
-  static int v = -1;
-  if (v < 0) {
-    const char *e = std::getenv("ILBM_PIPE_STAGES");
-    v = e ? std::atoi(e) : 0;
-    if (v != 0 && v != 2 && v != 3) v = 0;
-  }
-  return v;
-}
-
-template <class L, int S, int ST>
-static bool launch_ws_n(ilbm_ctx *ctx, const StepArgs &a, cudaStream_t st, bool with_ghosts) {
-  using T = typename Store<S>::T;
-  constexpr int E = 16 / (int)sizeof(T);
-  const int nx = a.rhi[0] - a.rlo[0] + 1, ny = a.rhi[1] - a.rlo[1] + 1;
-  const int nz = (L::D == 3) ? a.rhi[2] - a.rlo[2] + 1 : 1;
-  const int W = nx >= 256 ? 256 : ((nx + 31) / 32) * 32;
-  const int segE = W + 2 * E;
-  const size_t smem = (size_t)ST * L::Q * segE * sizeof(T);
-  if (smem > 200 * 1024) return false;
-  // the copies reach fewer than E elements beyond either end of a row
-  // segment: inside the grown box as long as a row plus its ghost is longer
-  if (a.fs0 < E) return false;
-  static int attr_set[64] = {0};  // the attribute is per device; setting it twice is harmless
-  const int dev = ctx->device & 63;
-  if (!attr_set[dev]) {
-    if (cudaFuncSetAttribute(k_step_ws<L, S, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             200 * 1024) != cudaSuccess) {
-      cudaGetLastError();
-      return false;
-    }
-    attr_set[dev] = 1;
-  }
-  int occ = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_step_ws<L, S, ST>, W + 32, smem) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  if (occ < 1) return false;
-  const int nseg = (nx + W - 1) / W;
-  const int nitems = nseg * ny * nz;
-  int ghost_blocks = 0;
-  if (with_ghosts) {
-    const int64_t w = ghost_work<L>(a);
-    ghost_blocks = (int)std::min<int64_t>(512, (w + W - 1) / W);
-  }
-  const int plane_aligned = (a.fs2 % E) == 0 ? 1 : 0;
-  const int pipes = std::max(1, std::min(nitems, occ * ctx->sms));
-  k_step_ws<L, S, ST><<<ghost_blocks + pipes, W + 32, smem, st>>>(a, nitems, nseg, W, segE, ghost_blocks,
-                                                                    plane_aligned, ctx->d_flag);
-  ctx->launches++;
-  return true;
-}
-
-// the level step of [rlo, rhi] through k_step_ws when it applies (f_in on a
-// 16-byte boundary); false: the caller uses k_step
-template <class L, int S>
-static bool launch_ws(ilbm_ctx *ctx, const StepArgs &a, cudaStream_t st, bool with_ghosts) {
-  if ((reinterpret_cast<uintptr_t>(a.f_in) & 15) != 0) return false;
-  const int ns = pipe_stages();
-  if (ns == 3) return launch_ws_n<L, S, 3>(ctx, a, st, with_ghosts);
-  if (ns == 2) return launch_ws_n<L, S, 2>(ctx, a, st, with_ghosts);
-  return false;
-}
-
 // k_step over [rlo, rhi] (minus the skip box), with the ghost shell push in
 // leading z-slices when with_ghosts is set
 template <class L, int S>
@@ -1126,7 +1007,7 @@ static void launch_cells(ilbm_ctx *ctx, const StepArgs &a_in, cudaStream_t st, b
 template <class L, int S>
 static int launch_step(ilbm_ctx *ctx, const StepArgs &a, const ilbm_level_params *p) {
   (void)p;
-  if (!launch_ws<L, S>(ctx, a, ctx->stream, true)) launch_cells<L, S>(ctx, a, ctx->stream, true);
+  launch_cells<L, S>(ctx, a, ctx->stream, true);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "level step launch");
   return ILBM_OK;
@@ -1152,7 +1033,7 @@ static int launch_step_split(ilbm_ctx *ctx, const StepArgs &a, const int *blo, c
     outer.slo[d] = blo[d];
     outer.shi[d] = bhi[d];
   }
-  if (!launch_ws<L, S>(ctx, outer, ctx->stream, true)) launch_cells<L, S>(ctx, outer, ctx->stream, true);
+  launch_cells<L, S>(ctx, outer, ctx->stream, true);
   cudaError_t e = cudaStreamWaitEvent(ctx->stream, band_ready, 0);
   if (e != cudaSuccess) return cuda_fail(e, "cudaStreamWaitEvent");
   StepArgs inner = a;
@@ -1692,8 +1573,6 @@ int ilbm_create(const ilbm_lattice *lat, int storage, int device, void *cuda_str
     }
   }
   e = cudaMallocHost(&c->host_pinned, 64 * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&c->d_flag, 16);
-  if (e == cudaSuccess) e = cudaMemset(c->d_flag, 0, 16);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) {
     cudaMemPoolProps pp = {};
@@ -1723,7 +1602,6 @@ int ilbm_destroy(ilbm_ctx *ctx) {
   delete[] ctx->xev;
   if (ctx->scratch) cudaFree(ctx->scratch);
   if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
-  if (ctx->d_flag) cudaFree(ctx->d_flag);
   if (ctx->side) {
     cudaStreamSynchronize(ctx->side);
     cudaStreamDestroy(ctx->side);
@@ -1742,14 +1620,6 @@ int ilbm_sync(ilbm_ctx *ctx) {
   if (!ctx) return ILBM_ERR_ARG;
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "stream synchronize");
-  int flag = 0;
-  e = cudaMemcpy(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return cuda_fail(e, "level-step status");
-  if (flag) {
-    cudaMemset(ctx->d_flag, 0, sizeof(int));
-    set_error("level step: a bulk copy into shared memory did not complete (step abandoned)");
-    return ILBM_ERR_CUDA;
-  }
   return ILBM_OK;
 }
 

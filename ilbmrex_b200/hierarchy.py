@@ -18,8 +18,8 @@ import torch
 
 from . import capi
 from .cases import MarkerIB, TwoLevelCase
-from .level import (_REAL_DT, _TORCH_DT, Context, LevelSolver, ib_params, level_geom,
-                    level_params)
+from .level import (_REAL_DT, _TORCH_DT, Context, LevelSolver, alloc_populations, ib_params,
+                    level_geom, level_params)
 
 
 class _Level:
@@ -36,8 +36,8 @@ class _Level:
         fdt, rdt = _TORCH_DT[storage], _REAL_DT[storage]
         fsh = (q, gz_f, ny + 2 * self.gf, nx + 2 * self.gf)
         msh = (gz_m, ny + 2 * self.gm, nx + 2 * self.gm)
-        self.f = torch.zeros(fsh, dtype=fdt, device=dev)
-        self.f_next = torch.zeros(fsh, dtype=fdt, device=dev)
+        self.f = alloc_populations(*fsh, fdt, dev, ngrow=self.gf)
+        self.f_next = alloc_populations(*fsh, fdt, dev, ngrow=self.gf)
         self.m = torch.zeros((4,) + msh, dtype=rdt, device=dev)
         self.m_next = torch.zeros((4,) + msh, dtype=rdt, device=dev)
         self.fa = torch.zeros((3,) + msh, dtype=rdt, device=dev) if with_force else None

@@ -163,8 +163,10 @@ int ilbm_storage_bytes(const ilbm_ctx *ctx, int *storage_bytes, int *real_bytes)
 
 /* ---- level step --------------------------------------------------------- */
 /* One level step on nbox boxes: BGK collision with Guo forcing on valid cells,
- * halfway bounce-back for user_1 faces and pull streaming into f_out, with the
- * reference's ghost semantics.  If macro_out is set, rho/u of f^{n+1} are
+ * halfway bounce-back for user_1 faces and streaming into f_out (each cell
+ * pushes its post-collision populations to its neighbours, which gives the
+ * same f_out as the reference's pull stream), with the reference's ghost
+ * semantics.  If macro_out is set, rho/u of f^{n+1} are
  * written as well (calculateMacroForcing with F^n). */
 int ilbm_level_step(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox,
                     const ilbm_level_params *p);
@@ -279,7 +281,9 @@ int ilbm_force_integrals(ilbm_ctx *ctx, const ilbm_box *box, const void *force,
  *     without launching anything.
  *   - The first call on a device does a one-time set-up (it looks up the
  *     array's device address, which may load the library's device code on
- *     that device); make it before any stream capture begins.
+ *     that device); make it before any stream capture begins.  The address
+ *     is cached for the life of the process: a process that resets a device
+ *     (cudaDeviceReset) must not call this entry point on that device again.
  *   - There is one array per device: calls that overlap on a device (from
  *     two host threads, or on two contexts of the same device) race on it
  *     and give wrong sums.  Each call synchronises the context's stream
@@ -403,7 +407,11 @@ int ilbm_average_down(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_pa
  *   f16 storage keeps its raw half bits: restore with the same f16_scale.
  * Both synchronise the context's stream.  Errors: ILBM_ERR_IO (file, short
  * read, hash mismatch), ILBM_ERR_ARG (the file does not match the lattice,
- * storage, box, body or the sections asked for). */
+ * storage, box, body or the sections asked for).  A read is checked section
+ * by section as it is restored: when ilbm_checkpoint_read fails with
+ * ILBM_ERR_IO after its header was accepted, the box arrays and the body may
+ * already be partly overwritten and are undefined; restore them from
+ * another checkpoint or re-initialise them. */
 #define ILBM_ERR_IO (-7)
 #define ILBM_CKPT_MACRO 1 /* flags: the file holds stored macro fields */
 #define ILBM_CKPT_FORCE 2 /*        F^{n-1} */
