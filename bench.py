@@ -159,21 +159,22 @@ def barrier(world: int):
         dist.barrier()
 
 
-def cpu_reference_steps(steps: int, warmup: int, threads: int | None = None):
+def cpu_reference_levels(levels, steps: int, warmup: int, threads: int | None = None,
+                         budget_s: float = 120.0):
     """Times the reference's own CPU level step (oracle/_ref: Source/LBM,
-    Source/BC compiled in place, FP32 3D build, OpenMP) on the levels of the
-    same hierarchy: the coarse level and the fine box each advanced as a
-    level; MLUPS = updates of one coarse step (coarse + 2 x fine cells) over
-    (coarse step time + 2 x fine step time).  Returns (MLUPS, seconds per
-    coarse step, threads, kind, sample text)."""
-    from ilbmrex_b200 import cases
+    Source/BC compiled in place, float build, the restated AdvancePhiAtLevel
+    pass structure, OpenMP) on each (case, init, weight) of `levels`: per
+    level `warmup` untimed steps, then up to `steps` timed ones (fewer when
+    the first timed step shows that `steps` would exceed budget_s in all).
+    Returns (seconds per weighted step = sum of weight x level step time,
+    threads, kind, steps timed)."""
     from oracle import checker
     from oracle.checker import CpuLevel
-    tl, ib, ic, if_ = sphere_hierarchy()
-    kind = "reference" if checker.available("ref", 3, fp32=True) else "port"
+    dim = levels[0][0].dim
+    kind = "reference" if checker.available("ref", dim, fp32=True) else "port"
     threads = threads or os.cpu_count() or 1
-    t = []
-    for case, init in ((tl.coarse, ic), (tl.fine_box(), if_)):
+    total, timed = 0.0, steps
+    for case, init, weight in levels:
         if kind == "reference":
             L = CpuLevel(case, "ref", fp32=True, threads=threads)
         else:
@@ -183,37 +184,107 @@ def cpu_reference_steps(steps: int, warmup: int, threads: int | None = None):
         L.init_equilibrium()
         L.step(max(1, warmup))
         t0 = time.perf_counter()
-        L.step(steps)
-        t.append((time.perf_counter() - t0) / steps)
+        L.step(1)
+        first = time.perf_counter() - t0
+        n = max(1, min(timed, int(budget_s / max(first * len(levels) * weight, 1e-9))))
+        timed = min(timed, n)
+        if n > 1:
+            t0 = time.perf_counter()
+            L.step(n - 1)
+            per = (first + time.perf_counter() - t0) / n
+        else:
+            per = first
+        total += weight * per
         L.close()
-    dt = t[0] + 2.0 * t[1]
+    return total, threads, kind, timed
+
+
+def cpu_reference_steps(steps: int, warmup: int, threads: int | None = None):
+    """The reference's CPU level step on the levels of the sphere hierarchy:
+    MLUPS = updates of one coarse step (coarse + 2 x fine cells) over (coarse
+    step time + 2 x fine step time).  Returns (MLUPS, seconds per coarse
+    step, threads, kind, steps timed, sample text)."""
+    tl, ib, ic, if_ = sphere_hierarchy()
+    dt, threads, kind, timed = cpu_reference_levels(
+        [(tl.coarse, ic, 1.0), (tl.fine_box(), if_, 2.0)], steps, warmup, threads)
     updates = tl.coarse.cells + 2 * int(np.prod(tl.fine_n_cell))
-    sample = (f"{steps} level steps each of the coarse level ({tl.coarse.cells} cells) and of the fine box "
+    sample = (f"{timed} level steps each of the coarse level ({tl.coarse.cells} cells) and of the fine box "
               f"({int(np.prod(tl.fine_n_cell))} cells) after {max(1, warmup)} warm-up step(s), timed as "
-              "coarse + 2 x fine per coarse step; the body's forcing (12.9k-marker IVC, whose dense LU "
-              "alone runs for minutes on the host) and the coarse-fine fill are not included; "
+              "coarse + 2 x fine per coarse step; "
               + ("reference sources (Source/LBM, Source/BC) compiled in place, float, restated "
                  "AdvancePhiAtLevel pass structure, OpenMP" if kind == "reference"
                  else "plain-C oracle port, FP64, 1 thread"))
-    return updates / dt / 1e6, dt, threads, kind, sample
+    return updates / dt / 1e6, dt, threads, kind, timed, sample
+
+
+REFERENCE_SCOPE = ("the reference's level step (collide with Guo forcing, bounce-back, stream, "
+                   "macro) on both levels of the hierarchy, float build on all host cores; NOT "
+                   "included: the immersed body's update_forcing (its 12,869-marker dense LU alone runs "
+                   "for minutes on the host; see with_body_single_level for its per-step cost on the "
+                   "single-level sphere) and the coarse-fine fill / average-down (AMReX's)")
+
+
+def cpu_reference_body(warmup: int, steps: int = 3, threads: int | None = None):
+    """The reference's CPU path WITH its body on the sphere's base level
+    alone (3,218 markers): IBMarkerDF::update_forcing compiled in place (its
+    one-time dense LU inside the untimed warm-up) plus the level step, against
+    the same level without the body."""
+    from oracle import checker
+    from oracle.checker import CpuLevel
+    from ilbmrex_b200 import cases
+    if not checker.available("ref", 3, fp32=True):
+        return None
+    w = WORKLOAD
+    case, ib, init = cases.sphere(w["nx"], w["ny"], w["nz"], D=w["D"], center=w["center"], U=w["U"],
+                                  Re=w["Re"])
+    threads = threads or os.cpu_count() or 1
+    out = {}
+    for with_body in (False, True):
+        L = CpuLevel(case, "ref", fp32=True, threads=threads)
+        L.set_macro(*init())
+        L.init_equilibrium()
+        if with_body:
+            L.ib_create(ib)
+        L.step(max(1, warmup))
+        t0 = time.perf_counter()
+        L.step(steps)
+        out[with_body] = (time.perf_counter() - t0) / steps
+        if with_body:
+            n_mark = L.num_markers()
+        L.close()
+    return {"mlups": round(case.cells / out[True] / 1e6, 3), "ms_per_step": round(out[True] * 1e3, 1),
+            "ms_per_step_without_body": round(out[False] * 1e3, 1),
+            "ib_ms_per_step": round((out[True] - out[False]) * 1e3, 1), "markers": int(n_mark),
+            "cores": threads, "steps": steps,
+            "sample": f"sphere base level {w['nx']}x{w['ny']}x{w['nz']} alone, {steps} steps with and "
+                      f"without its body after {max(1, warmup)} warm-up step(s) (the IVC dense LU in the "
+                      "first); reference sources incl. Source/IBM/IBMarkerDF.cpp compiled in place, float, "
+                      "OpenMP"}
 
 
 def run_reference(args):
     world, rank, local = dist_setup()
     if rank != 0:
         return
-    steps = max(1, min(args.steps, 3))
-    warm = max(3, min(args.warmup, 5))  # at least three, at most five host steps
-    mlups, dt, threads, kind, sample = cpu_reference_steps(steps, warm)
+    warm = max(3, args.warmup)
+    mlups, dt, threads, kind, timed, sample = cpu_reference_steps(max(1, args.steps), warm)
+    body = cpu_reference_body(3)
+    config = dict(workload_config(args))
+    config["reference_scope"] = REFERENCE_SCOPE
     line = {"metric": METRIC, "value": round(mlups, 3), "unit": UNIT, "n_gpus": args.gpus,
-            "steps": steps, "warmup": warm, "ms_per_step": round(dt * 1e3, 3),
+            "steps": timed, "warmup": warm, "ms_per_step": round(dt * 1e3, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
-            "config": workload_config(args),
+            "config": config,
             "cpu_baseline": {"value": round(mlups, 3), "unit": UNIT, "cores": threads,
                              "kind": kind, "sample": sample},
             "e2e": {"value": round(mlups, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "with_body_single_level": body}
+    if timed < args.steps:
+        line["steps_requested"] = args.steps
+        line["steps_note"] = ("fewer timed steps than requested: the requested count would exceed the "
+                              "120 s budget of the CPU sample")
     print(json.dumps(line), flush=True)
 
 
@@ -376,8 +447,8 @@ def run_two_level(args, world, device):
     reference's refinement rule (1 R upstream, 4 R downstream, 2 R across,
     plus a 6-cell pad) carrying the marker IBM with markers ~1 fine dx apart,
     FP32 storage.  Cell updates per coarse step: coarse cells + 2 x fine
-    cells.  Beside it, the oracle's two-level driver (plain C, FP64, one
-    thread) on coarse steps of the same hierarchy."""
+    cells.  Beside it, the reference's CPU level step on the same two levels
+    (all host cores)."""
     from ilbmrex_b200 import cases
     from ilbmrex_b200.hierarchy import TwoLevelSolver
     R, pad = 20.0, 6.0
@@ -408,20 +479,13 @@ def run_two_level(args, world, device):
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         try:
-            from oracle.checker import CpuTwoLevel
-            T = CpuTwoLevel(tl)
-            T.set_macro(0, *ic())
-            T.set_macro(1, *if_())
-            T.init_equilibrium()
-            T.ib_create(ib)
-            T.step(1)  # includes the one-time dense LU of the IVC operator
-            t0 = time.perf_counter()
-            T.step(2)
-            dt = (time.perf_counter() - t0) / 2
-            cpu = {"value": round(updates / dt / 1e6, 3), "unit": "MLUPS", "cores": 1, "kind": "port",
-                   "sample": "two coarse steps of the same hierarchy (coarse step + 2 fine substeps "
-                             "+ average-down) after one warm-up step, oracle two-level driver, FP64"}
-            T.close()
+            dt, threads, kind, timed = cpu_reference_levels([(tl.coarse, ic, 1.0), (tl.fine_box(), if_, 2.0)],
+                                                            5, 3, budget_s=30.0)
+            cpu = {"value": round(updates / dt / 1e6, 3), "unit": "MLUPS", "cores": threads, "kind": kind,
+                   "sample": f"{timed} level steps each of the coarse level and of the fine box after 3 "
+                             "warm-up steps, timed as coarse + 2 x fine per coarse step (the body's forcing, "
+                             "the coarse-fine fill and the average-down not included); reference sources "
+                             "compiled in place, float, OpenMP"}
         except Exception as e:  # the checker is optional at run time
             cpu = {"value": None, "unit": "MLUPS", "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
     return {"metric": "two-level MLUPS (D2Q9 cylinder wake 1024x512 + 1 refined level, FP32)",
@@ -489,6 +553,49 @@ def run_served(args, world, device):
                         f"1e5-3e7 cells x 1000-20000 steps shrunk to a bench-sized run)"}
 
 
+def level_step_ms(L, ctx, box, params, K: int) -> float:
+    """Mean device time (CUDA events on the library stream) of K launches of
+    ilbm_level_step on one box, after two untimed ones; the box's f_in is
+    read and its f_out written each time, so the state is left as it was."""
+    from ilbmrex_b200 import capi
+    for r in range(K + 2):
+        if r >= 2:
+            ctx.record(16 + 2 * (r - 2))
+        capi.check(L.ilbm_level_step(ctx.h, C.byref(box), 1, C.byref(params)), "level step")
+        if r >= 2:
+            ctx.record(17 + 2 * (r - 2))
+    ctx.sync()
+    return float(np.mean([ctx.elapsed_ms(16 + 2 * r, 17 + 2 * r) for r in range(K)]))
+
+
+def run_roofline_only(args):
+    """The dominant kernel alone, for profiling: the level step of the
+    sphere's 256 x 128 x 128 base level (no body, the headline's storage
+    form, the library's population layout) launched --steps times after
+    --warmup level steps; prints one JSON line with its roofline figures."""
+    import torch
+    from ilbmrex_b200 import cases
+    from ilbmrex_b200.level import LevelSolver
+    w = WORKLOAD
+    case, _, init = cases.sphere(w["nx"], w["ny"], w["nz"], D=w["D"], center=w["center"], U=w["U"],
+                                 Re=w["Re"])
+    S = LevelSolver(case, args.storage, ib=None)
+    S.set_macro(*init())
+    S.step(max(3, args.warmup))
+    S.ctx.sync()
+    sbytes = {"f64": 8, "f32": 4, "f16": 2}[args.storage]
+    B_cell = 2 * case.lattice.q * sbytes
+    ms = level_step_ms(S.L, S.ctx, S._box(S.f, S.f_next), S.params, max(1, args.steps))
+    peak, kind = peaks()
+    achieved = B_cell * case.cells / (ms * 1e-3) / 1e9
+    print(json.dumps({"roofline_only": True, "kernel": f"k_step<D3Q{case.lattice.q},{args.storage}>",
+                      "cells": case.cells, "bytes_per_cell": B_cell, "kernel_ms": round(ms, 4),
+                      "achieved_gbs": round(achieved, 1), "peak_gbs": peak, "peak_source": kind,
+                      "frac": round(achieved / peak, 4), "launches": max(1, args.steps) + 2}), flush=True)
+    S.close()
+    torch.cuda.synchronize()
+
+
 def run_b200(args):
     import torch
     world, rank, local = dist_setup()
@@ -551,16 +658,7 @@ def run_b200(args):
     # (4,194,304 cells), from the current state into the scratch buffer (the
     # hierarchy's state is left as it was) ------------------------------------
     Cl = S.C
-    bk = Cl.box(Cl.f, Cl.f_next)
-    Kr = max(3, min(K, 20))
-    for r in range(Kr + 2):
-        if r >= 2:
-            ctx.record(16 + 2 * (r - 2))
-        capi.check(S.L.ilbm_level_step(ctx.h, C.byref(bk), 1, C.byref(S.pc)), "level step")
-        if r >= 2:
-            ctx.record(17 + 2 * (r - 2))
-    ctx.sync()
-    kern_ms = float(np.mean([ctx.elapsed_ms(16 + 2 * r, 17 + 2 * r) for r in range(Kr)]))
+    kern_ms = level_step_ms(S.L, ctx, Cl.box(Cl.f, Cl.f_next), S.pc, max(3, min(K, 20)))
     peak, peak_kind = peaks()
     achieved = B_cell * cells_c / (kern_ms * 1e-3) / 1e9
 
@@ -598,9 +696,9 @@ def run_b200(args):
     cpu_base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            mlups, dt, threads, kind, sample = cpu_reference_steps(2, 3)
+            mlups, dt, threads, kind, timed, sample = cpu_reference_steps(2, 3)
             cpu_base = {"value": round(mlups, 3), "unit": UNIT, "cores": threads, "kind": kind,
-                        "sample": sample}
+                        "sample": sample, "scope": REFERENCE_SCOPE}
         except Exception as e:  # the checker is optional at run time
             cpu_base = {"value": None, "unit": UNIT, "cores": 0, "kind": "port",
                         "sample": f"unavailable: {e}"}
@@ -686,11 +784,15 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=40)
     ap.add_argument("--batch-plain-steps", type=int, default=8)
     ap.add_argument("--batch-check-cases", type=int, default=4)
+    ap.add_argument("--roofline-only", action="store_true",
+                    help="time only the level step of the sphere's base level (profiling aid)")
     args = ap.parse_args()
     if args.nx:
         set_workload_size(args.nx, args.ny or args.nx // 2, args.nz or args.nx // 2)
     if args.impl == "reference":
         run_reference(args)
+    elif args.roofline_only:
+        run_roofline_only(args)
     else:
         run_b200(args)
 

@@ -1,7 +1,7 @@
 """ctypes binding of the C ABI declared in ``include/ilbm_b200.h``.
 
-This is the same binding a host of the library would write (see
-INTEGRATION.md); the package's drivers go through it.  The shared object is
+This is the same binding a host of the library would write; the package's
+drivers go through it.  The shared object is
 the in-tree ``ilbmrex_b200/lib/libilbm_b200.so``; there is no fallback: if it
 cannot be loaded every entry point raises.
 """
@@ -19,6 +19,7 @@ ILBM_ERR_NOMEM, ILBM_ERR_SOLVER, ILBM_ERR_RANGE = -4, -5, -6
 ILBM_ERR_IO = -7
 CKPT_MACRO, CKPT_FORCE, CKPT_BODY = 1, 2, 4
 TWO_LEVEL_FIRST_STEP = 1
+HIERARCHY_FIRST_STEP = 1
 STORAGE = {"f64": 0, "f32": 1, "f16": 2}
 GHOST_SELF, GHOST_CALLER = 0, 1
 IVC_AUTO, IVC_CG, IVC_DENSE = 0, 1, 2
@@ -41,7 +42,7 @@ EXPORTS = [
     "ilbm_batch_tune", "ilbm_batch_size", "ilbm_batch_progress",
     "ilbm_derived_fields", "ilbm_tag_cells",
     "ilbm_checkpoint_write", "ilbm_checkpoint_read", "ilbm_plotfile_write",
-    "ilbm_advance_two_level", "ilbm_average_down",
+    "ilbm_advance_two_level", "ilbm_average_down", "ilbm_advance_hierarchy",
 ]
 
 
@@ -147,15 +148,15 @@ def lib():
         "ilbm_ib_destroy": (I, [P]),
         "ilbm_ib_num_markers": (I, [P, C.POINTER(I64)]),
         "ilbm_ib_force_region": (I, [P, ip3, ip3]),
-        "ilbm_ib_update_forcing": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), D, D]),
+        "ilbm_ib_update_forcing": (I, [P, C.POINTER(Box_t), I, C.POINTER(LevelParams_t), D, D]),
         "ilbm_advance_level": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P, D, D]),
         "ilbm_ib_last_marker_force_sum": (I, [P, dp]),
         "ilbm_ib_solver_stats": (I, [P, C.POINTER(I)]),
         "ilbm_ib_set_ivc_solver": (I, [P, I]),
         "ilbm_ib_markers": (I, [P, dp, dp, dp]),
-        "ilbm_force_integrals": (I, [P, C.POINTER(Box_t), P, ip3, ip3, dp]),
+        "ilbm_force_integrals": (I, [P, C.POINTER(Box_t), I, ip3, ip3, dp]),
         "ilbm_force_integrals_noalloc": (I, [P, C.POINTER(Box_t), P, ip3, ip3, dp]),
-        "ilbm_force_record_async": (I, [P, C.POINTER(Box_t), P, P, ip3, ip3, P]),
+        "ilbm_force_record_async": (I, [P, C.POINTER(Box_t), I, P, ip3, ip3, P]),
         "ilbm_batch_create": (I, [P, I, C.POINTER(P)]),
         "ilbm_batch_destroy": (I, [P]),
         "ilbm_batch_add": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P, D, D, I,
@@ -175,11 +176,12 @@ def lib():
                                        C.POINTER(LevelParams_t), P, D, D, I]),
         "ilbm_average_down": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), C.POINTER(Box_t),
                                   C.POINTER(LevelParams_t)]),
+        "ilbm_advance_hierarchy": (I, [P, I, C.POINTER(Box_t), C.POINTER(LevelParams_t), P, D, D, I]),
         "ilbm_checkpoint_write": (I, [P, C.POINTER(Box_t), P, C.POINTER(CheckpointMeta_t), C.c_char_p]),
         "ilbm_checkpoint_read": (I, [P, C.POINTER(Box_t), P, C.POINTER(CheckpointMeta_t), C.c_char_p]),
         "ilbm_plotfile_write": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t),
                                     C.POINTER(PlotInfo_t), C.c_char_p]),
-        "ilbm_momentum_exchange": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P,
+        "ilbm_momentum_exchange": (I, [P, C.POINTER(Box_t), I, C.POINTER(LevelParams_t),
                                        D, D, D, D, dp, dp, I, dp]),
     }
     for name, (res, args) in sigs.items():

@@ -39,7 +39,7 @@ int batch_step_occupancy(const ilbm_ctx *ctx, int w, int *per_sm);
 // the Eulerian force sum of ilbm_force_integrals enqueued on ctx->stream; the
 // three sums land at *d_sum (context scratch, with 8 spare doubles after
 // them) when the stream gets there
-int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *box, const void *force, const int lo[3],
+int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const int lo[3],
                       const int hi[3], double **d_sum);
 
 // ---- ib.cu ----------------------------------------------------------------

@@ -7,6 +7,7 @@
 #include <atomic>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "batch_internal.h"
 #include "ilbm_common.cuh"
@@ -57,6 +58,56 @@ __global__ void __launch_bounds__(kRedThreads) k_force_partial(RegionArgs a, con
   }
 }
 
+// The same partial sums over several boxes: the regions' cells are taken as
+// one sequence (region by region, each in i-fastest order) cut into equal
+// chunks, one per block, so the summation order depends on the box list only.
+struct SumRegion {
+  RegionArgs a;
+  const void *F;
+};
+
+template <class R>
+__global__ void __launch_bounds__(kRedThreads) k_force_partial_multi(const SumRegion *__restrict__ regs,
+                                                                     int nregs, const int64_t *off,
+                                                                     double *partial) {
+  __shared__ double sh[3][kRedThreads / 32];
+  const int64_t total = off[nregs];
+  const int64_t per = (total + gridDim.x - 1) / gridDim.x;
+  const int64_t t0 = (int64_t)blockIdx.x * per, t1 = min(total, t0 + per);
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+    int r = 0, hi = nregs - 1;
+    while (r < hi) {
+      const int mid = (r + hi + 1) >> 1;
+      if (off[mid] <= t) r = mid;
+      else hi = mid - 1;
+    }
+    const RegionArgs &a = regs[r].a;
+    const R *F = static_cast<const R *>(regs[r].F);
+    const int64_t u = t - off[r];
+    const int i = a.lo[0] + (int)(u % a.n[0]);
+    const int j = a.lo[1] + (int)((u / a.n[0]) % a.n[1]);
+    const int k = a.lo[2] + (int)(u / ((int64_t)a.n[0] * a.n[1]));
+    const int64_t m = (int64_t)(i - a.mgl[0]) + (int64_t)(j - a.mgl[1]) * a.ms0 +
+                      (int64_t)(k - a.mgl[2]) * a.ms1;
+    acc[0] += double(F[m]);
+    acc[1] += double(F[m + a.ms2]);
+    if (a.dim == 3) acc[2] += double(F[m + 2 * a.ms2]);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int c = 0; c < 3; ++c) {
+    double v = acc[c];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[c][wid] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double s = 0.0;
+    for (int w = 0; w < kRedThreads / 32; ++w) s += sh[threadIdx.x][w];
+    partial[blockIdx.x * 3 + threadIdx.x] = s;
+  }
+}
+
 __global__ void k_final_sum(const double *partial, int nparts, double *out) {
   if (threadIdx.x < 3) {
     double s = 0.0;
@@ -66,14 +117,20 @@ __global__ void k_final_sum(const double *partial, int nparts, double *out) {
 }
 
 struct MEArgs {
-  int lo[3], hi[3];
-  int fgl[3];
-  int64_t fs0, fs1, fs2;
+  int dlo[3], dhi[3];
   int periodic[3];
   double plo[3], dx[3];
   double x0, y0, z0, R;
   int one_sided;
   float f16_scale;
+  int nbox;
+};
+
+// one box of the level: valid region, allocated lower corner and strides of f
+struct MEBox {
+  int lo[3], hi[3], fgl[3];
+  int64_t fs0, fs1, fs2;
+  const void *f;
 };
 
 __device__ __forceinline__ double sdist(const MEArgs &a, int D, double x, double y, double z) {
@@ -86,57 +143,80 @@ __device__ __forceinline__ double sdist(const MEArgs &a, int D, double x, double
   return X::sub(__dsqrt_rn(s), a.R);
 }
 
+__device__ __forceinline__ bool box_holds(const MEBox &b, int D, int i, int j, int k, int grow) {
+  return i >= b.lo[0] - grow && i <= b.hi[0] + grow && j >= b.lo[1] - grow && j <= b.hi[1] + grow &&
+         (D == 2 || (k >= b.lo[2] - grow && k <= b.hi[2] + grow));
+}
+
+// Link-wise momentum exchange over the valid cells of every box, taken as one
+// sequence cut into equal chunks (fixed summation order for a given box
+// list).  The population of a solid neighbour comes from the box whose valid
+// region holds it, else from this box's caller-filled ghost layer; a link
+// whose neighbour neither reaches is left out.
 template <class L, int S>
-__global__ void __launch_bounds__(kRedThreads) k_me_partial(MEArgs a, const void *fptr,
-                                                            double *partial) {
+__global__ void __launch_bounds__(kRedThreads) k_me_partial(MEArgs a, const MEBox *__restrict__ boxes,
+                                                            const int64_t *off, double *partial) {
   using T = typename Store<S>::T;
-  const T *f = static_cast<const T *>(fptr);
   __shared__ double sh[3][kRedThreads / 32];
-  const int nx = a.hi[0] - a.lo[0] + 1, ny = a.hi[1] - a.lo[1] + 1;
-  const int nz = (L::D == 3) ? a.hi[2] - a.lo[2] + 1 : 1;
-  const int64_t total = (int64_t)nx * ny * nz;
+  const int64_t total = off[a.nbox];
   const int64_t per = (total + gridDim.x - 1) / gridDim.x;
   const int64_t t0 = (int64_t)blockIdx.x * per, t1 = min(total, t0 + per);
   double acc[3] = {0.0, 0.0, 0.0};
-  auto load = [&](int i, int j, int k, int q) -> double {
-    const int64_t b = (int64_t)(i - a.fgl[0]) + (int64_t)(j - a.fgl[1]) * a.fs0 +
-                      (int64_t)(k - a.fgl[2]) * a.fs1 + q * a.fs2;
+  auto load = [&](const MEBox &b, int i, int j, int k, int q) -> double {
+    const int64_t e = (int64_t)(i - b.fgl[0]) + (int64_t)(j - b.fgl[1]) * b.fs0 +
+                      (int64_t)(k - b.fgl[2]) * b.fs1 + q * b.fs2;
     const float s = (S == ILBM_STORAGE_F16_SCALED) ? float(L::w(q)) / a.f16_scale : 1.0f;
-    double v = double(Store<S>::load(f + b, s));
+    double v = double(Store<S>::load(static_cast<const T *>(b.f) + e, s));
     if (Store<S>::shifted) v += L::w(q);
     return v;
   };
+  const int nn[3] = {a.dhi[0] - a.dlo[0] + 1, a.dhi[1] - a.dlo[1] + 1, a.dhi[2] - a.dlo[2] + 1};
   for (int64_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
-    const int i = a.lo[0] + (int)(t % nx);
-    const int j = a.lo[1] + (int)((t / nx) % ny);
-    const int k = (L::D == 3) ? a.lo[2] + (int)(t / ((int64_t)nx * ny)) : 0;
+    int bi = 0, hi = a.nbox - 1;
+    while (bi < hi) {
+      const int mid = (bi + hi + 1) >> 1;
+      if (off[mid] <= t) bi = mid;
+      else hi = mid - 1;
+    }
+    const MEBox &B = boxes[bi];
+    const int nx = B.hi[0] - B.lo[0] + 1, ny = B.hi[1] - B.lo[1] + 1;
+    const int64_t u = t - off[bi];
+    const int i = B.lo[0] + (int)(u % nx);
+    const int j = B.lo[1] + (int)((u / nx) % ny);
+    const int k = (L::D == 3) ? B.lo[2] + (int)(u / ((int64_t)nx * ny)) : 0;
     const double xc = X::add(a.plo[0], X::mul(X::add(double(i), 0.5), a.dx[0]));
     const double yc = X::add(a.plo[1], X::mul(X::add(double(j), 0.5), a.dx[1]));
     const double zc = (L::D == 3) ? X::add(a.plo[2], X::mul(X::add(double(k), 0.5), a.dx[2])) : 0.0;
     if (!(sdist(a, L::D, xc, yc, zc) > 0.0)) continue;
 #pragma unroll
     for (int q = 1; q < L::Q; ++q) {
-      int in = i + L::cx(q), jn = j + L::cy(q), kn = k + L::cz(q);
-      const int nn[3] = {nx, ny, nz};
-      int c[3] = {in, jn, kn};
-      const int lo[3] = {a.lo[0], a.lo[1], a.lo[2]}, hi[3] = {a.hi[0], a.hi[1], a.hi[2]};
+      int c[3] = {i + L::cx(q), j + L::cy(q), k + L::cz(q)};
       bool skip = false;
 #pragma unroll
       for (int d = 0; d < L::D; ++d) {
-        if (c[d] < lo[d] || c[d] > hi[d]) {
-          if (a.periodic[d]) c[d] = (c[d] < lo[d]) ? c[d] + nn[d] : c[d] - nn[d];
+        if (c[d] < a.dlo[d] || c[d] > a.dhi[d]) {
+          if (a.periodic[d]) c[d] = (c[d] < a.dlo[d]) ? c[d] + nn[d] : c[d] - nn[d];
           else skip = true;
         }
       }
       if (skip) continue;
+      if (L::D != 3) c[2] = 0;
       const double xn = X::add(a.plo[0], X::mul(X::add(double(c[0]), 0.5), a.dx[0]));
       const double yn = X::add(a.plo[1], X::mul(X::add(double(c[1]), 0.5), a.dx[1]));
       const double zn = (L::D == 3) ? X::add(a.plo[2], X::mul(X::add(double(c[2]), 0.5), a.dx[2])) : 0.0;
       if (!(sdist(a, L::D, xn, yn, zn) <= 0.0)) continue;
-      const double fo = load(i, j, k, q);
+      const double fo = load(B, i, j, k, q);
       double dm;
-      if (a.one_sided) dm = X::mul(2.0, fo);
-      else dm = X::add(fo, load(c[0], c[1], L::D == 3 ? c[2] : 0, opposite<L>(q)));
+      if (a.one_sided) {
+        dm = X::mul(2.0, fo);
+      } else {
+        int src = box_holds(B, L::D, c[0], c[1], c[2], 0) ? bi : -1;
+        for (int b = 0; b < a.nbox && src < 0; ++b)
+          if (box_holds(boxes[b], L::D, c[0], c[1], c[2], 0)) src = b;
+        if (src < 0 && box_holds(B, L::D, c[0], c[1], c[2], B.lo[0] - B.fgl[0])) src = bi;
+        if (src < 0) continue;
+        dm = X::add(fo, load(boxes[src], c[0], c[1], c[2], opposite<L>(q)));
+      }
       acc[0] += dm * double(L::cx(q));
       acc[1] += dm * double(L::cy(q));
       acc[2] += dm * double(L::cz(q));
@@ -157,8 +237,9 @@ __global__ void __launch_bounds__(kRedThreads) k_me_partial(MEArgs a, const void
 }
 
 template <class L, int S>
-int launch_me(ilbm_ctx *ctx, const MEArgs &a, const void *f, double *partial) {
-  k_me_partial<L, S><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(a, f, partial);
+int launch_me(ilbm_ctx *ctx, const MEArgs &a, const MEBox *boxes, const int64_t *off,
+              double *partial) {
+  k_me_partial<L, S><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(a, boxes, off, partial);
   ctx->launches++;
   return ILBM_OK;
 }
@@ -167,14 +248,14 @@ int launch_me(ilbm_ctx *ctx, const MEArgs &a, const void *f, double *partial) {
 
 extern "C" {
 
-int ilbm_force_integrals(ilbm_ctx *ctx, const ilbm_box *box, const void *force, const int lo[3],
+int ilbm_force_integrals(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const int lo[3],
                          const int hi[3], double out_sum[3]) {
-  if (!ctx || !box || !force || !out_sum) {
+  if (!ctx || !boxes || nbox < 1 || !out_sum) {
     set_error("ilbm_force_integrals: null argument");
     return ILBM_ERR_ARG;
   }
   double *d_sum = nullptr;
-  int rc = force_sum_enqueue(ctx, box, force, lo, hi, &d_sum);
+  int rc = force_sum_enqueue(ctx, boxes, nbox, lo, hi, &d_sum);
   if (rc) return rc;
   cudaMemcpyAsync(ctx->host_pinned, d_sum, 3 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
@@ -187,8 +268,9 @@ int ilbm_force_integrals(ilbm_ctx *ctx, const ilbm_box *box, const void *force, 
 
 namespace ilbm {
 
-int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *box, const void *force, const int lo[3],
-                      const int hi[3], double **d_sum) {
+// valid cells of `box` inside [lo, hi] (NULL: the whole box)
+static RegionArgs clip_region(const ilbm_ctx *ctx, const ilbm_box &box, const int lo[3],
+                              const int hi[3]) {
   RegionArgs a;
   std::memset(&a, 0, sizeof(a));
   a.dim = ctx->dim;
@@ -199,30 +281,70 @@ int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *box, const void *force, con
       a.mgl[d] = 0;
       continue;
     }
-    const int l = std::max(lo ? lo[d] : box->lo[d], box->lo[d]);
-    const int h = std::min(hi ? hi[d] : box->hi[d], box->hi[d]);
+    const int l = std::max(lo ? lo[d] : box.lo[d], box.lo[d]);
+    const int h = std::min(hi ? hi[d] : box.hi[d], box.hi[d]);
     a.lo[d] = l;
     a.n[d] = std::max(0, h - l + 1);
-    a.mgl[d] = box->lo[d] - box->ngrow_m;
+    a.mgl[d] = box.lo[d] - box.ngrow_m;
   }
-  a.ms0 = box->mstride[0];
-  a.ms1 = box->mstride[1];
-  a.ms2 = box->mstride[2];
-  double *scr = static_cast<double *>(ilbm_ctx_scratch(ctx, (kRedBlocks * 3 + 16) * sizeof(double)));
+  a.ms0 = box.mstride[0];
+  a.ms1 = box.mstride[1];
+  a.ms2 = box.mstride[2];
+  return a;
+}
+
+int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const int lo[3],
+                      const int hi[3], double **d_sum) {
+  std::vector<SumRegion> regs;
+  std::vector<int64_t> off(1, 0);
+  for (int b = 0; b < nbox; ++b) {
+    if (!boxes[b].force) {
+      set_error("ilbm_force_integrals: box->force (the array to integrate) is required");
+      return ILBM_ERR_ARG;
+    }
+    const RegionArgs a = clip_region(ctx, boxes[b], lo, hi);
+    const int64_t cells = (int64_t)a.n[0] * a.n[1] * a.n[2];
+    if (cells == 0) continue;
+    regs.push_back({a, boxes[b].force});
+    off.push_back(off.back() + cells);
+  }
+  const int nregs = (int)regs.size();
+  // partials, the result (+ a record slot after it), then the region table
+  const size_t head = (size_t)kRedBlocks * 3 + 16;
+  const size_t table = nregs > 1 ? nregs * sizeof(SumRegion) + (nregs + 1) * sizeof(int64_t) : 0;
+  double *scr = static_cast<double *>(ilbm_ctx_scratch(ctx, head * sizeof(double) + table + 16));
   if (!scr) {
     set_error("ilbm_force_integrals: scratch allocation failed");
     return ILBM_ERR_NOMEM;
   }
   *d_sum = scr + kRedBlocks * 3;
-  if ((int64_t)a.n[0] * a.n[1] * a.n[2] == 0) {
+  if (nregs == 0) {
     cudaError_t e = cudaMemsetAsync(*d_sum, 0, 3 * sizeof(double), ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals");
     return ILBM_OK;
   }
-  if (ctx->storage == ILBM_STORAGE_F64)
-    k_force_partial<double><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(a, static_cast<const double *>(force), scr);
-  else
-    k_force_partial<float><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(a, static_cast<const float *>(force), scr);
+  const bool f64 = ctx->storage == ILBM_STORAGE_F64;
+  if (nregs == 1) {
+    if (f64)
+      k_force_partial<double><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(
+          regs[0].a, static_cast<const double *>(regs[0].F), scr);
+    else
+      k_force_partial<float><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(
+          regs[0].a, static_cast<const float *>(regs[0].F), scr);
+  } else {
+    SumRegion *d_regs = reinterpret_cast<SumRegion *>(scr + head);
+    int64_t *d_off = reinterpret_cast<int64_t *>(d_regs + nregs);
+    cudaError_t e = cudaMemcpyAsync(d_regs, regs.data(), nregs * sizeof(SumRegion),
+                                    cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(d_off, off.data(), (nregs + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
+                          ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals: region table");
+    if (f64)
+      k_force_partial_multi<double><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(d_regs, nregs, d_off, scr);
+    else
+      k_force_partial_multi<float><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(d_regs, nregs, d_off, scr);
+  }
   k_final_sum<<<1, 32, 0, ctx->stream>>>(scr, kRedBlocks, *d_sum);
   ctx->launches += 2;
   cudaError_t e = cudaGetLastError();
@@ -234,63 +356,94 @@ int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *box, const void *force, con
 
 extern "C" {
 
-int ilbm_momentum_exchange(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
-                           const void *f, double x0, double y0, double z0, double R,
+int ilbm_momentum_exchange(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox,
+                           const ilbm_level_params *p, double x0, double y0, double z0, double R,
                            const double prob_lo[3], const double dx[3], int one_sided,
                            double out[3]) {
-  if (!ctx || !box || !p || !f || !out || !prob_lo || !dx) {
+  if (!ctx || !boxes || nbox < 1 || !p || !out || !prob_lo || !dx) {
     set_error("ilbm_momentum_exchange: null argument");
     return ILBM_ERR_ARG;
   }
-  for (int d = 0; d < ctx->dim; ++d)
-    if (box->lo[d] != p->domain_lo[d] || box->hi[d] != p->domain_hi[d]) {
-      set_error("ilbm_momentum_exchange: the box must cover the level domain");
-      return ILBM_ERR_ARG;
-    }
   MEArgs a;
   std::memset(&a, 0, sizeof(a));
   for (int d = 0; d < 3; ++d) {
     const bool use = d < ctx->dim;
-    a.lo[d] = use ? box->lo[d] : 0;
-    a.hi[d] = use ? box->hi[d] : 0;
-    a.fgl[d] = use ? box->lo[d] - box->ngrow_f : 0;
+    a.dlo[d] = use ? p->domain_lo[d] : 0;
+    a.dhi[d] = use ? p->domain_hi[d] : 0;
     a.periodic[d] = use ? p->periodic[d] : 0;
     a.plo[d] = prob_lo[d];
     a.dx[d] = dx[d];
   }
-  a.fs0 = box->fstride[0];
-  a.fs1 = box->fstride[1];
-  a.fs2 = box->fstride[2];
   a.x0 = x0;
   a.y0 = y0;
   a.z0 = (ctx->dim == 3) ? z0 : 0.0;
   a.R = R;
   a.one_sided = one_sided;
   a.f16_scale = (p->f16_scale > 0) ? float(p->f16_scale) : 1024.0f;
-  double *scr = static_cast<double *>(ilbm_ctx_scratch(ctx, (kRedBlocks * 3 + 8) * sizeof(double)));
+  a.nbox = nbox;
+  std::vector<MEBox> mb(nbox);
+  std::vector<int64_t> off(nbox + 1, 0);
+  for (int b = 0; b < nbox; ++b) {
+    const ilbm_box &x = boxes[b];
+    if (!x.f_in) {
+      set_error("ilbm_momentum_exchange: box->f_in is required");
+      return ILBM_ERR_ARG;
+    }
+    int64_t cells = 1;
+    for (int d = 0; d < 3; ++d) {
+      const bool use = d < ctx->dim;
+      mb[b].lo[d] = use ? x.lo[d] : 0;
+      mb[b].hi[d] = use ? x.hi[d] : 0;
+      mb[b].fgl[d] = use ? x.lo[d] - x.ngrow_f : 0;
+      cells *= (int64_t)(mb[b].hi[d] - mb[b].lo[d] + 1);
+    }
+    if (cells <= 0) {
+      set_error("ilbm_momentum_exchange: empty box");
+      return ILBM_ERR_ARG;
+    }
+    mb[b].fs0 = x.fstride[0];
+    mb[b].fs1 = x.fstride[1];
+    mb[b].fs2 = x.fstride[2];
+    mb[b].f = x.f_in;
+    off[b + 1] = off[b] + cells;
+  }
+  const size_t head = (size_t)kRedBlocks * 3 + 8;
+  char *scr = static_cast<char *>(ilbm_ctx_scratch(
+      ctx, head * sizeof(double) + nbox * sizeof(MEBox) + (nbox + 1) * sizeof(int64_t)));
   if (!scr) {
     set_error("ilbm_momentum_exchange: scratch allocation failed");
     return ILBM_ERR_NOMEM;
   }
+  double *part = reinterpret_cast<double *>(scr);
+  MEBox *d_boxes = reinterpret_cast<MEBox *>(scr + head * sizeof(double));
+  int64_t *d_off = reinterpret_cast<int64_t *>(d_boxes + nbox);
+  cudaError_t e = cudaMemcpyAsync(d_boxes, mb.data(), nbox * sizeof(MEBox), cudaMemcpyHostToDevice,
+                                  ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_off, off.data(), (nbox + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
+                        ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_momentum_exchange: box table");
   int rc;
   switch (ctx->q * 4 + ctx->storage) {
-    case 9 * 4 + 0: rc = launch_me<Lat<9>, 0>(ctx, a, f, scr); break;
-    case 9 * 4 + 1: rc = launch_me<Lat<9>, 1>(ctx, a, f, scr); break;
-    case 9 * 4 + 2: rc = launch_me<Lat<9>, 2>(ctx, a, f, scr); break;
-    case 19 * 4 + 0: rc = launch_me<Lat<19>, 0>(ctx, a, f, scr); break;
-    case 19 * 4 + 1: rc = launch_me<Lat<19>, 1>(ctx, a, f, scr); break;
-    case 19 * 4 + 2: rc = launch_me<Lat<19>, 2>(ctx, a, f, scr); break;
-    case 27 * 4 + 0: rc = launch_me<Lat<27>, 0>(ctx, a, f, scr); break;
-    case 27 * 4 + 1: rc = launch_me<Lat<27>, 1>(ctx, a, f, scr); break;
-    case 27 * 4 + 2: rc = launch_me<Lat<27>, 2>(ctx, a, f, scr); break;
+    case 9 * 4 + 0: rc = launch_me<Lat<9>, 0>(ctx, a, d_boxes, d_off, part); break;
+    case 9 * 4 + 1: rc = launch_me<Lat<9>, 1>(ctx, a, d_boxes, d_off, part); break;
+    case 9 * 4 + 2: rc = launch_me<Lat<9>, 2>(ctx, a, d_boxes, d_off, part); break;
+    case 19 * 4 + 0: rc = launch_me<Lat<19>, 0>(ctx, a, d_boxes, d_off, part); break;
+    case 19 * 4 + 1: rc = launch_me<Lat<19>, 1>(ctx, a, d_boxes, d_off, part); break;
+    case 19 * 4 + 2: rc = launch_me<Lat<19>, 2>(ctx, a, d_boxes, d_off, part); break;
+    case 27 * 4 + 0: rc = launch_me<Lat<27>, 0>(ctx, a, d_boxes, d_off, part); break;
+    case 27 * 4 + 1: rc = launch_me<Lat<27>, 1>(ctx, a, d_boxes, d_off, part); break;
+    case 27 * 4 + 2: rc = launch_me<Lat<27>, 2>(ctx, a, d_boxes, d_off, part); break;
     default: set_error("unsupported lattice/storage"); return ILBM_ERR_UNSUPPORTED;
   }
   if (rc) return rc;
-  k_final_sum<<<1, 32, 0, ctx->stream>>>(scr, kRedBlocks, scr + kRedBlocks * 3);
+  k_final_sum<<<1, 32, 0, ctx->stream>>>(part, kRedBlocks, part + kRedBlocks * 3);
   ctx->launches++;
-  cudaMemcpyAsync(ctx->host_pinned, scr + kRedBlocks * 3, 3 * sizeof(double),
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_momentum_exchange");
+  cudaMemcpyAsync(ctx->host_pinned, part + kRedBlocks * 3, 3 * sizeof(double),
                   cudaMemcpyDeviceToHost, ctx->stream);
-  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "ilbm_momentum_exchange");
   for (int c = 0; c < 3; ++c) out[c] = -ctx->host_pinned[c];
   return ILBM_OK;

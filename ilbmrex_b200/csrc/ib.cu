@@ -34,6 +34,10 @@ namespace cgrp = cooperative_groups;
 namespace ilbm {
 int band_macro(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p, const int *blo,
                const int *bn, double *EV, double *RHO, cudaStream_t st);
+int box_step_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p,
+                  StepArgs *out);
+int band_macro_boxes(ilbm_ctx *ctx, const StepArgs *d_args, int nargs, const int *blo,
+                     const int *bn, double *EV, double *RHO, cudaStream_t st);
 int level_step_split(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p,
                      const int *blo, const int *bhi, cudaEvent_t band_ready);
 }
@@ -1294,6 +1298,61 @@ __global__ void k_export(IBArgs a, const double *EFT, const double *RHO, R *F, i
     export_cell<R>(a, EFT, RHO, F, mgl0, mgl1, mgl2, ms0, ms1, ms2, t);
 }
 
+// export to a level held in several boxes: the force of a band cell goes to
+// the box whose valid region holds it (cells no box holds are dropped, as
+// the reference's SumBoundary drops spread force outside the level's valid
+// cells, IBMarkerDF.cpp:1511) and, as FillBoundary of the force before the
+// collision does (Source/Core/AdvanceLBMAtLevel.cpp:187-194), to every box
+// whose grown force array holds the cell or one of its periodic images as a
+// ghost.
+template <class R>
+__global__ void k_export_boxes(IBArgs a, const double *EFT, const double *RHO,
+                               const StepArgs *__restrict__ args, int nargs) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < a.nb;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int g[3] = {a.blo[0] + (int)(t % a.bn[0]), a.blo[1] + (int)((t / a.bn[0]) % a.bn[1]),
+                      a.blo[2] + (int)(t / ((int64_t)a.bn[0] * a.bn[1]))};
+    bool inside = true;
+    for (int d = 0; d < a.dim; ++d) inside = inside && g[d] >= a.dlo[d] && g[d] <= a.dhi[d];
+    if (!inside) continue;
+    bool owned = false;
+    for (int b = 0; b < nargs && !owned; ++b) {
+      const StepArgs &x = args[b];
+      owned = g[0] >= x.lo[0] && g[0] <= x.hi[0] && g[1] >= x.lo[1] && g[1] <= x.hi[1] &&
+              (a.dim == 2 || (g[2] >= x.lo[2] && g[2] <= x.hi[2]));
+    }
+    if (!owned) continue;
+    const double dr = X::mul(a.dt, RHO[t]);
+    const R fx = R(X::mul(dr, EFT[t])), fy = R(X::mul(dr, EFT[t + a.nb]));
+    const R fz = R(a.dim == 3 ? X::mul(dr, EFT[t + 2 * a.nb]) : 0.0);
+    // shifts by whole domain lengths along periodic directions (0 included)
+    const int n[3] = {a.dhi[0] - a.dlo[0] + 1, a.dhi[1] - a.dlo[1] + 1, a.dhi[2] - a.dlo[2] + 1};
+    for (int s = 0; s < 27; ++s) {
+      const int sh[3] = {s % 3 - 1, (s / 3) % 3 - 1, s / 9 - 1};
+      bool ok = true;
+      for (int d = 0; d < 3; ++d)
+        if (sh[d] != 0 && (d >= a.dim || !a.periodic[d])) ok = false;
+      if (!ok) continue;
+      const int c[3] = {g[0] + sh[0] * n[0], g[1] + sh[1] * n[1], g[2] + sh[2] * n[2]};
+      for (int b = 0; b < nargs; ++b) {
+        const StepArgs &x = args[b];
+        bool in = true;
+        for (int d = 0; d < a.dim; ++d) {
+          const int w = x.lo[d] - x.mgl[d];
+          in = in && c[d] >= x.lo[d] - w && c[d] <= x.hi[d] + w;
+        }
+        if (!in) continue;
+        R *F = static_cast<R *>(const_cast<void *>(x.force));
+        const int64_t m = (int64_t)(c[0] - x.mgl[0]) + (int64_t)(c[1] - x.mgl[1]) * x.ms0 +
+                          (int64_t)(a.dim == 3 ? c[2] - x.mgl[2] : 0) * x.ms1;
+        F[m] = fx;
+        F[m + x.ms2] = fy;
+        if (a.dim == 3) F[m + 2 * x.ms2] = fz;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1331,6 +1390,10 @@ struct ilbm_ib {
   double *d_Ainv = nullptr, *d_gj = nullptr, *d_rhs = nullptr;
   float *d_Ainv32 = nullptr;  // FP32 copy of A^-1 for the 4- and 2-byte storage forms
   bool fsum_deferred = false;  // marker force sum still to be launched (ib_finish)
+  // a level held in several boxes: the StepArgs of the boxes near the band
+  std::vector<StepArgs> h_boxargs;
+  StepArgs *d_boxargs = nullptr;
+  int boxargs_cap = 0;
   std::vector<void *> allocs;
 };
 
@@ -1791,36 +1854,102 @@ static int launch_cg(ilbm_ib *ib, const IBArgs &a_in, cudaStream_t s) {
 // defer_sum: with one MDF iteration, leave the marker force sum (which only
 // the force evaluation reads) to ib_finish, so it can run after the exported
 // force has been handed to the level step
-static int ib_update(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *lp, double dt,
-                     double time, cudaStream_t s, bool defer_sum) {
-  if (!ib || !box || !box->force) {
-    set_error("ilbm_ib_update_forcing: ib, box and box->force are required");
+// boxes of a level whose grown arrays meet the body's band (or a periodic
+// image of it): their StepArgs go to ib->d_boxargs (stream-ordered on s)
+static int ib_box_table(ilbm_ib *ib, const ilbm_box *boxes, int nbox, const ilbm_level_params *lp,
+                        cudaStream_t s) {
+  ilbm_ctx *ctx = ib->ctx;
+  ib->h_boxargs.clear();
+  for (int b = 0; b < nbox; ++b) {
+    const ilbm_box &x = boxes[b];
+    if (!x.force) {
+      set_error("ilbm_ib_update_forcing: every box needs its force array");
+      return ILBM_ERR_ARG;
+    }
+    if (!x.macro_in && !x.f_in) {
+      set_error("ilbm_ib_update_forcing: every box needs macro_in or f_in");
+      return ILBM_ERR_ARG;
+    }
+    const int w = std::max(x.ngrow_f, x.ngrow_m);
+    bool meets = false;
+    for (int m = 0; m < 27 && !meets; ++m) {
+      const int sh[3] = {m % 3 - 1, (m / 3) % 3 - 1, m / 9 - 1};
+      bool ok = true, hit = true;
+      for (int d = 0; d < 3; ++d) {
+        if (sh[d] != 0 && (d >= ib->dim || !ib->g.periodic[d])) ok = false;
+        if (d >= ib->dim) continue;
+        const int lo = ib->blo[d] + sh[d] * ib->g.n_cell[d], hi = lo + ib->bn[d] - 1;
+        hit = hit && hi >= x.lo[d] - w && lo <= x.hi[d] + w;
+      }
+      meets = ok && hit;
+    }
+    if (!meets) continue;
+    StepArgs a;
+    int rc = box_step_args(ctx, x, lp, &a);
+    if (rc) return rc;
+    ib->h_boxargs.push_back(a);
+  }
+  const int n = (int)ib->h_boxargs.size();
+  if (n > ib->boxargs_cap) {
+    const int cap = std::max(n, 2 * ib->boxargs_cap);
+    int rc = dmalloc(ib, &ib->d_boxargs, (size_t)cap);
+    if (rc) return rc;
+    ib->boxargs_cap = cap;
+  }
+  if (n > 0) {
+    cudaError_t e = cudaMemcpyAsync(ib->d_boxargs, ib->h_boxargs.data(), n * sizeof(StepArgs),
+                                    cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_fail(e, "ilbm_ib_update_forcing: box table");
+  }
+  return ILBM_OK;
+}
+
+static int ib_update(ilbm_ib *ib, const ilbm_box *boxes, int nbox, const ilbm_level_params *lp,
+                     double dt, double time, cudaStream_t s, bool defer_sum) {
+  if (!ib || !boxes || nbox < 1 || !lp) {
+    set_error("ilbm_ib_update_forcing: ib, boxes (nbox >= 1) and level params are required");
     return ILBM_ERR_ARG;
   }
   ilbm_ctx *ctx = ib->ctx;
-  // one box per level: the whole domain, or (a fine box of a two-level
-  // hierarchy) a box whose valid cells hold the body's whole support band,
-  // so every band cell the IB reads or writes lies inside the box's arrays
-  bool whole = true, holds_band = true;
+  const ilbm_box *box = boxes;
+  // One box: the whole domain, or a box whose valid cells hold the body's
+  // whole support band (the fine box of a two-level hierarchy), so every
+  // band cell the IB reads or writes lies inside the box's arrays.  Any
+  // other level takes the box-table path (caller-filled ghosts).
+  bool whole = nbox == 1, holds_band = nbox == 1;
   for (int d = 0; d < ib->dim; ++d) {
     whole = whole && box->lo[d] == 0 && box->hi[d] == ib->g.n_cell[d] - 1;
     holds_band = holds_band && ib->blo[d] >= box->lo[d] && ib->blo[d] + ib->bn[d] - 1 <= box->hi[d];
   }
-  if (!whole && !holds_band) {
-    set_error("ilbm_ib_update_forcing: the box must cover the level domain, or hold the body's "
-              "whole support band in its valid cells");
+  const bool multi = !whole && !holds_band;
+  if (multi && lp->ghost_mode != ILBM_GHOST_CALLER) {
+    set_error("ilbm_ib_update_forcing: a level that is not one box holding the body's support "
+              "band needs caller-filled ghosts (ILBM_GHOST_CALLER)");
     return ILBM_ERR_ARG;
   }
-  if (box->macro_in && box->ngrow_m < 2) {
-    set_error("ilbm_ib_update_forcing: macro_in needs at least two filled ghost layers");
-    return ILBM_ERR_ARG;
+  for (int b = 0; b < nbox; ++b) {
+    if (!boxes[b].force) {
+      set_error("ilbm_ib_update_forcing: box->force is required");
+      return ILBM_ERR_ARG;
+    }
+    if (boxes[b].macro_in && boxes[b].ngrow_m < 2) {
+      set_error("ilbm_ib_update_forcing: macro_in needs at least two filled ghost layers");
+      return ILBM_ERR_ARG;
+    }
+    if (!boxes[b].macro_in && !boxes[b].f_in) {
+      set_error("ilbm_ib_update_forcing: need macro_in or f_in");
+      return ILBM_ERR_ARG;
+    }
   }
-  if (!box->macro_in && !box->f_in) {
-    set_error("ilbm_ib_update_forcing: need macro_in or f_in");
-    return ILBM_ERR_ARG;
+  // EulerVel / rho on the band (:1541-1566, FillBoundary :702-703)
+  int rc;
+  if (multi) {
+    if ((rc = ib_box_table(ib, boxes, nbox, lp, s))) return rc;
+    rc = band_macro_boxes(ctx, ib->d_boxargs, (int)ib->h_boxargs.size(), ib->blo, ib->bn, ib->d_EV,
+                          ib->d_RHO, s);
+  } else {
+    rc = band_macro(ctx, *box, lp, ib->blo, ib->bn, ib->d_EV, ib->d_RHO, s);
   }
-  // EulerVel / rho on the band (:1541-1566)
-  int rc = band_macro(ctx, *box, lp, ib->blo, ib->bn, ib->d_EV, ib->d_RHO, s);
   if (rc) return rc;
   IBArgs a = make_args(ib, dt, time);
   const int nthr = 128, nblk = (ib->n + nthr - 1) / nthr;
@@ -1910,7 +2039,13 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *
   const double *EFT = single ? ib->d_EFI : ib->d_EFT;
   const int mgl0 = box->lo[0] - box->ngrow_m, mgl1 = box->lo[1] - box->ngrow_m;
   const int mgl2 = (ib->dim == 3) ? box->lo[2] - box->ngrow_m : 0;
-  if (ctx->storage == ILBM_STORAGE_F64)
+  if (multi) {
+    const int nargs = (int)ib->h_boxargs.size();
+    if (ctx->storage == ILBM_STORAGE_F64)
+      k_export_boxes<double><<<gb, 256, 0, s>>>(a, EFT, ib->d_RHO, ib->d_boxargs, nargs);
+    else
+      k_export_boxes<float><<<gb, 256, 0, s>>>(a, EFT, ib->d_RHO, ib->d_boxargs, nargs);
+  } else if (ctx->storage == ILBM_STORAGE_F64)
     k_export<double><<<gb, 256, 0, s>>>(a, EFT, ib->d_RHO, static_cast<double *>(box->force),
                                         mgl0, mgl1, mgl2, box->mstride[0], box->mstride[1], box->mstride[2]);
   else
@@ -1954,7 +2089,7 @@ int advance_begin(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p
   for (int d = 0; d < ctx->dim; ++d)
     band_inside = band_inside && sp->lo[d] >= box->lo[d] && sp->hi[d] <= box->hi[d];
   sp->serial = (p->ghost_mode != ILBM_GHOST_SELF && !band_inside);
-  if (sp->serial) return ib_update(ib, box, &sp->q, dt, time, ctx->stream, false);
+  if (sp->serial) return ib_update(ib, box, 1, &sp->q, dt, time, ctx->stream, false);
   // validate like ilbm_level_step does before anything is launched
   if ((p->ghost_mode == ILBM_GHOST_SELF && box->lo[0] != p->domain_lo[0]) || box->f_in == box->f_out) {
     set_error("ilbm_advance_level: self-fill needs one box equal to the domain, f_in != f_out");
@@ -1965,7 +2100,7 @@ int advance_begin(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p
   cudaError_t e = cudaEventRecord(ctx->ev_fork, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0);
   if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level fork");
-  int rc = ib_update(ib, box, &sp->q, dt, time, ctx->side, true);
+  int rc = ib_update(ib, box, 1, &sp->q, dt, time, ctx->side, true);
   if (rc) return rc;
   e = cudaEventRecord(ctx->ev_join, ctx->side);
   if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_level join");
@@ -1991,13 +2126,13 @@ int advance_end(ilbm_ctx *ctx, const ilbm_box *box, const AdvanceSplit *sp) {
 
 extern "C" {
 
-int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *lp,
-                           double dt, double time) {
+int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *boxes, int nbox,
+                           const ilbm_level_params *lp, double dt, double time) {
   if (!ib) {
     set_error("ilbm_ib_update_forcing: null ib");
     return ILBM_ERR_ARG;
   }
-  return ib_update(ib, box, lp, dt, time, ib->ctx->stream, false);
+  return ib_update(ib, boxes, nbox, lp, dt, time, ib->ctx->stream, false);
 }
 
 int ilbm_advance_level(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
@@ -2041,9 +2176,9 @@ int ilbm_ib_last_marker_force_sum(ilbm_ib *ib, double out[3]) {
   return ILBM_OK;
 }
 
-int ilbm_force_record_async(ilbm_ctx *ctx, const ilbm_box *box, const void *force, ilbm_ib *ib,
+int ilbm_force_record_async(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, ilbm_ib *ib,
                             const int lo[3], const int hi[3], double *out) {
-  if (!ctx || !box || !force || !ib || !out) {
+  if (!ctx || !boxes || nbox < 1 || !ib || !out) {
     set_error("ilbm_force_record_async: null argument");
     return ILBM_ERR_ARG;
   }
@@ -2052,7 +2187,7 @@ int ilbm_force_record_async(ilbm_ctx *ctx, const ilbm_box *box, const void *forc
     return ILBM_ERR_ARG;
   }
   double *d_sum = nullptr;
-  int rc = force_sum_enqueue(ctx, box, force, lo, hi, &d_sum);
+  int rc = force_sum_enqueue(ctx, boxes, nbox, lo, hi, &d_sum);
   if (rc) return rc;
   double *d_rec = d_sum + 8;  // spare scratch after the sums
   k_record_pack<<<1, 32, 0, ctx->stream>>>(d_sum, ib->d_fsum, ib->d_status, d_rec);

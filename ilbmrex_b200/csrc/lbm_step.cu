@@ -858,6 +858,71 @@ __global__ void __launch_bounds__(256) k_band_macro_batch(const StepArgs *args, 
   }
 }
 
+// Band macro of a level held in several boxes (caller-filled ghosts), the
+// EulerVel of IBMarkerDF::update_forcing (Source/IBM/IBMarkerDF.cpp:1541-1566)
+// followed by its FillBoundary (:702-703): a band cell takes rho, u from the
+// box whose valid region holds it; a cell that no box holds (a coarse-fine or
+// physical ghost of the level) takes the caller-filled ghost value of the
+// first box whose grown arrays reach it; a cell that none reaches gets the
+// reference's initial EulerVel, zero velocity (and unit density).
+template <class L>
+__device__ __forceinline__ bool valid_at(const StepArgs &a, int i, int j, int k) {
+  return i >= a.lo[0] && i <= a.hi[0] && j >= a.lo[1] && j <= a.hi[1] &&
+         (L::D == 2 || (k >= a.lo[2] && k <= a.hi[2]));
+}
+
+// the cell can be read from the box's grown arrays: macro_in grown by
+// ngrow_m, else f_in and force_prev grown by the smaller of their widths
+template <class L>
+__device__ __forceinline__ bool readable_at(const StepArgs &a, int i, int j, int k) {
+  const int g[3] = {i, j, k};
+#pragma unroll
+  for (int d = 0; d < L::D; ++d) {
+    const int gm = a.lo[d] - a.mgl[d], gf = a.lo[d] - a.fgl[d];
+    const int w = a.macro_in ? gm : min(gm, gf);
+    if (g[d] < a.lo[d] - w || g[d] > a.hi[d] + w) return false;
+  }
+  return true;
+}
+
+template <class L, int S>
+__global__ void __launch_bounds__(256) k_band_macro_boxes(const StepArgs *__restrict__ args, int nargs,
+                                                          int blo0, int blo1, int blo2, int bn0,
+                                                          int bn1, int bn2, double *EV, double *RHO) {
+  const int64_t nb = (int64_t)bn0 * bn1 * bn2;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nb;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = blo0 + (int)(t % bn0);
+    const int j = blo1 + (int)((t / bn0) % bn1);
+    const int k = (L::D == 3) ? blo2 + (int)(t / ((int64_t)bn0 * bn1)) : 0;
+    int src = -1;
+    for (int b = 0; b < nargs && src < 0; ++b)
+      if (valid_at<L>(args[b], i, j, k)) src = b;
+    for (int b = 0; b < nargs && src < 0; ++b)
+      if (readable_at<L>(args[b], i, j, k)) src = b;
+    double m4[4] = {1.0, 0.0, 0.0, 0.0};
+    if (src >= 0) macro_at<L, S>(args[src], i, j, k, m4);
+    EV[t] = m4[1];
+    EV[t + nb] = m4[2];
+    EV[t + 2 * nb] = (L::D == 3) ? m4[3] : 0.0;
+    RHO[t] = m4[0];
+  }
+}
+
+template <class L, int S>
+static int launch_band_macro_boxes(ilbm_ctx *ctx, const StepArgs *d_args, int nargs,
+                                   const int *blo, const int *bn, double *EV, double *RHO,
+                                   cudaStream_t st) {
+  const int64_t nb = (int64_t)bn[0] * bn[1] * bn[2];
+  const int blocks = (int)std::min<int64_t>((nb + 255) / 256, 2048);
+  k_band_macro_boxes<L, S><<<blocks, 256, 0, st>>>(d_args, nargs, blo[0], blo[1], blo[2], bn[0],
+                                                   bn[1], bn[2], EV, RHO);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "band macro launch");
+  return ILBM_OK;
+}
+
 template <class L, int S>
 static int launch_band_macro(ilbm_ctx *ctx, const StepArgs &a, const int *blo, const int *bn,
                              double *EV, double *RHO, cudaStream_t st) {
@@ -1124,6 +1189,18 @@ int band_macro(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p, con
   int rc = fill_args(ctx, b, p, a);
   if (rc) return rc;
   return ILBM_DISPATCH(ctx, launch_band_macro, ctx, a, blo, bn, EV, RHO, st);
+}
+
+// StepArgs of one box of a level, for kernels that take several boxes
+int box_step_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p,
+                  StepArgs *out) {
+  return fill_args(ctx, b, p, *out);
+}
+
+// Band macro over several boxes whose StepArgs are in device memory.
+int band_macro_boxes(ilbm_ctx *ctx, const StepArgs *d_args, int nargs, const int *blo,
+                     const int *bn, double *EV, double *RHO, cudaStream_t st) {
+  return ILBM_DISPATCH(ctx, launch_band_macro_boxes, ctx, d_args, nargs, blo, bn, EV, RHO, st);
 }
 
 // Level step with the band [blo,bhi] deferred until `band_ready`.

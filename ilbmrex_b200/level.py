@@ -344,10 +344,10 @@ class LevelSolver:
     # ---- force evaluation (ComputeIBForce, AmrCoreLBM.cpp:456-631) --------
     def compute_ib_force(self):
         lo, hi = self.force_region
-        b = self._box(self.f, None)
+        b = self._box(self.f, None, force=self.force_prev)
         s = (C.c_double * 3)()
-        capi.check(self.L.ilbm_force_integrals(self.ctx.h, C.byref(b), self.force_prev.data_ptr(),
-                                               capi.ivec3(lo), capi.ivec3(hi), s), "force_integrals")
+        capi.check(self.L.ilbm_force_integrals(self.ctx.h, C.byref(b), 1, capi.ivec3(lo),
+                                               capi.ivec3(hi), s), "force_integrals")
         m = (C.c_double * 3)()
         capi.check(self.L.ilbm_ib_last_marker_force_sum(self.ib, m), "marker_force_sum")
         self.rec = self.force_record(np.array([s[0], s[1], s[2]]), np.array([m[0], m[1], m[2]]))
@@ -600,8 +600,8 @@ class LevelSolver:
         b = self._box(self.f, None)
         out = (C.c_double * 3)()
         dx = [self.case.dx] * 3
-        capi.check(self.L.ilbm_momentum_exchange(self.ctx.h, C.byref(b), C.byref(self.params),
-                                                 self.f.data_ptr(), x0, y0, z0, R,
+        capi.check(self.L.ilbm_momentum_exchange(self.ctx.h, C.byref(b), 1, C.byref(self.params),
+                                                 x0, y0, z0, R,
                                                  capi.dvec3(self.case.prob_lo), capi.dvec3(dx),
                                                  int(one_sided), out), "momentum_exchange")
         return np.array([out[0], out[1], out[2]])

@@ -225,12 +225,30 @@ int ilbm_ib_destroy(ilbm_ib *ib);
 int ilbm_ib_num_markers(const ilbm_ib *ib, int64_t *n);
 /* Lower/upper corner (inclusive) of the cells whose force the IB may write. */
 int ilbm_ib_force_region(const ilbm_ib *ib, int lo[3], int hi[3]);
-/* update_forcing: reads rho,u (from box->macro_in incl. 2 ghost layers when
- * set, else from box->f_in + box->force_prev), writes box->force = dt*rho*a on
- * valid cells of the force region.  Cells of box->force outside that region
- * are not touched (keep them zero). */
-int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *box, const ilbm_level_params *p,
-                           double dt, double time);
+/* update_forcing on a level held in nbox boxes (IBMarkerDF::update_forcing,
+ * Source/IBM/IBMarkerDF.H:76-87, IBMarkerDF.cpp:1522-1917): reads rho, u of
+ * every cell of the body's support band and writes box->force = dt*rho*a on
+ * the valid cells of the force region (ilbm_ib_force_region).  Cells of the
+ * force arrays outside that region are not touched (keep them zero).
+ *   - One box that covers the level domain (self-filled or caller-filled
+ *     ghosts), or one box whose valid cells hold the whole band: rho, u come
+ *     from box->macro_in (two filled ghost layers) when set, else from f_in
+ *     and force_prev.
+ *   - Any other level (ILBM_GHOST_CALLER, e.g. an AMReX level cut by
+ *     max_grid_size): a band cell takes rho, u from the box whose valid
+ *     region holds it (the reference's EulerVel + FillBoundary,
+ *     IBMarkerDF.cpp:1541-1566, 702-703), else from the caller-filled ghost
+ *     of a box whose grown arrays reach it (macro_in grown by ngrow_m, or
+ *     f_in / force_prev).  The force of a band cell goes to its box and, as
+ *     the reference's FillBoundary of the force before the collision does
+ *     (Source/Core/AdvanceLBMAtLevel.cpp:187-194), into the ghost cells of
+ *     every other box whose grown force array holds the cell or a periodic
+ *     image of it; force spread outside every box's valid cells is dropped
+ *     (SumBoundary, IBMarkerDF.cpp:1511).  The boxes that meet the band are
+ *     copied to the device in stream order; their arrays must stay valid
+ *     until the call's work has run. */
+int ilbm_ib_update_forcing(ilbm_ib *ib, const ilbm_box *boxes, int nbox,
+                           const ilbm_level_params *p, double dt, double time);
 /* One whole AdvancePhiAtLevel of a level with an immersed body
  * (Source/Core/AdvanceLBMAtLevel.cpp:20-394): update_forcing into box->force,
  * then the level step with that force.  In self-fill mode the IB chain runs on
@@ -266,10 +284,15 @@ int ilbm_ib_set_ivc_solver(ilbm_ib *ib, int solver);
 int ilbm_ib_markers(ilbm_ib *ib, double *xyz, double *uvw, double *force);
 
 /* ---- force evaluation ---------------------------------------------------- */
-/* sum of the force array over valid cells of [lo,hi] (3 doubles, synchronous) */
-int ilbm_force_integrals(ilbm_ctx *ctx, const ilbm_box *box, const void *force,
-                         const int lo[3], const int hi[3], double out_sum[3]);
-/* The same sum as ilbm_force_integrals, for callers that cannot allocate
+/* Sum of boxes[b].force (3 components, the real type) over the valid cells of
+ * every box inside [lo, hi] (NULL: whole boxes); 3 doubles, synchronous.  The
+ * Eulerian forcing integral of ComputeIBForce is this sum times -dV/dt
+ * (Source/Core/AmrCoreLBM.cpp:489-509).  The summation order is fixed for a
+ * given list of boxes, so repeated calls return identical bits. */
+int ilbm_force_integrals(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const int lo[3],
+                         const int hi[3], double out_sum[3]);
+/* The same sum as ilbm_force_integrals over one box whose force array is
+ * `force`, for callers that cannot allocate
  * device memory while they run (no counterpart in the reference).  Hosts
  * such as AMReX reserve most of the device memory in their own arena at
  * start-up, serving loops admit work against a fixed memory budget, and
@@ -296,7 +319,8 @@ int ilbm_force_integrals_noalloc(ilbm_ctx *ctx, const ilbm_box *box, const void 
 /* The force record of a step, without synchronising (no counterpart in the
  * reference, whose ComputeIBForce returns the sums at once,
  * Source/Core/AmrCoreLBM.cpp:456-631): enqueues on the context's stream the
- * Eulerian sum of ilbm_force_integrals over [lo, hi] and copies it, the
+ * Eulerian sum of ilbm_force_integrals (boxes[b].force over [lo, hi]) and
+ * copies it, the
  * body's last marker force sum (ilbm_ib_last_marker_force_sum) and the body's
  * two status words into out[8] = {Eulerian sum (3), marker sum (3),
  * status word 0, status word 1}.  out should be pinned host memory (or device
@@ -307,11 +331,20 @@ int ilbm_force_integrals_noalloc(ilbm_ctx *ctx, const ilbm_box *box, const void 
  * the IVC operator's nonzero capacity, bit 2 CG not converged; word 1 bit 3 a
  * non-positive pivot of the stored inverse.  The next call on the context
  * reuses the record's device slot after this copy, in stream order. */
-int ilbm_force_record_async(ilbm_ctx *ctx, const ilbm_box *box, const void *force, ilbm_ib *ib,
+int ilbm_force_record_async(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, ilbm_ib *ib,
                             const int lo[3], const int hi[3], double *out);
-/* link-wise momentum exchange on f (IBForceEval); out = body force (3) */
-int ilbm_momentum_exchange(ilbm_ctx *ctx, const ilbm_box *box, const ilbm_level_params *p,
-                           const void *f, double x0, double y0, double z0, double R,
+/* Link-wise momentum exchange (IBForceEval::ComputeMomentumExchangeBodyForce,
+ * Source/IBM/IBForceEval.H:24-32, IBForceEval.cpp:28-191) on the populations
+ * boxes[b].f_in of a level held in nbox boxes, for a circle / sphere body
+ * (x0, y0, z0, R); out = the reaction force on the body (3, synchronous).
+ * Each fluid->solid link of a valid cell counts once; the opposite population
+ * of the solid cell comes from the box whose valid region holds it (the
+ * domain wrapped along periodic directions), else from the ghost layer of
+ * the cell's own box, and a link neither reaches is left out.  With one box
+ * covering the domain this is the reference's loop; summation order is
+ * fixed for a given list of boxes. */
+int ilbm_momentum_exchange(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox,
+                           const ilbm_level_params *p, double x0, double y0, double z0, double R,
                            const double prob_lo[3], const double dx[3], int one_sided,
                            double out[3]);
 
@@ -382,9 +415,41 @@ int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_lev
                            const ilbm_box *fine, const ilbm_level_params *pf, ilbm_ib *ib,
                            double dt, double time, int flags);
 /* average-down alone (InitData's AverageDown after the levels are made,
- * AmrCoreLBM.cpp:710-720): fine f_in / macro_in onto coarse f_in / macro_in */
+ * AmrCoreLBM.cpp:710-720): fine f_in / macro_in onto coarse f_in / macro_in,
+ * for any two adjacent levels of a hierarchy (the coarse one self-filled and
+ * equal to its domain, or one box in caller mode holding the fine box two
+ * coarse cells inside it) */
 int ilbm_average_down(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_params *pc,
                       const ilbm_box *fine, const ilbm_level_params *pf);
+
+/* ---- static hierarchy of any depth --------------------------------------
+ * nlev levels (2..8), one box each: level 0 equal to its domain
+ * (ILBM_GHOST_SELF), level l > 0 a box of the domain of level l-1 refined by
+ * 2 (ILBM_GHOST_CALLER, lo even and hi odd, coarsened at least two cells
+ * inside the box of level l-1), advanced as AmrCoreLBM::
+ * timeStepWithSubcycling does (Source/Core/AmrCoreLBM.cpp:1690-1755): a
+ * level's step by its dt (dt / 2^l), then two substeps of level l+1 at t and
+ * t + dt/2 whose ghost cells are filled from level l's macro fields at that
+ * time (as ilbm_advance_two_level's fine level), then the average-down of
+ * level l+1 onto level l (AverageDownTo, :1519-1527); recursively.  The body
+ * `ib` (or NULL) lives on the finest level, whose steps overlap its forcing
+ * chain with the cells outside its band.
+ * Buffers: every level with a finer one carries stored macro fields
+ * (macro_in, macro_out; kept on the finer box coarsened and grown by two
+ * cells after the first step); the finest level's f_in, and every finer
+ * level's f_in / macro_in, hold the new state on return (an even number of
+ * steps swaps them back); level 0's new state is in its f_out / macro_out and
+ * the caller swaps that pair.  force / force_prev of the finest level: the
+ * force of its last substep is in force_prev on return.  With flags
+ * ILBM_HIERARCHY_FIRST_STEP each level's first step reads its initial macro
+ * fields everywhere (after ilbm_init_equilibrium and ilbm_average_down from
+ * the finest level up).  nlev = 2 is the schedule of ilbm_advance_two_level
+ * without its overlap of the coarse step with the fine level's forcing.
+ * Asynchronous on the context's stream. */
+#define ILBM_HIERARCHY_FIRST_STEP 1
+int ilbm_advance_hierarchy(ilbm_ctx *ctx, int nlev, const ilbm_box *boxes,
+                           const ilbm_level_params *params, ilbm_ib *ib, double dt, double time,
+                           int flags);
 
 /* ---- state I/O ----------------------------------------------------------
  * Checkpoint and restart of one level box (and its immersed body): the

@@ -18,8 +18,15 @@ from ilbmrex_b200.level import Context, LevelSolver  # noqa: E402
 
 
 def _sum(L, fn, ctx, box, force_ptr, lo, hi):
+    """ilbm_force_integrals takes the force array in the box (a list of one
+    box here); the no-allocation entry point takes one box and the array."""
     out = (C.c_double * 3)()
-    rc = getattr(L, fn)(ctx, C.byref(box), force_ptr, capi.ivec3(lo), capi.ivec3(hi), out)
+    if fn == "ilbm_force_integrals":
+        b = capi.Box_t.from_buffer_copy(box)
+        b.force = force_ptr
+        rc = L.ilbm_force_integrals(ctx, C.byref(b), 1, capi.ivec3(lo), capi.ivec3(hi), out)
+    else:
+        rc = getattr(L, fn)(ctx, C.byref(box), force_ptr, capi.ivec3(lo), capi.ivec3(hi), out)
     return rc, np.array([out[0], out[1], out[2]])
 
 
