@@ -397,3 +397,147 @@ def sphere_two_level(nx=256, ny=128, nz=128, D=32.0, center=(64.0, 64.0, 64.0), 
     tl = TwoLevelCase(case, lo, hi, name=f"sphere{nx}x{ny}x{nz}_2lev")
     init_f = uniform_init(tl.fine_box(), 1.0, (U, 0.0, 0.0))
     return tl, ib, init_c, init_f
+
+
+@dataclass
+class HierarchyCase:
+    """A coarse level equal to the domain and one fixed box on each finer
+    level (refinement ratio 2 between levels): ``boxes[l - 1]`` = (lo, hi) of
+    level l in that level's own cell indices (lo even, hi odd; coarsened, at
+    least two cells inside the box of level l - 1, or inside the domain for
+    level 1).  Each level steps twice per step of the level above
+    (timeStepWithSubcycling, Source/Core/AmrCoreLBM.cpp:1690-1755); a body
+    lives on the finest level."""
+    coarse: LevelCase
+    boxes: tuple
+    name: str = "hierarchy"
+
+    def __post_init__(self):
+        d = self.coarse.dim
+        norm = []
+        for lo, hi in self.boxes:
+            lo = tuple(int(v) for v in lo) + (0,) * (3 - len(lo))
+            hi = tuple(int(v) for v in hi) + (0,) * (3 - len(hi))
+            norm.append((lo[:3], hi[:3]))
+        self.boxes = tuple(norm)
+        for l in range(1, self.nlev):
+            lo, hi = self.boxes[l - 1]
+            plo, phi = self.box_lohi(l - 1)
+            for a in range(d):
+                if lo[a] % 2 or hi[a] % 2 == 0 or hi[a] < lo[a]:
+                    raise ValueError(f"level {l}: the box must cover whole cells of level {l - 1}")
+                if lo[a] // 2 < plo[a] + 2 or hi[a] // 2 > phi[a] - 2:
+                    raise ValueError(f"level {l}: the box must lie two cells inside level {l - 1}'s box")
+
+    @property
+    def nlev(self) -> int:
+        return 1 + len(self.boxes)
+
+    @property
+    def dim(self) -> int:
+        return self.coarse.dim
+
+    def box_lohi(self, l: int):
+        if l == 0:
+            c = self.coarse
+            return (0, 0, 0), tuple(c.n_cell[a] - 1 if a < c.dim else 0 for a in range(3))
+        return self.boxes[l - 1]
+
+    def n_cell_of(self, l: int) -> tuple:
+        lo, hi = self.box_lohi(l)
+        return tuple((hi[a] - lo[a] + 1) if a < self.dim else 1 for a in range(3))
+
+    def level_case(self, l: int) -> LevelCase:
+        """Level l's whole domain (2^l times the coarse cells, same geometry)."""
+        c = self.coarse
+        n = tuple((2 ** l) * c.n_cell[a] if a < c.dim else 1 for a in range(3))
+        return replace(c, n_cell=n, name=f"{c.name}_lev{l}")
+
+    def box_case(self, l: int) -> LevelCase:
+        """Level l's box as a level of its own (its cells and physical extent),
+        for initial fields evaluated at its cell centres."""
+        c = self.coarse
+        if l == 0:
+            return c
+        lo, hi = self.boxes[l - 1]
+        dx = c.dx / (2 ** l)
+        plo = tuple(c.prob_lo[a] + dx * lo[a] if a < c.dim else c.prob_lo[a] for a in range(3))
+        phi = tuple(c.prob_lo[a] + dx * (hi[a] + 1) if a < c.dim else c.prob_hi[a] for a in range(3))
+        return replace(c, n_cell=self.n_cell_of(l), prob_lo=plo, prob_hi=phi, periodic=(False,) * 3,
+                       name=f"{c.name}_box{l}")
+
+    def cells(self, l: int) -> int:
+        return int(np.prod(self.n_cell_of(l)[: self.dim]))
+
+    def updates_per_coarse_step(self) -> int:
+        """Cell updates of one coarse step: level l steps 2^l times."""
+        return sum((2 ** l) * self.cells(l) for l in range(self.nlev))
+
+
+def nested_boxes(finest_lo, finest_hi, nlev: int, n_cell, dim: int, grow: int = 8):
+    """Boxes of levels 1 .. nlev - 1 around a finest-level box (given in the
+    finest level's indices): each coarser box is the finer one coarsened and
+    grown by `grow` cells, aligned to whole cells of the level above."""
+    L = nlev - 1
+    boxes = [None] * L
+    lo = [int(v) for v in finest_lo[:dim]]
+    hi = [int(v) for v in finest_hi[:dim]]
+    lo = [v - (v % 2) for v in lo]
+    hi = [v + (1 - v % 2) for v in hi]
+    boxes[L - 1] = (tuple(lo), tuple(hi))
+    for l in range(L - 1, 0, -1):
+        lo = [v // 2 - grow for v in lo]
+        hi = [v // 2 + grow for v in hi]
+        lo = [v - (v % 2) for v in lo]
+        hi = [v + (1 - v % 2) for v in hi]
+        boxes[l - 1] = (tuple(lo), tuple(hi))
+    # keep level 1 two coarse cells inside the domain
+    lo1, hi1 = boxes[0]
+    for a in range(dim):
+        if lo1[a] // 2 < 2 or hi1[a] // 2 > n_cell[a] - 3:
+            raise ValueError("the refined boxes reach the domain boundary; use a larger domain")
+    return tuple(boxes)
+
+
+def cylinder_hierarchy(nx=1024, ny=512, D=40.0, center=(256.0, 256.0), U=0.05, Re=100.0, nlev=3,
+                       upstream=1.0, downstream=4.0, cross=1.5, grow=8):
+    """The reference's 2D cylinder deck on nlev levels (Examples/Cylinder_flow/
+    inputs, ref_ratio 2): coarse level as ``cylinder``; the finest box around
+    the body and its near wake (upstream / downstream / cross extents in
+    diameters from the centre), every level in between the finer box
+    coarsened and grown by `grow` of its cells.  The marker IBM runs on the
+    finest level with markers about one finest cell apart."""
+    case, ib, init_c = cylinder(nx=nx, ny=ny, D=D, center=center, U=U, Re=Re)
+    r = 2 ** (nlev - 1)
+    dx = case.dx
+    flo = [int(math.floor((center[0] - upstream * D) / dx * r)), int(math.floor((center[1] - cross * D) / dx * r))]
+    fhi = [int(math.ceil((center[0] + downstream * D) / dx * r)) - 1,
+           int(math.ceil((center[1] + cross * D) / dx * r)) - 1]
+    boxes = nested_boxes(flo, fhi, nlev, case.n_cell, 2, grow)
+    hc = HierarchyCase(case, boxes, name=f"cylinder{nx}x{ny}_{nlev}lev")
+    inits = [init_c] + [uniform_init(hc.box_case(l), 1.0, (U, 0.0, 0.0)) for l in range(1, nlev)]
+    return hc, ib, inits
+
+
+def shear_layer_hierarchy(n=64, U0=0.02, nu=0.01, nlev=3, lattice: Lattice = D2Q9):
+    """Periodic box with a perturbed double shear layer and nested boxes
+    around its centre on every finer level (no body): velocity gradients
+    cross every coarse-fine boundary."""
+    dims = (n, n, n if lattice.dim == 3 else 1)
+    coarse = LevelCase(lattice, dims, periodic=(True, True, True), nu=nu, name=f"shear{n}")
+    L = nlev - 1
+    r = 2 ** L
+    c = n * r // 2
+    half = n * r // 8
+    boxes = nested_boxes([c - half] * lattice.dim, [c + half - 1] * lattice.dim, nlev, dims,
+                         lattice.dim, grow=4)
+    hc = HierarchyCase(coarse, boxes, name=f"shear{n}_{nlev}lev")
+    Lx = float(n)
+
+    def fn(X, Y, Z):
+        u = U0 * np.tanh(30.0 * (np.abs(Y / Lx - 0.5) - 0.25))
+        v = 0.05 * U0 * np.sin(2.0 * np.pi * X / Lx)
+        w = 0.02 * U0 * np.sin(2.0 * np.pi * Z / Lx) if lattice.dim == 3 else 0.0 * X
+        return 1.0 + 0.0 * X, u, v, w
+
+    return hc, [field_init(hc.box_case(l), fn) for l in range(nlev)]

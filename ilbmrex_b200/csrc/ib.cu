@@ -168,10 +168,12 @@ __global__ void k_markers(IBArgs a, double *xyz, const double *ref, double *tgt,
 }
 
 // velocity_interpolation_cic, :612-695; clip box = domain grown by 2.
-// One warp per marker: the 5 kernel weights per direction are evaluated once
-// (the reference re-evaluates the same values inside its loops) and the 5^d
-// stencil points are spread over the lanes; products keep the reference's
-// (tU*tV)*tW order, the sum is a fixed-order warp reduction.
+// One warp per marker (the batched stages): the 5 kernel weights per
+// direction are evaluated once (the reference re-evaluates the same values
+// inside its loops) and the 5^d stencil points are spread over the lanes;
+// products keep the reference's (tU*tV)*tW order, the sum is a fixed-order
+// warp reduction.  The single-body path sums in the reference's own order
+// (interp_seq below).
 __device__ __forceinline__ void marker_weights(const IBArgs &a, double px, double py, double pz,
                                                int lane, int &i0, int &j0, int &k0,
                                                double &wx, double &wy, double &wz) {
@@ -257,14 +259,6 @@ __device__ __forceinline__ void interp_one(const IBArgs &a, int m, int lane, con
   }
 }
 
-__global__ void __launch_bounds__(128) k_interp(IBArgs a, const double *xyz, const double *EV,
-                                                double *uvw, int *status, const double *tgt,
-                                                double *rhs, int ld) {
-  const int lane = threadIdx.x & 31;
-  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (m >= a.n) return;
-  interp_one(a, m, lane, xyz, EV, uvw, status, tgt, rhs, ld);
-}
 
 // rigid_target_velocity / box_target_velocity, :147-182
 __device__ __forceinline__ void rigid_target(const IBArgs &a, double x, double y, double z,
@@ -1154,6 +1148,166 @@ __global__ void __launch_bounds__(128) k_spread(IBArgs a, const double *xyz, con
   spread_one(a, m, lane, xyz, F, EFI, status);
 }
 
+// ---------------------------------------------------------------------------
+// Interpolation and spreading in the reference's summation order.
+// velocity_interpolation_cic sums a marker's stencil sequentially (i, then
+// j, then k innermost, IBMarkerDF.cpp:612-695); force_spreading adds the
+// markers' contributions to each cell in marker order (the loop over
+// particles, :1331-1448).  The kernels below keep both orders: one thread per
+// marker for the interpolation, and for a body whose markers do not move a
+// gather over a cell -> marker table built once (markers in increasing
+// order), so each cell's force is the reference's sum, computed once, with
+// no atomics.  FP64 results then equal the reference's bit for bit wherever
+// the rest of the chain does (explicit and explicit_diag coupling).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void interp_seq(const IBArgs &a, int m, const double *xyz,
+                                           const double *EV, double *uvw, int *status,
+                                           const double *tgt, double *rhs, int ld) {
+  const double px = xyz[m], py = xyz[m + a.n], pz = xyz[m + 2 * a.n];
+  const double d = (a.dim == 3) ? X::mul(X::mul(a.dx[0], a.dx[1]), a.dx[2]) : X::mul(a.dx[0], a.dx[1]);
+  const int i0 = cell_of(px, a.plo[0], a.dx[0]), j0 = cell_of(py, a.plo[1], a.dx[1]);
+  const int k0 = (a.dim == 3) ? cell_of(pz, a.plo[2], a.dx[2]) : 0;
+  double wx[5], wy[5], wz[5];
+#pragma unroll
+  for (int o = 0; o < 5; ++o) {
+    wx[o] = delta_fn(cell_center(a.plo[0], i0 + o - 2, a.dx[0]), px, a.dx[0], a.kt);
+    wy[o] = delta_fn(cell_center(a.plo[1], j0 + o - 2, a.dx[1]), py, a.dx[1], a.kt);
+    wz[o] = (a.dim == 3) ? delta_fn(cell_center(a.plo[2], k0 + o - 2, a.dx[2]), pz, a.dx[2], a.kt) : 1.0;
+  }
+  const int ilo = a.dlo[0] - 2, ihi = a.dhi[0] + 2, jlo = a.dlo[1] - 2, jhi = a.dhi[1] + 2;
+  const int klo = (a.dim == 3) ? a.dlo[2] - 2 : 0, khi = (a.dim == 3) ? a.dhi[2] + 2 : 0;
+  const int nk = (a.dim == 3) ? 5 : 1;
+  double u = 0.0, v = 0.0, w = 0.0, part = 0.0;
+  bool outside = false;
+  for (int ii = 0; ii < 5; ++ii) {
+    const int ip = i0 + ii - 2;
+    if (ip < ilo || ip > ihi || wx[ii] == 0.0) continue;
+    for (int jj = 0; jj < 5; ++jj) {
+      const int jp = j0 + jj - 2;
+      if (jp < jlo || jp > jhi || wy[jj] == 0.0) continue;
+      for (int kk = 0; kk < nk; ++kk) {
+        const int kp = (a.dim == 3) ? k0 + kk - 2 : 0;
+        if (kp < klo || kp > khi) continue;
+        const double dvl = (a.dim == 3) ? X::mul(X::mul(wx[ii], wy[jj]), wz[kk]) : X::mul(wx[ii], wy[jj]);
+        // points outside the kernel's support add signed zeros to sums that
+        // start at +0: skipping them leaves every sum bit for bit as it was
+        if (dvl == 0.0) continue;
+        if (!in_band(a, ip, jp, kp)) {
+          outside = true;
+          continue;
+        }
+        const int64_t e = bidx(a, ip, jp, kp);
+        part = X::add(part, X::mul(dvl, d));
+        u = X::add(u, X::mul(X::mul(dvl, EV[e]), d));
+        v = X::add(v, X::mul(X::mul(dvl, EV[e + a.nb]), d));
+        if (a.dim == 3) w = X::add(w, X::mul(X::mul(dvl, EV[e + 2 * a.nb]), d));
+      }
+    }
+  }
+  if (outside) atomicOr(status, 1);
+  if (a.renorm_interp && part > 0.0) {
+    u = X::div(u, part);
+    v = X::div(v, part);
+    w = X::div(w, part);
+  }
+  u = X::add(uvw[m], u);
+  v = X::add(uvw[m + a.n], v);
+  w = X::add(uvw[m + 2 * a.n], w);
+  uvw[m] = u;
+  uvw[m + a.n] = v;
+  uvw[m + 2 * a.n] = w;
+  if (rhs) {
+    double Ux, Uy, Uz;
+    target_of(a, m, xyz, tgt, Ux, Uy, Uz);
+    rhs[m] = X::div(X::sub(Ux, u), a.dt);
+    rhs[m + ld] = X::div(X::sub(Uy, v), a.dt);
+    rhs[m + 2 * ld] = X::div(X::sub(Uz, w), a.dt);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_interp_seq(IBArgs a, const double *xyz, const double *EV,
+                                                    double *uvw, int *status, const double *tgt,
+                                                    double *rhs, int ld) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.n) return;
+  interp_seq(a, m, xyz, EV, uvw, status, tgt, rhs, ld);
+}
+
+// per marker: its five kernel weights per direction and the spreading scale
+// (1, or 1 / partition with renormalize_delta, the partition summed in the
+// reference's order over the clipped stencil, :1336-1410)
+struct SpreadW {
+  double w[3][5];
+  double scale;
+};
+
+__global__ void __launch_bounds__(128) k_spread_weights(IBArgs a, const double *xyz, SpreadW *W) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= a.n) return;
+  const double p[3] = {xyz[m], xyz[m + a.n], xyz[m + 2 * a.n]};
+  SpreadW sw;
+  int c0[3];
+  for (int dd = 0; dd < 3; ++dd) {
+    c0[dd] = (dd < a.dim) ? cell_of(p[dd], a.plo[dd], a.dx[dd]) : 0;
+    for (int o = 0; o < 5; ++o)
+      sw.w[dd][o] = (dd < a.dim) ? delta_fn(cell_center(a.plo[dd], c0[dd] + o - 2, a.dx[dd]), p[dd],
+                                             a.dx[dd], a.kt)
+                                 : 1.0;
+  }
+  sw.scale = 1.0;
+  if (a.renorm_spread) {
+    const double d = (a.dim == 3) ? X::mul(X::mul(a.dx[0], a.dx[1]), a.dx[2]) : X::mul(a.dx[0], a.dx[1]);
+    const int nk = (a.dim == 3) ? 5 : 1;
+    double part = 0.0;
+    for (int ii = 0; ii < 5; ++ii) {
+      const int ip = c0[0] + ii - 2;
+      if (ip < a.dlo[0] - 2 || ip > a.dhi[0] + 2) continue;
+      for (int jj = 0; jj < 5; ++jj) {
+        const int jp = c0[1] + jj - 2;
+        if (jp < a.dlo[1] - 2 || jp > a.dhi[1] + 2) continue;
+        for (int kk = 0; kk < nk; ++kk) {
+          const int kp = c0[2] + kk - 2;
+          if (a.dim == 3 && (kp < a.dlo[2] - 2 || kp > a.dhi[2] + 2)) continue;
+          const double t3 = (a.dim == 3) ? X::mul(X::mul(sw.w[0][ii], sw.w[1][jj]), sw.w[2][kk])
+                                         : X::mul(sw.w[0][ii], sw.w[1][jj]);
+          part = X::add(part, X::mul(t3, d));
+        }
+      }
+    }
+    if (part > 0.0) sw.scale = X::div(1.0, part);
+  }
+  W[m] = sw;
+}
+
+// one thread per band cell that some stencil reaches: its markers' force
+// contributions in increasing marker order.  ent: marker << 9 | ii << 6 |
+// jj << 3 | kk.
+__global__ void __launch_bounds__(128) k_spread_gather(IBArgs a, const SpreadW *__restrict__ W,
+                                                       const double *__restrict__ F,
+                                                       const int64_t *__restrict__ cells,
+                                                       const int *__restrict__ rowptr,
+                                                       const int *__restrict__ ent, int ncell,
+                                                       double *EFI) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= ncell) return;
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  for (int e = rowptr[r]; e < rowptr[r + 1]; ++e) {
+    const int pk = ent[e];
+    const int m = pk >> 9, ii = (pk >> 6) & 7, jj = (pk >> 3) & 7, kk = pk & 7;
+    const SpreadW &w = W[m];
+    const double t3 = (a.dim == 3) ? X::mul(X::mul(w.w[0][ii], w.w[1][jj]), w.w[2][kk])
+                                   : X::mul(w.w[0][ii], w.w[1][jj]);
+    const double dvl = X::mul(t3, w.scale);
+    ax = X::add(ax, X::mul(dvl, X::mul(F[m], a.dv)));
+    ay = X::add(ay, X::mul(dvl, X::mul(F[m + a.n], a.dv)));
+    if (a.dim == 3) az = X::add(az, X::mul(dvl, X::mul(F[m + 2 * a.n], a.dv)));
+  }
+  const int64_t t = cells[r];
+  EFI[t] = ax;
+  EFI[t + a.nb] = ay;
+  if (a.dim == 3) EFI[t + 2 * a.nb] = az;
+}
+
 // SumBoundary (periodic): ghost-cell contributions added into their valid image
 __device__ __forceinline__ void sum_boundary_cell(const IBArgs &a, double *EFI, int64_t t) {
   {
@@ -1390,6 +1544,13 @@ struct ilbm_ib {
   double *d_Ainv = nullptr, *d_gj = nullptr, *d_rhs = nullptr;
   float *d_Ainv32 = nullptr;  // FP32 copy of A^-1 for the 4- and 2-byte storage forms
   bool fsum_deferred = false;  // marker force sum still to be launched (ib_finish)
+  // fixed-order spreading of a body whose markers do not move: the band cells
+  // its stencils reach, their marker lists (CSR) and the markers' weights
+  bool gather = false;
+  int gather_cells = 0;
+  int64_t *d_gcell = nullptr;
+  int *d_growptr = nullptr, *d_gent = nullptr;
+  void *d_sw = nullptr;  // SpreadW per marker
   // a level held in several boxes: the StepArgs of the boxes near the band
   std::vector<StepArgs> h_boxargs;
   StepArgs *d_boxargs = nullptr;
@@ -1596,6 +1757,85 @@ void build_band(ilbm_ib *ib) {
   ib->nb = (int64_t)ib->bn[0] * ib->bn[1] * ib->bn[2];
 }
 
+// The cell -> marker table of the fixed-order spreading (k_spread_gather)
+// for a body whose markers do not move: every band cell within the kernel's
+// support of a marker, with its markers in increasing order.  The host
+// repeats the device's cell and distance arithmetic (IEEE double, no
+// contraction), so the table holds exactly the stencil points whose weight
+// is nonzero (plus, at worst, a few of weight zero, which add signed zeros).
+int build_gather(ilbm_ib *ib) {
+  const int n = ib->n, dim = ib->dim;
+  if (ib->moving || n <= 0 || n >= (1 << 22)) return ILBM_OK;
+  const double R = (ib->kt == 0) ? 2.0 : 1.5;
+  const ilbm_level_geom &g = ib->g;
+  std::vector<std::pair<int64_t, int>> pairs;
+  pairs.reserve((size_t)n * (dim == 3 ? 64 : 16));
+  for (int m = 0; m < n; ++m) {
+    const double p[3] = {ib->hx[m], ib->hy[m], ib->hz[m]};
+    int c0[3] = {0, 0, 0};
+    bool sup[3][5];
+    for (int d = 0; d < 3; ++d)
+      for (int o = 0; o < 5; ++o) sup[d][o] = (d >= dim && o == 2);
+    for (int d = 0; d < dim; ++d) {
+      c0[d] = (int)std::floor((p[d] - g.prob_lo[d]) / ib->dx[d]);
+      for (int o = 0; o < 5; ++o) {
+        const double xc = g.prob_lo[d] + ((double)(c0[d] + o - 2) + 0.5) * ib->dx[d];
+        const double rr = std::fabs(xc - p[d]) / ib->dx[d];
+        sup[d][o] = rr < R * (1.0 + 1e-12);
+      }
+    }
+    for (int ii = 0; ii < 5; ++ii)
+      for (int jj = 0; jj < 5; ++jj)
+        for (int kk = 0; kk < 5; ++kk) {
+          if (!sup[0][ii] || !sup[1][jj] || !sup[2][kk]) continue;
+          const int c[3] = {c0[0] + ii - 2, c0[1] + jj - 2, dim == 3 ? c0[2] + kk - 2 : 0};
+          bool ok = true;
+          for (int d = 0; d < dim; ++d) {
+            if (c[d] < -2 || c[d] > g.n_cell[d] + 1) ok = false;  // clip: domain grown by 2
+            if (c[d] < ib->blo[d] || c[d] >= ib->blo[d] + ib->bn[d]) ok = false;
+          }
+          if (!ok) continue;
+          const int64_t t = (int64_t)(c[0] - ib->blo[0]) + (int64_t)(c[1] - ib->blo[1]) * ib->bn[0] +
+                            (int64_t)(c[2] - ib->blo[2]) * ib->bn[0] * ib->bn[1];
+          pairs.push_back({t, (m << 9) | (ii << 6) | (jj << 3) | (dim == 3 ? kk : 0)});
+        }
+  }
+  std::stable_sort(pairs.begin(), pairs.end(),
+                   [](const std::pair<int64_t, int> &x, const std::pair<int64_t, int> &y) {
+                     return x.first < y.first;
+                   });
+  std::vector<int64_t> cells;
+  std::vector<int> rowptr, ent(pairs.size());
+  for (size_t e = 0; e < pairs.size(); ++e) {
+    if (e == 0 || pairs[e].first != pairs[e - 1].first) {
+      cells.push_back(pairs[e].first);
+      rowptr.push_back((int)e);
+    }
+    ent[e] = pairs[e].second;
+  }
+  rowptr.push_back((int)pairs.size());
+  const int nc = (int)cells.size();
+  int rc;
+  double *sw = nullptr;
+  const size_t sw_doubles = (size_t)n * (sizeof(SpreadW) / sizeof(double));
+  if ((rc = dmalloc(ib, &ib->d_gcell, (size_t)std::max(nc, 1))) ||
+      (rc = dmalloc(ib, &ib->d_growptr, (size_t)nc + 1)) ||
+      (rc = dmalloc(ib, &ib->d_gent, std::max<size_t>(ent.size(), 1))) ||
+      (rc = dmalloc(ib, &sw, sw_doubles)))
+    return rc;
+  ib->d_sw = sw;
+  cudaStream_t st = ib->ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(ib->d_gcell, cells.data(), nc * sizeof(int64_t), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ib->d_growptr, rowptr.data(), (nc + 1) * sizeof(int), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && !ent.empty())
+    e = cudaMemcpyAsync(ib->d_gent, ent.data(), ent.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_ib_create: spreading table");
+  ib->gather_cells = nc;
+  ib->gather = true;
+  return ILBM_OK;
+}
+
 IBArgs make_args(const ilbm_ib *ib, double dt, double time) {
   IBArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -1721,6 +1961,10 @@ int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom
   }
   cudaMemsetAsync(ib->d_status, 0, 2 * sizeof(int), ctx->stream);
   cudaMemsetAsync(ib->d_fsum, 0, 4 * sizeof(double), ctx->stream);
+  if ((rc = build_gather(ib))) {
+    ilbm_ib_destroy(ib);
+    return rc;
+  }
   if (p->coupling_method == 1) {
     // neighbours per row: at most (9 cells)^d of markers within +-4 cells;
     // keep a generous cap and report overflow through the status word
@@ -1972,8 +2216,8 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *boxes, int nbox, const ilbm_le
     cudaMemsetAsync(ib->d_EFI, 0, 3 * ib->nb * sizeof(double), s);
     k_markers<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_ref, ib->d_tgt, ib->d_uvw, ib->d_F);
     if (any_periodic_band) k_fill_boundary<<<gb, 256, 0, s>>>(a, ib->d_EV);
-    k_interp<<<wblk, 128, 0, s>>>(a, ib->d_xyz, ib->d_EV, ib->d_uvw, ib->d_status, ib->d_tgt,
-                                  use_dense ? ib->d_rhs : nullptr, ib->ld);
+    k_interp_seq<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_EV, ib->d_uvw, ib->d_status, ib->d_tgt,
+                                       use_dense ? ib->d_rhs : nullptr, ib->ld);
     ctx->launches += 2 + (any_periodic_band ? 1 : 0);
     if (ivc) {
       if (!ib->csr_ready || ib->moving || ib->p.ivc_rebuild_matrix > 0) {
@@ -2020,8 +2264,16 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *boxes, int nbox, const ilbm_le
       k_force_explicit<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_F);
       ctx->launches++;
     }
-    k_spread<<<wblk, 128, 0, s>>>(a, ib->d_xyz, ib->d_F, ib->d_EFI, ib->d_status);
-    ctx->launches++;
+    if (ib->gather) {
+      SpreadW *sw = static_cast<SpreadW *>(ib->d_sw);
+      k_spread_weights<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, sw);
+      k_spread_gather<<<(ib->gather_cells + 127) / 128, 128, 0, s>>>(
+          a, sw, ib->d_F, ib->d_gcell, ib->d_growptr, ib->d_gent, ib->gather_cells, ib->d_EFI);
+      ctx->launches += 2;
+    } else {
+      k_spread<<<wblk, 128, 0, s>>>(a, ib->d_xyz, ib->d_F, ib->d_EFI, ib->d_status);
+      ctx->launches++;
+    }
     if (any_periodic_band) {
       k_sum_boundary<<<gb, 256, 0, s>>>(a, ib->d_EFI);
       ctx->launches++;

@@ -27,6 +27,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
+#include <vector>
 
 #include "batch_internal.h"
 #include "ilbm_b200.h"
@@ -415,8 +417,20 @@ int ilbm_average_down(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_pa
   }
   ilbm_box c = *coarse, f = *fine;
   c.macro_out = c.macro_in;
-  int rc = check_two_level(ctx, &c, pc, &f, pf);
-  if (rc) return rc;
+  // any pair of adjacent levels of a hierarchy: the coarser one equal to its
+  // domain (self-filled) or one box of a level in between
+  int rc;
+  if (pc->ghost_mode == ILBM_GHOST_SELF) {
+    if ((rc = check_two_level(ctx, &c, pc, &f, pf))) return rc;
+  } else {
+    for (int d = 0; d < ctx->dim; ++d)
+      if ((f.lo[d] & 1) || !(f.hi[d] & 1) || f.lo[d] / 2 < c.lo[d] + 2 || f.hi[d] / 2 > c.hi[d] - 2 ||
+          pf->domain_lo[d] != 2 * pc->domain_lo[d] || pf->domain_hi[d] != 2 * pc->domain_hi[d] + 1) {
+        set_error("ilbm_average_down: the fine box must cover whole coarse cells two cells inside the "
+                  "coarse box, on the coarse domain refined by 2");
+        return ILBM_ERR_ARG;
+      }
+  }
   const AvgArgs g = avg_args(ctx, &c, &f, f.f_in, f.macro_in, c.f_in, c.macro_in, pf);
   return ILBM_DISPATCH(ctx, launch_avg_down, ctx, g);
 }
@@ -545,6 +559,200 @@ int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_lev
     }
   }
   return ILBM_DISPATCH(ctx, launch_avg_down, ctx, a);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Static hierarchy of any depth: AmrCoreLBM::timeStepWithSubcycling's
+// recursion (Source/Core/AmrCoreLBM.cpp:1690-1755).  A level's step, then
+// (below the finest level) two substeps of the next finer level, each with
+// its ghost cells filled from this level's macro fields at the substep's
+// time, then the average-down of that level onto this one (AverageDownTo,
+// :1519-1527).  The body, if any, lives on the finest level, whose steps
+// overlap the body's forcing chain with the cells outside its band.
+// ---------------------------------------------------------------------------
+namespace ilbm {
+namespace {
+
+struct HLevel {
+  ilbm_box b;                     // current buffers (swapped after each step)
+  const ilbm_level_params *p;
+  bool first;                     // the level's first step reads its stored macro everywhere
+  int mlo[3], mhi[3];             // stored macro region: the finer box coarsened, grown by 2
+  double t_old, t_new;            // the level's current step
+};
+
+int hier_check(const ilbm_ctx *ctx, int nlev, const ilbm_box *boxes, const ilbm_level_params *ps) {
+  auto fail = [](const char *m) {
+    set_error(std::string("hierarchy: ") + m);
+    return ILBM_ERR_ARG;
+  };
+  if (nlev < 2 || nlev > 8) return fail("2 to 8 levels");
+  if (ps[0].ghost_mode != ILBM_GHOST_SELF) return fail("the coarsest level self-fills its ghosts");
+  for (int l = 0; l < nlev; ++l) {
+    const ilbm_box &b = boxes[l];
+    if (!b.f_in || !b.f_out || b.f_in == b.f_out) return fail("every level needs distinct f_in and f_out");
+    if (b.ngrow_f < 1 || b.ngrow_m < 1) return fail("ghost widths must be at least 1");
+    if (l + 1 < nlev && (!b.macro_in || !b.macro_out))
+      return fail("every level with a finer one carries stored macro fields (macro_in and macro_out)");
+    if (l == 0) {
+      for (int d = 0; d < ctx->dim; ++d)
+        if (b.lo[d] != ps[0].domain_lo[d] || b.hi[d] != ps[0].domain_hi[d])
+          return fail("the coarsest box must equal its domain");
+      continue;
+    }
+    const ilbm_box &c = boxes[l - 1];
+    if (ps[l].ghost_mode != ILBM_GHOST_CALLER)
+      return fail("finer levels take their ghosts from the level above (ILBM_GHOST_CALLER)");
+    if (ps[l].nlevel_boxes > 1) return fail("one box per level");
+    for (int d = 0; d < ctx->dim; ++d) {
+      if (ps[l].domain_lo[d] != 2 * ps[l - 1].domain_lo[d] ||
+          ps[l].domain_hi[d] != 2 * ps[l - 1].domain_hi[d] + 1)
+        return fail("each domain must be the one above refined by 2");
+      if ((b.lo[d] & 1) || !(b.hi[d] & 1) || b.hi[d] < b.lo[d])
+        return fail("each box must cover whole cells of the level above");
+      if (b.lo[d] / 2 < c.lo[d] + 2 || b.hi[d] / 2 > c.hi[d] - 2)
+        return fail("each box must lie two cells of the level above inside that level's box");
+    }
+  }
+  return ILBM_OK;
+}
+
+// ghost cells of level `lev` for a step at time t, from level lev-1's macro
+// fields at its step's start (macro_in) and end (macro_out)
+int hier_cf_fill(ilbm_ctx *ctx, const HLevel &C, const HLevel &F, double t, bool reads_macro) {
+  CFArgs g;
+  std::memset(&g, 0, sizeof(g));
+  for (int d = 0; d < 3; ++d) {
+    const bool use = d < ctx->dim;
+    g.lo[d] = use ? F.b.lo[d] : 0;
+    g.hi[d] = use ? F.b.hi[d] : 0;
+    g.clo[d] = use ? C.b.lo[d] : 0;
+  }
+  g.gf = F.b.ngrow_f;
+  g.gm = F.b.ngrow_m;
+  g.fs0 = F.b.fstride[0]; g.fs1 = F.b.fstride[1]; g.fs2 = F.b.fstride[2];
+  g.ms0 = F.b.mstride[0]; g.ms1 = F.b.mstride[1]; g.ms2 = F.b.mstride[2];
+  g.cgm = C.b.ngrow_m;
+  g.cs0 = C.b.mstride[0]; g.cs1 = C.b.mstride[1]; g.cs2 = C.b.mstride[2];
+  g.cold = C.b.macro_in;
+  g.cnew = C.b.macro_out;
+  g.f16_scale = (float)f16_scale_of(F.p);
+  // GetDataMacro(lev-1, t): the data at t_new, at t_old, or both
+  const double teps = std::max(1.e-12, std::fabs(C.t_new - C.t_old) * 1.e-3);
+  if (t >= C.t_new - teps && t <= C.t_new + teps) {
+    g.mode = 1;
+  } else if (t >= C.t_old - teps && t <= C.t_old + teps) {
+    g.mode = 0;
+  } else {
+    g.mode = 2;
+    g.a = (C.t_new - t) / (C.t_new - C.t_old);
+    g.b = (t - C.t_old) / (C.t_new - C.t_old);
+  }
+  g.f = F.b.f_in;
+  g.m = reads_macro ? F.b.macro_in : nullptr;
+  return ILBM_DISPATCH(ctx, launch_cf_fill, ctx, g);
+}
+
+int hier_advance(ilbm_ctx *ctx, std::vector<HLevel> &H, int lev, ilbm_ib *ib, double dt, double t) {
+  const int nlev = (int)H.size();
+  const bool finest = lev == nlev - 1;
+  HLevel &L = H[lev];
+  L.t_old = t;
+  L.t_new = t + dt;
+  int rc;
+  ilbm_box b = L.b;
+  if (finest) {
+    b.macro_in = L.first ? L.b.macro_in : nullptr;
+    b.macro_out = nullptr;
+  }
+  if (lev > 0 && (rc = hier_cf_fill(ctx, H[lev - 1], L, t, finest && L.first))) return rc;
+  if (!finest) {
+    // stored macro fields: on the coarsest level on the region the finer
+    // level's ghost fill and average-down use (everywhere on its first step);
+    // on a level in between everywhere, since the average-down onto the level
+    // above takes its stored values (which hold the finer level's average on
+    // the covered cells)
+    const bool whole = L.first || lev > 0;
+    if ((rc = level_step_impl(ctx, &b, 1, L.p, whole ? nullptr : L.mlo, whole ? nullptr : L.mhi, 0)))
+      return rc;
+  } else if (ib) {
+    AdvanceSplit sp;
+    if ((rc = advance_begin(ctx, &b, L.p, ib, dt, t, &sp))) return rc;
+    if ((rc = advance_end(ctx, &b, &sp))) return rc;
+  } else {
+    if ((rc = ilbm_level_step(ctx, &b, 1, L.p))) return rc;
+  }
+  L.first = false;
+  if (!finest) {
+    const double dtf = 0.5 * dt;
+    for (int sub = 0; sub < 2; ++sub)
+      if ((rc = hier_advance(ctx, H, lev + 1, ib, dtf, t + (double)sub * dtf))) return rc;
+    // the finer level's state is back in its f_in after its two substeps;
+    // average it down onto this level's new state
+    const HLevel &F = H[lev + 1];
+    // a finer level that has a finer one itself passes its stored macro
+    // fields (AverageDownTo averages macro_new, which there holds the average
+    // of the level below on its covered cells); the finest level's macro
+    // fields are those of its populations
+    const void *fm = (lev + 1 < nlev - 1) ? F.b.macro_in : nullptr;
+    AvgArgs a = avg_args(ctx, &L.b, &F.b, F.b.f_in, fm, L.b.f_out, L.b.macro_out, F.p);
+    if (lev + 1 == nlev - 1 && ib) {
+      a.fF = F.b.force_prev;  // the force of the finest level's last substep
+      a.use_uniform = 0;
+      int lo[3], hi[3];
+      ilbm_ib_force_region(ib, lo, hi);
+      for (int d = 0; d < 3; ++d) {
+        a.rlo[d] = lo[d];
+        a.rhi[d] = hi[d];
+      }
+    }
+    if ((rc = ILBM_DISPATCH(ctx, launch_avg_down, ctx, a))) return rc;
+  }
+  // the new state becomes the current one
+  std::swap(L.b.f_in, L.b.f_out);
+  std::swap(L.b.macro_in, L.b.macro_out);
+  if (finest && ib) std::swap(L.b.force, L.b.force_prev);
+  return ILBM_OK;
+}
+
+}  // namespace
+}  // namespace ilbm
+
+extern "C" {
+
+int ilbm_advance_hierarchy(ilbm_ctx *ctx, int nlev, const ilbm_box *boxes,
+                           const ilbm_level_params *params, ilbm_ib *ib, double dt, double time,
+                           int flags) {
+  if (!ctx || !boxes || !params) {
+    set_error("ilbm_advance_hierarchy: null argument");
+    return ILBM_ERR_ARG;
+  }
+  int rc = hier_check(ctx, nlev, boxes, params);
+  if (rc) return rc;
+  const ilbm_box &fb = boxes[nlev - 1];
+  if (ib && (!fb.force || !fb.force_prev)) {
+    set_error("ilbm_advance_hierarchy: a body needs the finest level's force and force_prev");
+    return ILBM_ERR_ARG;
+  }
+  const bool first = (flags & ILBM_HIERARCHY_FIRST_STEP) != 0;
+  if (first && !fb.macro_in) {
+    set_error("ilbm_advance_hierarchy: the first step reads the finest level's stored macro_in");
+    return ILBM_ERR_ARG;
+  }
+  std::vector<HLevel> H(nlev);
+  for (int l = 0; l < nlev; ++l) {
+    H[l].b = boxes[l];
+    H[l].p = &params[l];
+    H[l].first = first;
+    for (int d = 0; d < 3; ++d) {
+      const bool use = d < ctx->dim && l + 1 < nlev;
+      H[l].mlo[d] = use ? boxes[l + 1].lo[d] / 2 - 2 : 0;
+      H[l].mhi[d] = use ? boxes[l + 1].hi[d] / 2 + 2 : 0;
+    }
+  }
+  return hier_advance(ctx, H, 0, ib, dt, time);
 }
 
 }  // extern "C"

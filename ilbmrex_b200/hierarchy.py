@@ -1,12 +1,14 @@
-"""A static two-level hierarchy on the GPU through the C ABI.
+"""Static hierarchies on the GPU through the C ABI.
 
-``TwoLevelSolver`` holds a coarse level equal to the domain and one fixed
-fine box of refinement ratio 2 (``cases.TwoLevelCase``) in device memory and
-advances them with ``ilbm_advance_two_level``: one coarse step, two fine
-substeps whose ghost cells come from the coarse macro fields on the device,
-then average-down (AmrCoreLBM::timeStepWithSubcycling,
-Source/Core/AmrCoreLBM.cpp:1690-1755, for max_level = 1 without regrid).  A
-marker body lives on the fine level, the finest one
+``HierarchySolver`` holds a coarse level equal to the domain and one fixed
+box on each finer level (refinement ratio 2, ``cases.HierarchyCase``) in
+device memory and advances them with ``ilbm_advance_hierarchy``: a level's
+step, two substeps of the next finer level whose ghost cells come from this
+level's macro fields on the device, then average-down, recursively
+(AmrCoreLBM::timeStepWithSubcycling, Source/Core/AmrCoreLBM.cpp:1690-1755,
+without regrid).  ``TwoLevelSolver`` is the two-level case advanced by
+``ilbm_advance_two_level``, whose schedule overlaps the coarse step with the
+fine level's body forcing.  A marker body lives on the finest level
 (Source/Core/AdvanceLBMAtLevel.cpp:30, 73-93).
 """
 from __future__ import annotations
@@ -17,7 +19,7 @@ import numpy as np
 import torch
 
 from . import capi
-from .cases import MarkerIB, TwoLevelCase
+from .cases import HierarchyCase, MarkerIB, TwoLevelCase
 from .level import (_REAL_DT, _TORCH_DT, Context, LevelSolver, alloc_populations, ib_params,
                     level_geom, level_params)
 
@@ -65,31 +67,48 @@ class _Level:
         return t[..., :, g:g + ny, g:g + nx]
 
 
-class TwoLevelSolver:
-    """Coarse level + one fine box (ratio 2) stepped on the GPU."""
+class HierarchySolver:
+    """A static hierarchy (``cases.HierarchyCase``: coarse level = the domain,
+    one box per finer level, ratio 2) stepped on the GPU through
+    ``ilbm_advance_hierarchy``; a marker body lives on the finest level."""
 
-    def __init__(self, tl: TwoLevelCase, storage: str = "f64", ib: MarkerIB | None = None,
+    def __init__(self, hc: HierarchyCase, storage: str = "f64", ib: MarkerIB | None = None,
                  device: int = 0, f16_scale: float = 1024.0):
         if not torch.cuda.is_available():
-            raise capi.IlbmError("TwoLevelSolver needs a CUDA device")
-        self.tl = tl
+            raise capi.IlbmError("HierarchySolver needs a CUDA device")
+        self.hc = hc
+        self.nlev = hc.nlev
         self.storage = storage
         self.dev = torch.device("cuda", device)
-        c = tl.coarse
-        self.case = tl.fine_level()          # the finest level (force record, body)
+        c = hc.coarse
+        top = hc.nlev - 1
+        self.case = hc.level_case(top)          # the finest level (force record, body)
         self.ib_case = ib
         self.dim = c.dim
         self.ctx = Context(c.lattice, storage, device)
         self.L = self.ctx.L
         q = c.lattice.q
-        self.C = _Level(q, c.dim, c.n_cell, (0, 0, 0), storage, self.dev, False)
-        self.F = _Level(q, c.dim, tl.fine_n_cell, tl.fine_lo, storage, self.dev, ib is not None)
-        self.pc = level_params(c, uniform_force=True, f16_scale=f16_scale)
-        self.pf = level_params(self.case, uniform_force=ib is None, f16_scale=f16_scale)
-        self.pf.ghost_mode = capi.GHOST_CALLER
-        self._fine_boxes = (C.c_int * 6)(*tl.fine_lo, *tl.fine_hi)
-        self.pf.level_boxes = C.cast(self._fine_boxes, C.POINTER(C.c_int))
-        self.pf.nlevel_boxes = 1
+        self.levels = []
+        self.params = []
+        self._lb = []
+        for l in range(hc.nlev):
+            lo, _ = hc.box_lohi(l)
+            self.levels.append(_Level(q, c.dim, hc.n_cell_of(l), lo, storage, self.dev,
+                                      ib is not None and l == top))
+            if l == 0:
+                p = level_params(c, uniform_force=True, f16_scale=f16_scale)
+            else:
+                p = level_params(hc.level_case(l), uniform_force=(ib is None or l < top),
+                                 f16_scale=f16_scale)
+                p.ghost_mode = capi.GHOST_CALLER
+                lo, hi = hc.box_lohi(l)
+                lb = (C.c_int * 6)(*lo, *hi)
+                self._lb.append(lb)
+                p.level_boxes = C.cast(lb, C.POINTER(C.c_int))
+                p.nlevel_boxes = 1
+            self.params.append(p)
+        self.C, self.F = self.levels[0], self.levels[top]
+        self.pc, self.pf = self.params[0], self.params[top]
         self.ib = None
         if ib is not None:
             self._geom = level_geom(self.case)
@@ -115,44 +134,58 @@ class TwoLevelSolver:
         self._pending = None
 
     # ---- initialisation (MakeNewLevelFromScratch per level + InitData) ----
-    def set_macro(self, init_coarse, init_fine):
-        """Initial (rho, u, v, w) of each level on its valid cells; each
-        level's populations become their equilibrium, then the fine level is
-        averaged down onto the coarse one (InitData, AmrCoreLBM.cpp:704-722)."""
-        for lvl, vals in ((self.C, init_coarse), (self.F, init_fine)):
+    def set_macro(self, *inits):
+        """Initial (rho, u, v, w) of each level on its valid cells, coarsest
+        first (one argument per level, or one list of them); each level's
+        populations become their equilibrium, then every level is averaged
+        down onto the one above, finest first (InitData,
+        AmrCoreLBM.cpp:704-722)."""
+        if len(inits) == 1 and len(inits[0]) == self.nlev and not isinstance(inits[0][0], np.ndarray):
+            inits = tuple(inits[0])
+        for lvl, vals in zip(self.levels, inits):
             v = lvl.valid(lvl.m, lvl.gm)
             for n in range(4 if self.dim == 3 else 3):
                 v[n].copy_(torch.as_tensor(np.asarray(vals[n]), dtype=lvl.m.dtype))
             torch.cuda.synchronize(self.dev)
             b = lvl.box(lvl.f, lvl.f_next, m_in=lvl.m)
             capi.check(self.L.ilbm_init_equilibrium(self.ctx.h, C.byref(b)), "init_equilibrium")
-        bc = self.C.box(self.C.f, None, m_in=self.C.m)
-        bf = self.F.box(self.F.f, None, m_in=self.F.m)
-        capi.check(self.L.ilbm_average_down(self.ctx.h, C.byref(bc), C.byref(self.pc), C.byref(bf),
-                                            C.byref(self.pf)), "average_down")
+        for l in range(self.nlev - 1, 0, -1):
+            crs, fin = self.levels[l - 1], self.levels[l]
+            bc = crs.box(crs.f, None, m_in=crs.m)
+            bf = fin.box(fin.f, None, m_in=fin.m)
+            capi.check(self.L.ilbm_average_down(self.ctx.h, C.byref(bc), C.byref(self.params[l - 1]),
+                                                C.byref(bf), C.byref(self.params[l])), "average_down")
         self.ctx.sync()
         self.time, self.istep = 0.0, 0
         self.first_step = True
 
     # ---- one coarse step ---------------------------------------------------
+    def _launch_step(self):
+        top = self.nlev - 1
+        arr = (capi.Box_t * self.nlev)()
+        for l, lvl in enumerate(self.levels):
+            if l < top:
+                arr[l] = lvl.box(lvl.f, lvl.f_next, m_in=lvl.m, m_out=lvl.m_next)
+            else:
+                arr[l] = lvl.box(lvl.f, lvl.f_next, m_in=lvl.m if self.first_step else None,
+                                 force=lvl.fa, force_prev=lvl.fb)
+        pa = (capi.LevelParams_t * self.nlev)(*self.params)
+        flags = capi.HIERARCHY_FIRST_STEP if self.first_step else 0
+        capi.check(self.L.ilbm_advance_hierarchy(self.ctx.h, self.nlev, arr, pa, self.ib,
+                                                 self.hc.coarse.dt, self.time, flags),
+                   "advance_hierarchy")
+
     def advance(self, record_force: bool = False, pipelined: bool = False):
         """One coarse step.  record_force: the force record (self.rec) of the
         step; pipelined: its sums are copied to the host without waiting, and
         the record of the previous step is taken instead (flush_records takes
         the last one), so the next step is queued before the host waits."""
-        Cl, Fl = self.C, self.F
-        bc = Cl.box(Cl.f, Cl.f_next, m_in=Cl.m, m_out=Cl.m_next)
-        bf = Fl.box(Fl.f, Fl.f_next, m_in=Fl.m if self.first_step else None,
-                    force=Fl.fa, force_prev=Fl.fb)
-        flags = capi.TWO_LEVEL_FIRST_STEP if self.first_step else 0
-        capi.check(self.L.ilbm_advance_two_level(self.ctx.h, C.byref(bc), C.byref(self.pc),
-                                                 C.byref(bf), C.byref(self.pf), self.ib,
-                                                 self.tl.coarse.dt, self.time, flags),
-                   "advance_two_level")
+        self._launch_step()
+        Cl = self.C
         Cl.f, Cl.f_next = Cl.f_next, Cl.f
         Cl.m, Cl.m_next = Cl.m_next, Cl.m
         self.first_step = False
-        self.time += self.tl.coarse.dt
+        self.time += self.hc.coarse.dt
         self.istep += 1
         if record_force and self.ib is not None:
             if pipelined:
@@ -171,11 +204,11 @@ class TwoLevelSolver:
             self._rec_bufs = [torch.empty(8, dtype=torch.float64, pin_memory=True) for _ in range(2)]
             self._stream = torch.cuda.ExternalStream(self.L.ilbm_stream(self.ctx.h), device=self.dev)
         lo, hi = self.force_region
-        b = self.F.box(self.F.f, None)
+        b = self.F.box(self.F.f, None, force=self.F.fb)
         buf = self._rec_bufs[self._rec_slot]
         self._rec_slot ^= 1
-        capi.check(self.L.ilbm_force_record_async(self.ctx.h, C.byref(b), self.F.fb.data_ptr(), self.ib,
-                                                  capi.ivec3(lo), capi.ivec3(hi), buf.data_ptr()),
+        capi.check(self.L.ilbm_force_record_async(self.ctx.h, C.byref(b), 1, self.ib, capi.ivec3(lo),
+                                                  capi.ivec3(hi), buf.data_ptr()),
                    "force_record_async")
         ev = torch.cuda.Event()
         ev.record(self._stream)
@@ -207,10 +240,10 @@ class TwoLevelSolver:
         """ComputeIBForce on the finest level (AmrCoreLBM.cpp:456-631) with
         the force of the last fine substep."""
         lo, hi = self.force_region
-        b = self.F.box(self.F.f, None)
+        b = self.F.box(self.F.f, None, force=self.F.fb)
         s = (C.c_double * 3)()
-        capi.check(self.L.ilbm_force_integrals(self.ctx.h, C.byref(b), self.F.fb.data_ptr(),
-                                               capi.ivec3(lo), capi.ivec3(hi), s), "force_integrals")
+        capi.check(self.L.ilbm_force_integrals(self.ctx.h, C.byref(b), 1, capi.ivec3(lo),
+                                               capi.ivec3(hi), s), "force_integrals")
         m = (C.c_double * 3)()
         capi.check(self.L.ilbm_ib_last_marker_force_sum(self.ib, m), "marker_force_sum")
         self.rec = LevelSolver.force_record(self, np.array([s[0], s[1], s[2]]),
@@ -219,14 +252,14 @@ class TwoLevelSolver:
 
     # ---- read-back ---------------------------------------------------------
     def _lvl(self, lev):
-        return self.F if lev else self.C
+        return self.levels[lev]
 
     def get_f(self, lev: int) -> np.ndarray:
         self.ctx.sync()
         lvl = self._lvl(lev)
         v = lvl.valid(lvl.f, lvl.gf).to(torch.float64)
         if self.storage != "f64":
-            w = torch.tensor(self.tl.coarse.lattice.w, dtype=torch.float64, device=self.dev).view(-1, 1, 1, 1)
+            w = torch.tensor(self.hc.coarse.lattice.w, dtype=torch.float64, device=self.dev).view(-1, 1, 1, 1)
             if self.storage == "f16":
                 v = v * (w / self.pc.f16_scale)
             v = v + w
@@ -242,17 +275,21 @@ class TwoLevelSolver:
             return lvl.valid(lvl.m, lvl.gm).to(torch.float64).cpu().numpy()
         out = torch.zeros_like(lvl.m)
         b = lvl.box(lvl.f, None)
-        force = self.F.fb if (lev == 1 and self.ib is not None) else None
-        p = self.pf if lev == 1 else self.pc
+        top = self.nlev - 1
+        force = self.F.fb if (lev == top and self.ib is not None) else None
+        p = self.params[lev]
         capi.check(self.L.ilbm_compute_macro(self.ctx.h, C.byref(b), C.byref(p), lvl.f.data_ptr(),
                                              force.data_ptr() if force is not None else None,
                                              out.data_ptr(), None, None), "compute_macro")
         self.ctx.sync()
         m = lvl.valid(out, lvl.gm).to(torch.float64).cpu().numpy()
-        if lev == 0:
+        if lev < top:
+            # the covered cells hold the averaged-down values (stored macro)
             st = lvl.valid(lvl.m, lvl.gm).to(torch.float64).cpu().numpy()
-            lo = [v // 2 for v in self.tl.fine_lo]
-            hi = [v // 2 + 1 for v in self.tl.fine_hi]
+            blo, _ = self.hc.box_lohi(lev)
+            flo, fhi = self.hc.box_lohi(lev + 1)
+            lo = [flo[a] // 2 - blo[a] for a in range(3)]
+            hi = [fhi[a] // 2 + 1 - blo[a] for a in range(3)]
             if self.dim == 3:
                 sl = (slice(None), slice(lo[2], hi[2]), slice(lo[1], hi[1]), slice(lo[0], hi[0]))
             else:
@@ -274,3 +311,29 @@ class TwoLevelSolver:
             self.L.ilbm_ib_destroy(self.ib)
             self.ib = None
         self.ctx.close()
+
+
+class TwoLevelSolver(HierarchySolver):
+    """A coarse level + one fine box (ratio 2) stepped by
+    ``ilbm_advance_two_level``, whose schedule overlaps the coarse step with
+    the fine level's body forcing."""
+
+    def __init__(self, tl: TwoLevelCase, storage: str = "f64", ib: MarkerIB | None = None,
+                 device: int = 0, f16_scale: float = 1024.0):
+        self.tl = tl
+        hc = HierarchyCase(tl.coarse, ((tl.fine_lo, tl.fine_hi),), name=tl.name)
+        super().__init__(hc, storage, ib, device, f16_scale)
+
+    def set_macro(self, init_coarse, init_fine):
+        super().set_macro(init_coarse, init_fine)
+
+    def _launch_step(self):
+        Cl, Fl = self.C, self.F
+        bc = Cl.box(Cl.f, Cl.f_next, m_in=Cl.m, m_out=Cl.m_next)
+        bf = Fl.box(Fl.f, Fl.f_next, m_in=Fl.m if self.first_step else None,
+                    force=Fl.fa, force_prev=Fl.fb)
+        flags = capi.TWO_LEVEL_FIRST_STEP if self.first_step else 0
+        capi.check(self.L.ilbm_advance_two_level(self.ctx.h, C.byref(bc), C.byref(self.pc),
+                                                 C.byref(bf), C.byref(self.pf), self.ib,
+                                                 self.tl.coarse.dt, self.time, flags),
+                   "advance_two_level")

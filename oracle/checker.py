@@ -342,37 +342,43 @@ class CpuLevel:
         return float(self.lib.orc_ib_dv(self.h))
 
 
-class CpuTwoLevel:
-    """A static two-level hierarchy advanced by the oracle (orc2_*): coarse
-    level = the domain, one fine box of ratio 2, two fine substeps per coarse
-    step with coarse-fine ghosts from the coarse macro fields, average-down."""
+class CpuHierarchy:
+    """A static hierarchy advanced by the oracle (orcN_*): coarse level = the
+    domain, one box per finer level (ratio 2, properly nested), two substeps
+    of each finer level per step of the level above with coarse-fine ghosts
+    from that level's macro fields, average-down after them.  `hc` has
+    ``coarse`` (LevelCase), ``boxes`` ((lo, hi) per finer level in its own
+    domain indices), ``nlev`` and ``box_case(l)``."""
 
-    def __init__(self, tl):
-        self.tl = tl
-        self.lib = _load("oracle", tl.dim)
+    def __init__(self, hc):
+        self.hc = hc
+        self.nlev = hc.nlev
+        self.lib = _load("oracle", hc.coarse.dim)
         lib = self.lib
-        P, I, dp = C.c_void_p, C.c_int, C.POINTER(C.c_double)
+        P, I = C.c_void_p, C.c_int
         ip = C.POINTER(C.c_int)
-        for name, res, args in [("orc2_create", P, [C.POINTER(IlbmCase), ip, ip]),
-                                ("orc2_destroy", None, [P]), ("orc2_level", P, [P, I]),
-                                ("orc2_step", I, [P, I]), ("orc2_init_equilibrium", I, [P])]:
+        for name, res, args in [("orcN_create", P, [C.POINTER(IlbmCase), I, ip]),
+                                ("orcN_destroy", None, [P]), ("orcN_level", P, [P, I]),
+                                ("orcN_step", I, [P, I]), ("orcN_init_equilibrium", I, [P])]:
             fn = getattr(lib, name)
             fn.restype, fn.argtypes = res, args
-        self._case = to_case(tl.coarse)
-        lo = (C.c_int * 3)(*tl.fine_lo)
-        hi = (C.c_int * 3)(*tl.fine_hi)
-        self.h = lib.orc2_create(C.byref(self._case), lo, hi)
+        self._case = to_case(hc.coarse)
+        flat = []
+        for lo, hi in hc.boxes:
+            flat += list(lo) + list(hi)
+        arr = (C.c_int * max(1, len(flat)))(*flat)
+        self.h = lib.orcN_create(C.byref(self._case), self.nlev, arr)
         if not self.h:
-            raise RuntimeError("orc2_create refused the fine box")
-        self.q = tl.coarse.lattice.q
-        self.shapes = (tl.coarse.shape, tl.fine_box().shape)
+            raise RuntimeError("orcN_create refused the level boxes")
+        self.q = hc.coarse.lattice.q
+        self.shapes = tuple(hc.box_case(l).shape for l in range(self.nlev))
 
     def level(self, lev: int):
-        return self.lib.orc2_level(self.h, lev)
+        return self.lib.orcN_level(self.h, lev)
 
     def close(self):
         if self.h:
-            self.lib.orc2_destroy(self.h)
+            self.lib.orcN_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -390,18 +396,19 @@ class CpuTwoLevel:
         self.lib.orc_set_macro(self.level(lev), _dp(m))
 
     def init_equilibrium(self):
-        self.lib.orc2_init_equilibrium(self.h)
+        self.lib.orcN_init_equilibrium(self.h)
 
     def ib_create(self, ib):
+        """The body lives on the finest level."""
         if getattr(ib, "airfoil", None) is not None:
             p = np.ascontiguousarray(np.asarray(ib.airfoil, dtype=np.float64))
             self.lib.orc_set_airfoil(_dp(p))
         self._ib = to_ib_case(ib)
-        if self.lib.orc_ib_create(self.level(1), C.byref(self._ib)) != 0:
+        if self.lib.orc_ib_create(self.level(self.nlev - 1), C.byref(self._ib)) != 0:
             raise RuntimeError("oracle: ib_create failed")
 
     def step(self, n: int = 1):
-        self.lib.orc2_step(self.h, int(n))
+        self.lib.orcN_step(self.h, int(n))
 
     def get_f(self, lev):
         out = np.zeros((self.q,) + self.shapes[lev])
@@ -415,19 +422,33 @@ class CpuTwoLevel:
 
     def force_record(self):
         out = np.zeros(FORCE_REC)
-        self.lib.orc_force_record(self.level(1), _dp(out))
+        self.lib.orc_force_record(self.level(self.nlev - 1), _dp(out))
         return out
 
     def marker_force_sum(self):
         out = np.zeros(3)
-        self.lib.orc_ib_marker_force_sum(self.level(1), _dp(out))
+        self.lib.orc_ib_marker_force_sum(self.level(self.nlev - 1), _dp(out))
         return out
 
 
-# ---------------------------------------------------------------------------
-# Derived fields and refinement tags, restated for checking (numpy, FP64, the
-# reference's operation order; every operation is one IEEE rounding)
-# ---------------------------------------------------------------------------
+class CpuTwoLevel(CpuHierarchy):
+    """The two-level hierarchy of a ``cases.TwoLevelCase``: coarse level = the
+    domain, one fine box of ratio 2."""
+
+    class _HC:
+        def __init__(self, tl):
+            self.coarse, self.nlev = tl.coarse, 2
+            self.boxes = ((tl.fine_lo, tl.fine_hi),)
+            self._tl = tl
+
+        def box_case(self, l):
+            return self.coarse if l == 0 else self._tl.fine_box()
+
+    def __init__(self, tl):
+        self.tl = tl
+        super().__init__(CpuTwoLevel._HC(tl))
+
+
 def vorticity_pressure(mg, ng: int, dim: int, dx: float, dy: float, dz: float):
     """vorticityDiagnostic / visPara (Source/LBM/visPara.H:10-54) on the valid
     cells of a FillPatched macro array mg[comp, k, j, i] (comps rho, u, v, w,

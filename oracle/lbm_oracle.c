@@ -296,7 +296,10 @@ static void fill_boundary(const orc_level *L, double *a, int nc) {
  * MultiFab::LinComb, a*old + b*new) */
 static double cf_coarse(const orc_level *F, int n, int i, int j, int k) {
   const orc_level *C = F->cf;
-  const long e = IX(C, i, j, k) + (long)n * C->gcells;
+  /* (i,j,k) in the coarse level's domain index space; C's own box starts at
+   * C->cflo there (0 for the coarsest level) */
+  const long e = IX(C, i - C->cflo[0], j - C->cflo[1], (C->dim == 3) ? k - C->cflo[2] : 0) +
+                 (long)n * C->gcells;
   if (F->cf_mode == 0) return C->mac_old[e];
   if (F->cf_mode == 1) return C->mac_new[e];
   return F->cf_a * C->mac_old[e] + F->cf_b * C->mac_new[e];
@@ -1469,120 +1472,169 @@ double orc_overlap(double xa, double xb, double h, int type, double plo, int ilo
 }
 
 /* ------------------------------------------------------------------------ */
-/* static two-level hierarchy: AmrCoreLBM::timeStepWithSubcycling           */
+/* static hierarchy: AmrCoreLBM::timeStepWithSubcycling                     */
 /* (Source/Core/AmrCoreLBM.cpp:1690-1755) for a coarse level equal to the   */
-/* domain and one fine box of ratio 2 inside it, fixed (no regrid)          */
+/* domain and one box per finer level (ratio 2, properly nested), fixed (no */
+/* regrid)                                                                  */
 /* ------------------------------------------------------------------------ */
+#define ORC_MAX_LEV 8
 typedef struct {
-  orc_level *C, *F;
-  int flo[3], fhi[3]; /* fine box in fine-domain index space */
-} orc_two;
+  int n;
+  orc_level *lv[ORC_MAX_LEV];
+  int lo[ORC_MAX_LEV][3], hi[ORC_MAX_LEV][3]; /* level boxes in their own domain indices */
+} orc_hier;
 
 /* amrex::average_down of ratio 2 (AverageDownTo, AmrCoreLBM.cpp:1519-1527):
- * each covered coarse cell gets the mean of its fine cells, summed k, j, i
- * inner and scaled by the volume fraction */
-static void average_down(const orc_two *T, const double *fine, double *crse, int nc) {
-  const orc_level *C = T->C, *F = T->F;
+ * each coarse cell covered by the fine box [flo, fhi] gets the mean of its
+ * fine cells, summed k, j, i inner and scaled by the volume fraction */
+static void average_down(const orc_level *C, const orc_level *F, const int *flo, const int *fhi,
+                         const double *fine, double *crse, int nc) {
   const int kr = (C->dim == 3) ? 2 : 1;
   const double volfrac = (C->dim == 3) ? 0.125 : 0.25;
-  const int ck0 = (C->dim == 3) ? T->flo[2] / 2 : 0, ck1 = (C->dim == 3) ? T->fhi[2] / 2 : 0;
+  const int ck0 = (C->dim == 3) ? flo[2] / 2 : 0, ck1 = (C->dim == 3) ? fhi[2] / 2 : 0;
+  const int cz = (C->dim == 3) ? C->cflo[2] : 0;
   for (int n = 0; n < nc; ++n)
     for (int kc = ck0; kc <= ck1; ++kc)
-      for (int jc = T->flo[1] / 2; jc <= T->fhi[1] / 2; ++jc)
-        for (int ic = T->flo[0] / 2; ic <= T->fhi[0] / 2; ++ic) {
+      for (int jc = flo[1] / 2; jc <= fhi[1] / 2; ++jc)
+        for (int ic = flo[0] / 2; ic <= fhi[0] / 2; ++ic) {
           double c = 0.0;
           for (int kk = 0; kk < kr; ++kk)
             for (int jj = 0; jj < 2; ++jj)
               for (int ii = 0; ii < 2; ++ii) {
-                const int fi = 2 * ic + ii - T->flo[0], fj = 2 * jc + jj - T->flo[1];
-                const int fk = (C->dim == 3) ? 2 * kc + kk - T->flo[2] : 0;
+                const int fi = 2 * ic + ii - flo[0], fj = 2 * jc + jj - flo[1];
+                const int fk = (C->dim == 3) ? 2 * kc + kk - flo[2] : 0;
                 c += fine[IX(F, fi, fj, fk) + (long)n * F->gcells];
               }
-          crse[IX(C, ic, jc, kc) + (long)n * C->gcells] = volfrac * c;
+          crse[IX(C, ic - C->cflo[0], jc - C->cflo[1], kc - cz) + (long)n * C->gcells] = volfrac * c;
         }
 }
 
-/* coarse case c, fine box [flo, fhi] (fine-domain indices, even lo, odd hi,
- * at least two coarse cells away from every face of the domain) */
-void *orc2_create(const ilbm_case *c, const int *flo, const int *fhi) {
-  for (int d = 0; d < c->dim; ++d) {
-    if ((flo[d] & 1) || !(fhi[d] & 1) || fhi[d] < flo[d]) return NULL;
-    if (flo[d] / 2 < 2 || fhi[d] / 2 > c->n_cell[d] - 3) return NULL;
-  }
-  orc_two *T = (orc_two *)calloc(1, sizeof(orc_two));
-  T->C = (orc_level *)orc_create(c);
-  ilbm_case fc = *c;
-  const double dxf = (c->prob_hi[0] - c->prob_lo[0]) / (double)c->n_cell[0] / 2.0;
+/* coarse case c and nlev - 1 finer boxes: box l (l = 1..nlev-1) is
+ * lohi[6(l-1) .. 6(l-1)+5] = lo xyz, hi xyz in level l's domain indices (even
+ * lo, odd hi, its coarsened box at least two cells inside level l-1's box,
+ * and inside the domain by two cells for level 1) */
+void *orcN_create(const ilbm_case *c, int nlev, const int *lohi) {
+  if (nlev < 1 || nlev > ORC_MAX_LEV) return NULL;
+  orc_hier *H = (orc_hier *)calloc(1, sizeof(orc_hier));
+  H->n = nlev;
   for (int d = 0; d < 3; ++d) {
-    T->flo[d] = (d < c->dim) ? flo[d] : 0;
-    T->fhi[d] = (d < c->dim) ? fhi[d] : 0;
-    if (d < c->dim) {
-      fc.n_cell[d] = fhi[d] - flo[d] + 1;
-      fc.prob_lo[d] = c->prob_lo[d] + dxf * (double)flo[d];
-      fc.prob_hi[d] = c->prob_lo[d] + dxf * (double)(fhi[d] + 1);
-    }
-    fc.periodic[d] = 0;
-    fc.bc_lo[d] = fc.bc_hi[d] = BC_FOEXTRAP; /* unused: every ghost is coarse-fine */
+    H->lo[0][d] = 0;
+    H->hi[0][d] = (d < c->dim) ? c->n_cell[d] - 1 : 0;
   }
-  T->F = (orc_level *)orc_create(&fc);
-  if (!T->C || !T->F) return NULL;
-  T->F->cf = T->C;
-  for (int d = 0; d < 3; ++d) T->F->cflo[d] = T->flo[d];
-  return T;
-}
-
-void orc2_destroy(void *h) {
-  orc_two *T = (orc_two *)h;
-  orc_destroy(T->C);
-  orc_destroy(T->F);
-  free(T);
-}
-
-void *orc2_level(void *h, int lev) { orc_two *T = (orc_two *)h; return lev ? T->F : T->C; }
-
-/* one coarse step: the coarse level, two fine substeps with their coarse-fine
- * ghosts at times t and t + dt/2, average-down; the force record of the fine
- * level once per coarse step (Evolve, AmrCoreLBM.cpp:361-420) */
-int orc2_step(void *h, int nsteps) {
-  orc_two *T = (orc_two *)h;
-  orc_level *C = T->C, *F = T->F;
-  for (int s = 0; s < nsteps; ++s) {
-    const double t_old = C->time, t_new = C->time + C->dt;
-    level_step(C);
-    C->time = t_new;
-    C->step += 1;
-    for (int sub = 0; sub < 2; ++sub) {
-      const double t = t_old + (double)sub * F->dt;
-      /* GetDataMacro(0, t): within teps of t_new / t_old, else both */
-      const double teps = dmax(1.e-12, fabs(t_new - t_old) * 1.e-3);
-      if (t >= t_new - teps && t <= t_new + teps) F->cf_mode = 1;
-      else if (t >= t_old - teps && t <= t_old + teps) F->cf_mode = 0;
-      else {
-        F->cf_mode = 2;
-        F->cf_a = (t_new - t) / (t_new - t_old);
-        F->cf_b = (t - t_old) / (t_new - t_old);
+  for (int l = 1; l < nlev; ++l)
+    for (int d = 0; d < 3; ++d) {
+      H->lo[l][d] = (d < c->dim) ? lohi[6 * (l - 1) + d] : 0;
+      H->hi[l][d] = (d < c->dim) ? lohi[6 * (l - 1) + 3 + d] : 0;
+      if (d >= c->dim) continue;
+      const int plo = H->lo[l - 1][d], phi = H->hi[l - 1][d];
+      if ((H->lo[l][d] & 1) || !(H->hi[l][d] & 1) || H->hi[l][d] < H->lo[l][d] ||
+          H->lo[l][d] / 2 < plo + 2 || H->hi[l][d] / 2 > phi - 2) {
+        free(H);
+        return NULL;
       }
-      F->time = t;
-      level_step(F);
-      F->step += 1;
     }
-    F->time = t_new;
-    average_down(T, F->f_new, C->f_new, C->Q);
-    average_down(T, F->mac_new, C->mac_new, 6);
-    compute_ib_force(F);
+  H->lv[0] = (orc_level *)orc_create(c);
+  if (!H->lv[0]) { free(H); return NULL; }
+  double dx = (c->prob_hi[0] - c->prob_lo[0]) / (double)c->n_cell[0];
+  for (int l = 1; l < nlev; ++l) {
+    dx *= 0.5;
+    ilbm_case fc = *c;
+    for (int d = 0; d < 3; ++d) {
+      if (d < c->dim) {
+        fc.n_cell[d] = H->hi[l][d] - H->lo[l][d] + 1;
+        fc.prob_lo[d] = c->prob_lo[d] + dx * (double)H->lo[l][d];
+        fc.prob_hi[d] = c->prob_lo[d] + dx * (double)(H->hi[l][d] + 1);
+      }
+      fc.periodic[d] = 0;
+      fc.bc_lo[d] = fc.bc_hi[d] = BC_FOEXTRAP; /* unused: every ghost is coarse-fine */
+    }
+    H->lv[l] = (orc_level *)orc_create(&fc);
+    if (!H->lv[l]) return NULL;
+    H->lv[l]->cf = H->lv[l - 1];
+    for (int d = 0; d < 3; ++d) H->lv[l]->cflo[d] = H->lo[l][d];
+  }
+  return H;
+}
+
+void orcN_destroy(void *h) {
+  orc_hier *H = (orc_hier *)h;
+  for (int l = 0; l < H->n; ++l) orc_destroy(H->lv[l]);
+  free(H);
+}
+
+void *orcN_level(void *h, int lev) { return ((orc_hier *)h)->lv[lev]; }
+
+/* timeStepWithSubcycling(lev): the level's step from its current time, then
+ * (below the finest level) two substeps of the next finer level with their
+ * coarse-fine ghosts at t and t + dt/2, then the average-down onto it */
+static void orcN_advance(orc_hier *H, int lev) {
+  orc_level *L = H->lv[lev];
+  const double t_old = L->time, t_new = L->time + L->dt;
+  level_step(L);
+  L->time = t_new;
+  L->step += 1;
+  if (lev + 1 >= H->n) return;
+  orc_level *F = H->lv[lev + 1];
+  for (int sub = 0; sub < 2; ++sub) {
+    const double t = t_old + (double)sub * F->dt;
+    /* GetDataMacro(lev, t): within teps of t_new / t_old, else both */
+    const double teps = dmax(1.e-12, fabs(t_new - t_old) * 1.e-3);
+    if (t >= t_new - teps && t <= t_new + teps) F->cf_mode = 1;
+    else if (t >= t_old - teps && t <= t_old + teps) F->cf_mode = 0;
+    else {
+      F->cf_mode = 2;
+      F->cf_a = (t_new - t) / (t_new - t_old);
+      F->cf_b = (t - t_old) / (t_new - t_old);
+    }
+    F->time = t;
+    orcN_advance(H, lev + 1);
+  }
+  F->time = t_new;
+  average_down(L, F, H->lo[lev + 1], H->hi[lev + 1], F->f_new, L->f_new, L->Q);
+  average_down(L, F, H->lo[lev + 1], H->hi[lev + 1], F->mac_new, L->mac_new, 6);
+}
+
+/* coarse steps of the whole hierarchy; the force record of the finest level
+ * once per coarse step (Evolve, AmrCoreLBM.cpp:361-420) */
+int orcN_step(void *h, int nsteps) {
+  orc_hier *H = (orc_hier *)h;
+  for (int s = 0; s < nsteps; ++s) {
+    orcN_advance(H, 0);
+    compute_ib_force(H->lv[H->n - 1]);
   }
   return 0;
 }
 
-/* InitData for two levels (AmrCoreLBM.cpp:704-722): each level's equilibrium
- * from its own macro fields, then AverageDown and macro_old = macro_new */
-int orc2_init_equilibrium(void *h) {
-  orc_two *T = (orc_two *)h;
-  orc_init_equilibrium(T->C);
-  orc_init_equilibrium(T->F);
-  average_down(T, T->F->f_new, T->C->f_new, T->C->Q);
-  average_down(T, T->F->mac_new, T->C->mac_new, 6);
-  memcpy(T->C->mac_old, T->C->mac_new, sizeof(double) * 6 * T->C->gcells);
-  memcpy(T->C->f_old, T->C->f_new, sizeof(double) * T->C->Q * T->C->gcells);
+/* InitData (AmrCoreLBM.cpp:704-722): each level's equilibrium from its own
+ * macro fields, then AverageDown from the finest level to the coarsest and
+ * macro_old = macro_new on the levels that have a finer one */
+int orcN_init_equilibrium(void *h) {
+  orc_hier *H = (orc_hier *)h;
+  for (int l = 0; l < H->n; ++l) orc_init_equilibrium(H->lv[l]);
+  for (int l = H->n - 1; l > 0; --l) {
+    orc_level *C = H->lv[l - 1], *F = H->lv[l];
+    average_down(C, F, H->lo[l], H->hi[l], F->f_new, C->f_new, C->Q);
+    average_down(C, F, H->lo[l], H->hi[l], F->mac_new, C->mac_new, 6);
+  }
+  for (int l = 0; l + 1 < H->n; ++l) {
+    orc_level *C = H->lv[l];
+    memcpy(C->mac_old, C->mac_new, sizeof(double) * 6 * C->gcells);
+    memcpy(C->f_old, C->f_new, sizeof(double) * C->Q * C->gcells);
+  }
   return 0;
 }
+
+/* the two-level hierarchy of the same driver: coarse case c, fine box
+ * [flo, fhi] (fine-domain indices) */
+void *orc2_create(const ilbm_case *c, const int *flo, const int *fhi) {
+  int lohi[6];
+  for (int d = 0; d < 3; ++d) {
+    lohi[d] = (d < c->dim) ? flo[d] : 0;
+    lohi[3 + d] = (d < c->dim) ? fhi[d] : 0;
+  }
+  return orcN_create(c, 2, lohi);
+}
+void orc2_destroy(void *h) { orcN_destroy(h); }
+void *orc2_level(void *h, int lev) { return orcN_level(h, lev); }
+int orc2_step(void *h, int nsteps) { return orcN_step(h, nsteps); }
+int orc2_init_equilibrium(void *h) { return orcN_init_equilibrium(h); }

@@ -83,6 +83,22 @@ def _order_sensitivity(name):
             "force": rel_l2(Fb, Fa), "cdcl": float(np.max(np.abs(rb[3:5] - ra[3:5]) / np.abs(ra[3])))}
 
 
+EXPLICIT = [n for n in WITH_IB if GOLDEN_CASES[n][0]()[2].coupling_method in (0, 2)]
+
+
+@pytest.mark.parametrize("name", EXPLICIT)
+def test_fp64_explicit_coupling_bit_exact(name):
+    """Explicit and explicit_diag coupling of a body whose markers do not move:
+    interpolation sums each stencil in the reference's order and spreading
+    adds the markers to each cell in marker order, so the FP64 populations,
+    macro fields and forces equal the reference build's bit for bit."""
+    cpu, gpu, ib = _pair(name)
+    np.testing.assert_array_equal(gpu.get_f(), cpu.get_f())
+    np.testing.assert_array_equal(gpu.get_macro(), cpu.get_macro())
+    np.testing.assert_array_equal(gpu.get_force(), cpu.get_force())
+    gpu.close()
+
+
 @pytest.mark.parametrize("name", WITH_IB)
 def test_fp64_ib_parity(name):
     """relative L2 <= 1e-12 (force field 1e-11, Cd / Cl 1e-9), or four times
