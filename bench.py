@@ -440,31 +440,45 @@ def run_batched(args, world, device):
                         "each case steps through its own IB (stored IVC inverse or CG)"}
 
 
-def run_two_level(args, world, device):
-    """The D2Q9 cylinder wake on two levels: base grid 1024 x 512, D = 40
-    base cells centred at (256, 256), inflow U = 0.05, Re = 100, one refined
-    level (ratio 2, max_level 1) over the fixed body-and-wake box of the
-    reference's refinement rule (1 R upstream, 4 R downstream, 2 R across,
-    plus a 6-cell pad) carrying the marker IBM with markers ~1 fine dx apart,
-    FP32 storage.  Cell updates per coarse step: coarse cells + 2 x fine
-    cells.  Beside it, the reference's CPU level step on the same two levels
-    (all host cores)."""
+def strouhal(cl: np.ndarray, dt: float, D: float, U: float):
+    """Shedding Strouhal number f D / U from a lift series: the mean period
+    between upward zero crossings of Cl - mean(Cl) (None without at least
+    two full periods)."""
+    x = np.asarray(cl, dtype=np.float64) - float(np.mean(cl))
+    up = np.nonzero((x[:-1] < 0.0) & (x[1:] >= 0.0))[0]
+    if len(up) < 3:
+        return None
+    # linear interpolation of each crossing
+    tc = up + x[up] / (x[up] - x[up + 1])
+    period = float(np.mean(np.diff(tc))) * dt
+    return D / (U * period) if period > 0 else None
+
+
+def run_cylinder(args, world, device):
+    """The D2Q9 cylinder wake of the 'two AMR levels' configuration: base grid
+    1024 x 512, D = 40 base cells centred at (256, 256), inflow U = 0.05,
+    Re = 100, max_level = 2 (ratio 2): the finest level over the body and near
+    wake (1 R upstream, 4 R downstream, 2 R across plus 6 base cells), the
+    middle level around it; the marker IBM on the finest level (markers ~1
+    finest dx apart), FP32 storage.  Cell updates per coarse step: coarse
+    cells + 2 x level-1 cells + 4 x level-2 cells.  MLUPS over --cyl-steps
+    coarse steps; then the Cd / Cl series of the configuration's 20,000 coarse
+    steps (time-centred body force, one record per coarse step taken while
+    the next step runs) with its mean Cd, rms Cl and Strouhal number.  Beside
+    it, the reference's CPU level step on the same three levels."""
     from ilbmrex_b200 import cases
-    from ilbmrex_b200.hierarchy import TwoLevelSolver
-    R, pad = 20.0, 6.0
-    tl, ib, ic, if_ = cases.cylinder_two_level(nx=1024, ny=512, D=2 * R, center=(256.0, 256.0), U=0.05,
-                                               Re=100.0, upstream=(R + pad) / (2 * R),
-                                               downstream=(4 * R + pad) / (2 * R),
-                                               cross=(2 * R + pad) / (2 * R))
-    nc = tl.coarse.cells
-    nf = int(np.prod(tl.fine_n_cell[: tl.dim]))
-    updates = nc + 2 * nf
-    S = TwoLevelSolver(tl, "f32", ib=ib, device=device.index or 0)
-    S.set_macro(ic(), if_())
+    from ilbmrex_b200.hierarchy import HierarchySolver
+    R, pad, U, D = 20.0, 6.0, 0.05, 40.0
+    hc, ib, inits = cases.cylinder_hierarchy(nx=1024, ny=512, D=D, center=(256.0, 256.0), U=U, Re=100.0,
+                                             nlev=3, upstream=(R + pad) / D, downstream=(4 * R + pad) / D,
+                                             cross=(2 * R + pad) / D)
+    updates = hc.updates_per_coarse_step()
+    S = HierarchySolver(hc, "f32", ib=ib, device=device.index or 0)
+    S.set_macro([init() for init in inits])
     S.step(3)
     S.ctx.sync()
     barrier(world)
-    K = args.two_level_steps
+    K = args.cyl_steps
     l0 = S.ctx.launches()
     S.ctx.record(8)
     S.step(K)
@@ -473,26 +487,56 @@ def run_two_level(args, world, device):
     launches = S.ctx.launches() - l0
     t = allreduce_max(S.ctx.elapsed_ms(8, 9), world, device)
     mlups = world * updates * K / (t * 1e-3) / 1e6
-    S.step(1, record_force=True)
-    cd = float(S.rec[3])
+    series = None
+    if args.cyl_series_steps > 0:
+        n = args.cyl_series_steps - S.istep
+        cd, cl = np.zeros(n), np.zeros(n)
+        t0 = time.perf_counter()
+        prev = None
+        for i in range(n):
+            S.advance(record_force=True, pipelined=True)
+            if prev is not None:
+                cd[i - 1], cl[i - 1] = S.rec[3], S.rec[4]
+            prev = i
+        S.flush_records()
+        cd[n - 1], cl[n - 1] = S.rec[3], S.rec[4]
+        wall = time.perf_counter() - t0
+        tail = slice(3 * n // 4, n)
+        cdm = float(np.mean(cd[tail]))
+        clr = float(np.std(cl[tail]))
+        # a Strouhal number needs an oscillating lift (shedding): below 1e-3 Cd
+        # the lift is round-off around the symmetric state
+        st = strouhal(cl[tail], 1.0, D, U) if clr > 1e-3 * abs(cdm) else None
+        series = {"coarse_steps": int(S.istep), "wall_s": round(wall, 2),
+                  "cd_mean_last_quarter": round(cdm, 4), "cl_rms_last_quarter": float(f"{clr:.3e}"),
+                  "shedding": st is not None,
+                  "strouhal_last_quarter": None if st is None else round(st, 4),
+                  "cd_in_band_1.2_1.8": bool(1.2 <= cdm <= 1.8),
+                  "strouhal_at_least_0.14": None if st is None else bool(st >= 0.14),
+                  "band_source": "Examples/Cylinder_flow/analyze_force.py:29-32, 148-151",
+                  "cd_every_1000": [round(float(v), 4) for v in cd[999::1000]],
+                  "cl_every_1000": [round(float(v), 4) for v in cl[999::1000]]}
+    n_mark = C.c_int64()
+    S.L.ilbm_ib_num_markers(S.ib, C.byref(n_mark))
     S.close()
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         try:
-            dt, threads, kind, timed = cpu_reference_levels([(tl.coarse, ic, 1.0), (tl.fine_box(), if_, 2.0)],
-                                                            5, 3, budget_s=30.0)
+            levels = [(hc.box_case(l), inits[l], float(2 ** l)) for l in range(hc.nlev)]
+            dt, threads, kind, timed = cpu_reference_levels(levels, 5, 3, budget_s=30.0)
             cpu = {"value": round(updates / dt / 1e6, 3), "unit": "MLUPS", "cores": threads, "kind": kind,
-                   "sample": f"{timed} level steps each of the coarse level and of the fine box after 3 "
-                             "warm-up steps, timed as coarse + 2 x fine per coarse step (the body's forcing, "
-                             "the coarse-fine fill and the average-down not included); reference sources "
-                             "compiled in place, float, OpenMP"}
+                   "sample": f"{timed} level steps of each level after 3 warm-up steps, timed as coarse + "
+                             "2 x level 1 + 4 x level 2 per coarse step (the body's forcing, the coarse-fine "
+                             "fill and the average-down not included); reference sources compiled in place, "
+                             "float, OpenMP"}
         except Exception as e:  # the checker is optional at run time
             cpu = {"value": None, "unit": "MLUPS", "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
-    return {"metric": "two-level MLUPS (D2Q9 cylinder wake 1024x512 + 1 refined level, FP32)",
+    return {"metric": "MLUPS, D2Q9 cylinder wake 1024x512 with 2 refined levels (max_level 2), FP32",
             "value": round(mlups, 2), "unit": "MLUPS", "ms_per_coarse_step": round(t / K, 4),
-            "coarse_cells": nc, "fine_cells": nf, "fine_box": [list(tl.fine_lo[:2]), list(tl.fine_hi[:2])],
+            "levels": [{"box": [list(hc.box_lohi(l)[0][:2]), list(hc.box_lohi(l)[1][:2])],
+                        "cells": hc.cells(l)} for l in range(hc.nlev)],
             "updates_per_coarse_step": updates, "steps": K, "gpu_launches": int(launches),
-            "cd_after": round(cd, 5), "cpu_baseline": cpu}
+            "ib_markers": int(n_mark.value), "cd_cl_series": series, "cpu_baseline": cpu}
 
 
 def run_served(args, world, device):
@@ -604,9 +648,9 @@ def run_b200(args):
     from ilbmrex_b200 import capi, cases
     from ilbmrex_b200.level import LevelSolver
 
-    if args.only_batched or args.only_served or args.only_two_level:  # profiling aids: one workload alone
-        if args.only_two_level:
-            out = run_two_level(args, world, device)
+    if args.only_batched or args.only_served or args.only_cylinder:  # profiling aids: one workload alone
+        if args.only_cylinder:
+            out = run_cylinder(args, world, device)
         else:
             out = run_batched(args, world, device) if args.only_batched else run_served(args, world, device)
         if rank == 0:
@@ -661,6 +705,12 @@ def run_b200(args):
     kern_ms = level_step_ms(S.L, ctx, Cl.box(Cl.f, Cl.f_next), S.pc, max(3, min(K, 20)))
     peak, peak_kind = peaks()
     achieved = B_cell * cells_c / (kern_ms * 1e-3) / 1e9
+    # the same kernel on the fine level as the hierarchy runs it (caller-filled
+    # ghosts, the body's force arrays on its band)
+    Fl = S.F
+    fine_ms = level_step_ms(S.L, ctx, Fl.box(Fl.f, Fl.f_next, force=Fl.fa, force_prev=Fl.fb), S.pf,
+                            max(3, min(K, 20)))
+    fine_achieved = B_cell * cells_f / (fine_ms * 1e-3) / 1e9
 
     # ---- end-to-end through the public call: per coarse step the host
     # parameter structs go down and the force record (Eulerian and marker
@@ -711,9 +761,9 @@ def run_b200(args):
     served = None
     if not args.no_served:
         served = run_served(args, world, device)
-    two_level = None
-    if not args.no_two_level:
-        two_level = run_two_level(args, world, device)
+    cylinder = None
+    if not args.no_cylinder:
+        cylinder = run_cylinder(args, world, device)
 
     if rank == 0:
         line = {
@@ -728,7 +778,12 @@ def run_b200(args):
                                    "leading blocks), timed alone on the 256x128x128 coarse level",
                          "kernel_ms": round(kern_ms, 4), "bytes_per_cell": B_cell,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
-                         if peak_kind == "measured" else "fallback 6650 GB/s"},
+                         if peak_kind == "measured" else "fallback 6650 GB/s",
+                         "fine_level": {"kernel_ms": round(fine_ms, 4), "cells": cells_f,
+                                        "achieved": round(fine_achieved, 1),
+                                        "frac": round(fine_achieved / peak, 4),
+                                        "what": "k_step on the 192x128x128 fine box (caller-filled "
+                                                "ghosts, body force arrays on its band)"}},
             "cpu_baseline": cpu_base,
             "e2e": {"value": round(e2e, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -742,7 +797,7 @@ def run_b200(args):
             "single_level": single,
             "batched": batched,
             "served": served,
-            "two_level": two_level,
+            "cylinder_three_levels": cylinder,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -766,10 +821,12 @@ def main():
     ap.add_argument("--no-precision", action="store_true", help="skip the storage-form error check")
     ap.add_argument("--precision-steps", type=int, default=200)
     ap.add_argument("--no-served", action="store_true", help="skip the served workload")
-    ap.add_argument("--no-two-level", action="store_true", help="skip the two-level cylinder workload")
-    ap.add_argument("--two-level-steps", type=int, default=100)
-    ap.add_argument("--only-two-level", action="store_true",
-                    help="run only the two-level cylinder workload and print its result (profiling aid)")
+    ap.add_argument("--no-cylinder", action="store_true", help="skip the three-level cylinder workload")
+    ap.add_argument("--cyl-steps", type=int, default=200, help="timed coarse steps of the cylinder")
+    ap.add_argument("--cyl-series-steps", type=int, default=20000,
+                    help="coarse steps of the cylinder's Cd / Cl series (0: none)")
+    ap.add_argument("--only-cylinder", action="store_true",
+                    help="run only the three-level cylinder workload and print its result (profiling aid)")
     ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-rate", type=float, default=200.0, help="arrivals per second")
     ap.add_argument("--serve-scale", type=float, default=0.5)

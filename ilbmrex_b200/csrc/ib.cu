@@ -172,8 +172,8 @@ __global__ void k_markers(IBArgs a, double *xyz, const double *ref, double *tgt,
 // direction are evaluated once (the reference re-evaluates the same values
 // inside its loops) and the 5^d stencil points are spread over the lanes;
 // products keep the reference's (tU*tV)*tW order, the sum is a fixed-order
-// warp reduction.  The single-body path sums in the reference's own order
-// (interp_seq below).
+// warp reduction.  With FP64 storage the single-body path sums in the
+// reference's own order instead (interp_seq below).
 __device__ __forceinline__ void marker_weights(const IBArgs &a, double px, double py, double pz,
                                                int lane, int &i0, int &j0, int &k0,
                                                double &wx, double &wy, double &wz) {
@@ -1146,6 +1146,15 @@ __global__ void __launch_bounds__(128) k_spread(IBArgs a, const double *xyz, con
   const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (m >= a.n) return;
   spread_one(a, m, lane, xyz, F, EFI, status);
+}
+
+__global__ void __launch_bounds__(128) k_interp(IBArgs a, const double *xyz, const double *EV,
+                                                double *uvw, int *status, const double *tgt,
+                                                double *rhs, int ld) {
+  const int lane = threadIdx.x & 31;
+  const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (m >= a.n) return;
+  interp_one(a, m, lane, xyz, EV, uvw, status, tgt, rhs, ld);
 }
 
 // ---------------------------------------------------------------------------
@@ -2212,12 +2221,21 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *boxes, int nbox, const ilbm_le
   bool any_periodic_band = false;
   for (int d = 0; d < ib->dim; ++d)
     any_periodic_band = any_periodic_band || (ib->g.periodic[d] && ib->blo[d] < 0);
+  // FP64 storage (the parity form) sums interpolation and spreading in the
+  // reference's order; the 4- and 2-byte forms use the warp-parallel
+  // interpolation and atomic spreading, which are faster and whose rounding
+  // order is far below those forms' own precision
+  const bool ordered = ctx->storage == ILBM_STORAGE_F64;
   for (int it = 0; it < nloop; ++it) {
     cudaMemsetAsync(ib->d_EFI, 0, 3 * ib->nb * sizeof(double), s);
     k_markers<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_ref, ib->d_tgt, ib->d_uvw, ib->d_F);
     if (any_periodic_band) k_fill_boundary<<<gb, 256, 0, s>>>(a, ib->d_EV);
-    k_interp_seq<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_EV, ib->d_uvw, ib->d_status, ib->d_tgt,
-                                       use_dense ? ib->d_rhs : nullptr, ib->ld);
+    if (ordered)
+      k_interp_seq<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_EV, ib->d_uvw, ib->d_status, ib->d_tgt,
+                                         use_dense ? ib->d_rhs : nullptr, ib->ld);
+    else
+      k_interp<<<wblk, 128, 0, s>>>(a, ib->d_xyz, ib->d_EV, ib->d_uvw, ib->d_status, ib->d_tgt,
+                                    use_dense ? ib->d_rhs : nullptr, ib->ld);
     ctx->launches += 2 + (any_periodic_band ? 1 : 0);
     if (ivc) {
       if (!ib->csr_ready || ib->moving || ib->p.ivc_rebuild_matrix > 0) {
@@ -2264,7 +2282,7 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *boxes, int nbox, const ilbm_le
       k_force_explicit<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_F);
       ctx->launches++;
     }
-    if (ib->gather) {
+    if (ordered && ib->gather) {
       SpreadW *sw = static_cast<SpreadW *>(ib->d_sw);
       k_spread_weights<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, sw);
       k_spread_gather<<<(ib->gather_cells + 127) / 128, 128, 0, s>>>(
