@@ -341,6 +341,35 @@ class LevelSolver:
         for _ in range(n):
             self.advance_phi_at_level(record_force=record_force)
 
+    def run_recorded(self, n: int) -> np.ndarray:
+        """n steps queued back to back, each followed by its force record
+        copied to pinned host memory in stream order
+        (ilbm_force_record_async), with one synchronisation at the end;
+        returns the n force records (the rows of force_record).  Without a
+        body it is n plain steps and returns an empty array."""
+        if self.ib is None:
+            self.step(n)
+            self.ctx.sync()
+            return np.zeros((0, 18))
+        buf = torch.empty((n, 8), dtype=torch.float64, pin_memory=True)
+        lo, hi = self.force_region
+        lo3, hi3 = capi.ivec3(lo), capi.ivec3(hi)
+        for i in range(n):
+            self.advance_phi_at_level()
+            b = self._box(self.f, None, force=self.force_prev)
+            capi.check(self.L.ilbm_force_record_async(self.ctx.h, C.byref(b), 1, self.ib, lo3, hi3,
+                                                      buf[i].data_ptr()), "force_record_async")
+        self.ctx.sync()
+        r = buf.numpy().copy()
+        for w, bit, msg in ((0, 1, "IB stencil left the support band"), (0, 2, "IVC operator capacity"),
+                            (0, 4, "IVC conjugate gradient did not converge"),
+                            (1, 8, "IVC operator has a non-positive pivot")):
+            if np.any(r[:, 6 + w].astype(np.int64) & bit):
+                raise capi.IlbmError(f"force_record_async: {msg}")
+        recs = self.force_records(r[:, 0:3], r[:, 3:6])
+        self.rec = recs[-1].copy()
+        return recs
+
     # ---- force evaluation (ComputeIBForce, AmrCoreLBM.cpp:456-631) --------
     def compute_ib_force(self):
         lo, hi = self.force_region

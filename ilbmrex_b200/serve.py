@@ -217,16 +217,15 @@ class Server:
 
 
 def run_alone(req: Request, storage: str = "f32", device: int = 0, keep_f: bool = False) -> Request:
-    """The same request through the plain single-case call, for comparison."""
+    """The same request through the plain single-case call, for comparison:
+    its steps queued back to back through ilbm_advance_level, each step's
+    force record copied to pinned memory in stream order and read once at
+    the end (LevelSolver.run_recorded)."""
     S = LevelSolver(req.case, storage, ib=req.ib, device=device)
     S.set_macro(*req.init())
-    cd = []
-    for _ in range(req.steps):
-        S.advance_phi_at_level(record_force=req.ib is not None)
-        if req.ib is not None:
-            cd.append(S.rec[3:5].copy())
+    recs = S.run_recorded(req.steps)
     out = Request(req.rid, req.kind, req.case, req.ib, req.init, req.steps, req.arrival)
-    out.cd_cl = np.array(cd) if cd else None
+    out.cd_cl = recs[:, 3:5].copy() if req.ib is not None else None
     out.mean_u = S.mean_velocity()
     out.f_final = S.get_f() if keep_f else None
     S.close()
