@@ -156,14 +156,17 @@ def uniform_init(case: LevelCase, rho=1.0, u=(0.0, 0.0, 0.0)):
 
 
 def cylinder(nx=1024, ny=512, D=40.0, center=(256.0, 256.0), U=0.05, Re=100.0, dx=1.0,
-             coupling=1, n_marker=0):
+             coupling=1, n_marker=0, inflow_uy=0.0):
     """2D flow past a cylinder: ext_dir inflow (rho=1, u=U) at x-lo,
-    foextrap outflow at x-hi, periodic in y, marker IBM with IVC coupling."""
+    foextrap outflow at x-hi, periodic in y, marker IBM with IVC coupling.
+    `inflow_uy` is the inflow's transverse velocity (the deck's
+    amrbc.bc_lo_0_uy_val, 1e-4 in Examples/Cylinder_flow/inputs), which breaks
+    the symmetry so that the wake starts shedding within the run."""
     nu = U * D / Re
     case = LevelCase(D2Q9, (nx, ny, 1), prob_hi=(nx * dx, ny * dx, 1.0),
                      periodic=(False, True, True), bc_lo=(EXT_DIR, INT_DIR, INT_DIR),
                      bc_hi=(FOEXTRAP, INT_DIR, INT_DIR),
-                     bc_lo_val=(_bcv(1.0, U), _bcv(0.0), _bcv(0.0)), nu=nu,
+                     bc_lo_val=(_bcv(1.0, U, inflow_uy), _bcv(0.0), _bcv(0.0)), nu=nu,
                      name=f"cylinder{nx}x{ny}")
     ib = MarkerIB(coupling_method=coupling, delta_type=4, loop_ns=1, ivc_diag_reg=1.3,
                   x0=center[0], y0=center[1], R=D / 2.0, U0=U, n_marker=n_marker)
@@ -500,14 +503,14 @@ def nested_boxes(finest_lo, finest_hi, nlev: int, n_cell, dim: int, grow: int = 
 
 
 def cylinder_hierarchy(nx=1024, ny=512, D=40.0, center=(256.0, 256.0), U=0.05, Re=100.0, nlev=3,
-                       upstream=1.0, downstream=4.0, cross=1.5, grow=8):
+                       upstream=1.0, downstream=4.0, cross=1.5, grow=8, inflow_uy=0.0):
     """The reference's 2D cylinder deck on nlev levels (Examples/Cylinder_flow/
     inputs, ref_ratio 2): coarse level as ``cylinder``; the finest box around
     the body and its near wake (upstream / downstream / cross extents in
     diameters from the centre), every level in between the finer box
     coarsened and grown by `grow` of its cells.  The marker IBM runs on the
     finest level with markers about one finest cell apart."""
-    case, ib, init_c = cylinder(nx=nx, ny=ny, D=D, center=center, U=U, Re=Re)
+    case, ib, init_c = cylinder(nx=nx, ny=ny, D=D, center=center, U=U, Re=Re, inflow_uy=inflow_uy)
     r = 2 ** (nlev - 1)
     dx = case.dx
     flo = [int(math.floor((center[0] - upstream * D) / dx * r)), int(math.floor((center[1] - cross * D) / dx * r))]
