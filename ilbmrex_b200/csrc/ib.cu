@@ -38,6 +38,9 @@ int box_step_args(const ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_param
                   StepArgs *out);
 int band_macro_boxes(ilbm_ctx *ctx, const StepArgs *d_args, int nargs, const int *blo,
                      const int *bn, double *EV, double *RHO, cudaStream_t st);
+int band_macro_list(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p, const int *blo,
+                    const int *bn, const int64_t *cells, int ncells, double *EV, double *RHO,
+                    cudaStream_t st);
 int level_step_split(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p,
                      const int *blo, const int *bhi, cudaEvent_t band_ready);
 }
@@ -1353,11 +1356,13 @@ __device__ __forceinline__ double table_weight(const SpreadW *W, int m, int lane
   return (lane < 16) ? reinterpret_cast<const double *>(W + m)[lane] : 0.0;
 }
 
+// fresh: the markers' velocities and forces start from zero here (the
+// zeroing of k_markers, for bodies whose positions need no update)
 __global__ void __launch_bounds__(128) k_interp_w(IBArgs a, const double *xyz,
                                                   const SpreadW *__restrict__ W,
                                                   const double *__restrict__ EV, double *uvw,
-                                                  int *status, const double *tgt, double *rhs,
-                                                  int ld) {
+                                                  double *F, int fresh, int *status,
+                                                  const double *tgt, double *rhs, int ld) {
   const int lane = threadIdx.x & 31;
   const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (m >= a.n) return;
@@ -1406,9 +1411,15 @@ __global__ void __launch_bounds__(128) k_interp_w(IBArgs a, const double *xyz,
       v /= part;
       w /= part;
     }
-    u += uvw[m];
-    v += uvw[m + a.n];
-    w += uvw[m + 2 * a.n];
+    if (fresh) {
+      F[m] = 0.0;
+      F[m + a.n] = 0.0;
+      F[m + 2 * a.n] = 0.0;
+    } else {
+      u += uvw[m];
+      v += uvw[m + a.n];
+      w += uvw[m + 2 * a.n];
+    }
     uvw[m] = u;
     uvw[m + a.n] = v;
     uvw[m + 2 * a.n] = w;
@@ -2117,6 +2128,9 @@ int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom
   }
   cudaMemsetAsync(ib->d_status, 0, 2 * sizeof(int), ctx->stream);
   cudaMemsetAsync(ib->d_fsum, 0, 4 * sizeof(double), ctx->stream);
+  // band fields finite everywhere (a fixed body forms them on its stencils only)
+  cudaMemsetAsync(ib->d_EV, 0, 3 * (size_t)ib->nb * sizeof(double), ctx->stream);
+  cudaMemsetAsync(ib->d_RHO, 0, (size_t)ib->nb * sizeof(double), ctx->stream);
   if ((rc = build_gather(ib))) {
     ilbm_ib_destroy(ib);
     return rc;
@@ -2341,12 +2355,24 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *boxes, int nbox, const ilbm_le
       return ILBM_ERR_ARG;
     }
   }
-  // EulerVel / rho on the band (:1541-1566, FillBoundary :702-703)
+  const bool ivc_ = ib->p.coupling_method == 1;
+  const bool single_ = ivc_ || std::max(ib->p.loop_ns, 1) == 1;
+  bool periodic_band = false;
+  for (int d = 0; d < ib->dim; ++d)
+    periodic_band = periodic_band || (ib->g.periodic[d] && ib->blo[d] < 0);
+  // EulerVel / rho on the band (:1541-1566, FillBoundary :702-703).  A body
+  // whose markers do not move reads them only on the cells its stencils
+  // reach (its spreading table): only those are formed.  The rest of the band
+  // keeps finite values (zero at creation), which meet a zero spread force
+  // in the export.
   int rc;
   if (multi) {
     if ((rc = ib_box_table(ib, boxes, nbox, lp, s))) return rc;
     rc = band_macro_boxes(ctx, ib->d_boxargs, (int)ib->h_boxargs.size(), ib->blo, ib->bn, ib->d_EV,
                           ib->d_RHO, s);
+  } else if (ib->gather && single_ && !periodic_band) {
+    rc = band_macro_list(ctx, *box, lp, ib->blo, ib->bn, ib->d_gcell, ib->gather_cells, ib->d_EV,
+                         ib->d_RHO, s);
   } else {
     rc = band_macro(ctx, *box, lp, ib->blo, ib->bn, ib->d_EV, ib->d_RHO, s);
   }
@@ -2384,18 +2410,21 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *boxes, int nbox, const ilbm_le
   const bool table = ib->gather && !ordered;
   for (int it = 0; it < nloop; ++it) {
     cudaMemsetAsync(ib->d_EFI, 0, 3 * ib->nb * sizeof(double), s);
-    k_markers<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_ref, ib->d_tgt, ib->d_uvw, ib->d_F);
+    // a fixed body's markers need no position update: the table-driven
+    // interpolation zeroes their velocities and forces itself
+    const bool fresh = table && ib->p.geometry_type != 2;
+    if (!fresh) k_markers<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_ref, ib->d_tgt, ib->d_uvw, ib->d_F);
     if (any_periodic_band) k_fill_boundary<<<gb, 256, 0, s>>>(a, ib->d_EV);
     if (ordered)
       k_interp_seq<<<nblk, nthr, 0, s>>>(a, ib->d_xyz, ib->d_EV, ib->d_uvw, ib->d_status, ib->d_tgt,
                                          use_dense ? ib->d_rhs : nullptr, ib->ld);
     else if (table)
-      k_interp_w<<<wblk, 128, 0, s>>>(a, ib->d_xyz, sw, ib->d_EV, ib->d_uvw, ib->d_status, ib->d_tgt,
-                                      use_dense ? ib->d_rhs : nullptr, ib->ld);
+      k_interp_w<<<wblk, 128, 0, s>>>(a, ib->d_xyz, sw, ib->d_EV, ib->d_uvw, ib->d_F, fresh ? 1 : 0,
+                                      ib->d_status, ib->d_tgt, use_dense ? ib->d_rhs : nullptr, ib->ld);
     else
       k_interp<<<wblk, 128, 0, s>>>(a, ib->d_xyz, ib->d_EV, ib->d_uvw, ib->d_status, ib->d_tgt,
                                     use_dense ? ib->d_rhs : nullptr, ib->ld);
-    ctx->launches += 2 + (any_periodic_band ? 1 : 0);
+    ctx->launches += (fresh ? 1 : 2) + (any_periodic_band ? 1 : 0);
     if (ivc) {
       if (!ib->csr_ready || ib->moving || ib->p.ivc_rebuild_matrix > 0) {
         const int cb = std::min(4096, (ib->n * 32 + 255) / 256);

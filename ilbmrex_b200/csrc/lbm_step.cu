@@ -841,6 +841,18 @@ __global__ void __launch_bounds__(256) k_band_macro(StepArgs a, int blo0, int bl
     band_macro_cell<L, S>(a, blo0, blo1, blo2, bn0, bn1, nb, t, EV, RHO);
 }
 
+// the band cells of a list (band indices): the cells a fixed body's stencils
+// reach, which are all that its interpolation and export read
+template <class L, int S>
+__global__ void __launch_bounds__(256) k_band_macro_list(StepArgs a, int blo0, int blo1, int blo2,
+                                                         int bn0, int bn1, int bn2,
+                                                         const int64_t *__restrict__ cells,
+                                                         int ncells, double *EV, double *RHO) {
+  const int64_t nb = (int64_t)bn0 * bn1 * bn2;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < ncells; r += gridDim.x * blockDim.x)
+    band_macro_cell<L, S>(a, blo0, blo1, blo2, bn0, bn1, nb, cells[r], EV, RHO);
+}
+
 template <class L, int S>
 __global__ void __launch_bounds__(256) k_band_macro_batch(const StepArgs *args, const BandDesc *bands,
                                                           const int64_t *off, int ncase,
@@ -930,6 +942,20 @@ static int launch_band_macro(ilbm_ctx *ctx, const StepArgs &a, const int *blo, c
   const int blocks = (int)std::min<int64_t>((nb + 255) / 256, 2048);
   k_band_macro<L, S><<<blocks, 256, 0, st>>>(a, blo[0], blo[1], blo[2], bn[0], bn[1], bn[2], EV,
                                               RHO);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "band macro launch");
+  return ILBM_OK;
+}
+
+template <class L, int S>
+static int launch_band_macro_list(ilbm_ctx *ctx, const StepArgs &a, const int *blo, const int *bn,
+                                  const int64_t *cells, int ncells, double *EV, double *RHO,
+                                  cudaStream_t st) {
+  if (ncells <= 0) return ILBM_OK;
+  const int blocks = std::min((ncells + 255) / 256, 2048);
+  k_band_macro_list<L, S><<<blocks, 256, 0, st>>>(a, blo[0], blo[1], blo[2], bn[0], bn[1], bn[2],
+                                                   cells, ncells, EV, RHO);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "band macro launch");
@@ -1189,6 +1215,16 @@ int band_macro(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p, con
   int rc = fill_args(ctx, b, p, a);
   if (rc) return rc;
   return ILBM_DISPATCH(ctx, launch_band_macro, ctx, a, blo, bn, EV, RHO, st);
+}
+
+// Band macro on the listed band cells only.
+int band_macro_list(ilbm_ctx *ctx, const ilbm_box &b, const ilbm_level_params *p, const int *blo,
+                    const int *bn, const int64_t *cells, int ncells, double *EV, double *RHO,
+                    cudaStream_t st) {
+  StepArgs a;
+  int rc = fill_args(ctx, b, p, a);
+  if (rc) return rc;
+  return ILBM_DISPATCH(ctx, launch_band_macro_list, ctx, a, blo, bn, cells, ncells, EV, RHO, st);
 }
 
 // StepArgs of one box of a level, for kernels that take several boxes
