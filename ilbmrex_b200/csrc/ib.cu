@@ -453,24 +453,35 @@ constexpr int kCgSharedN = 1024;
 // block.  warm: start from the previous solution in X_ (the force changes
 // little from one step to the next), else from zero.  Per iteration two
 // fused reductions (p.Ap; r.z and r.r) keep the block barriers to five.
+// hist: the solutions the start may use (0: none, 1: X, 2: X and Xh), kept
+// on the device so that the batched solves and the body's own alternate
+// freely; x0 = 0, X, or the extrapolation 2 X - Xh
 __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz, const double *tgt,
                                              const double *uvw, const int *rowptr, const int *col,
                                              const double *val, const double *diag, double *X_,
-                                             double *work, double *F, int maxit, double tol,
-                                             int *status, int *iters, int warm) {
+                                             double *Xh, int *hist, double *work, double *F,
+                                             int maxit, double tol, int *status, int *iters) {
   __shared__ double sh3[kMaxWarps][3], sh6[kMaxWarps][6];
   __shared__ double p_sh[3 * kCgSharedN];
+  __shared__ int sh_hist;
   const int n = a.n;
   double *r = work, *z = work + 3 * n, *Ap = work + 9 * n;
   double *p = (n <= kCgSharedN) ? p_sh : work + 6 * n;
-  // b (kept in Ap until the residual is formed), x0 = 0 or the previous x
+  if (threadIdx.x == 0) sh_hist = *hist;
+  __syncthreads();
+  const int h = sh_hist;
+  const int warm = h < 2 ? h : 2;
+  // b (kept in Ap until the residual is formed), x0
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double Ux, Uy, Uz;
     target_of(a, i, xyz, tgt, Ux, Uy, Uz);
     const double U[3] = {Ux, Uy, Uz};
     for (int c = 0; c < 3; ++c) {
       Ap[i + c * n] = X::div(X::sub(U[c], uvw[i + c * n]), a.dt);
-      if (!warm) X_[i + c * n] = 0.0;
+      const double xc = X_[i + c * n];
+      if (warm >= 2) X_[i + c * n] = X::sub(X::mul(2.0, xc), Xh[i + c * n]);
+      else if (!warm) X_[i + c * n] = 0.0;
+      if (warm) Xh[i + c * n] = xc;
     }
   }
   __syncthreads();
@@ -545,6 +556,7 @@ __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz,
   if (threadIdx.x == 0) {
     *iters = it;
     if (!done) atomicOr(status, 4);
+    *hist = (h + 1 < 2) ? h + 1 : 2;
   }
   __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x)
@@ -554,11 +566,11 @@ __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz,
 __global__ void __launch_bounds__(kCgThreads) k_ivc_cg(IBArgs a, const double *xyz, const double *tgt,
                                                  const double *uvw, const int *rowptr,
                                                  const int *col, const double *val,
-                                                 const double *diag, double *X_, double *work,
-                                                 double *F, int maxit, double tol, int *status,
-                                                 int *iters, int warm) {
-  ivc_cg_block(a, xyz, tgt, uvw, rowptr, col, val, diag, X_, work, F, maxit, tol, status, iters,
-               warm);
+                                                 const double *diag, double *X_, double *Xh,
+                                                 int *hist, double *work, double *F, int maxit,
+                                                 double tol, int *status, int *iters) {
+  ivc_cg_block(a, xyz, tgt, uvw, rowptr, col, val, diag, X_, Xh, hist, work, F, maxit, tol, status,
+               iters);
 }
 
 // ---------------------------------------------------------------------------
@@ -718,9 +730,13 @@ __device__ __forceinline__ void cg_grid_body(cgrp::grid_group &grid, const IBArg
                                              const int *col, const double *val,
                                              const double *diag, double *X_, double *Xh,
                                              double *work, double *F, double *partial, int maxit,
-                                             double tol, int warm, int *status, int *iters,
+                                             double tol, int *hist, int *status, int *iters,
                                              double (*sh)[8], double *red) {
   const int n = a.n;
+  // the start (hist, as the block solve keeps it): read by every block before
+  // the first grid barrier, advanced by one thread after the last
+  const int h = *hist;
+  const int warm = h < 2 ? h : 2;
   double *r = work, *z = work + 3 * n, *Ap = work + 9 * n;
   double *P[2] = {work + 6 * n, work + 12 * n};
   const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gsz = gridDim.x * blockDim.x;
@@ -861,6 +877,7 @@ __device__ __forceinline__ void cg_grid_body(cgrp::grid_group &grid, const IBArg
   if (gtid == 0) {
     *iters = it;
     if (!done) atomicOr(status, 4);
+    *hist = (h + 1 < 2) ? h + 1 : 2;
   }
   for (int i = gtid; i < n; i += gsz)
     for (int c = 0; c < 3; ++c) F[i + c * n] = X::add(F[i + c * n], X_[i + c * n]);
@@ -871,13 +888,13 @@ __global__ void __launch_bounds__(256, 4) k_ivc_cg_grid(IBArgs a, const double *
                                                      const int *col, const double *val,
                                                      const double *diag, double *X_, double *Xh,
                                                      double *work, double *F, double *partial,
-                                                     int maxit, double tol, int warm, int *status,
+                                                     int maxit, double tol, int *hist, int *status,
                                                      int *iters) {
   cgrp::grid_group grid = cgrp::this_grid();
   __shared__ double sh[8][8];
   __shared__ double red[8];
   cg_grid_body(grid, a, xyz, tgt, uvw, rowptr, col, val, diag, X_, Xh, work, F, partial, maxit, tol,
-               warm, status, iters, sh, red);
+               hist, status, iters, sh, red);
 }
 
 // ---------------------------------------------------------------------------
@@ -1700,8 +1717,9 @@ struct ilbm_ib {
   bool csr_ready = false;
   double *d_partial = nullptr;  // CG block partials
   int cg_blocks = 0;
-  bool cg_warm = false;  // previous IVC solution available as the CG start
-  bool cg_hist2 = false; // and the one before it (d_Xh), for the extrapolated start
+  // the IVC solutions the next CG start may use (device int, 0-2): d_X the
+  // last, d_Xh the one before it; the solves themselves advance it
+  int *d_hist = nullptr;
   double *d_Xh = nullptr;
   // fixed operator solved through its stored inverse (k_ivc_dense)
   int ivc_solver = ILBM_IVC_AUTO;
@@ -2143,10 +2161,12 @@ int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom
     if ((rc = dmalloc(ib, &ib->d_rowptr, (size_t)n + 1)) || (rc = dmalloc(ib, &ib->d_col, (size_t)ib->nnz_cap)) ||
         (rc = dmalloc(ib, &ib->d_val, (size_t)ib->nnz_cap)) || (rc = dmalloc(ib, &ib->d_diag, (size_t)n)) ||
         (rc = dmalloc(ib, &ib->d_X, 3 * (size_t)n)) || (rc = dmalloc(ib, &ib->d_Xh, 3 * (size_t)n)) ||
+        (rc = dmalloc(ib, &ib->d_hist, 1)) ||
         (rc = dmalloc(ib, &ib->d_work, 15 * (size_t)n))) {
       ilbm_ib_destroy(ib);
       return rc;
     }
+    cudaMemsetAsync(ib->d_hist, 0, sizeof(int), ctx->stream);
     // grid-wide CG: as many co-resident blocks as the device holds, at most 2
     // per SM (measured fastest beside the level step it overlaps)
     int dev = 0, sms = 0, per_sm = 0;
@@ -2237,9 +2257,8 @@ static int launch_cg(ilbm_ib *ib, const IBArgs &a_in, cudaStream_t s) {
   const double cg_tol = ivc_cg_tolerance(ctx->storage);
   if (ib->n <= 1024) {
     k_ivc_cg<<<1, kCgThreads, 0, s>>>(a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_rowptr, ib->d_col,
-                                ib->d_val, ib->d_diag, ib->d_X, ib->d_work, ib->d_F, 500, cg_tol,
-                                ib->d_status, ib->d_iters, ib->cg_warm ? 1 : 0);
-    ib->cg_warm = true;  // later solves start from this one
+                                ib->d_val, ib->d_diag, ib->d_X, ib->d_Xh, ib->d_hist, ib->d_work,
+                                ib->d_F, 500, cg_tol, ib->d_status, ib->d_iters);
     return ILBM_OK;
   }
   const double *xyz = ib->d_xyz, *tgt = ib->d_tgt, *uvw = ib->d_uvw, *val = ib->d_val,
@@ -2248,17 +2267,14 @@ static int launch_cg(ilbm_ib *ib, const IBArgs &a_in, cudaStream_t s) {
   double *Xv = ib->d_X, *Xh = ib->d_Xh, *work = ib->d_work, *Fm = ib->d_F, *partial = ib->d_partial;
   int maxit = 500;
   double tol = cg_tol;
-  int warm = ib->cg_warm ? (ib->cg_hist2 ? 2 : 1) : 0;
-  int *status = ib->d_status, *iters = ib->d_iters;
+  int *hist = ib->d_hist, *status = ib->d_status, *iters = ib->d_iters;
   void *args[] = {&a, &xyz, &tgt, &uvw, &rowptr, &col, &val, &diag, &Xv, &Xh, &work, &Fm,
-                  &partial, &maxit, &tol, &warm, &status, &iters};
+                  &partial, &maxit, &tol, &hist, &status, &iters};
   // one warp per ~2 rows keeps the SpMV latency-tolerant; more blocks than
   // that only make the grid barriers dearer
   const int blocks = std::max(8, std::min(ib->cg_blocks, (ib->n + 15) / 16));
   cudaError_t ce = cudaLaunchCooperativeKernel((const void *)k_ivc_cg_grid, dim3(blocks), dim3(256),
                                                args, 0, s);
-  ib->cg_hist2 = ib->cg_warm;  // Xh now holds the previous solution
-  ib->cg_warm = true;  // the next solve starts from this one (an initial guess only)
   if (ce != cudaSuccess) return cuda_fail(ce, "cooperative CG launch");
   return ILBM_OK;
 }
@@ -2683,8 +2699,10 @@ int ilbm_ib_set_ivc_solver(ilbm_ib *ib, int solver) {
     if (rc) return rc;
   }
   ib->ivc_solver = solver;
-  ib->cg_warm = false;
-  ib->cg_hist2 = false;
+  if (ib->d_hist) {  // the next solve starts from zero
+    cudaError_t e = cudaMemsetAsync(ib->d_hist, 0, sizeof(int), ib->ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "ilbm_ib_set_ivc_solver");
+  }
   return ILBM_OK;
 }
 
@@ -2715,13 +2733,19 @@ void ib_state(ilbm_ib *ib, IBState *out) {
   out->fsum = ib->d_fsum;
   out->X = ib->d_X;
   out->Xh = ib->d_Xh;
-  out->cg_warm = ib->cg_warm;
-  out->cg_hist2 = ib->cg_hist2;
+  // the solves keep the history count on the device (the caller has
+  // synchronised the context's stream)
+  int h = 0;
+  if (ib->d_hist && cudaMemcpy(&h, ib->d_hist, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    h = 0;
+  out->cg_warm = h >= 1;
+  out->cg_hist2 = h >= 2;
 }
 
 void ib_set_cg_warm(ilbm_ib *ib, bool warm, bool hist2) {
-  ib->cg_warm = warm && ib->d_X != nullptr;
-  ib->cg_hist2 = ib->cg_warm && hist2 && ib->d_Xh != nullptr;
+  if (!ib->d_hist) return;
+  const int h = (warm && ib->d_X) ? ((hist2 && ib->d_Xh) ? 2 : 1) : 0;
+  cudaMemcpy(ib->d_hist, &h, sizeof(int), cudaMemcpyHostToDevice);
 }
 
 }  // namespace ilbm
@@ -2750,7 +2774,8 @@ struct IBCase {
   int rebuild;  // CG operator rebuilt every step (moving markers / ivc_rebuild_matrix)
   int moving, periodic_band;
   int *rowptr, *col;
-  double *val, *diag, *X, *work;
+  double *val, *diag, *X, *Xh, *work;
+  int *hist;
   int nnz_cap;
   double reg, cg_tol;
   const double *Ainv;
@@ -2849,8 +2874,8 @@ __global__ void __launch_bounds__(kCgThreads) k_b_cg(const IBCase *cs, const int
   if (stage == 0) {
     if (k.rebuild) csr_scan_block(k.a.n, k.rowptr, k.nnz_cap, k.status);
   } else {
-    ivc_cg_block(k.a, k.xyz, k.tgt, k.uvw, k.rowptr, k.col, k.val, k.diag, k.X, k.work, k.F, 500,
-                 k.cg_tol, k.status, k.iters, 1);
+    ivc_cg_block(k.a, k.xyz, k.tgt, k.uvw, k.rowptr, k.col, k.val, k.diag, k.X, k.Xh, k.hist, k.work,
+                 k.F, 500, k.cg_tol, k.status, k.iters);
   }
 }
 
@@ -3068,6 +3093,8 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
     k.val = ib->d_val;
     k.diag = ib->d_diag;
     k.X = ib->d_X;
+    k.Xh = ib->d_Xh;
+    k.hist = ib->d_hist;
     k.work = ib->d_work;
     k.nnz_cap = ib->nnz_cap;
     k.reg = ib->p.ivc_diag_reg;

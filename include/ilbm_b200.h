@@ -271,8 +271,11 @@ int ilbm_ib_solver_stats(ilbm_ib *ib, int *cg_iterations);
  * is the device counterpart: A^-1 is formed once per body (in-place
  * Gauss-Jordan on the GPU, n*n doubles, n <= ILBM_IVC_DENSE_MAX) and each step
  * solves with one dense matvec.  ILBM_IVC_CG solves every step by
- * preconditioned CG on the sparse operator (warm-started; used for moving
- * markers and ivc_rebuild_matrix > 0).  ILBM_IVC_AUTO (the default) takes the
+ * preconditioned CG on the sparse operator (used for moving markers and
+ * ivc_rebuild_matrix > 0), started from the linear extrapolation of the
+ * body's last two solutions (the body keeps them, with their count, on the
+ * device, so its own solves and a batch's alternate freely; selecting a
+ * solver restarts from zero).  ILBM_IVC_AUTO (the default) takes the
  * stored inverse whenever it applies.  Selecting ILBM_IVC_DENSE where it does
  * not apply returns ILBM_ERR_UNSUPPORTED. */
 #define ILBM_IVC_AUTO 0
