@@ -30,6 +30,7 @@ BC_INT_DIR, BC_FOEXTRAP, BC_EXT_DIR, BC_USER_1, BC_USER_2 = 0, 2, 3, 1001, 1002
 EXPORTS = [
     "ilbm_create", "ilbm_destroy", "ilbm_last_error", "ilbm_sync", "ilbm_stream",
     "ilbm_event_record", "ilbm_event_elapsed_ms", "ilbm_kernel_launches", "ilbm_storage_bytes",
+    "ilbm_graph_begin", "ilbm_graph_end", "ilbm_graph_launch", "ilbm_graph_destroy",
     "ilbm_level_step", "ilbm_compute_macro", "ilbm_init_equilibrium",
     "ilbm_ib_create", "ilbm_ib_destroy", "ilbm_ib_num_markers", "ilbm_ib_force_region",
     "ilbm_ib_update_forcing", "ilbm_advance_level", "ilbm_ib_last_marker_force_sum",
@@ -140,6 +141,10 @@ def lib():
         "ilbm_event_record": (I, [P, I]),
         "ilbm_event_elapsed_ms": (I, [P, I, I, C.POINTER(C.c_float)]),
         "ilbm_kernel_launches": (I64, [P]),
+        "ilbm_graph_begin": (I, [P]),
+        "ilbm_graph_end": (I, [P, C.POINTER(P)]),
+        "ilbm_graph_launch": (I, [P, P]),
+        "ilbm_graph_destroy": (I, [P]),
         "ilbm_storage_bytes": (I, [P, ip3, ip3]),
         "ilbm_level_step": (I, [P, C.POINTER(Box_t), I, C.POINTER(LevelParams_t)]),
         "ilbm_compute_macro": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), P, P, P, ip3, ip3]),

@@ -397,6 +397,7 @@ struct ilbm_ctx {
   cudaEvent_t *xev = nullptr;
   int nxev = 0;
   int64_t launches = 0;
+  int64_t capture_launch0 = -1;  // launch count when a graph capture began (-1: none)
   // reusable scratch (reductions, level box tables)
   void *scratch = nullptr;
   size_t scratch_bytes = 0;

@@ -25,6 +25,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "ilbm_common.cuh"
 #include "step_args.cuh"
@@ -1737,6 +1738,82 @@ int ilbm_sync(ilbm_ctx *ctx) {
 }
 
 void *ilbm_stream(ilbm_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+}  // extern "C"
+
+// a recorded sequence of the context's launches, instantiated once
+struct ilbm_graph {
+  cudaGraphExec_t exec = nullptr;
+  int64_t kernels = 0;  // kernel nodes: what one replay adds to the launch count
+};
+
+extern "C" {
+
+int ilbm_graph_begin(ilbm_ctx *ctx) {
+  if (!ctx) return ILBM_ERR_ARG;
+  if (ctx->capture_launch0 >= 0) {
+    set_error("ilbm_graph_begin: a capture is already open on this context");
+    return ILBM_ERR_ARG;
+  }
+  cudaSetDevice(ctx->device);
+  // thread-local: launches other host threads make meanwhile are not recorded
+  cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_graph_begin");
+  ctx->capture_launch0 = ctx->launches;
+  return ILBM_OK;
+}
+
+int ilbm_graph_end(ilbm_ctx *ctx, ilbm_graph **out) {
+  if (!ctx || !out) return ILBM_ERR_ARG;
+  *out = nullptr;
+  if (ctx->capture_launch0 < 0) {
+    set_error("ilbm_graph_end: no capture open on this context");
+    return ILBM_ERR_ARG;
+  }
+  ctx->launches = ctx->capture_launch0;  // the recorded launches did not run
+  ctx->capture_launch0 = -1;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  if (e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return cuda_fail(e != cudaSuccess ? e : cudaErrorStreamCaptureInvalidated, "ilbm_graph_end");
+  }
+  size_t nn = 0;
+  e = cudaGraphGetNodes(g, nullptr, &nn);
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (e == cudaSuccess && nn) e = cudaGraphGetNodes(g, nodes.data(), &nn);
+  int64_t kernels = 0;
+  for (size_t i = 0; e == cudaSuccess && i < nn; ++i) {
+    cudaGraphNodeType t;
+    e = cudaGraphNodeGetType(nodes[i], &t);
+    if (e == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kernels;
+  }
+  cudaGraphExec_t exec = nullptr;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_graph_end: instantiate");
+  ilbm_graph *h = new ilbm_graph;
+  h->exec = exec;
+  h->kernels = kernels;
+  *out = h;
+  return ILBM_OK;
+}
+
+int ilbm_graph_launch(ilbm_ctx *ctx, const ilbm_graph *g) {
+  if (!ctx || !g || !g->exec) return ILBM_ERR_ARG;
+  cudaError_t e = cudaGraphLaunch(g->exec, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "ilbm_graph_launch");
+  ctx->launches += g->kernels;
+  return ILBM_OK;
+}
+
+int ilbm_graph_destroy(ilbm_graph *g) {
+  if (!g) return ILBM_OK;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  delete g;
+  return ILBM_OK;
+}
 
 static cudaEvent_t *event_slot(ilbm_ctx *ctx, int slot) {
   if (slot < 0 || slot >= 16 + 8192) return nullptr;

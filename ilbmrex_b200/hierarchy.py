@@ -73,9 +73,17 @@ class HierarchySolver:
     ``ilbm_advance_hierarchy``; a marker body lives on the finest level."""
 
     def __init__(self, hc: HierarchyCase, storage: str = "f64", ib: MarkerIB | None = None,
-                 device: int = 0, f16_scale: float = 1024.0):
+                 device: int = 0, f16_scale: float = 1024.0, graphs: bool = False):
+        """graphs: step(n) replays two coarse steps recorded once as a CUDA
+        graph (``ilbm_graph_*``) instead of issuing every launch from the
+        host, when the body (if any) does not move and the step is not the
+        first after initialisation; the results are those of the same steps
+        taken one call at a time."""
         if not torch.cuda.is_available():
             raise capi.IlbmError("HierarchySolver needs a CUDA device")
+        self.use_graphs = graphs
+        self._graph = None
+        self._graph_failed = False
         self.hc = hc
         self.nlev = hc.nlev
         self.storage = storage
@@ -195,9 +203,53 @@ class HierarchySolver:
                 self.compute_ib_force()
 
     def step(self, n: int = 1, record_force: bool = False, pipelined: bool = False):
+        if n >= 2 and not record_force and self._graph_ok():
+            g = self._two_steps()
+            if g is not None:
+                dt = self.hc.coarse.dt
+                while n >= 2:
+                    capi.check(self.L.ilbm_graph_launch(self.ctx.h, g), "graph_launch")
+                    self.time += 2 * dt
+                    self.istep += 2
+                    n -= 2
         for _ in range(n):
             self.advance(record_force=record_force, pipelined=pipelined)
         self.flush_records()
+
+    def _graph_ok(self) -> bool:
+        return (self.use_graphs and not self._graph_failed and not self.first_step and
+                (self.ib_case is None or self.ib_case.geometry_type != 2))
+
+    def _two_steps(self):
+        """The graph of two coarse steps from the current buffers (which two
+        steps bring back to their places), recorded once; None if recording
+        fails (the steps are then taken one call at a time)."""
+        if self._graph is not None:
+            return self._graph
+        time0, istep0 = self.time, self.istep
+        capi.check(self.L.ilbm_graph_begin(self.ctx.h), "graph_begin")
+        g = C.c_void_p()
+        try:
+            for _ in range(2):
+                self._launch_step()
+                Cl = self.C
+                Cl.f, Cl.f_next = Cl.f_next, Cl.f
+                Cl.m, Cl.m_next = Cl.m_next, Cl.m
+        except Exception:
+            self.L.ilbm_graph_end(self.ctx.h, C.byref(g))
+            if g.value:
+                self.L.ilbm_graph_destroy(g)
+            # a call that cannot be recorded: the steps go one call at a
+            # time (which reports a genuine error of the call itself)
+            self._graph_failed = True
+            return None
+        finally:
+            self.time, self.istep = time0, istep0
+        if self.L.ilbm_graph_end(self.ctx.h, C.byref(g)) != 0 or not g.value:
+            self._graph_failed = True
+            return None
+        self._graph = g
+        return g
 
     def _record_async(self):
         if self._rec_bufs is None:
@@ -307,6 +359,9 @@ class HierarchySolver:
         return np.array([m[0], m[1], m[2]])
 
     def close(self):
+        if self._graph is not None:
+            self.L.ilbm_graph_destroy(self._graph)
+            self._graph = None
         if self.ib is not None:
             self.L.ilbm_ib_destroy(self.ib)
             self.ib = None
@@ -319,10 +374,10 @@ class TwoLevelSolver(HierarchySolver):
     the fine level's body forcing."""
 
     def __init__(self, tl: TwoLevelCase, storage: str = "f64", ib: MarkerIB | None = None,
-                 device: int = 0, f16_scale: float = 1024.0):
+                 device: int = 0, f16_scale: float = 1024.0, graphs: bool = False):
         self.tl = tl
         hc = HierarchyCase(tl.coarse, ((tl.fine_lo, tl.fine_hi),), name=tl.name)
-        super().__init__(hc, storage, ib, device, f16_scale)
+        super().__init__(hc, storage, ib, device, f16_scale, graphs)
 
     def set_macro(self, init_coarse, init_fine):
         super().set_macro(init_coarse, init_fine)

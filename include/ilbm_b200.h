@@ -156,8 +156,29 @@ void *ilbm_stream(ilbm_ctx *ctx);
  * slots from 16 up are created on first use). */
 int ilbm_event_record(ilbm_ctx *ctx, int slot);
 int ilbm_event_elapsed_ms(ilbm_ctx *ctx, int slot_a, int slot_b, float *ms);
-/* number of kernels this context has launched since creation */
+/* number of kernels this context has launched since creation (a graph
+ * replay counts the kernels it holds) */
 int64_t ilbm_kernel_launches(const ilbm_ctx *ctx);
+/* CUDA graphs of a context's steps (no counterpart in the reference, whose
+ * steps are host loops over ParallelFor launches).  Between ilbm_graph_begin
+ * and ilbm_graph_end the launches that calls on the context issue (level
+ * steps, hierarchy steps, the body's forcing, on the context's stream and its
+ * side stream) are recorded instead of run; ilbm_graph_launch replays them on
+ * the context's stream, as one submission, with the arguments they were
+ * recorded with: the buffers, boxes and parameters must be the same at every
+ * replay (a hierarchy's buffers are back in place after two coarse steps), and
+ * whatever the recorded calls keep on the device (a body's solver history)
+ * carries on from replay to replay.  Calls that synchronise, read results back
+ * or allocate cannot be recorded: they fail, the capture is invalidated, and
+ * ilbm_graph_end reports it (ILBM_ERR_CUDA) and ends the capture.  A recorded
+ * step must therefore not be the first one of a level or body (which builds
+ * tables and reads a bound back).  ilbm_kernel_launches counts recorded
+ * kernels only when they are replayed. */
+typedef struct ilbm_graph ilbm_graph;
+int ilbm_graph_begin(ilbm_ctx *ctx);
+int ilbm_graph_end(ilbm_ctx *ctx, ilbm_graph **out);
+int ilbm_graph_launch(ilbm_ctx *ctx, const ilbm_graph *g);
+int ilbm_graph_destroy(ilbm_graph *g);
 /* storage element size in bytes and real (macro/force) element size */
 int ilbm_storage_bytes(const ilbm_ctx *ctx, int *storage_bytes, int *real_bytes);
 
