@@ -172,7 +172,7 @@ int64_t ilbm_kernel_launches(const ilbm_ctx *ctx);
  * or allocate cannot be recorded: they fail, the capture is invalidated, and
  * ilbm_graph_end reports it (ILBM_ERR_CUDA) and ends the capture.  A recorded
  * step must therefore not be the first one of a level or body (which builds
- * tables and reads a bound back).  ilbm_kernel_launches counts recorded
+ * the body's tables and allocates).  ilbm_kernel_launches counts recorded
  * kernels only when they are replayed. */
 typedef struct ilbm_graph ilbm_graph;
 int ilbm_graph_begin(ilbm_ctx *ctx);
