@@ -193,16 +193,33 @@ __device__ __forceinline__ void target_of(const IBArgs &a, int m, const double *
                                           const double *tgt, double &ux, double &uy,
                                           double &uz);
 
+// A step's kernel-weight table of the markers (the batched stages): marker m's
+// weight at offset o - 2 from its cell in direction d is tw[kTabStride m +
+// 5 d + o] (1.0 in the third direction of a 2D lattice), its cell tc[m].  The
+// interpolation's lanes 0-4 write it; the spreading and the IVC operator
+// build of the same step read it instead of evaluating the kernel again, with
+// the very values marker_weights / overlap_1d would compute.
+constexpr int kTabStride = 16;
+
 // rhs (optional, row stride ld): the IVC right-hand side (U_target - U)/dt of
-// the marker, written once here instead of by every block of the solve
+// the marker, written once here instead of by every block of the solve;
+// tw / tc (optional): the weight table above
 __device__ __forceinline__ void interp_one(const IBArgs &a, int m, int lane, const double *xyz,
                                            const double *EV, double *uvw, int *status,
-                                           const double *tgt, double *rhs, int ld) {
+                                           const double *tgt, double *rhs, int ld,
+                                           double *tw = nullptr, int4 *tc = nullptr) {
   const double px = xyz[m], py = xyz[m + a.n], pz = xyz[m + 2 * a.n];
   const double d = (a.dim == 3) ? X::mul(X::mul(a.dx[0], a.dx[1]), a.dx[2]) : X::mul(a.dx[0], a.dx[1]);
   int i0, j0, k0;
   double wxl, wyl, wzl;
   marker_weights(a, px, py, pz, lane, i0, j0, k0, wxl, wyl, wzl);
+  if (tw && lane < 5) {
+    double *row = tw + (int64_t)kTabStride * m;
+    row[lane] = wxl;
+    row[5 + lane] = wyl;
+    row[10 + lane] = wzl;
+  }
+  if (tc && lane == 0) tc[m] = make_int4(i0, j0, k0, 0);
   const int ilo = a.dlo[0] - 2, ihi = a.dhi[0] + 2, jlo = a.dlo[1] - 2, jhi = a.dhi[1] + 2;
   const int klo = (a.dim == 3) ? a.dlo[2] - 2 : 0, khi = (a.dim == 3) ? a.dhi[2] + 2 : 0;
   const int npts = (a.dim == 3) ? 125 : 25;
@@ -365,6 +382,36 @@ __device__ double ivc_entry(const IBArgs &a, const double *xyz, int i, int j, do
   const double sz = (a.dim == 3) ? overlap_1d(xyz[i + 2 * a.n], xyz[j + 2 * a.n], a.dx[2], a.kt,
                                               a.plo[2], a.dlo[2], a.dhi[2])
                                  : 1.0;
+  double val = X::mul(X::mul(X::mul(a.dv, sx), sy), sz);
+  if (i == j) val = X::add(val, reg);
+  return val;
+}
+
+// the same coupling test and entry from the step's weight table (kTabStride):
+// overlap_1d's nodes, clipping, products and summation order, with the kernel
+// values read instead of evaluated
+__device__ __forceinline__ int tab_cell(const int4 &c, int d) {
+  return d == 0 ? c.x : (d == 1 ? c.y : c.z);
+}
+__device__ __forceinline__ bool may_couple_tab(const IBArgs &a, const int4 *tc, int i, int j) {
+  const int4 ci = tc[i], cj = tc[j];
+  return abs(ci.x - cj.x) <= 4 && abs(ci.y - cj.y) <= 4 && (a.dim < 3 || abs(ci.z - cj.z) <= 4);
+}
+__device__ double ivc_entry_tab(const IBArgs &a, const double *tw, const int4 *tc, int i, int j,
+                                double reg) {
+  const int4 ci = tc[i], cj = tc[j];
+  const double *wi = tw + (int64_t)kTabStride * i, *wj = tw + (int64_t)kTabStride * j;
+  auto overlap = [&](int d) {
+    const int ia = tab_cell(ci, d), ib = tab_cell(cj, d);
+    int lo = max(ia - 2, ib - 2), hi = min(ia + 2, ib + 2);
+    lo = max(lo, a.dlo[d]);
+    hi = min(hi, a.dhi[d]);
+    double sum = 0.0;  // stays 0 when lo > hi, as overlap_1d
+    for (int q = lo; q <= hi; ++q)
+      sum = X::add(sum, X::mul(X::mul(wi[5 * d + q - ia + 2], wj[5 * d + q - ib + 2]), a.dx[d]));
+    return sum;
+  };
+  const double sx = overlap(0), sy = overlap(1), sz = (a.dim == 3) ? overlap(2) : 1.0;
   double val = X::mul(X::mul(X::mul(a.dv, sx), sy), sz);
   if (i == j) val = X::add(val, reg);
   return val;
@@ -576,19 +623,24 @@ __global__ void __launch_bounds__(kCgThreads) k_ivc_cg(IBArgs a, const double *x
 // ---------------------------------------------------------------------------
 // Multi-CTA CSR build (warp per row) and grid-wide CG for large marker sets
 // ---------------------------------------------------------------------------
+// tc / tw (optional): the step's weight table, read instead of the positions
 __device__ __forceinline__ void csr_count_row(const IBArgs &a, const double *xyz, int *rowptr, int i,
-                                              int lane) {
+                                              int lane, const int4 *tc = nullptr) {
   int c = 0;
-  for (int j = lane; j < a.n; j += 32) c += may_couple(a, xyz, i, j) ? 1 : 0;
+  if (tc)
+    for (int j = lane; j < a.n; j += 32) c += may_couple_tab(a, tc, i, j) ? 1 : 0;
+  else
+    for (int j = lane; j < a.n; j += 32) c += may_couple(a, xyz, i, j) ? 1 : 0;
   for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
   if (lane == 0) rowptr[i + 1] = c;
 }
 
-__global__ void __launch_bounds__(256) k_csr_count(IBArgs a, const double *xyz, int *rowptr) {
+__global__ void __launch_bounds__(256) k_csr_count(IBArgs a, const double *xyz, int *rowptr,
+                                                   const int4 *tc) {
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += nw)
-    csr_count_row(a, xyz, rowptr, i, lane);
+    csr_count_row(a, xyz, rowptr, i, lane, tc);
 }
 
 // exclusive scan of the row counts; if the total exceeds the capacity the
@@ -639,16 +691,17 @@ __global__ void __launch_bounds__(1024) k_csr_scan(int n, int *rowptr, int cap, 
 
 __device__ __forceinline__ void csr_fill_row(const IBArgs &a, const double *xyz, double reg,
                                              const int *rowptr, int *col, double *val,
-                                             double *diag, int i, int lane) {
+                                             double *diag, int i, int lane,
+                                             const double *tw = nullptr, const int4 *tc = nullptr) {
   {
     int p = rowptr[i];
     for (int j0 = 0; j0 < a.n; j0 += 32) {
       const int j = j0 + lane;
-      const bool c = (j < a.n) && may_couple(a, xyz, i, j);
+      const bool c = (j < a.n) && (tc ? may_couple_tab(a, tc, i, j) : may_couple(a, xyz, i, j));
       const unsigned m = __ballot_sync(0xffffffffu, c);
       if (c) {
         const int slot = p + __popc(m & ((1u << lane) - 1u));
-        const double v = ivc_entry(a, xyz, i, j, reg);
+        const double v = tc ? ivc_entry_tab(a, tw, tc, i, j, reg) : ivc_entry(a, xyz, i, j, reg);
         col[slot] = j;
         val[slot] = v;
         if (i == j) diag[i] = v;
@@ -658,14 +711,16 @@ __device__ __forceinline__ void csr_fill_row(const IBArgs &a, const double *xyz,
   }
 }
 
+// tw / tc: the step's weight table when the interpolation wrote one, else null
 __global__ void __launch_bounds__(256) k_csr_fill(IBArgs a, const double *xyz, double reg,
                                                   const int *rowptr, int *col, double *val,
-                                                  double *diag, int cap, int *status) {
+                                                  double *diag, int cap, int *status,
+                                                  const double *tw, const int4 *tc) {
   if ((*status & 2) || rowptr[a.n] > cap) return;  // capacity exceeded (k_csr_scan)
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += nw)
-    csr_fill_row(a, xyz, reg, rowptr, col, val, diag, i, lane);
+    csr_fill_row(a, xyz, reg, rowptr, col, val, diag, i, lane, tw, tc);
 }
 
 // fixed-order reduction of per-block partials (nb blocks x 8 slots); every
@@ -1115,15 +1170,13 @@ __global__ void __launch_bounds__(256) k_to_f32(const double *src, float *dst, i
 }
 
 // force_spreading_cic, :1331-1448 (dv folded in, 2D spreads x and y only);
-// one warp per marker, lanes over the stencil points, FP64 atomics
-__device__ __forceinline__ void spread_one(const IBArgs &a, int m, int lane, const double *xyz,
-                                           const double *F, double *EFI, int *status) {
+// one warp per marker, lanes over the stencil points, FP64 atomics; the
+// marker's cell and lane's kernel weights (marker_weights) are given
+__device__ __forceinline__ void spread_core(const IBArgs &a, int m, int lane, const double *F,
+                                            double *EFI, int *status, int i0, int j0, int k0,
+                                            double wxl, double wyl, double wzl) {
   const double fx = X::mul(F[m], a.dv), fy = X::mul(F[m + a.n], a.dv), fz = X::mul(F[m + 2 * a.n], a.dv);
-  const double px = xyz[m], py = xyz[m + a.n], pz = xyz[m + 2 * a.n];
   const double d = (a.dim == 3) ? X::mul(X::mul(a.dx[0], a.dx[1]), a.dx[2]) : X::mul(a.dx[0], a.dx[1]);
-  int i0, j0, k0;
-  double wxl, wyl, wzl;
-  marker_weights(a, px, py, pz, lane, i0, j0, k0, wxl, wyl, wzl);
   const int ilo = a.dlo[0] - 2, ihi = a.dhi[0] + 2, jlo = a.dlo[1] - 2, jhi = a.dhi[1] + 2;
   const int klo = (a.dim == 3) ? a.dlo[2] - 2 : 0, khi = (a.dim == 3) ? a.dhi[2] + 2 : 0;
   const int npts = (a.dim == 3) ? 125 : 25;
@@ -1174,21 +1227,44 @@ __device__ __forceinline__ void spread_one(const IBArgs &a, int m, int lane, con
   }
 }
 
+__device__ __forceinline__ void spread_one(const IBArgs &a, int m, int lane, const double *xyz,
+                                           const double *F, double *EFI, int *status) {
+  int i0, j0, k0;
+  double wxl, wyl, wzl;
+  marker_weights(a, xyz[m], xyz[m + a.n], xyz[m + 2 * a.n], lane, i0, j0, k0, wxl, wyl, wzl);
+  spread_core(a, m, lane, F, EFI, status, i0, j0, k0, wxl, wyl, wzl);
+}
+
+// the same from the step's weight table (kTabStride)
+__device__ __forceinline__ void spread_one_tab(const IBArgs &a, int m, int lane, const double *tw,
+                                               const int4 *tc, const double *F, double *EFI,
+                                               int *status) {
+  const double *row = tw + (int64_t)kTabStride * m;
+  const int o = lane % 5;
+  const int4 c = tc[m];
+  spread_core(a, m, lane, F, EFI, status, c.x, c.y, c.z, row[o], row[5 + o], row[10 + o]);
+}
+
+// tw / tc: the step's weight table when the interpolation wrote one, else null
 __global__ void __launch_bounds__(128) k_spread(IBArgs a, const double *xyz, const double *F,
-                                                double *EFI, int *status) {
+                                                double *EFI, int *status, const double *tw,
+                                                const int4 *tc) {
   const int lane = threadIdx.x & 31;
   const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (m >= a.n) return;
-  spread_one(a, m, lane, xyz, F, EFI, status);
+  if (tc)
+    spread_one_tab(a, m, lane, tw, tc, F, EFI, status);
+  else
+    spread_one(a, m, lane, xyz, F, EFI, status);
 }
 
 __global__ void __launch_bounds__(128) k_interp(IBArgs a, const double *xyz, const double *EV,
                                                 double *uvw, int *status, const double *tgt,
-                                                double *rhs, int ld) {
+                                                double *rhs, int ld, double *tw, int4 *tc) {
   const int lane = threadIdx.x & 31;
   const int m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (m >= a.n) return;
-  interp_one(a, m, lane, xyz, EV, uvw, status, tgt, rhs, ld);
+  interp_one(a, m, lane, xyz, EV, uvw, status, tgt, rhs, ld, tw, tc);
 }
 
 // ---------------------------------------------------------------------------
@@ -1736,6 +1812,10 @@ struct ilbm_ib {
   int *d_growptr = nullptr, *d_gent = nullptr;
   void *d_sw = nullptr;  // SpreadW per marker
   bool sw_ready = false;  // d_sw holds the (fixed) markers' weights
+  // a step's marker weight table (kTabStride per marker) and cells, written
+  // by the warp-parallel interpolation for the spreading and operator build
+  double *d_tw = nullptr;
+  int4 *d_tc = nullptr;
   // a level held in several boxes: the StepArgs of the boxes near the band
   std::vector<StepArgs> h_boxargs;
   StepArgs *d_boxargs = nullptr;
@@ -2162,7 +2242,8 @@ int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom
         (rc = dmalloc(ib, &ib->d_val, (size_t)ib->nnz_cap)) || (rc = dmalloc(ib, &ib->d_diag, (size_t)n)) ||
         (rc = dmalloc(ib, &ib->d_X, 3 * (size_t)n)) || (rc = dmalloc(ib, &ib->d_Xh, 3 * (size_t)n)) ||
         (rc = dmalloc(ib, &ib->d_hist, 1)) ||
-        (rc = dmalloc(ib, &ib->d_work, 15 * (size_t)n))) {
+        (rc = dmalloc(ib, &ib->d_work, 15 * (size_t)n)) ||
+        (rc = dmalloc(ib, &ib->d_tw, (size_t)kTabStride * n)) || (rc = dmalloc(ib, &ib->d_tc, (size_t)n))) {
       ilbm_ib_destroy(ib);
       return rc;
     }
@@ -2424,6 +2505,10 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *boxes, int nbox, const ilbm_le
     ib->sw_ready = true;
   }
   const bool table = ib->gather && !ordered;
+  // the warp-parallel interpolation (k_interp) writes the step's weight table
+  // of an IVC body, which its operator build and spreading then read
+  double *tw = (!ordered && !table) ? ib->d_tw : nullptr;
+  int4 *tc = tw ? ib->d_tc : nullptr;
   for (int it = 0; it < nloop; ++it) {
     cudaMemsetAsync(ib->d_EFI, 0, 3 * ib->nb * sizeof(double), s);
     // a fixed body's markers need no position update: the table-driven
@@ -2439,15 +2524,15 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *boxes, int nbox, const ilbm_le
                                       ib->d_status, ib->d_tgt, use_dense ? ib->d_rhs : nullptr, ib->ld);
     else
       k_interp<<<wblk, 128, 0, s>>>(a, ib->d_xyz, ib->d_EV, ib->d_uvw, ib->d_status, ib->d_tgt,
-                                    use_dense ? ib->d_rhs : nullptr, ib->ld);
+                                    use_dense ? ib->d_rhs : nullptr, ib->ld, tw, tc);
     ctx->launches += (fresh ? 1 : 2) + (any_periodic_band ? 1 : 0);
     if (ivc) {
       if (!ib->csr_ready || ib->moving || ib->p.ivc_rebuild_matrix > 0) {
         const int cb = std::min(4096, (ib->n * 32 + 255) / 256);
-        k_csr_count<<<cb, 256, 0, s>>>(a, ib->d_xyz, ib->d_rowptr);
+        k_csr_count<<<cb, 256, 0, s>>>(a, ib->d_xyz, ib->d_rowptr, tc);
         k_csr_scan<<<1, 1024, 0, s>>>(ib->n, ib->d_rowptr, ib->nnz_cap, ib->d_status);
         k_csr_fill<<<cb, 256, 0, s>>>(a, ib->d_xyz, ib->p.ivc_diag_reg, ib->d_rowptr, ib->d_col,
-                                      ib->d_val, ib->d_diag, ib->nnz_cap, ib->d_status);
+                                      ib->d_val, ib->d_diag, ib->nnz_cap, ib->d_status, tw, tc);
         ctx->launches += 3;
         ib->csr_ready = true;
       }
@@ -2494,7 +2579,7 @@ static int ib_update(ilbm_ib *ib, const ilbm_box *boxes, int nbox, const ilbm_le
       k_spread_w<<<wblk, 128, 0, s>>>(a, ib->d_xyz, sw, ib->d_F, ib->d_EFI, ib->d_status);
       ctx->launches++;
     } else {
-      k_spread<<<wblk, 128, 0, s>>>(a, ib->d_xyz, ib->d_F, ib->d_EFI, ib->d_status);
+      k_spread<<<wblk, 128, 0, s>>>(a, ib->d_xyz, ib->d_F, ib->d_EFI, ib->d_status, tw, tc);
       ctx->launches++;
     }
     if (any_periodic_band) {
@@ -2785,6 +2870,8 @@ struct IBCase {
   const double *kin;  // per step: komega, cos, sin, 0
   int kin_steps;
   double *rec;        // rec_slots x 8: Eulerian force sum (3), marker force sum (3), step, 0
+  double *tw;         // the step's marker weight table (kTabStride per marker) and cells
+  int4 *tc;
 };
 
 // a case that has taken all the steps it was added for sits out
@@ -2839,10 +2926,12 @@ __global__ void __launch_bounds__(256) k_b_band(const IBCase *cs, const int64_t 
   }
 }
 
-// one warp per marker; stage 0 interpolation, 1 explicit force, 2 spreading,
-// 3 CSR row count, 4 CSR row fill
+// one warp per marker; stage 0 interpolation (writes the weight table), 1
+// explicit force, 2 spreading, 3 CSR row count, 4 CSR row fill (2-4 read the
+// table)
+template <int stage>
 __global__ void __launch_bounds__(128) k_b_marker_warp(const IBCase *cs, const int64_t *off, int nc,
-                                                       int stage, const int *steps, const int *limit) {
+                                                       const int *steps, const int *limit) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < off[nc]; w += nw) {
@@ -2850,18 +2939,18 @@ __global__ void __launch_bounds__(128) k_b_marker_warp(const IBCase *cs, const i
     if (!live(steps, limit, c)) continue;
     const IBCase &k = cs[c];
     const int m = (int)(w - off[c]);
-    if (stage == 0) {
+    if constexpr (stage == 0) {
       interp_one(k.a, m, lane, k.xyz, k.EV, k.uvw, k.status, k.tgt, k.mode == 1 ? k.rhs : nullptr,
-                 k.ld);
-    } else if (stage == 1) {
+                 k.ld, k.tw, k.tc);
+    } else if constexpr (stage == 1) {
       if (k.mode == 0 && lane == 0) force_explicit_one(k.a, m, k.xyz, k.tgt, k.uvw, k.F);
-    } else if (stage == 2) {
-      spread_one(k.a, m, lane, k.xyz, k.F, k.EFI, k.status);
-    } else if (stage == 3) {
-      if (k.mode == 2 && k.rebuild) csr_count_row(k.a, k.xyz, k.rowptr, m, lane);
+    } else if constexpr (stage == 2) {
+      spread_one_tab(k.a, m, lane, k.tw, k.tc, k.F, k.EFI, k.status);
+    } else if constexpr (stage == 3) {
+      if (k.mode == 2 && k.rebuild) csr_count_row(k.a, k.xyz, k.rowptr, m, lane, k.tc);
     } else {
       if (k.mode == 2 && k.rebuild && !(k.status[0] & 2) && k.rowptr[k.a.n] <= k.nnz_cap)
-        csr_fill_row(k.a, k.xyz, k.reg, k.rowptr, k.col, k.val, k.diag, m, lane);
+        csr_fill_row(k.a, k.xyz, k.reg, k.rowptr, k.col, k.val, k.diag, m, lane, k.tw, k.tc);
     }
   }
 }
@@ -3168,6 +3257,19 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
   for (int c = 0; c < b->nc; ++c) hc[c].rec = rec + (size_t)c * b->rec_slots * 8;
   b->total_m = moff.back();
   b->total_b = boff.back();
+  {
+    double *tw = nullptr;
+    int4 *tc = nullptr;
+    if ((rc = bmalloc(b, &tw, (size_t)std::max<int64_t>(1, b->total_m) * kTabStride)) ||
+        (rc = bmalloc(b, &tc, (size_t)std::max<int64_t>(1, b->total_m)))) {
+      ib_batch_destroy(b);
+      return rc;
+    }
+    for (int c = 0; c < b->nc; ++c) {
+      hc[c].tw = tw + (size_t)moff[c] * kTabStride;
+      hc[c].tc = tc + moff[c];
+    }
+  }
   b->nd = (int)dcase.size();
   b->total_drows = doff.back();
   b->ncg = (int)cgcase.size();
@@ -3202,12 +3304,12 @@ int ib_batch_forcing(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
     k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 1, st, lm);
     ctx->launches++;
   }
-  k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 0, st, lm);
+  k_b_marker_warp<0><<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, st, lm);
   ctx->launches++;
   if (b->any_rebuild) {
-    k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 3, st, lm);
+    k_b_marker_warp<3><<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, st, lm);
     k_b_cg<<<b->ncg, kCgThreads, 0, s>>>(b->d_cases, b->d_cgcase, 0, st, lm);
-    k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 4, st, lm);
+    k_b_marker_warp<4><<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, st, lm);
     ctx->launches += 3;
   }
   if (b->nd > 0) {
@@ -3220,10 +3322,10 @@ int ib_batch_forcing(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
     ctx->launches++;
   }
   if (b->any_explicit) {
-    k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 1, st, lm);
+    k_b_marker_warp<1><<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, st, lm);
     ctx->launches++;
   }
-  k_b_marker_warp<<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, 2, st, lm);
+  k_b_marker_warp<2><<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, st, lm);
   ctx->launches++;
   if (b->any_periodic) {
     k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 2, st, lm);
