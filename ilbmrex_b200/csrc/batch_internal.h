@@ -28,10 +28,10 @@ int batch_ghost_chunks(const ilbm_ctx *ctx, const StepArgs &a, int w);
 // blocks); cases with steps[c] >= limit[c] are skipped
 int batch_step_launch(ilbm_ctx *ctx, const StepArgs *d_args, const StepTile *d_tiles, int ntiles,
                       int w, int blocks, const int *steps, const int *limit, cudaStream_t st);
-// band macro of every case's body (same skipping)
+// band macro of every case's body over its band tiles (same skipping)
 int batch_band_macro_launch(ilbm_ctx *ctx, const StepArgs *d_args, const BandDesc *d_bands,
-                            const int64_t *d_off, int ncase, int64_t total, const int *steps,
-                            const int *limit, cudaStream_t st);
+                            const ItemRef *d_tiles, int ntiles, const int *steps, const int *limit,
+                            cudaStream_t st);
 // resident blocks of w threads per SM of k_step_batch
 int batch_step_occupancy(const ilbm_ctx *ctx, int w, int *per_sm);
 

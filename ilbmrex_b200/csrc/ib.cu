@@ -493,7 +493,8 @@ __device__ __forceinline__ void thread_row_dot3(const int *col, const double *va
   }
 }
 
-// systems up to this size keep the search direction in shared memory
+// systems up to this size keep the search direction in shared memory (p_sh,
+// 3 kCgSharedN doubles of the calling kernel)
 constexpr int kCgSharedN = 1024;
 
 // Jacobi-preconditioned CG for the three force components at once, one
@@ -507,9 +508,9 @@ __device__ __forceinline__ void ivc_cg_block(const IBArgs &a, const double *xyz,
                                              const double *uvw, const int *rowptr, const int *col,
                                              const double *val, const double *diag, double *X_,
                                              double *Xh, int *hist, double *work, double *F,
-                                             int maxit, double tol, int *status, int *iters) {
+                                             int maxit, double tol, int *status, int *iters,
+                                             double *p_sh) {
   __shared__ double sh3[kMaxWarps][3], sh6[kMaxWarps][6];
-  __shared__ double p_sh[3 * kCgSharedN];
   __shared__ int sh_hist;
   const int n = a.n;
   double *r = work, *z = work + 3 * n, *Ap = work + 9 * n;
@@ -616,8 +617,9 @@ __global__ void __launch_bounds__(kCgThreads) k_ivc_cg(IBArgs a, const double *x
                                                  const double *diag, double *X_, double *Xh,
                                                  int *hist, double *work, double *F, int maxit,
                                                  double tol, int *status, int *iters) {
+  __shared__ double p_sh[3 * kCgSharedN];
   ivc_cg_block(a, xyz, tgt, uvw, rowptr, col, val, diag, X_, Xh, hist, work, F, maxit, tol, status,
-               iters);
+               iters, p_sh);
 }
 
 // ---------------------------------------------------------------------------
@@ -2338,8 +2340,8 @@ static int launch_cg(ilbm_ib *ib, const IBArgs &a_in, cudaStream_t s) {
   const double cg_tol = ivc_cg_tolerance(ctx->storage);
   if (ib->n <= 1024) {
     k_ivc_cg<<<1, kCgThreads, 0, s>>>(a, ib->d_xyz, ib->d_tgt, ib->d_uvw, ib->d_rowptr, ib->d_col,
-                                ib->d_val, ib->d_diag, ib->d_X, ib->d_Xh, ib->d_hist, ib->d_work,
-                                ib->d_F, 500, cg_tol, ib->d_status, ib->d_iters);
+                                      ib->d_val, ib->d_diag, ib->d_X, ib->d_Xh, ib->d_hist,
+                                      ib->d_work, ib->d_F, 500, cg_tol, ib->d_status, ib->d_iters);
     return ILBM_OK;
   }
   const double *xyz = ib->d_xyz, *tgt = ib->d_tgt, *uvw = ib->d_uvw, *val = ib->d_val,
@@ -2838,9 +2840,10 @@ void ib_set_cg_warm(ilbm_ib *ib, bool warm, bool hist2) {
 
 // ---------------------------------------------------------------------------
 // Batched update_forcing for the batch engine (batch.cu): every stage runs as
-// one launch over all cases.  The items of a stage (markers, band cells, rows
-// of a stored inverse) are concatenated over the cases and mapped back with
-// case_of; each case's IBArgs and arrays sit in a device table.  Cases have
+// one launch over all cases.  The items of a stage (markers, band tiles, rows
+// of a stored inverse) come from work lists of (case, item) built when the
+// batch is formed; each case's IBArgs and arrays sit in a device table, and
+// the operator build runs over the markers of rebuilding bodies only.  Cases have
 // taken their first step through ib_update already (operator and inverse
 // built), use one MDF iteration, and read the time-dependent pitching
 // kinematics from a per-step table filled on the host with the same
@@ -2879,14 +2882,15 @@ __device__ __forceinline__ bool live(const int *steps, const int *limit, int c) 
   return steps[c] < limit[c];
 }
 
-__global__ void __launch_bounds__(256) k_b_markers(const IBCase *cs, const int64_t *off, int nc,
+__global__ void __launch_bounds__(256) k_b_markers(const IBCase *cs, const ItemRef *list, int64_t cnt,
                                                    const int *steps, const int *limit) {
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < off[nc];
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < cnt;
        t += (int64_t)gridDim.x * blockDim.x) {
-    const int c = case_of(off, nc, t);
+    const ItemRef e = list[t];
+    const int c = e.c;
     if (!live(steps, limit, c)) continue;
     const IBCase &k = cs[c];
-    const int m = (int)(t - off[c]);
+    const int m = e.u;
     if (m == 0) {
       k.fsum[0] = k.fsum[1] = k.fsum[2] = 0.0;
       k.status[0] = 0;
@@ -2906,14 +2910,16 @@ __global__ void __launch_bounds__(256) k_b_markers(const IBCase *cs, const int64
   }
 }
 
-__global__ void __launch_bounds__(256) k_b_band(const IBCase *cs, const int64_t *off, int nc, int op,
-                                                const int *steps, const int *limit) {
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < off[nc];
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int c = case_of(off, nc, t);
+// one block of kItemTile threads per band tile
+__global__ void __launch_bounds__(kItemTile) k_b_band(const IBCase *cs, const ItemRef *tiles, int ntiles,
+                                                      int op, const int *steps, const int *limit) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const ItemRef e = tiles[t];
+    const int c = e.c;
     if (!live(steps, limit, c)) continue;
     const IBCase &k = cs[c];
-    const int64_t u = t - off[c];
+    const int64_t u = (int64_t)e.u + threadIdx.x;
+    if (u >= k.a.nb) continue;
     if (op == 0) {
       k.EFI[u] = 0.0;
       k.EFI[u + k.a.nb] = 0.0;
@@ -2930,15 +2936,16 @@ __global__ void __launch_bounds__(256) k_b_band(const IBCase *cs, const int64_t 
 // explicit force, 2 spreading, 3 CSR row count, 4 CSR row fill (2-4 read the
 // table)
 template <int stage>
-__global__ void __launch_bounds__(128) k_b_marker_warp(const IBCase *cs, const int64_t *off, int nc,
+__global__ void __launch_bounds__(128) k_b_marker_warp(const IBCase *cs, const ItemRef *list, int64_t cnt,
                                                        const int *steps, const int *limit) {
   const int lane = threadIdx.x & 31;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < off[nc]; w += nw) {
-    const int c = case_of(off, nc, w);
+  for (int64_t w = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < cnt; w += nw) {
+    const ItemRef e = list[w];
+    const int c = e.c;
     if (!live(steps, limit, c)) continue;
     const IBCase &k = cs[c];
-    const int m = (int)(w - off[c]);
+    const int m = e.u;
     if constexpr (stage == 0) {
       interp_one(k.a, m, lane, k.xyz, k.EV, k.uvw, k.status, k.tgt, k.mode == 1 ? k.rhs : nullptr,
                  k.ld, k.tw, k.tc);
@@ -2955,44 +2962,50 @@ __global__ void __launch_bounds__(128) k_b_marker_warp(const IBCase *cs, const i
   }
 }
 
-// one block per CG case: the CSR scan, or the whole solve
-__global__ void __launch_bounds__(kCgThreads) k_b_cg(const IBCase *cs, const int *cg_case, int stage,
-                                               const int *steps, const int *limit) {
+// one block per CG case: the CSR scan of a rebuilding body
+__global__ void __launch_bounds__(kCgThreads) k_b_scan(const IBCase *cs, const int *cg_case,
+                                                 const int *steps, const int *limit) {
   if (!live(steps, limit, cg_case[blockIdx.x])) return;
   const IBCase &k = cs[cg_case[blockIdx.x]];
-  if (stage == 0) {
-    if (k.rebuild) csr_scan_block(k.a.n, k.rowptr, k.nnz_cap, k.status);
-  } else {
-    ivc_cg_block(k.a, k.xyz, k.tgt, k.uvw, k.rowptr, k.col, k.val, k.diag, k.X, k.Xh, k.hist, k.work,
-                 k.F, 500, k.cg_tol, k.status, k.iters);
-  }
+  if (k.rebuild) csr_scan_block(k.a.n, k.rowptr, k.nnz_cap, k.status);
 }
 
-// one block per row of every stored inverse
-__global__ void __launch_bounds__(kDenseThreads) k_b_dense(const IBCase *cs, const int *dcase,
-                                                           const int64_t *doff, int nd,
+// one block per CG case: the solve
+__global__ void __launch_bounds__(kCgThreads) k_b_cg(const IBCase *cs, const int *cg_case,
+                                                     const int *steps, const int *limit) {
+  __shared__ double p_sh[3 * kCgSharedN];
+  if (!live(steps, limit, cg_case[blockIdx.x])) return;
+  const IBCase &k = cs[cg_case[blockIdx.x]];
+  ivc_cg_block(k.a, k.xyz, k.tgt, k.uvw, k.rowptr, k.col, k.val, k.diag, k.X, k.Xh, k.hist, k.work,
+               k.F, 500, k.cg_tol, k.status, k.iters, p_sh);
+}
+
+// one block per row of every stored inverse (list: case, row)
+__global__ void __launch_bounds__(kDenseThreads) k_b_dense(const IBCase *cs, const ItemRef *rows,
                                                            const int *steps, const int *limit) {
-  const int di = case_of(doff, nd, blockIdx.x);
-  if (!live(steps, limit, dcase[di])) return;
-  const IBCase &k = cs[dcase[di]];
+  const ItemRef e = rows[blockIdx.x];
+  if (!live(steps, limit, e.c)) return;
+  const IBCase &k = cs[e.c];
   if (k.Ainv32)
-    dense_row32(k.a, k.rhs, k.Ainv32, k.ld, k.F, (int)(blockIdx.x - doff[di]));
+    dense_row32(k.a, k.rhs, k.Ainv32, k.ld, k.F, e.u);
   else
-    dense_row(k.a, k.rhs, k.Ainv, k.ld, k.F, (int)(blockIdx.x - doff[di]));
+    dense_row(k.a, k.rhs, k.Ainv, k.ld, k.F, e.u);
 }
 
 template <class R>
-__global__ void __launch_bounds__(256) k_b_export(const IBCase *cs, const int64_t *off, int nc,
-                                                  const StepArgs *args, const int *steps,
-                                                  const int *limit) {
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < off[nc];
-       t += (int64_t)gridDim.x * blockDim.x) {
-    const int c = case_of(off, nc, t);
+__global__ void __launch_bounds__(kItemTile) k_b_export(const IBCase *cs, const ItemRef *tiles,
+                                                        int ntiles, const StepArgs *args,
+                                                        const int *steps, const int *limit) {
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const ItemRef e = tiles[t];
+    const int c = e.c;
     if (!live(steps, limit, c)) continue;
     const IBCase &k = cs[c];
+    const int64_t u = (int64_t)e.u + threadIdx.x;
+    if (u >= k.a.nb) continue;
     const StepArgs &sa = args[c];
     export_cell<R>(k.a, k.EFI, k.RHO, static_cast<R *>(const_cast<void *>(sa.force)), sa.mgl[0],
-                   sa.mgl[1], sa.mgl[2], sa.ms0, sa.ms1, sa.ms2, t - off[c]);
+                   sa.mgl[1], sa.mgl[2], sa.ms0, sa.ms1, sa.ms2, u);
   }
 }
 
@@ -3078,10 +3091,14 @@ struct IBBatch {
   std::vector<void *> allocs;
   IBCase *d_cases = nullptr;
   BandDesc *d_bands = nullptr;
-  int64_t *d_moff = nullptr, *d_boff = nullptr, *d_doff = nullptr;
-  int64_t total_m = 0, total_b = 0, total_drows = 0;
-  int *d_dcase = nullptr, *d_cgcase = nullptr;
-  int nd = 0, ncg = 0;
+  int64_t total_m = 0, total_b = 0, total_drows = 0, total_rm = 0;
+  int nbt = 0;  // band tiles
+  // work lists: every marker, the markers of bodies whose operator is
+  // rebuilt each step, every row of a stored inverse (case, item), and the
+  // band tiles (case, first cell)
+  ItemRef *d_mlist = nullptr, *d_rlist = nullptr, *d_dlist = nullptr, *d_btiles = nullptr;
+  int *d_cgcase = nullptr;
+  int ncg = 0;
   bool any_periodic = false, any_explicit = false, any_rebuild = false;
   int *d_steps = nullptr, *d_limit = nullptr;
   double *d_rec = nullptr, *d_part = nullptr;
@@ -3101,7 +3118,7 @@ static int bmalloc(IBBatch *b, T **p, size_t count) {
 }
 template <class T>
 static int bupload(IBBatch *b, T **p, const std::vector<T> &h) {
-  int rc = bmalloc(b, p, h.size());
+  int rc = bmalloc(b, p, std::max<size_t>(1, h.size()));
   if (rc) return rc;
   if (!h.empty()) {
     cudaError_t e = cudaMemcpyAsync(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice,
@@ -3129,8 +3146,9 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
   b->rec_slots = std::max(1, rec_slots);
   std::vector<IBCase> hc(b->nc);
   std::vector<BandDesc> hb(b->nc);
-  std::vector<int64_t> moff(b->nc + 1, 0), boff(b->nc + 1, 0), doff(1, 0);
-  std::vector<int> dcase, cgcase;
+  std::vector<int64_t> moff(b->nc + 1, 0), boff(b->nc + 1, 0);
+  std::vector<int> cgcase;
+  std::vector<ItemRef> mlist, rlist, dlist, btiles;
   std::vector<std::vector<double>> kin(b->nc);
   for (int c = 0; c < b->nc; ++c) {
     IBCase &k = hc[c];
@@ -3211,6 +3229,12 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
     }
     moff[c + 1] = moff[c] + ib->n;
     boff[c + 1] = boff[c] + ib->nb;
+    for (int m = 0; m < ib->n; ++m) {
+      mlist.push_back({c, m});
+      if (k.rebuild) rlist.push_back({c, m});
+      if (k.mode == 1) dlist.push_back({c, m});
+    }
+    for (int64_t u = 0; u < ib->nb; u += kItemTile) btiles.push_back({c, (int)u});
     for (int d = 0; d < 3; ++d) {
       bd.blo[d] = ib->blo[d];
       bd.bn[d] = ib->bn[d];
@@ -3219,10 +3243,6 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
     bd.EV = ib->d_EV;
     bd.RHO = ib->d_RHO;
     bd.EFI = ib->d_EFI;
-    if (k.mode == 1) {
-      dcase.push_back(c);
-      doff.push_back(doff.back() + ib->n);
-    }
     if (k.mode == 2) cgcase.push_back(c);
     b->any_periodic = b->any_periodic || k.periodic_band;
     b->any_explicit = b->any_explicit || k.mode == 0;
@@ -3270,12 +3290,13 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
       hc[c].tc = tc + moff[c];
     }
   }
-  b->nd = (int)dcase.size();
-  b->total_drows = doff.back();
+  b->total_drows = (int64_t)dlist.size();
+  b->total_rm = (int64_t)rlist.size();
+  b->nbt = (int)btiles.size();
   b->ncg = (int)cgcase.size();
   if ((rc = bupload(b, &b->d_cases, hc)) || (rc = bupload(b, &b->d_bands, hb)) ||
-      (rc = bupload(b, &b->d_moff, moff)) || (rc = bupload(b, &b->d_boff, boff)) ||
-      (rc = bupload(b, &b->d_doff, doff)) || (rc = bupload(b, &b->d_dcase, dcase)) ||
+      (rc = bupload(b, &b->d_mlist, mlist)) || (rc = bupload(b, &b->d_rlist, rlist)) ||
+      (rc = bupload(b, &b->d_dlist, dlist)) || (rc = bupload(b, &b->d_btiles, btiles)) ||
       (rc = bupload(b, &b->d_cgcase, cgcase))) {
     ib_batch_destroy(b);
     return rc;
@@ -3293,48 +3314,49 @@ int ib_batch_forcing(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
   ilbm_ctx *ctx = b->ctx;
   if (b->total_m == 0) return ILBM_OK;
   const int *st = b->d_steps, *lm = b->d_limit;
-  int rc = batch_band_macro_launch(ctx, d_args, b->d_bands, b->d_boff, b->nc, b->total_b, st, lm, s);
+  int rc = batch_band_macro_launch(ctx, d_args, b->d_bands, b->d_btiles, b->nbt, st, lm, s);
   if (rc) return rc;
-  const int gb = grid_for(b->total_b, 256), gm = grid_for(b->total_m, 256);
-  const int gw = grid_for(b->total_m * 32, 128);
+  const int gt = std::min(b->nbt, 4096), gm = grid_for(b->total_m, 256);
+  const int gw = grid_for(b->total_m * 32, 128), gr = grid_for(b->total_rm * 32, 128);
+  const ItemRef *ml = b->d_mlist, *rl = b->d_rlist;
+  const int64_t nm = b->total_m, nr = b->total_rm;
   // (the band macro also zeroed EFI)
-  k_b_markers<<<gm, 256, 0, s>>>(b->d_cases, b->d_moff, b->nc, st, lm);
+  k_b_markers<<<gm, 256, 0, s>>>(b->d_cases, ml, nm, st, lm);
   ctx->launches += 1;
   if (b->any_periodic) {
-    k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 1, st, lm);
+    k_b_band<<<gt, kItemTile, 0, s>>>(b->d_cases, b->d_btiles, b->nbt, 1, st, lm);
     ctx->launches++;
   }
-  k_b_marker_warp<0><<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, st, lm);
+  k_b_marker_warp<0><<<gw, 128, 0, s>>>(b->d_cases, ml, nm, st, lm);
   ctx->launches++;
-  if (b->any_rebuild) {
-    k_b_marker_warp<3><<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, st, lm);
-    k_b_cg<<<b->ncg, kCgThreads, 0, s>>>(b->d_cases, b->d_cgcase, 0, st, lm);
-    k_b_marker_warp<4><<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, st, lm);
+  if (nr > 0) {
+    k_b_marker_warp<3><<<gr, 128, 0, s>>>(b->d_cases, rl, nr, st, lm);
+    k_b_scan<<<b->ncg, kCgThreads, 0, s>>>(b->d_cases, b->d_cgcase, st, lm);
+    k_b_marker_warp<4><<<gr, 128, 0, s>>>(b->d_cases, rl, nr, st, lm);
     ctx->launches += 3;
   }
-  if (b->nd > 0) {
-    k_b_dense<<<(unsigned)b->total_drows, kDenseThreads, 0, s>>>(b->d_cases, b->d_dcase, b->d_doff,
-                                                                 b->nd, st, lm);
+  if (b->total_drows > 0) {
+    k_b_dense<<<(unsigned)b->total_drows, kDenseThreads, 0, s>>>(b->d_cases, b->d_dlist, st, lm);
     ctx->launches++;
   }
   if (b->ncg > 0) {
-    k_b_cg<<<b->ncg, kCgThreads, 0, s>>>(b->d_cases, b->d_cgcase, 1, st, lm);
+    k_b_cg<<<b->ncg, kCgThreads, 0, s>>>(b->d_cases, b->d_cgcase, st, lm);
     ctx->launches++;
   }
   if (b->any_explicit) {
-    k_b_marker_warp<1><<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, st, lm);
+    k_b_marker_warp<1><<<gw, 128, 0, s>>>(b->d_cases, ml, nm, st, lm);
     ctx->launches++;
   }
-  k_b_marker_warp<2><<<gw, 128, 0, s>>>(b->d_cases, b->d_moff, b->nc, st, lm);
+  k_b_marker_warp<2><<<gw, 128, 0, s>>>(b->d_cases, ml, nm, st, lm);
   ctx->launches++;
   if (b->any_periodic) {
-    k_b_band<<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, 2, st, lm);
+    k_b_band<<<gt, kItemTile, 0, s>>>(b->d_cases, b->d_btiles, b->nbt, 2, st, lm);
     ctx->launches++;
   }
   if (ctx->storage == ILBM_STORAGE_F64)
-    k_b_export<double><<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, d_args, st, lm);
+    k_b_export<double><<<gt, kItemTile, 0, s>>>(b->d_cases, b->d_btiles, b->nbt, d_args, st, lm);
   else
-    k_b_export<float><<<gb, 256, 0, s>>>(b->d_cases, b->d_boff, b->nc, d_args, st, lm);
+    k_b_export<float><<<gt, kItemTile, 0, s>>>(b->d_cases, b->d_btiles, b->nbt, d_args, st, lm);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "batched update_forcing");

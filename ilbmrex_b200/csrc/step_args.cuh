@@ -74,16 +74,12 @@ struct BandDesc {
   double *EV, *RHO, *EFI;
 };
 
-// Case owning item t of a concatenation whose case c starts at off[c]
-// (off has ncase + 1 entries, nondecreasing).
-__device__ __forceinline__ int case_of(const int64_t *off, int ncase, int64_t t) {
-  int lo = 0, hi = ncase - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (off[mid] <= t) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
+// Work lists of the batched immersed-body stages: one entry per marker
+// (case, marker) and tiles of kItemTile band cells of one case (case, first
+// cell), so an item finds its case with one load.
+struct ItemRef {
+  int c, u;
+};
+constexpr int kItemTile = 256;
 
 }  // namespace ilbm
