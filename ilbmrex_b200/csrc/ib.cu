@@ -1689,7 +1689,8 @@ __global__ void k_fill_boundary(IBArgs a, double *EV) {
 template <class R>
 __device__ __forceinline__ void export_cell(const IBArgs &a, const double *EFT, const double *RHO,
                                             R *F, int mgl0, int mgl1, int mgl2, int64_t ms0,
-                                            int64_t ms1, int64_t ms2, int64_t t) {
+                                            int64_t ms1, int64_t ms2, int64_t t,
+                                            double *stored = nullptr) {
   const int i = a.blo[0] + (int)(t % a.bn[0]);
   const int j = a.blo[1] + (int)((t / a.bn[0]) % a.bn[1]);
   const int k = a.blo[2] + (int)(t / ((int64_t)a.bn[0] * a.bn[1]));
@@ -1699,9 +1700,19 @@ __device__ __forceinline__ void export_cell(const IBArgs &a, const double *EFT, 
   if (!inside) return;
   const int64_t m = (int64_t)(i - mgl0) + (int64_t)(j - mgl1) * ms0 + (int64_t)(k - mgl2) * ms1;
   const double dr = X::mul(a.dt, RHO[t]);
-  F[m] = R(X::mul(dr, EFT[t]));
-  F[m + ms2] = R(X::mul(dr, EFT[t + a.nb]));
-  if (a.dim == 3) F[m + 2 * ms2] = R(X::mul(dr, EFT[t + 2 * a.nb]));
+  const R fx = R(X::mul(dr, EFT[t])), fy = R(X::mul(dr, EFT[t + a.nb]));
+  F[m] = fx;
+  F[m + ms2] = fy;
+  R fz = R(0);
+  if (a.dim == 3) {
+    fz = R(X::mul(dr, EFT[t + 2 * a.nb]));
+    F[m + 2 * ms2] = fz;
+  }
+  if (stored) {  // the values as stored (the force region is the band inside the domain)
+    stored[0] = double(fx);
+    stored[1] = double(fy);
+    stored[2] = double(fz);
+  }
 }
 
 template <class R>
@@ -2875,6 +2886,7 @@ struct IBCase {
   double *rec;        // rec_slots x 8: Eulerian force sum (3), marker force sum (3), step, 0
   double *tw;         // the step's marker weight table (kTabStride per marker) and cells
   int4 *tc;
+  int tile0, ntile;   // the case's band tiles in the batch's tile list
 };
 
 // a case that has taken all the steps it was added for sits out
@@ -2993,76 +3005,55 @@ __global__ void __launch_bounds__(kDenseThreads) k_b_dense(const IBCase *cs, con
 }
 
 template <class R>
+// each tile also leaves the fixed-order sum of the force it stored (tpart,
+// 3 per tile): the case's Eulerian force sum, combined by k_b_record
 __global__ void __launch_bounds__(kItemTile) k_b_export(const IBCase *cs, const ItemRef *tiles,
                                                         int ntiles, const StepArgs *args,
-                                                        const int *steps, const int *limit) {
+                                                        const int *steps, const int *limit,
+                                                        double *tpart) {
+  __shared__ double shr[kMaxWarps][3];
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const ItemRef e = tiles[t];
     const int c = e.c;
-    if (!live(steps, limit, c)) continue;
+    if (!live(steps, limit, c)) continue;  // uniform over the block
     const IBCase &k = cs[c];
     const int64_t u = (int64_t)e.u + threadIdx.x;
-    if (u >= k.a.nb) continue;
-    const StepArgs &sa = args[c];
-    export_cell<R>(k.a, k.EFI, k.RHO, static_cast<R *>(const_cast<void *>(sa.force)), sa.mgl[0],
-                   sa.mgl[1], sa.mgl[2], sa.ms0, sa.ms1, sa.ms2, u);
+    double v[3] = {0.0, 0.0, 0.0};
+    if (u < k.a.nb) {
+      const StepArgs &sa = args[c];
+      export_cell<R>(k.a, k.EFI, k.RHO, static_cast<R *>(const_cast<void *>(sa.force)), sa.mgl[0],
+                     sa.mgl[1], sa.mgl[2], sa.ms0, sa.ms1, sa.ms2, u, v);
+    }
+    double tot[3];
+    block_reduce<3>(v, shr, tot);
+    if (threadIdx.x == 0) {
+      tpart[3 * (int64_t)t] = tot[0];
+      tpart[3 * (int64_t)t + 1] = tot[1];
+      tpart[3 * (int64_t)t + 2] = tot[2];
+    }
+    __syncthreads();  // shr is read before the next tile's reduction writes it
   }
 }
 
-// kRecParts blocks per case: Eulerian force sum over the force region (the
-// band clipped to the domain) in fixed partial slots; the case's last block to
-// finish combines them in order, forms the marker force sum, writes the
-// case's record ring and advances its step counter
-constexpr int kRecParts = 8;
+// one block per case: its Eulerian force sum (the export's tile partials in
+// tile order), the marker force sum, a record ring entry and the step counter
 constexpr int kRecThreads = 256;
-template <class R>
-__global__ void __launch_bounds__(kRecThreads) k_b_record(const IBCase *cs, const StepArgs *args,
-                                                          int *steps, const int *limit,
-                                                          int rec_slots, double *part,
-                                                          unsigned *done) {
+__global__ void __launch_bounds__(kRecThreads) k_b_record(const IBCase *cs, int *steps,
+                                                          const int *limit, int rec_slots,
+                                                          const double *tpart) {
   __shared__ double sh[33];
-  __shared__ bool last;
-  const int c = blockIdx.x / kRecParts, pt = blockIdx.x % kRecParts;
-  if (!live(steps, limit, c)) return;  // uniform over the case's blocks
+  const int c = blockIdx.x;
+  if (!live(steps, limit, c)) return;
   const IBCase &k = cs[c];
-  const StepArgs &sa = args[c];
-  if (k.a.n > 0) {
-    const R *F = static_cast<const R *>(sa.force);
-    int lo[3], nn[3];
-    for (int d = 0; d < 3; ++d) {
-      const int l = (d < k.a.dim) ? max(k.a.blo[d], k.a.dlo[d]) : 0;
-      const int h = (d < k.a.dim) ? min(k.a.blo[d] + k.a.bn[d] - 1, k.a.dhi[d]) : 0;
-      lo[d] = l;
-      nn[d] = max(0, h - l + 1);
-    }
-    const int items = nn[0] * nn[1] * nn[2];
-    for (int comp = 0; comp < 3; ++comp) {
-      double sm = 0.0;
-      if (comp < k.a.dim) {
-        const R *Fc = F + comp * sa.ms2;
-        for (int f = pt * kRecThreads + threadIdx.x; f < items; f += kRecParts * kRecThreads) {
-          const int i = lo[0] + f % nn[0], r = f / nn[0];
-          const int j = lo[1] + r % nn[1], kk = lo[2] + r / nn[1];
-          sm += double(Fc[(int64_t)(i - sa.mgl[0]) + (int64_t)(j - sa.mgl[1]) * sa.ms0 +
-                          (int64_t)(kk - sa.mgl[2]) * sa.ms1]);
-        }
-      }
-      sm = block_sum(sm, sh);
-      if (threadIdx.x == 0) part[((size_t)c * kRecParts + pt) * 3 + comp] = sm;
-    }
-  }
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last = (atomicAdd(done + c, 1u) == kRecParts - 1);
-  }
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
   double fe[3] = {0.0, 0.0, 0.0};
   if (k.a.n > 0) {
     marker_sum_block(k.a, k.F, k.fsum);
-    for (int p2 = 0; p2 < kRecParts; ++p2)
-      for (int comp = 0; comp < 3; ++comp) fe[comp] += __ldcg(part + ((size_t)c * kRecParts + p2) * 3 + comp);
+    for (int comp = 0; comp < 3; ++comp) {
+      double sm = 0.0;
+      for (int q = threadIdx.x; q < k.ntile; q += blockDim.x)
+        sm += tpart[3 * (int64_t)(k.tile0 + q) + comp];
+      fe[comp] = block_sum(sm, sh);
+    }
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -3077,7 +3068,6 @@ __global__ void __launch_bounds__(kRecThreads) k_b_record(const IBCase *cs, cons
     r[6] = double(st);
     r[7] = 0.0;
     steps[c] = st + 1;
-    done[c] = 0u;  // ready for the next step
   }
 }
 
@@ -3101,8 +3091,7 @@ struct IBBatch {
   int ncg = 0;
   bool any_periodic = false, any_explicit = false, any_rebuild = false;
   int *d_steps = nullptr, *d_limit = nullptr;
-  double *d_rec = nullptr, *d_part = nullptr;
-  unsigned *d_done = nullptr;
+  double *d_rec = nullptr, *d_tpart = nullptr;  // record rings; the export's tile partials
   int *d_status_copy = nullptr;
   std::vector<int *> status_ptrs;
 };
@@ -3234,7 +3223,9 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
       if (k.rebuild) rlist.push_back({c, m});
       if (k.mode == 1) dlist.push_back({c, m});
     }
+    k.tile0 = (int)btiles.size();
     for (int64_t u = 0; u < ib->nb; u += kItemTile) btiles.push_back({c, (int)u});
+    k.ntile = (int)btiles.size() - k.tile0;
     for (int d = 0; d < 3; ++d) {
       bd.blo[d] = ib->blo[d];
       bd.bn[d] = ib->bn[d];
@@ -3258,13 +3249,12 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
   }
   double *rec = nullptr;
   if ((rc = bmalloc(b, &rec, (size_t)b->nc * b->rec_slots * 8)) || (rc = bmalloc(b, &b->d_steps, b->nc)) ||
-      (rc = bmalloc(b, &b->d_part, (size_t)b->nc * kRecParts * 3)) || (rc = bmalloc(b, &b->d_done, b->nc))) {
+      (rc = bmalloc(b, &b->d_tpart, 3 * std::max<size_t>(1, btiles.size())))) {
     ib_batch_destroy(b);
     return rc;
   }
   cudaMemsetAsync(rec, 0, (size_t)b->nc * b->rec_slots * 8 * sizeof(double), ctx->stream);
   cudaMemsetAsync(b->d_steps, 0, b->nc * sizeof(int), ctx->stream);
-  cudaMemsetAsync(b->d_done, 0, b->nc * sizeof(unsigned), ctx->stream);
   {
     std::vector<int> lim(b->nc);
     for (int c = 0; c < b->nc; ++c) lim[c] = std::max(0, cases[c].limit);
@@ -3354,24 +3344,21 @@ int ib_batch_forcing(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
     ctx->launches++;
   }
   if (ctx->storage == ILBM_STORAGE_F64)
-    k_b_export<double><<<gt, kItemTile, 0, s>>>(b->d_cases, b->d_btiles, b->nbt, d_args, st, lm);
+    k_b_export<double><<<gt, kItemTile, 0, s>>>(b->d_cases, b->d_btiles, b->nbt, d_args, st, lm,
+                                                 b->d_tpart);
   else
-    k_b_export<float><<<gt, kItemTile, 0, s>>>(b->d_cases, b->d_btiles, b->nbt, d_args, st, lm);
+    k_b_export<float><<<gt, kItemTile, 0, s>>>(b->d_cases, b->d_btiles, b->nbt, d_args, st, lm,
+                                                b->d_tpart);
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "batched update_forcing");
   return ILBM_OK;
 }
 
-int ib_batch_record(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
+int ib_batch_record(IBBatch *b, const StepArgs *, cudaStream_t s) {
   if (b->nc == 0) return ILBM_OK;
-  const unsigned g = (unsigned)b->nc * kRecParts;
-  if (b->ctx->storage == ILBM_STORAGE_F64)
-    k_b_record<double><<<g, kRecThreads, 0, s>>>(b->d_cases, d_args, b->d_steps, b->d_limit,
-                                                 b->rec_slots, b->d_part, b->d_done);
-  else
-    k_b_record<float><<<g, kRecThreads, 0, s>>>(b->d_cases, d_args, b->d_steps, b->d_limit,
-                                                b->rec_slots, b->d_part, b->d_done);
+  k_b_record<<<(unsigned)b->nc, kRecThreads, 0, s>>>(b->d_cases, b->d_steps, b->d_limit, b->rec_slots,
+                                                    b->d_tpart);
   b->ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "batched force record");
