@@ -3092,6 +3092,9 @@ struct IBBatch {
   bool any_periodic = false, any_explicit = false, any_rebuild = false;
   int *d_steps = nullptr, *d_limit = nullptr;
   double *d_rec = nullptr, *d_tpart = nullptr;  // record rings; the export's tile partials
+  // fork / join of the moving bodies' operator build and CG (on the context's
+  // high-priority side stream) beside the stored-inverse solves
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int *d_status_copy = nullptr;
   std::vector<int *> status_ptrs;
 };
@@ -3122,7 +3125,11 @@ static int grid_for(int64_t items, int threads) {
 
 void ib_batch_destroy(IBBatch *b) {
   if (!b) return;
+  // (the side stream's batch work joined the context's stream before any
+  // later work there: the frees are ordered after it)
   for (void *q : b->allocs) ilbm_ctx_free(b->ctx, q);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->ev_join) cudaEventDestroy(b->ev_join);
   delete b;
 }
 
@@ -3131,6 +3138,14 @@ int ib_batch_create(ilbm_ctx *ctx, const std::vector<IBBatchCase> &cases, int re
   *out = nullptr;
   auto *b = new IBBatch();
   b->ctx = ctx;
+  {
+    cudaError_t e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      ib_batch_destroy(b);
+      return cuda_fail(e, "IB batch events");
+    }
+  }
   b->nc = (int)cases.size();
   b->rec_slots = std::max(1, rec_slots);
   std::vector<IBCase> hc(b->nc);
@@ -3319,19 +3334,33 @@ int ib_batch_forcing(IBBatch *b, const StepArgs *d_args, cudaStream_t s) {
   }
   k_b_marker_warp<0><<<gw, 128, 0, s>>>(b->d_cases, ml, nm, st, lm);
   ctx->launches++;
+  // the moving bodies' operator build and CG (the longer chain) on the
+  // high-priority side stream, the stored-inverse solves beside them
+  const bool fork = b->ncg > 0 && b->total_drows > 0;
+  cudaStream_t cgs = fork ? ctx->side : s;
+  if (fork) {
+    cudaError_t e = cudaEventRecord(b->ev_fork, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(cgs, b->ev_fork, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "batched IVC fork");
+  }
   if (nr > 0) {
-    k_b_marker_warp<3><<<gr, 128, 0, s>>>(b->d_cases, rl, nr, st, lm);
-    k_b_scan<<<b->ncg, kCgThreads, 0, s>>>(b->d_cases, b->d_cgcase, st, lm);
-    k_b_marker_warp<4><<<gr, 128, 0, s>>>(b->d_cases, rl, nr, st, lm);
+    k_b_marker_warp<3><<<gr, 128, 0, cgs>>>(b->d_cases, rl, nr, st, lm);
+    k_b_scan<<<b->ncg, kCgThreads, 0, cgs>>>(b->d_cases, b->d_cgcase, st, lm);
+    k_b_marker_warp<4><<<gr, 128, 0, cgs>>>(b->d_cases, rl, nr, st, lm);
     ctx->launches += 3;
+  }
+  if (b->ncg > 0) {
+    k_b_cg<<<b->ncg, kCgThreads, 0, cgs>>>(b->d_cases, b->d_cgcase, st, lm);
+    ctx->launches++;
   }
   if (b->total_drows > 0) {
     k_b_dense<<<(unsigned)b->total_drows, kDenseThreads, 0, s>>>(b->d_cases, b->d_dlist, st, lm);
     ctx->launches++;
   }
-  if (b->ncg > 0) {
-    k_b_cg<<<b->ncg, kCgThreads, 0, s>>>(b->d_cases, b->d_cgcase, st, lm);
-    ctx->launches++;
+  if (fork) {
+    cudaError_t e = cudaEventRecord(b->ev_join, cgs);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b->ev_join, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "batched IVC join");
   }
   if (b->any_explicit) {
     k_b_marker_warp<1><<<gw, 128, 0, s>>>(b->d_cases, ml, nm, st, lm);
