@@ -162,21 +162,15 @@ int build(ilbm_batch *b) {
     }
     ibc[c] = IBBatchCase{k.ib, k.dt, k.time, std::max(1, k.max_steps), std::max(0, k.max_steps)};
   }
-  // tile table: every case's ghost-push chunks first (strided, slow), then
-  // its row segments
+  // tile table: every case's ghost-push chunks first (strided, slow), padded
+  // to a whole number of rounds of the persistent grid, then its row
+  // segments.  The kernel's block b takes entries b, b + blocks, ...: each
+  // case owns a share of the blocks proportional to its rows and its row
+  // segments are dealt round by round over its own blocks, so a block stays
+  // in one case (its arguments copied to shared memory once) while the
+  // case's blocks sweep neighbouring rows together.  Entries with c = -1
+  // fill the rounds and are skipped.
   const int W = b->tile_w;
-  std::vector<StepTile> tiles;
-  for (int c = 0; c < nc; ++c) {
-    const int nch = batch_ghost_chunks(ctx, args[c], W);
-    for (int ch = 0; ch < nch; ++ch) tiles.push_back(StepTile{c, -1 - ch, nch, 0});
-  }
-  for (int c = 0; c < nc; ++c) {
-    const StepArgs &a = args[c];
-    for (int k = a.lo[2]; k <= a.hi[2]; ++k)
-      for (int j = a.lo[1]; j <= a.hi[1]; ++j)
-        for (int i0 = a.lo[0]; i0 <= a.hi[0]; i0 += W) tiles.push_back(StepTile{c, i0, j, k});
-  }
-  b->ntiles = (int)tiles.size();
   int per_sm = 0;
   if ((rc = batch_step_occupancy(ctx, W, &per_sm))) return rc;
   if (per_sm < 1) {
@@ -184,7 +178,55 @@ int build(ilbm_batch *b) {
     return ILBM_ERR_UNSUPPORTED;
   }
   const int use = (b->ctas_per_sm > 0) ? std::min(b->ctas_per_sm, per_sm) : per_sm;
-  b->blocks = std::max(1, std::min(b->ntiles, use * b->sms));
+  std::vector<StepTile> tiles;
+  for (int c = 0; c < nc; ++c) {
+    const int nch = batch_ghost_chunks(ctx, args[c], W);
+    for (int ch = 0; ch < nch; ++ch) tiles.push_back(StepTile{c, -1 - ch, nch, 0});
+  }
+  std::vector<std::vector<StepTile>> rows(nc);
+  int64_t nrow = 0;
+  for (int c = 0; c < nc; ++c) {
+    const StepArgs &a = args[c];
+    for (int k = a.lo[2]; k <= a.hi[2]; ++k)
+      for (int j = a.lo[1]; j <= a.hi[1]; ++j)
+        for (int i0 = a.lo[0]; i0 <= a.hi[0]; i0 += W) rows[c].push_back(StepTile{c, i0, j, k});
+    nrow += (int64_t)rows[c].size();
+  }
+  const int G = (int)std::max<int64_t>(1, std::min<int64_t>(nrow + (int64_t)tiles.size(),
+                                                            (int64_t)use * b->sms));
+  b->blocks = G;
+  if (nc <= G) {
+    // blocks per case: proportional to its rows, at least one (largest remainders)
+    std::vector<int> nb(nc, 1);
+    int left = G - nc;
+    std::vector<std::pair<double, int>> rem;
+    for (int c = 0; c < nc; ++c) {
+      const double share = nrow ? double(left) * double(rows[c].size()) / double(nrow) : 0.0;
+      nb[c] += (int)share;
+      rem.push_back({share - (int)share, c});
+    }
+    int given = 0;
+    for (int c = 0; c < nc; ++c) given += nb[c] - 1;
+    std::sort(rem.begin(), rem.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+    for (int q = 0; q < left - given && q < (int)rem.size(); ++q) nb[rem[q].second]++;
+    int64_t rounds = 0;
+    for (int c = 0; c < nc; ++c)
+      rounds = std::max<int64_t>(rounds, ((int64_t)rows[c].size() + nb[c] - 1) / nb[c]);
+    while (tiles.size() % G) tiles.push_back(StepTile{-1, 0, 0, 0});
+    std::vector<int> owner(G), first(nc + 1, 0);
+    for (int c = 0; c < nc; ++c) first[c + 1] = first[c] + nb[c];
+    for (int c = 0; c < nc; ++c)
+      for (int s = first[c]; s < first[c + 1]; ++s) owner[s] = c;
+    for (int64_t r = 0; r < rounds; ++r)
+      for (int s = 0; s < G; ++s) {
+        const int c = owner[s];
+        const int64_t i = r * nb[c] + (s - first[c]);
+        tiles.push_back(i < (int64_t)rows[c].size() ? rows[c][(size_t)i] : StepTile{-1, 0, 0, 0});
+      }
+  } else {
+    for (int c = 0; c < nc; ++c) tiles.insert(tiles.end(), rows[c].begin(), rows[c].end());
+  }
+  b->ntiles = (int)tiles.size();
   // stream-ordered tables (pageable sources are staged before the copies return)
   cudaError_t e = ilbm_ctx_malloc(ctx, (void **)&b->d_args, args.size() * sizeof(StepArgs));
   if (e == cudaSuccess) e = ilbm_ctx_malloc(ctx, (void **)&b->d_tiles, tiles.size() * sizeof(StepTile));

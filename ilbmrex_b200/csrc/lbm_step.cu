@@ -648,12 +648,14 @@ __global__ void __launch_bounds__(256, BatchOcc<L, S>::value)
                  const int *steps, const int *limit) {
   __shared__ StepArgs sa;
   int cur = -1;  // every thread walks the same tiles, so this stays block-uniform
-  // strided over the table, so that the blocks in flight stream through
-  // neighbouring rows together (a contiguous run per block measured 2.2x
-  // slower: the push stores' split lines no longer meet in L2)
+  // strided over the table (block b takes entries b, b + gridDim.x, ...),
+  // which the batch lays out so that the blocks in flight stream through
+  // neighbouring rows together (a contiguous run of rows per block measured
+  // 2.2x slower: the push stores' split lines no longer meet in L2) while a
+  // block keeps to one case; c = -1 marks a filler entry
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const StepTile tl = tiles[t];
-    if (steps[tl.c] >= limit[tl.c]) continue;  // the case has taken all its steps
+    if (tl.c < 0 || steps[tl.c] >= limit[tl.c]) continue;  // filler, or a case that has taken all its steps
     if (tl.c != cur) {
       __syncthreads();  // every thread is done with the previous case's arguments
       const int *src = reinterpret_cast<const int *>(args + tl.c);
