@@ -162,14 +162,17 @@ int build(ilbm_batch *b) {
     }
     ibc[c] = IBBatchCase{k.ib, k.dt, k.time, std::max(1, k.max_steps), std::max(0, k.max_steps)};
   }
-  // tile table: every case's ghost-push chunks first (strided, slow), padded
-  // to a whole number of rounds of the persistent grid, then its row
-  // segments.  The kernel's block b takes entries b, b + blocks, ...: each
-  // case owns a share of the blocks proportional to its rows and its row
-  // segments are dealt round by round over its own blocks, so a block stays
-  // in one case (its arguments copied to shared memory once) while the
-  // case's blocks sweep neighbouring rows together.  Entries with c = -1
-  // fill the rounds and are skipped.
+  // tile table: every case's ghost-push chunks first (strided, slow), then
+  // its row segments; the kernel's block b takes entries b, b + blocks, ...
+  // When every case has the same number of steps left (none sits out before
+  // the batch is re-tabled), each case owns a share of the blocks
+  // proportional to its rows and its row segments are dealt round by round
+  // over its own blocks, so a block stays in one case (its arguments copied
+  // to shared memory once) while the case's blocks sweep neighbouring rows
+  // together; the ghost chunks are then padded to a whole number of rounds
+  // and entries with c = -1 fill the rounds (skipped).  Otherwise the row
+  // segments follow case after case, so that the blocks of a case that has
+  // finished its steps take the other cases' segments.
   const int W = b->tile_w;
   int per_sm = 0;
   if ((rc = batch_step_occupancy(ctx, W, &per_sm))) return rc;
@@ -195,7 +198,9 @@ int build(ilbm_batch *b) {
   const int G = (int)std::max<int64_t>(1, std::min<int64_t>(nrow + (int64_t)tiles.size(),
                                                             (int64_t)use * b->sms));
   b->blocks = G;
-  if (nc <= G) {
+  bool same_steps = true;
+  for (int c = 1; c < nc; ++c) same_steps = same_steps && b->cases[c].max_steps == b->cases[0].max_steps;
+  if (nc <= G && same_steps) {
     // blocks per case: proportional to its rows, at least one (largest remainders)
     std::vector<int> nb(nc, 1);
     int left = G - nc;
