@@ -108,11 +108,36 @@ __global__ void __launch_bounds__(kRedThreads) k_force_partial_multi(const SumRe
   }
 }
 
-__global__ void k_final_sum(const double *partial, int nparts, double *out) {
-  if (threadIdx.x < 3) {
-    double s = 0.0;
-    for (int b = 0; b < nparts; ++b) s += partial[b * 3 + threadIdx.x];
-    out[threadIdx.x] = s;
+// one warp: the partials' fixed-order total (lane l sums partials l, l + 32,
+// ..., whose loads are in flight together, then a fixed butterfly); with rec
+// set, also one force record: the total (3), the body's last marker force sum
+// (3) and its two status words as doubles
+__global__ void k_final_sum(const double *partial, int nparts, double *out,
+                            const double *fsum = nullptr, const int *status = nullptr,
+                            double *rec = nullptr) {
+  const int lane = threadIdx.x & 31;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int b = lane; b < nparts; b += 32) {
+    s0 += partial[b * 3];
+    s1 += partial[b * 3 + 1];
+    s2 += partial[b * 3 + 2];
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if (threadIdx.x != 0) return;
+  out[0] = s0;
+  out[1] = s1;
+  out[2] = s2;
+  if (rec) {
+    rec[0] = s0;
+    rec[1] = s1;
+    rec[2] = s2;
+    for (int c = 0; c < 3; ++c) rec[3 + c] = fsum[c];
+    rec[6] = (double)status[0];
+    rec[7] = (double)status[1];
   }
 }
 
@@ -294,7 +319,7 @@ static RegionArgs clip_region(const ilbm_ctx *ctx, const ilbm_box &box, const in
 }
 
 int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const int lo[3],
-                      const int hi[3], double **d_sum) {
+                      const int hi[3], double **d_sum, const double *fsum, const int *status) {
   std::vector<SumRegion> regs;
   std::vector<int64_t> off(1, 0);
   for (int b = 0; b < nbox; ++b) {
@@ -318,7 +343,15 @@ int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const int 
     return ILBM_ERR_NOMEM;
   }
   *d_sum = scr + kRedBlocks * 3;
+  double *rec = fsum ? *d_sum + 8 : nullptr;  // the record after the sums' spare slots
   if (nregs == 0) {
+    if (rec) {
+      k_final_sum<<<1, 32, 0, ctx->stream>>>(scr, 0, *d_sum, fsum, status, rec);
+      ctx->launches++;
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals");
+      return ILBM_OK;
+    }
     cudaError_t e = cudaMemsetAsync(*d_sum, 0, 3 * sizeof(double), ctx->stream);
     if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals");
     return ILBM_OK;
@@ -345,7 +378,7 @@ int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const int 
     else
       k_force_partial_multi<float><<<kRedBlocks, kRedThreads, 0, ctx->stream>>>(d_regs, nregs, d_off, scr);
   }
-  k_final_sum<<<1, 32, 0, ctx->stream>>>(scr, kRedBlocks, *d_sum);
+  k_final_sum<<<1, 32, 0, ctx->stream>>>(scr, kRedBlocks, *d_sum, fsum, status, rec);
   ctx->launches += 2;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_integrals");

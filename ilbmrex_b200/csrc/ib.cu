@@ -2319,19 +2319,6 @@ int ilbm_ib_force_region(const ilbm_ib *ib, int lo[3], int hi[3]) {
 
 }  // extern "C"
 
-// one force record: Eulerian sum (3), last marker force sum (3), the body's
-// two status words as doubles
-__global__ void k_record_pack(const double *sum3, const double *fsum, const int *status,
-                              double *rec) {
-  if (threadIdx.x != 0) return;
-  for (int c = 0; c < 3; ++c) {
-    rec[c] = sum3[c];
-    rec[3 + c] = fsum[c];
-  }
-  rec[6] = (double)status[0];
-  rec[7] = (double)status[1];
-}
-
 // Stopping tolerance of the IVC conjugate gradient (relative residual).  FP64
 // populations: 1e-14, so results meet the reference's dense LU at 1e-12.
 // FP32 and FP16 populations: 1e-6.  The right-hand side (U_target - U)/dt
@@ -2759,12 +2746,11 @@ int ilbm_force_record_async(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, ilbm
     set_error("ilbm_force_record_async: the IB object belongs to another context");
     return ILBM_ERR_ARG;
   }
+  // the sums' final launch also packs the record (after the sums' spare slots)
   double *d_sum = nullptr;
-  int rc = force_sum_enqueue(ctx, boxes, nbox, lo, hi, &d_sum);
+  int rc = force_sum_enqueue(ctx, boxes, nbox, lo, hi, &d_sum, ib->d_fsum, ib->d_status);
   if (rc) return rc;
-  double *d_rec = d_sum + 8;  // spare scratch after the sums
-  k_record_pack<<<1, 32, 0, ctx->stream>>>(d_sum, ib->d_fsum, ib->d_status, d_rec);
-  ctx->launches++;
+  double *d_rec = d_sum + 8;
   cudaError_t e = cudaMemcpyAsync(out, d_rec, 8 * sizeof(double), cudaMemcpyDefault, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_record_async");
   return ILBM_OK;
