@@ -39,11 +39,11 @@ int batch_step_occupancy(const ilbm_ctx *ctx, int w, int *per_sm);
 // the Eulerian force sum of ilbm_force_integrals enqueued on ctx->stream; the
 // three sums land at *d_sum (context scratch, with 8 spare doubles after
 // them) when the stream gets there; with fsum set, the same final launch also
-// packs a force record at *d_sum + 8 (the sums, fsum[0..2], status[0..1] as
-// doubles)
+// packs a force record (the sums, fsum[0..2], status[0..1] as doubles) at
+// rec_dst (a device-accessible address) or, without it, at *d_sum + 8
 int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const int lo[3],
                       const int hi[3], double **d_sum, const double *fsum = nullptr,
-                      const int *status = nullptr);
+                      const int *status = nullptr, double *rec_dst = nullptr);
 
 // ---- ib.cu ----------------------------------------------------------------
 // ilbm_advance_level in two halves: begin starts the body's update_forcing

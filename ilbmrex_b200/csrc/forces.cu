@@ -138,6 +138,7 @@ __global__ void k_final_sum(const double *partial, int nparts, double *out,
     for (int c = 0; c < 3; ++c) rec[3 + c] = fsum[c];
     rec[6] = (double)status[0];
     rec[7] = (double)status[1];
+    __threadfence_system();  // rec may be pinned host memory the host reads next
   }
 }
 
@@ -319,7 +320,8 @@ static RegionArgs clip_region(const ilbm_ctx *ctx, const ilbm_box &box, const in
 }
 
 int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const int lo[3],
-                      const int hi[3], double **d_sum, const double *fsum, const int *status) {
+                      const int hi[3], double **d_sum, const double *fsum, const int *status,
+                      double *rec_dst) {
   std::vector<SumRegion> regs;
   std::vector<int64_t> off(1, 0);
   for (int b = 0; b < nbox; ++b) {
@@ -343,7 +345,8 @@ int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const int 
     return ILBM_ERR_NOMEM;
   }
   *d_sum = scr + kRedBlocks * 3;
-  double *rec = fsum ? *d_sum + 8 : nullptr;  // the record after the sums' spare slots
+  // the record: rec_dst, else after the sums' spare slots
+  double *rec = fsum ? (rec_dst ? rec_dst : *d_sum + 8) : nullptr;
   if (nregs == 0) {
     if (rec) {
       k_final_sum<<<1, 32, 0, ctx->stream>>>(scr, 0, *d_sum, fsum, status, rec);

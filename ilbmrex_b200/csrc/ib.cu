@@ -2746,12 +2746,23 @@ int ilbm_force_record_async(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, ilbm
     set_error("ilbm_force_record_async: the IB object belongs to another context");
     return ILBM_ERR_ARG;
   }
-  // the sums' final launch also packs the record (after the sums' spare slots)
+  // the sums' final launch also packs the record: straight into `out` when it
+  // is pinned host memory the device can address (no copy on the stream),
+  // else into scratch, copied to `out` after it
+  double *direct = nullptr;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, out) == cudaSuccess) {
+    if (at.type == cudaMemoryTypeHost && at.devicePointer)
+      direct = static_cast<double *>(at.devicePointer);
+    else if (at.type == cudaMemoryTypeDevice && at.device == ctx->device)
+      direct = out;
+  }
+  cudaGetLastError();  // an unregistered pointer is not an error here
   double *d_sum = nullptr;
-  int rc = force_sum_enqueue(ctx, boxes, nbox, lo, hi, &d_sum, ib->d_fsum, ib->d_status);
+  int rc = force_sum_enqueue(ctx, boxes, nbox, lo, hi, &d_sum, ib->d_fsum, ib->d_status, direct);
   if (rc) return rc;
-  double *d_rec = d_sum + 8;
-  cudaError_t e = cudaMemcpyAsync(out, d_rec, 8 * sizeof(double), cudaMemcpyDefault, ctx->stream);
+  if (direct) return ILBM_OK;
+  cudaError_t e = cudaMemcpyAsync(out, d_sum + 8, 8 * sizeof(double), cudaMemcpyDefault, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(e, "ilbm_force_record_async");
   return ILBM_OK;
 }

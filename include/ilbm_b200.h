@@ -348,7 +348,8 @@ int ilbm_force_integrals_noalloc(ilbm_ctx *ctx, const ilbm_box *box, const void 
  * body's last marker force sum (ilbm_ib_last_marker_force_sum) and the body's
  * two status words into out[8] = {Eulerian sum (3), marker sum (3),
  * status word 0, status word 1}.  out should be pinned host memory (or device
- * memory); the values are there once the stream passes this point (an event
+ * memory), which the sums' last kernel writes directly (other memory gets a
+ * copy on the stream); the values are there once the stream passes this point (an event
  * recorded after the call, or ilbm_sync), so a host can issue the next step
  * before it reads this one's record.  Status bits as reported by
  * ilbm_ib_last_marker_force_sum: word 0 bit 0 a stencil left the band, bit 1
