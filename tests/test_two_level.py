@@ -141,3 +141,38 @@ def test_pipelined_force_records():
     assert abs(recs[-1][3]) > 0.0
     a.close()
     b.close()
+
+
+def test_force_record_into_pageable_pinned_and_device_memory():
+    """ilbm_force_record_async writes pinned host and device buffers from its
+    last kernel and copies into pageable memory: the three records are the
+    same bits, and equal ilbm_force_integrals and the last marker force sum
+    (the same fixed-order reduction)."""
+    import ctypes as C
+    from ilbmrex_b200 import capi
+    tl, ib, ic, if_ = cases.cylinder_two_level(nx=96, ny=64, D=12.0, center=(32.3, 31.7), U=0.05,
+                                               Re=40.0, upstream=1.0, downstream=2.0, cross=1.2)
+    s = TwoLevelSolver(tl, "f64", ib=ib)
+    s.set_macro(ic(), if_())
+    s.step(3)
+    lo, hi = s.force_region
+    b = s.F.box(s.F.f, None, force=s.F.fb)
+    page = np.full(8, np.nan)
+    pin = torch.full((8,), float("nan"), dtype=torch.float64).pin_memory()
+    dev = torch.full((8,), float("nan"), dtype=torch.float64, device="cuda")
+    for ptr in (page.ctypes.data, pin.data_ptr(), dev.data_ptr()):
+        capi.check(s.L.ilbm_force_record_async(s.ctx.h, C.byref(b), 1, s.ib, capi.ivec3(lo),
+                                               capi.ivec3(hi), C.c_void_p(ptr)), "force_record_async")
+    s.ctx.sync()
+    np.testing.assert_array_equal(pin.numpy(), page)
+    np.testing.assert_array_equal(dev.cpu().numpy(), page)
+    e = (C.c_double * 3)()
+    capi.check(s.L.ilbm_force_integrals(s.ctx.h, C.byref(b), 1, capi.ivec3(lo), capi.ivec3(hi), e),
+               "force_integrals")
+    m = (C.c_double * 3)()
+    capi.check(s.L.ilbm_ib_last_marker_force_sum(s.ib, m), "marker_force_sum")
+    np.testing.assert_array_equal(page[:3], np.array(e[:]))
+    np.testing.assert_array_equal(page[3:6], np.array(m[:]))
+    assert page[6] == 0.0 and page[7] == 0.0  # status words
+    assert abs(page[0]) > 0.0
+    s.close()
