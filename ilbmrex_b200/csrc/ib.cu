@@ -862,27 +862,54 @@ __device__ __forceinline__ void cg_grid_body(cgrp::grid_group &grid, const IBArg
     // before the row's products)
     double pap_c = 0.0;
     const double beta_c = (lane == 0) ? beta[0] : ((lane == 1) ? beta[1] : beta[2]);
-    for (int row = gw; row < n; row += nw) {
-      double zc = 0.0, pc = 0.0;
+    // a warp takes its rows two at a time (row and row + nw) with separate
+    // sums, so that the loads of both are in flight together; each row's sum
+    // and the order of the rows' p.Ap contributions are those of one row at
+    // a time
+    for (int row = gw; row < n; row += 2 * nw) {
+      const int rb = row + nw;
+      const bool two = rb < n;
+      double zc = 0.0, pc = 0.0, zb = 0.0, pb = 0.0;
       if (lane < 3) {
         zc = z[row + lane * n];
         if (it) pc = pold[row + lane * n];
+        if (two) {
+          zb = z[rb + lane * n];
+          if (it) pb = pold[rb + lane * n];
+        }
       }
-      double s0 = 0, s1 = 0, s2 = 0;
-      for (int e = rowptr[row] + lane; e < rowptr[row + 1]; e += 32) {
-        const double v = val[e];
-        const int j = col[e];
-        const double p0 = it ? __fma_rn(beta[0], pold[j], z[j]) : z[j];
-        const double p1 = it ? __fma_rn(beta[1], pold[j + n], z[j + n]) : z[j + n];
-        const double p2 = it ? __fma_rn(beta[2], pold[j + 2 * n], z[j + 2 * n]) : z[j + 2 * n];
-        s0 += v * p0;
-        s1 += v * p1;
-        s2 += v * p2;
+      const int ea1 = rowptr[row + 1];
+      const int eb0 = two ? rowptr[rb] : 0, eb1 = two ? rowptr[rb + 1] : 0;
+      double s0 = 0, s1 = 0, s2 = 0, t0 = 0, t1 = 0, t2 = 0;
+      for (int ea = rowptr[row] + lane, eb = eb0 + lane; ea < ea1 || eb < eb1; ea += 32, eb += 32) {
+        if (ea < ea1) {
+          const double v = val[ea];
+          const int j = col[ea];
+          const double p0 = it ? __fma_rn(beta[0], pold[j], z[j]) : z[j];
+          const double p1 = it ? __fma_rn(beta[1], pold[j + n], z[j + n]) : z[j + n];
+          const double p2 = it ? __fma_rn(beta[2], pold[j + 2 * n], z[j + 2 * n]) : z[j + 2 * n];
+          s0 += v * p0;
+          s1 += v * p1;
+          s2 += v * p2;
+        }
+        if (eb < eb1) {
+          const double v = val[eb];
+          const int j = col[eb];
+          const double p0 = it ? __fma_rn(beta[0], pold[j], z[j]) : z[j];
+          const double p1 = it ? __fma_rn(beta[1], pold[j + n], z[j + n]) : z[j + n];
+          const double p2 = it ? __fma_rn(beta[2], pold[j + 2 * n], z[j + 2 * n]) : z[j + 2 * n];
+          t0 += v * p0;
+          t1 += v * p1;
+          t2 += v * p2;
+        }
       }
       for (int o = 16; o > 0; o >>= 1) {
         s0 += __shfl_xor_sync(0xffffffffu, s0, o);
         s1 += __shfl_xor_sync(0xffffffffu, s1, o);
         s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+        t0 += __shfl_xor_sync(0xffffffffu, t0, o);
+        t1 += __shfl_xor_sync(0xffffffffu, t1, o);
+        t2 += __shfl_xor_sync(0xffffffffu, t2, o);
       }
       if (lane < 3) {
         const int ii = row + lane * n;
@@ -891,6 +918,14 @@ __device__ __forceinline__ void cg_grid_body(cgrp::grid_group &grid, const IBArg
         pnew[ii] = pv;
         Ap[ii] = sc;
         pap_c += pv * sc;
+        if (two) {
+          const int ib = rb + lane * n;
+          const double sb = (lane == 0) ? t0 : ((lane == 1) ? t1 : t2);
+          const double pvb = it ? __fma_rn(beta_c, pb, zb) : zb;
+          pnew[ib] = pvb;
+          Ap[ib] = sb;
+          pap_c += pvb * sb;
+        }
       }
     }
     double pap[3];
