@@ -193,7 +193,8 @@ __device__ __forceinline__ void target_of(const IBArgs &a, int m, const double *
                                           const double *tgt, double &ux, double &uy,
                                           double &uz);
 
-// A step's kernel-weight table of the markers (the batched stages): marker m's
+// A step's kernel-weight table of the markers (the batched stages, and an
+// IVC body on the single-case warp-parallel path): marker m's
 // weight at offset o - 2 from its cell in direction d is tw[kTabStride m +
 // 5 d + o] (1.0 in the third direction of a 2D lattice), its cell tc[m].  The
 // interpolation's lanes 0-4 write it; the spreading and the IVC operator
