@@ -43,7 +43,8 @@ EXPORTS = [
     "ilbm_batch_tune", "ilbm_batch_size", "ilbm_batch_progress",
     "ilbm_derived_fields", "ilbm_tag_cells",
     "ilbm_checkpoint_write", "ilbm_checkpoint_read", "ilbm_plotfile_write",
-    "ilbm_advance_two_level", "ilbm_average_down", "ilbm_advance_hierarchy",
+    "ilbm_advance_two_level", "ilbm_advance_two_level_recorded", "ilbm_average_down",
+    "ilbm_advance_hierarchy",
 ]
 
 
@@ -179,6 +180,9 @@ def lib():
         "ilbm_batch_progress": (I, [P, I, C.POINTER(I), C.POINTER(I64), C.POINTER(I), C.POINTER(I)]),
         "ilbm_advance_two_level": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), C.POINTER(Box_t),
                                        C.POINTER(LevelParams_t), P, D, D, I]),
+        "ilbm_advance_two_level_recorded": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t),
+                                                C.POINTER(Box_t), C.POINTER(LevelParams_t), P, D, D,
+                                                I, ip3, ip3, P]),
         "ilbm_average_down": (I, [P, C.POINTER(Box_t), C.POINTER(LevelParams_t), C.POINTER(Box_t),
                                   C.POINTER(LevelParams_t)]),
         "ilbm_advance_hierarchy": (I, [P, I, C.POINTER(Box_t), C.POINTER(LevelParams_t), P, D, D, I]),

@@ -44,6 +44,18 @@ int batch_step_occupancy(const ilbm_ctx *ctx, int w, int *per_sm);
 int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const int lo[3],
                       const int hi[3], double **d_sum, const double *fsum = nullptr,
                       const int *status = nullptr, double *rec_dst = nullptr);
+// one box's force record (region sum, fsum, status) written to rec (device-
+// accessible) by launches on stream st, using the caller's scratch of at
+// least force_record_scratch() doubles
+size_t force_record_scratch();
+int force_record_on(ilbm_ctx *ctx, const ilbm_box &box, const int lo[3], const int hi[3],
+                    const double *fsum, const int *status, double *rec, double *scr,
+                    cudaStream_t st);
+// the body's force record on stream st (the context's side stream, after
+// the body's forcing chain queued there, or its main stream): rec is
+// device-accessible; records ctx->ev_rec on st after it
+int ib_record_on(ilbm_ib *ib, const ilbm_box &box, const int lo[3], const int hi[3], double *rec,
+                 cudaStream_t st);
 
 // ---- ib.cu ----------------------------------------------------------------
 // ilbm_advance_level in two halves: begin starts the body's update_forcing

@@ -388,6 +388,38 @@ int force_sum_enqueue(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, const int 
   return ILBM_OK;
 }
 
+// one box's force record (the region sum, fsum[0..2], status[0..1]) into rec
+// (device-accessible) on stream st, with the caller's scratch (at least
+// force_record_scratch() doubles): the launches of force_sum_enqueue for one
+// region, in the same fixed order
+size_t force_record_scratch() { return (size_t)kRedBlocks * 3 + 16; }
+
+int force_record_on(ilbm_ctx *ctx, const ilbm_box &box, const int lo[3], const int hi[3],
+                    const double *fsum, const int *status, double *rec, double *scr,
+                    cudaStream_t st) {
+  if (!box.force) {
+    set_error("force record: box->force (the array to integrate) is required");
+    return ILBM_ERR_ARG;
+  }
+  const RegionArgs a = clip_region(ctx, box, lo, hi);
+  const int64_t cells = (int64_t)a.n[0] * a.n[1] * a.n[2];
+  double *sum = scr + kRedBlocks * 3;
+  int nparts = 0;
+  if (cells > 0) {
+    if (ctx->storage == ILBM_STORAGE_F64)
+      k_force_partial<double><<<kRedBlocks, kRedThreads, 0, st>>>(a, static_cast<const double *>(box.force), scr);
+    else
+      k_force_partial<float><<<kRedBlocks, kRedThreads, 0, st>>>(a, static_cast<const float *>(box.force), scr);
+    ctx->launches++;
+    nparts = kRedBlocks;
+  }
+  k_final_sum<<<1, 32, 0, st>>>(scr, nparts, sum, fsum, status, rec);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "force record");
+  return ILBM_OK;
+}
+
 }  // namespace ilbm
 
 extern "C" {

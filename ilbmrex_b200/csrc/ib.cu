@@ -1865,6 +1865,7 @@ struct ilbm_ib {
   // by the warp-parallel interpolation for the spreading and operator build
   double *d_tw = nullptr;
   int4 *d_tc = nullptr;
+  double *d_recscr = nullptr;  // scratch of a force record taken with the step
   // a level held in several boxes: the StepArgs of the boxes near the band
   std::vector<StepArgs> h_boxargs;
   StepArgs *d_boxargs = nullptr;
@@ -2278,6 +2279,10 @@ int ilbm_ib_create(ilbm_ctx *ctx, const ilbm_ib_params *p, const ilbm_level_geom
   // band fields finite everywhere (a fixed body forms them on its stencils only)
   cudaMemsetAsync(ib->d_EV, 0, 3 * (size_t)ib->nb * sizeof(double), ctx->stream);
   cudaMemsetAsync(ib->d_RHO, 0, (size_t)ib->nb * sizeof(double), ctx->stream);
+  if ((rc = dmalloc(ib, &ib->d_recscr, force_record_scratch()))) {
+    ilbm_ib_destroy(ib);
+    return rc;
+  }
   if ((rc = build_gather(ib))) {
     ilbm_ib_destroy(ib);
     return rc;
@@ -2771,6 +2776,20 @@ int ilbm_ib_last_marker_force_sum(ilbm_ib *ib, double out[3]) {
   }
   return ILBM_OK;
 }
+
+}  // extern "C"
+
+int ilbm::ib_record_on(ilbm_ib *ib, const ilbm_box &box, const int lo[3], const int hi[3],
+                       double *rec, cudaStream_t st) {
+  ilbm_ctx *ctx = ib->ctx;
+  int rc = force_record_on(ctx, box, lo, hi, ib->d_fsum, ib->d_status, rec, ib->d_recscr, st);
+  if (rc) return rc;
+  cudaError_t e = cudaEventRecord(ctx->ev_rec, st);
+  if (e != cudaSuccess) return cuda_fail(e, "force record event");
+  return ILBM_OK;
+}
+
+extern "C" {
 
 int ilbm_force_record_async(ilbm_ctx *ctx, const ilbm_box *boxes, int nbox, ilbm_ib *ib,
                             const int lo[3], const int hi[3], double *out) {

@@ -406,6 +406,7 @@ struct ilbm_ctx {
   // immersed-boundary chain
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_done = nullptr;
+  cudaEvent_t ev_rec = nullptr;  // a force record taken on the side stream is in place
   int sms = 0;
   // the context's own memory pool for stream-ordered allocations (IB arrays,
   // batch tables): freed memory stays in the pool for the next request

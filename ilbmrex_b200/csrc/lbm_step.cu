@@ -1698,6 +1698,7 @@ int ilbm_create(const ilbm_lattice *lat, int storage, int device, void *cuda_str
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_rec, cudaEventDisableTiming);
     if (e != cudaSuccess) {
       ilbm_destroy(c);
       return cuda_fail(e, "side stream");
@@ -1740,6 +1741,7 @@ int ilbm_destroy(ilbm_ctx *ctx) {
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->ev_done) cudaEventDestroy(ctx->ev_done);
+  if (ctx->ev_rec) cudaEventDestroy(ctx->ev_rec);
   // a pool with allocations outstanding is released once they are freed
   if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);

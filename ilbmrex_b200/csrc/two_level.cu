@@ -435,9 +435,20 @@ int ilbm_average_down(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_pa
   return ILBM_DISPATCH(ctx, launch_avg_down, ctx, g);
 }
 
-int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_params *pc,
+}  // extern "C"
+
+namespace {
+
+// a force record requested with the step: region [lo, hi] of the fine
+// level's force of the second substep, written to rec (device-accessible)
+struct StepRecord {
+  const int *lo, *hi;
+  double *rec;
+};
+
+int advance_two_level_impl(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_params *pc,
                            const ilbm_box *fine, const ilbm_level_params *pf, ilbm_ib *ib,
-                           double dt, double time, int flags) {
+                           double dt, double time, int flags, const StepRecord *record) {
   if (!ctx || !coarse || !pc || !fine || !pf) {
     set_error("ilbm_advance_two_level: null argument");
     return ILBM_ERR_ARG;
@@ -542,6 +553,13 @@ int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_lev
       std::swap(b1.f_in, b1.f_out);
       std::swap(b1.force, b1.force_prev);
       if ((rc = advance_begin(ctx, &b1, pf, ib, dtf, t_old + dtf, &sp1))) return rc;
+      // the record reads what the second substep's chain produces (its
+      // exported force, the marker force sum, the status): on the side
+      // stream right after it, beside the main stream's remaining work,
+      // which only reads those arrays
+      if (record && !sp1.serial &&
+          (rc = ib_record_on(ib, b1, record->lo, record->hi, record->rec, ctx->side)))
+        return rc;
       if ((rc = level_step_impl(ctx, coarse, 1, pc, cmlo, cmhi, 2))) return rc;
     }
   }
@@ -558,7 +576,60 @@ int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_lev
       a.rhi[d] = hi[d];
     }
   }
-  return ILBM_DISPATCH(ctx, launch_avg_down, ctx, a);
+  if ((rc = ILBM_DISPATCH(ctx, launch_avg_down, ctx, a))) return rc;
+  if (record) {
+    if (sp1.serial) {  // the chain ran on the main stream: the record follows it there
+      ilbm_box rb = *fine;
+      rb.force = fine->force_prev;
+      if ((rc = ib_record_on(ib, rb, record->lo, record->hi, record->rec, ctx->stream))) return rc;
+    }
+    // the step's end waits for the record taken beside it
+    cudaError_t e = cudaStreamWaitEvent(ctx->stream, ctx->ev_rec, 0);
+    if (e != cudaSuccess) return cuda_fail(e, "ilbm_advance_two_level_recorded");
+  }
+  return ILBM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_params *pc,
+                           const ilbm_box *fine, const ilbm_level_params *pf, ilbm_ib *ib,
+                           double dt, double time, int flags) {
+  return advance_two_level_impl(ctx, coarse, pc, fine, pf, ib, dt, time, flags, nullptr);
+}
+
+int ilbm_advance_two_level_recorded(ilbm_ctx *ctx, const ilbm_box *coarse,
+                                    const ilbm_level_params *pc, const ilbm_box *fine,
+                                    const ilbm_level_params *pf, ilbm_ib *ib, double dt,
+                                    double time, int flags, const int lo[3], const int hi[3],
+                                    double *out) {
+  if (!ctx || !ib || !fine || !lo || !hi || !out) {
+    set_error("ilbm_advance_two_level_recorded: null argument");
+    return ILBM_ERR_ARG;
+  }
+  // the record's last kernel writes `out` itself when the device can address
+  // it (pinned host memory, or memory of this device); other memory gets the
+  // step, then the record through ilbm_force_record_async
+  double *direct = nullptr;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, out) == cudaSuccess) {
+    if (at.type == cudaMemoryTypeHost && at.devicePointer)
+      direct = static_cast<double *>(at.devicePointer);
+    else if (at.type == cudaMemoryTypeDevice && at.device == ctx->device)
+      direct = out;
+  }
+  cudaGetLastError();  // an unregistered pointer is not an error here
+  if (!direct) {
+    int rc = advance_two_level_impl(ctx, coarse, pc, fine, pf, ib, dt, time, flags, nullptr);
+    if (rc) return rc;
+    ilbm_box rb = *fine;
+    rb.force = fine->force_prev;
+    return ilbm_force_record_async(ctx, &rb, 1, ib, lo, hi, out);
+  }
+  const StepRecord r{lo, hi, direct};
+  return advance_two_level_impl(ctx, coarse, pc, fine, pf, ib, dt, time, flags, &r);
 }
 
 }  // extern "C"

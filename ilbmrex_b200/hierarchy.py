@@ -168,7 +168,7 @@ class HierarchySolver:
         self.first_step = True
 
     # ---- one coarse step ---------------------------------------------------
-    def _launch_step(self):
+    def _launch_step(self, record_into=None):
         top = self.nlev - 1
         arr = (capi.Box_t * self.nlev)()
         for l, lvl in enumerate(self.levels):
@@ -187,8 +187,12 @@ class HierarchySolver:
         """One coarse step.  record_force: the force record (self.rec) of the
         step; pipelined: its sums are copied to the host without waiting, and
         the record of the previous step is taken instead (flush_records takes
-        the last one), so the next step is queued before the host waits."""
-        self._launch_step()
+        the last one), so the next step is queued before the host waits.
+        Where the solver can take the record with the step itself
+        (TwoLevelSolver), the pipelined record runs beside the step's end."""
+        fused = record_force and pipelined and self.ib is not None and self._records_with_step()
+        buf = self._next_rec_buf() if fused else None
+        self._launch_step(record_into=buf)
         Cl = self.C
         Cl.f, Cl.f_next = Cl.f_next, Cl.f
         Cl.m, Cl.m_next = Cl.m_next, Cl.m
@@ -197,7 +201,7 @@ class HierarchySolver:
         self.istep += 1
         if record_force and self.ib is not None:
             if pipelined:
-                self._record_async()
+                self._record_async(buf)
             else:
                 self.flush_records()
                 self.compute_ib_force()
@@ -251,17 +255,27 @@ class HierarchySolver:
         self._graph = g
         return g
 
-    def _record_async(self):
+    def _records_with_step(self) -> bool:
+        return False
+
+    def _next_rec_buf(self):
         if self._rec_bufs is None:
             self._rec_bufs = [torch.empty(8, dtype=torch.float64, pin_memory=True) for _ in range(2)]
             self._stream = torch.cuda.ExternalStream(self.L.ilbm_stream(self.ctx.h), device=self.dev)
-        lo, hi = self.force_region
-        b = self.F.box(self.F.f, None, force=self.F.fb)
         buf = self._rec_bufs[self._rec_slot]
         self._rec_slot ^= 1
-        capi.check(self.L.ilbm_force_record_async(self.ctx.h, C.byref(b), 1, self.ib, capi.ivec3(lo),
-                                                  capi.ivec3(hi), buf.data_ptr()),
-                   "force_record_async")
+        return buf
+
+    def _record_async(self, buf=None):
+        """The step's record into pinned memory (buf: already taken with the
+        step), its event on the library stream; the previous one is taken."""
+        if buf is None:
+            buf = self._next_rec_buf()
+            lo, hi = self.force_region
+            b = self.F.box(self.F.f, None, force=self.F.fb)
+            capi.check(self.L.ilbm_force_record_async(self.ctx.h, C.byref(b), 1, self.ib, capi.ivec3(lo),
+                                                      capi.ivec3(hi), buf.data_ptr()),
+                       "force_record_async")
         ev = torch.cuda.Event()
         ev.record(self._stream)
         prev, self._pending = self._pending, (buf, ev)
@@ -382,12 +396,22 @@ class TwoLevelSolver(HierarchySolver):
     def set_macro(self, init_coarse, init_fine):
         super().set_macro(init_coarse, init_fine)
 
-    def _launch_step(self):
+    def _records_with_step(self) -> bool:
+        return True
+
+    def _launch_step(self, record_into=None):
         Cl, Fl = self.C, self.F
         bc = Cl.box(Cl.f, Cl.f_next, m_in=Cl.m, m_out=Cl.m_next)
         bf = Fl.box(Fl.f, Fl.f_next, m_in=Fl.m if self.first_step else None,
                     force=Fl.fa, force_prev=Fl.fb)
         flags = capi.TWO_LEVEL_FIRST_STEP if self.first_step else 0
+        if record_into is not None:  # the step and its force record (ilbm_advance_two_level_recorded)
+            lo, hi = self.force_region
+            capi.check(self.L.ilbm_advance_two_level_recorded(
+                self.ctx.h, C.byref(bc), C.byref(self.pc), C.byref(bf), C.byref(self.pf), self.ib,
+                self.tl.coarse.dt, self.time, flags, capi.ivec3(lo), capi.ivec3(hi),
+                record_into.data_ptr()), "advance_two_level_recorded")
+            return
         capi.check(self.L.ilbm_advance_two_level(self.ctx.h, C.byref(bc), C.byref(self.pc),
                                                  C.byref(bf), C.byref(self.pf), self.ib,
                                                  self.tl.coarse.dt, self.time, flags),

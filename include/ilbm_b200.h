@@ -439,6 +439,24 @@ int ilbm_tag_cells(ilbm_ctx *ctx, const ilbm_box *box, const void *vor, double t
 int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_level_params *pc,
                            const ilbm_box *fine, const ilbm_level_params *pf, ilbm_ib *ib,
                            double dt, double time, int flags);
+
+/* ilbm_advance_two_level followed by the step's force record, taken as
+ * ilbm_force_record_async takes it (region [lo, hi] of the fine level's force
+ * of the second substep, fine->force_prev on return; the body's last marker
+ * force sum; its two status words) into out[8], with the same values: when
+ * out is pinned host memory (or memory of this device) the record's kernels
+ * run on the context's side stream right after the second substep's forcing,
+ * beside the rest of the step, which only reads what they read, and write out
+ * directly; the step's end on the context's stream waits for them, so out is
+ * ready once the stream passes this call.  Other memory gets the step, then
+ * ilbm_force_record_async.  Replaces the caller's ilbm_advance_two_level +
+ * ilbm_force_record_async pair (ComputeIBForce after the finest level's
+ * substeps, Source/Core/AmrCoreLBM.cpp:456-631). */
+int ilbm_advance_two_level_recorded(ilbm_ctx *ctx, const ilbm_box *coarse,
+                                    const ilbm_level_params *pc, const ilbm_box *fine,
+                                    const ilbm_level_params *pf, ilbm_ib *ib, double dt,
+                                    double time, int flags, const int lo[3], const int hi[3],
+                                    double *out);
 /* average-down alone (InitData's AverageDown after the levels are made,
  * AmrCoreLBM.cpp:710-720): fine f_in / macro_in onto coarse f_in / macro_in,
  * for any two adjacent levels of a hierarchy (the coarse one self-filled and

@@ -176,3 +176,43 @@ def test_force_record_into_pageable_pinned_and_device_memory():
     assert page[6] == 0.0 and page[7] == 0.0  # status words
     assert abs(page[0]) > 0.0
     s.close()
+
+
+def test_step_with_record_into_pageable_memory():
+    """ilbm_advance_two_level_recorded with a pageable buffer takes the step,
+    then ilbm_force_record_async: the record equals the force integrals and
+    the marker force sum of the step (the pinned-buffer form, whose record
+    runs beside the step's end, is what test_pipelined_force_records uses)."""
+    import ctypes as C
+    from ilbmrex_b200 import capi
+
+    class _Host:
+        def __init__(self, a):
+            self.a = a
+
+        def data_ptr(self):
+            return self.a.ctypes.data
+
+    tl, ib, ic, if_ = cases.cylinder_two_level(nx=96, ny=64, D=12.0, center=(32.3, 31.7), U=0.05,
+                                               Re=40.0, upstream=1.0, downstream=2.0, cross=1.2)
+    s = TwoLevelSolver(tl, "f64", ib=ib)
+    s.set_macro(ic(), if_())
+    s.step(2)
+    page = np.full(8, np.nan)
+    s._launch_step(record_into=_Host(page))
+    Cl = s.C
+    Cl.f, Cl.f_next = Cl.f_next, Cl.f
+    Cl.m, Cl.m_next = Cl.m_next, Cl.m
+    s.time += s.hc.coarse.dt
+    s.ctx.sync()
+    lo, hi = s.force_region
+    b = s.F.box(s.F.f, None, force=s.F.fb)
+    e = (C.c_double * 3)()
+    capi.check(s.L.ilbm_force_integrals(s.ctx.h, C.byref(b), 1, capi.ivec3(lo), capi.ivec3(hi), e),
+               "force_integrals")
+    m = (C.c_double * 3)()
+    capi.check(s.L.ilbm_ib_last_marker_force_sum(s.ib, m), "marker_force_sum")
+    np.testing.assert_array_equal(page[:3], np.array(e[:]))
+    np.testing.assert_array_equal(page[3:6], np.array(m[:]))
+    assert page[6] == 0.0 and page[7] == 0.0 and abs(page[0]) > 0.0
+    s.close()
