@@ -440,8 +440,9 @@ int ilbm_advance_two_level(ilbm_ctx *ctx, const ilbm_box *coarse, const ilbm_lev
                            const ilbm_box *fine, const ilbm_level_params *pf, ilbm_ib *ib,
                            double dt, double time, int flags);
 
-/* ilbm_advance_two_level followed by the step's force record, taken as
- * ilbm_force_record_async takes it (region [lo, hi] of the fine level's force
+/* ilbm_advance_two_level followed by the step's force record (ib must not be
+ * NULL), taken as ilbm_force_record_async takes it (region [lo, hi] of the
+ * fine level's force
  * of the second substep, fine->force_prev on return; the body's last marker
  * force sum; its two status words) into out[8], with the same values: when
  * out is pinned host memory (or memory of this device) the record's kernels
